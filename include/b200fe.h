@@ -1,0 +1,151 @@
+/*
+ * b200fe.h -- C ABI of the B200 fixed-effects absorber (libb200fe.so).
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status and
+ * never throws.  Status codes follow the reference's GPU status semantics
+ * (docs/gpu.md:159-161, src/fe_absorption.cpp:361-381):
+ *
+ *   B200FE_OK             0  solved; outputs written
+ *   B200FE_NOT_CONVERGED  1  outputs written, tolerance not reached (status 3 upstream)
+ *   B200FE_UNAVAILABLE    2  no usable CUDA device (status 2 upstream)
+ *   B200FE_CUDA_ERROR     3  a CUDA call or allocation failed (status 4 upstream)
+ *   B200FE_INVALID_ARG    4  bad sizes, ids out of range, non-finite input
+ *
+ * There is no CPU fallback behind any of these calls: a failure is returned
+ * to the caller, which decides (the reference's fail-closed contract,
+ * src/fe_absorption.cpp:9227-9237).
+ *
+ * Problem solved by every absorb call: for each column v of [y X] return the
+ * weighted within transform  v~ = v - D a,  where a solves the normal
+ * equations  D'W D a = D'W v  of the stacked FE dummies D = [D_1 ... D_m]
+ * (the projection the reference's absorbers compute; fe_absorption.hpp).
+ *
+ * Group ids are dense 0..G_d-1 per dimension (the reference's GpuFeInput
+ * contract, include/fe_absorption_cuda.hpp:12-22); X is column-major with
+ * leading dimension n (the reference rejects ld != n,
+ * src/fe_absorption_cuda.cu:2303-2306).
+ */
+#ifndef B200FE_H
+#define B200FE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200FE_OK 0
+#define B200FE_NOT_CONVERGED 1
+#define B200FE_UNAVAILABLE 2
+#define B200FE_CUDA_ERROR 3
+#define B200FE_INVALID_ARG 4
+
+#define B200FE_PREC_FP64 0   /* plain FP64 preconditioned CG                   */
+#define B200FE_PREC_MIXED 1  /* FP32 inner CG inside FP64 iterative refinement */
+
+#define B200FE_MAX_DIMS 8
+
+typedef struct b200fe_context b200fe_context;
+
+typedef struct b200fe_options {
+    double tol;            /* stop when max_c ||b_c - S a_c|| <= tol * ||b_c|| (default 1e-8)   */
+    int max_iter;          /* cap on PCG iterations, all refinement rounds together (10000)   */
+    int precision;         /* B200FE_PREC_FP64 or B200FE_PREC_MIXED (default MIXED)           */
+    int certify;           /* 1: compute abs_residual / abs_residual_rel on the device (1)    */
+    int check_interval;    /* PCG iterations between host convergence checks (default 4)      */
+    int reuse_structure;   /* 1: ids and weights equal those of the previous call (0)         */
+    double inner_tol;      /* MIXED: relative tolerance of each FP32 inner solve (1e-5)       */
+    int tolerance_mode;    /* certificate limit as the reference: 0 xhdfe-fast,
+                              1 reghdfe-comparable (tol_eff = min(tol, 1e-9)), 2 strict (1)  */
+    int max_outer;         /* MIXED: cap on refinement rounds (default 12)                    */
+} b200fe_options;
+
+typedef struct b200fe_result {
+    int status;
+    int iterations;          /* PCG iterations over all refinement rounds                  */
+    int outer_iterations;    /* FP64 refinement rounds (1 for FP64)                        */
+    int converged;
+    int precision_certified; /* converged and abs_residual_rel <= max(8 tol_eff, 64 eps)    */
+    int primary_dim;         /* FE dimension eliminated exactly (the largest)              */
+    int num_levels_present[B200FE_MAX_DIMS];
+    double abs_residual;     /* max_c ||D'W v~_c||_2  (src/fe_absorption.cpp:14942-15190) */
+    double abs_residual_rel; /* max_c ||D'W v~_c|| / (||D'W||_F ||v_c||)                   */
+    double rel_residual;     /* max_c ||b_c - S a_c|| / ||b_c|| at exit                      */
+    double setup_ms;         /* FE structure build (0 when reused)                          */
+    double solve_ms;         /* RHS pass + PCG + output pass (+ certificate)                */
+    double h2d_ms;
+    double d2h_ms;
+    long long kernel_launches;
+} b200fe_result;
+
+/* Library version, e.g. 10000 for 1.0.0. */
+int b200fe_version(void);
+
+/* 1 when a CUDA device is usable.
+ * Replaces hdfe::detail::cuda_backend_available()
+ * (include/fe_absorption_cuda.hpp:125, src/fe_absorption_cuda.cu:2281). */
+int b200fe_device_available(void);
+
+void b200fe_default_options(b200fe_options* opts);
+
+/* A context owns one CUDA stream and a grow-only device workspace.  One
+ * context per host thread (the reference keeps its workspace thread_local,
+ * src/fe_absorption_cuda.cu:1536). */
+int b200fe_context_create(int device, b200fe_context** out);
+void b200fe_context_destroy(b200fe_context* ctx);
+const char* b200fe_last_error(const b200fe_context* ctx);
+/* The context's cudaStream_t, as void*. */
+void* b200fe_context_stream(b200fe_context* ctx);
+
+/* Absorb host arrays: copies in, solves on the device, copies out.
+ * y: n doubles; X: n*k doubles column-major (may be NULL when k == 0);
+ * group_ids[d]: n int32 dense ids; num_groups[d]: G_d; weights: n doubles or
+ * NULL.  y_out / X_out receive the within transforms.
+ * Replaces hdfe::detail::absorb_fixed_effects_cuda
+ * (include/fe_absorption_cuda.hpp:127-134, src/fe_absorption_cuda.cu:2294). */
+int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X,
+                  int64_t n, int k, int num_dims,
+                  const int32_t* const* group_ids, const int32_t* num_groups,
+                  const double* weights, const b200fe_options* opts,
+                  double* y_out, double* X_out, b200fe_result* res);
+
+/* Absorb device arrays (no host copies).  d_v: column-major n x cols with the
+ * outcome in column 0; d_out: same shape (may alias nothing of the inputs).
+ * stream: a cudaStream_t as void*, or NULL for the context's stream.
+ * Same solver as b200fe_absorb. */
+int b200fe_absorb_device(b200fe_context* ctx, const double* d_v, int64_t n,
+                         int cols, int num_dims,
+                         const int32_t* const* d_group_ids,
+                         const int32_t* num_groups, const double* d_weights,
+                         const b200fe_options* opts, double* d_out,
+                         b200fe_result* res, void* stream);
+
+/* In-place demean of host arrays, the raw interface of the reference's
+ * block-PCG absorber: Y (n) and X (n x k column-major) are overwritten with
+ * their within transforms; iters_out receives the PCG iteration count.
+ * Returns 0 on success.  Unlike the reference it has no column limit.
+ * Replaces xhdfe::schwarz_demean_raw (include/schwarz_demean.hpp:30-34,
+ * src/schwarz_demean.cpp:419-438). */
+int b200fe_demean_raw(double* Y, double* X, int64_t n, int k, int num_dims,
+                      const int32_t* const* fe, const int32_t* nlev,
+                      double tol, int max_iter, int* iters_out);
+
+/* Max over FE dims of max_g |weighted mean_g(residual)| after a Gauss-Seidel
+ * pass over the dims in sweep_order (NULL: 0..m-1), each dim's means
+ * subtracted before the next.  Used to check that a recovered residual is
+ * orthogonal to every FE basis.
+ * Replaces hdfe::detail::fe_recovery_max_delta_cuda
+ * (include/fe_absorption_cuda.hpp:152-156, src/fe_absorption_cuda.cu:5227). */
+int b200fe_fe_recovery_max_delta(b200fe_context* ctx, const double* residual,
+                                 int64_t n, int num_dims,
+                                 const int32_t* const* group_ids,
+                                 const int32_t* num_groups,
+                                 const double* weights,
+                                 const int32_t* sweep_order,
+                                 double* out_max_delta);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200FE_H */

@@ -1,0 +1,228 @@
+"""ORACLE -- test infrastructure only.
+
+Python front of the two checkers built by oracle/Makefile:
+
+* ``liboracle.so``          -- the plain-C restatement of the reference's
+  absorber (demean_oracle.c): Irons-Tuck MAP with the honest stop, a tight
+  projection for pinning, and the normal-equation certificate;
+* ``_ref/libxhdfe_ref.so``  -- the reference's own CPU core compiled from its
+  unmodified sources, behind ref_driver.cpp.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package, and only as the checker (never as the measured or shipped path).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libxhdfe_ref.so"
+
+_vp, _i64, _int, _dbl = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double
+_olib = None
+_rlib = None
+
+
+def build_oracle() -> Path:
+    if not ORACLE_SO.exists() or ORACLE_SO.stat().st_mtime < (HERE / "demean_oracle.c").stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
+    return ORACLE_SO
+
+
+def olib() -> ctypes.CDLL:
+    global _olib
+    if _olib is None:
+        build_oracle()
+        lib = ctypes.CDLL(str(ORACLE_SO))
+        lib.oracle_demean_map.argtypes = [_i64, _int, _vp, _int, _vp, _vp, _vp, _vp, _dbl, _int,
+                                          _int, ctypes.POINTER(_int)]
+        lib.oracle_demean_map.restype = _int
+        lib.oracle_sweep.argtypes = [_i64, _int, _vp, _int, _vp, _vp, _vp, _vp]
+        lib.oracle_sweep.restype = None
+        lib.oracle_certify.argtypes = [_i64, _int, _vp, _vp, _int, _vp, _vp, _vp,
+                                       ctypes.POINTER(_dbl), ctypes.POINTER(_dbl)]
+        lib.oracle_certify.restype = None
+        _olib = lib
+    return _olib
+
+
+def _pack(y, X, fes, G, weights):
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    n = y.shape[0]
+    X = np.zeros((n, 0)) if X is None else np.asarray(X, dtype=np.float64).reshape(n, -1)
+    V = np.empty((n, 1 + X.shape[1]), dtype=np.float64, order="F")
+    V[:, 0] = y
+    V[:, 1:] = X
+    g = np.ascontiguousarray(np.stack([np.asarray(f, dtype=np.int32) for f in fes]) if fes
+                             else np.zeros((0, n), np.int32))
+    Ga = np.ascontiguousarray(G, dtype=np.int32)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    return V, g, Ga, w
+
+
+def map_demean(y, X, fes, G, weights=None, *, tol=1e-8, max_iter=100000, accel=True,
+               order=None):
+    """Reference-style IT-MAP demeaning.  Returns (V~ [n, C] Fortran, iters, converged)."""
+    V, g, Ga, w = _pack(y, X, fes, G, weights)
+    it = _int()
+    o = None if order is None else np.ascontiguousarray(order, dtype=np.int32)
+    conv = olib().oracle_demean_map(V.shape[0], V.shape[1], V.ctypes.data, len(fes),
+                                    g.ctypes.data, Ga.ctypes.data,
+                                    None if w is None else w.ctypes.data,
+                                    None if o is None else o.ctypes.data, float(tol),
+                                    int(max_iter), 1 if accel else 0, ctypes.byref(it))
+    return V, int(it.value), bool(conv)
+
+
+def project(y, X, fes, G, weights=None, *, tol=1e-14, max_iter=200000):
+    """Tightly converged within transform (the near-exact projection)."""
+    return map_demean(y, X, fes, G, weights, tol=tol, max_iter=max_iter, accel=True)
+
+
+def certify(V_orig, V_tilde, fes, G, weights=None):
+    """(abs_residual, abs_residual_rel) of the reference's certificate."""
+    Vo = np.asfortranarray(V_orig, dtype=np.float64)
+    Vt = np.asfortranarray(V_tilde, dtype=np.float64)
+    g = np.ascontiguousarray(np.stack([np.asarray(f, dtype=np.int32) for f in fes]))
+    Ga = np.ascontiguousarray(G, dtype=np.int32)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    a, r = _dbl(), _dbl()
+    olib().oracle_certify(Vo.shape[0], Vo.shape[1], Vo.ctypes.data, Vt.ctypes.data, len(fes),
+                          g.ctypes.data, Ga.ctypes.data, None if w is None else w.ctypes.data,
+                          ctypes.byref(a), ctypes.byref(r))
+    return float(a.value), float(r.value)
+
+
+# ---------------------------------------------------------------------------
+# The reference's own CPU core (oracle/_ref), when it was built here.
+# ---------------------------------------------------------------------------
+class XrefOptions(ctypes.Structure):
+    _fields_ = [("tol", _dbl), ("tolerance_mode", _int), ("absorption_method", _int),
+                ("num_threads", _int), ("max_iter", _int), ("drop_singletons", _int),
+                ("se_type", _int), ("fit_intercept", _int)]
+
+
+TOLERANCE_MODES = {"xhdfe-fast": 0, "reghdfe-comparable": 1, "strict-residual": 2}
+METHODS = {"auto": 0, "gauss-seidel": 1, "symmetric-gauss-seidel": 2, "jacobi": 3}
+SE_TYPES = {"unadjusted": 0, "robust": 1, "cluster": 2}
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def rlib() -> ctypes.CDLL:
+    global _rlib
+    if _rlib is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} not built (oracle/Makefile target 'ref')")
+        lib = ctypes.CDLL(str(REF_SO))
+        P = ctypes.POINTER
+        lib.xref_absorb.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, P(XrefOptions), _vp, _vp,
+                                    P(_int), P(_dbl), ctypes.c_char_p, _int]
+        lib.xref_absorb.restype = _int
+        lib.xref_partial_out.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, P(XrefOptions), _vp,
+                                         _vp, _vp, P(_int), P(_dbl), ctypes.c_char_p, _int]
+        lib.xref_partial_out.restype = _int
+        lib.xref_fit.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, _vp, P(XrefOptions), _vp,
+                                 _vp, P(_int), P(_dbl), ctypes.c_char_p, _int]
+        lib.xref_fit.restype = _int
+        _rlib = lib
+    return _rlib
+
+
+def _xopts(tol, tolerance_mode, method, threads, max_iter=0, drop_singletons=True,
+           se_type="unadjusted", fit_intercept=True):
+    o = XrefOptions()
+    o.tol = tol
+    o.tolerance_mode = TOLERANCE_MODES[tolerance_mode]
+    o.absorption_method = METHODS[method]
+    o.num_threads = threads
+    o.max_iter = max_iter
+    o.drop_singletons = 1 if drop_singletons else 0
+    o.se_type = SE_TYPES[se_type]
+    o.fit_intercept = 1 if fit_intercept else 0
+    return o
+
+
+def ref_absorb(y, X, fes, weights=None, *, tol=1e-8, tolerance_mode="reghdfe-comparable",
+               method="auto", threads=1, max_iter=0):
+    """Reference absorb_fixed_effects_v6 (raw ids, no singleton drop)."""
+    V, g, _, w = _pack(y, X, fes, [1] * len(fes), weights)
+    n, C = V.shape
+    Vo = np.empty_like(V, order="F")
+    info = (_int * 4)()
+    dinfo = (_dbl * 2)()
+    err = ctypes.create_string_buffer(512)
+    o = _xopts(tol, tolerance_mode, method, threads, max_iter)
+    rc = rlib().xref_absorb(V[:, 0].ctypes.data, V[:, 1:].ctypes.data if C > 1 else None, n, C - 1,
+                            g.ctypes.data, len(fes), None if w is None else w.ctypes.data,
+                            ctypes.byref(o), Vo[:, 0].ctypes.data,
+                            Vo[:, 1:].ctypes.data if C > 1 else None, info, dinfo, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return {"V": Vo, "iterations": info[0], "converged": bool(info[1]),
+            "precision_certified": bool(info[2]), "abs_residual": dinfo[0],
+            "abs_residual_rel": dinfo[1]}
+
+
+def ref_partial_out(y, X, fes, weights=None, *, tol=1e-8, tolerance_mode="reghdfe-comparable",
+                    threads=1, drop_singletons=True):
+    V, g, _, w = _pack(y, X, fes, [1] * len(fes), weights)
+    n, C = V.shape
+    Vo = np.zeros_like(V, order="F")
+    idx = np.zeros(n, dtype=np.int32)
+    info = (_int * 4)()
+    dinfo = (_dbl * 2)()
+    err = ctypes.create_string_buffer(512)
+    o = _xopts(tol, tolerance_mode, "auto", threads, 0, drop_singletons)
+    rc = rlib().xref_partial_out(V[:, 0].ctypes.data, V[:, 1:].ctypes.data if C > 1 else None, n,
+                                 C - 1, g.ctypes.data, len(fes),
+                                 None if w is None else w.ctypes.data, ctypes.byref(o),
+                                 Vo[:, 0].ctypes.data, Vo[:, 1:].ctypes.data if C > 1 else None,
+                                 idx.ctypes.data, info, dinfo, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    kept = info[3]
+    # partial_out writes kept rows contiguously into each output column of length n
+    Vk = np.empty((kept, C), order="F")
+    Vk[:, 0] = Vo[:kept, 0]
+    if C > 1:
+        flat = Vo[:, 1:].ravel(order="F")[: kept * (C - 1)]
+        Vk[:, 1:] = flat.reshape((kept, C - 1), order="F")
+    return {"V": Vk, "sample_index": idx[:kept].copy(), "iterations": info[0],
+            "converged": bool(info[1]), "precision_certified": bool(info[2]),
+            "abs_residual": dinfo[0], "abs_residual_rel": dinfo[1]}
+
+
+def ref_fit(y, X, fes, weights=None, cluster=None, *, tol=1e-8,
+            tolerance_mode="reghdfe-comparable", threads=1, se_type=None, fit_intercept=False,
+            drop_singletons=True):
+    V, g, _, w = _pack(y, X, fes, [1] * len(fes), weights)
+    n, C = V.shape
+    k = C - 1
+    coef = np.zeros(k + 2)
+    se = np.zeros(k + 2)
+    info = (_int * 6)()
+    dinfo = (_dbl * 4)()
+    err = ctypes.create_string_buffer(512)
+    st = se_type or ("cluster" if cluster is not None else "unadjusted")
+    o = _xopts(tol, tolerance_mode, "auto", threads, 0, drop_singletons, st, fit_intercept)
+    cl = None if cluster is None else np.ascontiguousarray(cluster, dtype=np.int32)
+    rc = rlib().xref_fit(V[:, 0].ctypes.data, V[:, 1:].ctypes.data, n, k, g.ctypes.data, len(fes),
+                         None if w is None else w.ctypes.data,
+                         None if cl is None else cl.ctypes.data, ctypes.byref(o),
+                         coef.ctypes.data, se.ctypes.data, info, dinfo, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    p = info[5]
+    return {"coef": coef[:p].copy(), "se": se[:p].copy(), "iterations": info[0],
+            "converged": bool(info[1]), "precision_certified": bool(info[2]), "nobs": info[3],
+            "num_singletons": info[4], "abs_residual_rel": dinfo[0], "rss": dinfo[1],
+            "r2_within": dinfo[2], "df_a": dinfo[3]}

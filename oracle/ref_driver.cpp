@@ -1,0 +1,219 @@
+// Test infrastructure only: a C-ABI driver over the reference's own CPU core.
+//
+// This file is compiled together with the reference's unmodified C++ sources
+// (src/fe_absorption.cpp, src/hdfe_regressor_v11.cpp, src/ols.cpp, src/iv.cpp,
+// src/schwarz_demean.cpp, src/akm_kss.cpp) by oracle/Makefile into
+// oracle/_ref/libxhdfe_ref.so.  It is the checker that pins the oracle and the
+// timed CPU baseline; nothing in the product links or loads it.
+//
+// Entry points mirror the reference's public calls:
+//   xref_absorb       -> hdfe::detail::absorb_fixed_effects_v6  (src/fe_absorption.cpp:8750)
+//   xref_partial_out  -> hdfe::v11::HdfeRegressorV11::partial_out (src/hdfe_regressor_v11.cpp:10275)
+//   xref_fit          -> hdfe::v11::HdfeRegressorV11::fit         (src/hdfe_regressor_v11.cpp:7522)
+// Every entry point catches all exceptions and returns a nonzero status with
+// the message copied into err (the reference's own fail-closed contract).
+
+#include <Eigen/Dense>
+
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+#include "fe_absorption.hpp"
+#include "hdfe/hdfe_regressor.hpp"
+#include "hdfe/hdfe_regressor_v11.hpp"
+
+namespace {
+
+using Eigen::Map;
+using Eigen::MatrixXd;
+using Eigen::VectorXd;
+using Eigen::VectorXi;
+
+struct XrefOptions {
+    double tol;
+    int tolerance_mode;   // 0 xhdfe-fast, 1 reghdfe-comparable, 2 strict-residual
+    int absorption_method;  // hdfe::AbsorptionMethod integer value
+    int num_threads;
+    int max_iter;
+    int drop_singletons;
+    int se_type;          // 0 homoskedastic, 1 robust, 2 cluster
+    int fit_intercept;
+};
+
+hdfe::HdfeOptions to_options(const XrefOptions* o) {
+    hdfe::HdfeOptions opts;
+    opts.tol = o->tol;
+    opts.tolerance_mode = static_cast<hdfe::ToleranceMode>(o->tolerance_mode);
+    opts.absorption_method = static_cast<hdfe::AbsorptionMethod>(o->absorption_method);
+    opts.num_threads = o->num_threads;
+    opts.num_threads_explicit = o->num_threads > 0;
+    if (o->max_iter > 0) {
+        opts.max_iter = o->max_iter;
+    }
+    opts.drop_singletons = o->drop_singletons != 0;
+    opts.se_type = static_cast<hdfe::StandardErrorType>(o->se_type);
+    opts.fit_intercept = o->fit_intercept != 0;
+    return opts;
+}
+
+std::vector<VectorXi> to_fes(const int32_t* fe_flat, int64_t n, int dims) {
+    std::vector<VectorXi> fes;
+    fes.reserve(static_cast<std::size_t>(dims));
+    for (int d = 0; d < dims; ++d) {
+        VectorXi v(n);
+        std::memcpy(v.data(), fe_flat + static_cast<std::size_t>(d) * n,
+                    sizeof(int32_t) * static_cast<std::size_t>(n));
+        fes.push_back(std::move(v));
+    }
+    return fes;
+}
+
+void set_err(char* err, int err_len, const char* msg) {
+    if (err && err_len > 0) {
+        std::strncpy(err, msg, static_cast<std::size_t>(err_len) - 1);
+        err[err_len - 1] = '\0';
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Demean y (n) and X (n x k, column-major) on all FE dims, no singleton drop.
+// info[0]=iterations info[1]=converged info[2]=precision_certified
+// dinfo[0]=abs_residual dinfo[1]=abs_residual_rel
+int xref_absorb(const double* y, const double* X, int64_t n, int k,
+                const int32_t* fe_flat, int dims, const double* w,
+                const XrefOptions* o, double* y_out, double* X_out,
+                int* info, double* dinfo, char* err, int err_len) {
+    try {
+        Map<const VectorXd> ym(y, n);
+        Map<const MatrixXd> Xm(X, n, k);
+        std::vector<VectorXi> fes = to_fes(fe_flat, n, dims);
+        VectorXd wv;
+        if (w) {
+            wv = Map<const VectorXd>(w, n);
+        }
+        hdfe::HdfeOptions opts = to_options(o);
+        hdfe::detail::AbsorptionResult r = hdfe::detail::absorb_fixed_effects_v6(
+            ym, Xm, fes, w ? &wv : nullptr, opts, opts.absorption_method);
+        std::memcpy(y_out, r.y_tilde.data(), sizeof(double) * static_cast<std::size_t>(n));
+        if (k > 0) {
+            std::memcpy(X_out, r.X_tilde.data(),
+                        sizeof(double) * static_cast<std::size_t>(n) * k);
+        }
+        info[0] = r.iterations;
+        info[1] = r.converged ? 1 : 0;
+        info[2] = r.precision_certified ? 1 : 0;
+        dinfo[0] = r.abs_residual;
+        dinfo[1] = r.abs_residual_rel;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+// HdfeRegressorV11::partial_out with singleton drop.  Outputs are sized n;
+// only the first info[3] rows are written.  sample_index receives the kept
+// 0-based row indices.
+int xref_partial_out(const double* y, const double* X, int64_t n, int k,
+                     const int32_t* fe_flat, int dims, const double* w,
+                     const XrefOptions* o, double* y_out, double* X_out,
+                     int32_t* sample_index, int* info, double* dinfo,
+                     char* err, int err_len) {
+    try {
+        Map<const VectorXd> ym(y, n);
+        Map<const MatrixXd> Xm(X, n, k);
+        std::vector<VectorXi> fes = to_fes(fe_flat, n, dims);
+        VectorXd wv;
+        if (w) {
+            wv = Map<const VectorXd>(w, n);
+        }
+        hdfe::HdfeOptions opts = to_options(o);
+        hdfe::v11::HdfeRegressorV11 reg(opts);
+        hdfe::detail::AbsorptionResult r =
+            reg.partial_out(ym, Xm, fes, w ? &wv : nullptr, nullptr, nullptr);
+        const hdfe::HdfeResults& res = reg.results();
+        const int64_t kept = r.y_tilde.size();
+        std::memcpy(y_out, r.y_tilde.data(), sizeof(double) * static_cast<std::size_t>(kept));
+        if (k > 0) {
+            std::memcpy(X_out, r.X_tilde.data(),
+                        sizeof(double) * static_cast<std::size_t>(kept) * k);
+        }
+        for (int64_t i = 0; i < kept && i < res.sample_index.size(); ++i) {
+            sample_index[i] = res.sample_index[i];
+        }
+        info[0] = r.iterations;
+        info[1] = r.converged ? 1 : 0;
+        info[2] = r.precision_certified ? 1 : 0;
+        info[3] = static_cast<int>(kept);
+        dinfo[0] = r.abs_residual;
+        dinfo[1] = r.abs_residual_rel;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+// HdfeRegressorV11::fit.  coef/se have room for k+1 entries (intercept last
+// when fit_intercept).  cluster may be null (then se_type must not be 2).
+// info[0]=iterations info[1]=converged info[2]=precision_certified
+// info[3]=nobs info[4]=num_singletons info[5]=number of coefficients
+// dinfo[0]=abs_residual_rel dinfo[1]=rss dinfo[2]=r2_within dinfo[3]=df_a
+int xref_fit(const double* y, const double* X, int64_t n, int k,
+             const int32_t* fe_flat, int dims, const double* w,
+             const int32_t* cluster, const XrefOptions* o, double* coef,
+             double* se, int* info, double* dinfo, char* err, int err_len) {
+    try {
+        Map<const VectorXd> ym(y, n);
+        Map<const MatrixXd> Xm(X, n, k);
+        std::vector<VectorXi> fes = to_fes(fe_flat, n, dims);
+        VectorXd wv;
+        if (w) {
+            wv = Map<const VectorXd>(w, n);
+        }
+        std::vector<VectorXi> clusters;
+        if (cluster) {
+            clusters = to_fes(cluster, n, 1);
+        }
+        hdfe::HdfeOptions opts = to_options(o);
+        hdfe::v11::HdfeRegressorV11 reg(opts);
+        reg.fit(ym, Xm, fes, w ? &wv : nullptr, cluster ? &clusters : nullptr);
+        const hdfe::HdfeResults& res = reg.results();
+        const int p = static_cast<int>(res.coefficients.size());
+        for (int j = 0; j < p; ++j) {
+            coef[j] = res.coefficients[j];
+            se[j] = res.std_errors[j];
+        }
+        info[0] = res.num_iterations;
+        info[1] = res.converged ? 1 : 0;
+        info[2] = res.precision_certified ? 1 : 0;
+        info[3] = res.nobs;
+        info[4] = res.num_singletons;
+        info[5] = p;
+        dinfo[0] = res.abs_residual_rel;
+        dinfo[1] = res.rss;
+        dinfo[2] = res.r2_within;
+        dinfo[3] = res.df_a;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+"""GPU parity of the absorber against the oracle, through the C ABI.
+
+Bar: for every column c, ||v~_c - v~*_c|| <= REL_TOL * ||v_c|| where v~* is the
+oracle's tightly converged projection (IT-MAP to 1e-13, pinned against the
+reference core by test_oracle_golden.py).  The solver's own stopping rule is
+the relative residual of the projected normal equations at 1e-10 here.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-8      # relative error of the within transform vs the oracle
+SOLVE_TOL = 1e-10   # solver tolerance used in these tests
+
+
+def _rel_err(V, ref, Vorig):
+    scale = np.linalg.norm(Vorig, axis=0)
+    scale[scale == 0] = 1.0
+    return float((np.linalg.norm(V - ref, axis=0) / scale).max())
+
+
+def _check(absorber, pkg, oracle_mod, y, X, fes, G, w=None, precision="mixed", tol=SOLVE_TOL):
+    o = pkg.make_options(tol=tol, precision=precision)
+    res = absorber.absorb(y, X, fes, G, w, o)
+    assert res.converged
+    V = np.column_stack([res.y_tilde, res.X_tilde])
+    Vorig = np.column_stack([y, X])
+    ref, _, ok = oracle_mod.project(y, X, fes, G, w, tol=1e-13)
+    assert ok
+    err = _rel_err(V, ref, Vorig)
+    assert err <= REL_TOL, f"relative error {err:.3e}"
+    # certificate agrees with the oracle's certificate of the same output
+    a, r = oracle_mod.certify(Vorig, V, fes, G, w)
+    assert res.abs_residual_rel <= max(1e-12, 10 * r) and r <= max(1e-12, 10 * res.abs_residual_rel)
+    return res, V
+
+
+def _akm(panels, n, three_way, seed=0, firms=500):
+    p = panels.akm_two_way(n, n_firms=firms, seed=seed, three_way=three_way)
+    return panels.subset(p, panels.drop_singletons(p.fes))
+
+
+def test_reference_packed_fixture(absorber, pkg, oracle_mod):
+    # tests/test_cg_breakdown.py:_packed_fixture of the reference
+    i = np.arange(120)
+    f1 = (i % 20).astype(np.int32)
+    f2 = ((i * 7 + i // 20) % 20).astype(np.int32)
+    y = 0.7 * np.sin(i / 3) + 0.2 * (f1 - 9.5) + 0.1 * (f2 - 9.5)
+    X = np.cos(i / 5)[:, None]
+    _check(absorber, pkg, oracle_mod, y, X, [f1, f2], [20, 20])
+
+
+def test_reference_soa_fixture_weighted(absorber, pkg, oracle_mod):
+    # tests/test_cg_breakdown.py:_soa_fixture of the reference (unit weights)
+    i = np.arange(40)
+    f1 = (i // 2).astype(np.int32)
+    f2 = ((i + 1) // 2).astype(np.int32)
+    y = np.sin(i / 3) + 0.2 * f1 - 0.1 * f2
+    X = np.cos(i / 5)[:, None]
+    _check(absorber, pkg, oracle_mod, y, X, [f1, f2], [20, 21], w=np.ones(40))
+
+
+def test_validate_backends_design(absorber, pkg, oracle_mod):
+    # tests/validation/VALIDATE_PYTHON_BACKENDS.py:43-54 design (unsorted primary)
+    rng = np.random.default_rng(20260605)
+    n = 50000
+    fe1 = (np.arange(n) % 1000).astype(np.int32)
+    fe2 = (np.arange(n) % 97).astype(np.int32)
+    x1 = rng.normal(size=n)
+    x2 = rng.normal(size=n)
+    X = np.column_stack([x1, x2])
+    y = 1.25 * x1 - 0.70 * x2 + 0.01 * fe1 - 0.02 * fe2 + rng.normal(scale=0.01, size=n)
+    _check(absorber, pkg, oracle_mod, y, X, [fe1, fe2], [1000, 97])
+
+
+@pytest.mark.parametrize("three_way", [False, True])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_akm_panel(absorber, pkg, oracle_mod, panels, three_way, precision):
+    p = _akm(panels, 30_000, three_way)
+    _check(absorber, pkg, oracle_mod, p.y, p.X, p.fes, p.levels, precision=precision)
+
+
+def test_akm_weighted(absorber, pkg, oracle_mod, panels):
+    p = _akm(panels, 30_000, True, seed=5)
+    w = np.random.default_rng(1).lognormal(0.0, 0.5, size=p.n)
+    _check(absorber, pkg, oracle_mod, p.y, p.X, p.fes, p.levels, w=w)
+
+
+def test_akm_shuffled_rows(absorber, pkg, oracle_mod, panels):
+    p = _akm(panels, 30_000, True, seed=7)
+    perm = np.random.default_rng(2).permutation(p.n)
+    fes = [f[perm] for f in p.fes]
+    _check(absorber, pkg, oracle_mod, p.y[perm], p.X[perm], fes, p.levels)
+
+
+def test_single_dimension(absorber, pkg, oracle_mod, panels):
+    p = _akm(panels, 10_000, False)
+    _check(absorber, pkg, oracle_mod, p.y, p.X, p.fes[:1], p.levels[:1])
+
+
+def test_four_dimensions_two_large(absorber, pkg, oracle_mod, panels):
+    p = _akm(panels, 30_000, True, seed=11)
+    fy = p.fes[1].astype(np.int64) * p.levels[2] + p.fes[2]
+    fy, gfy = pkg.dense_ids(fy)
+    fes = p.fes + [fy]
+    keep = panels.drop_singletons(fes)
+    fes = [pkg.dense_ids(f[keep])[0] for f in fes]
+    G = [int(f.max()) + 1 for f in fes]
+    _check(absorber, pkg, oracle_mod, p.y[keep], p.X[keep], fes, G)
+
+
+def test_many_columns_batches(absorber, pkg, oracle_mod, panels):
+    p = _akm(panels, 8_000, True, seed=13)
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((p.n, 39))  # 40 columns with y: two column batches
+    _check(absorber, pkg, oracle_mod, p.y, X, p.fes, p.levels)
+
+
+def test_empty_groups_zero_and_constant_columns(absorber, pkg, oracle_mod, panels):
+    p = _akm(panels, 10_000, True, seed=17)
+    G = [g + 5 for g in p.levels]  # levels without observations
+    X = np.column_stack([p.X, np.zeros(p.n), np.full(p.n, 3.0)])
+    res, V = _check(absorber, pkg, oracle_mod, p.y, X, p.fes, G)
+    assert np.all(V[:, -2] == 0.0)
+    assert np.abs(V[:, -1]).max() < 1e-12
+
+
+def test_bitwise_deterministic(absorber, pkg, panels):
+    p = _akm(panels, 30_000, True, seed=19)
+    o = pkg.make_options(tol=1e-10)
+    r1 = absorber.absorb(p.y, p.X, p.fes, p.levels, None, o)
+    r2 = absorber.absorb(p.y, p.X, p.fes, p.levels, None, o)
+    assert np.array_equal(r1.y_tilde, r2.y_tilde)
+    assert np.array_equal(r1.X_tilde, r2.X_tilde)
+    assert r1.iterations == r2.iterations

@@ -1,0 +1,20 @@
+"""B200-native fixed-effects absorber (drop-in for the reference's CUDA absorber).
+
+The package directory name contains a hyphen, so it is imported through
+``load_package()`` from the repository root helpers as ``xhdfe_xfe_b200``.
+"""
+
+from .absorber import (  # noqa: F401
+    Absorber,
+    AbsorberError,
+    AbsorptionResult,
+    absorb_fixed_effects,
+    cuda_backend_available,
+    demean_raw,
+    dense_ids,
+    drop_singletons_mask,
+    make_options,
+    partial_out,
+)
+
+__version__ = "1.0.0"

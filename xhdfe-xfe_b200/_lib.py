@@ -1,0 +1,126 @@
+"""ctypes binding of libb200fe.so (the C ABI declared in include/b200fe.h).
+
+The library is built in-tree by ``build.py`` next to this file.  Loading fails
+loudly when it is missing: there is no CPU fallback behind this package.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libb200fe.so"
+
+OK, NOT_CONVERGED, UNAVAILABLE, CUDA_ERROR, INVALID_ARG = 0, 1, 2, 3, 4
+PREC_FP64, PREC_MIXED = 0, 1
+MAX_DIMS = 8
+
+STATUS_NAMES = {
+    OK: "ok",
+    NOT_CONVERGED: "not converged",
+    UNAVAILABLE: "CUDA device unavailable",
+    CUDA_ERROR: "CUDA error",
+    INVALID_ARG: "invalid argument",
+}
+
+# Every symbol include/b200fe.h declares.
+EXPORTED_SYMBOLS = (
+    "b200fe_version",
+    "b200fe_device_available",
+    "b200fe_default_options",
+    "b200fe_context_create",
+    "b200fe_context_destroy",
+    "b200fe_last_error",
+    "b200fe_context_stream",
+    "b200fe_absorb",
+    "b200fe_absorb_device",
+    "b200fe_demean_raw",
+    "b200fe_fe_recovery_max_delta",
+)
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("certify", ctypes.c_int),
+        ("check_interval", ctypes.c_int),
+        ("reuse_structure", ctypes.c_int),
+        ("inner_tol", ctypes.c_double),
+        ("tolerance_mode", ctypes.c_int),
+        ("max_outer", ctypes.c_int),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("iterations", ctypes.c_int),
+        ("outer_iterations", ctypes.c_int),
+        ("converged", ctypes.c_int),
+        ("precision_certified", ctypes.c_int),
+        ("primary_dim", ctypes.c_int),
+        ("num_levels_present", ctypes.c_int * MAX_DIMS),
+        ("abs_residual", ctypes.c_double),
+        ("abs_residual_rel", ctypes.c_double),
+        ("rel_residual", ctypes.c_double),
+        ("setup_ms", ctypes.c_double),
+        ("solve_ms", ctypes.c_double),
+        ("h2d_ms", ctypes.c_double),
+        ("d2h_ms", ctypes.c_double),
+        ("kernel_launches", ctypes.c_longlong),
+    ]
+
+
+_LIB = None
+
+
+def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
+    """Load libb200fe.so and declare argument types.  Raises when missing."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise ImportError(
+            f"{p} is missing: build it with build.build() (nvcc, sm_100a); "
+            "this package has no CPU fallback")
+    lib = ctypes.CDLL(str(p))
+    vp, i64, c_int = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    lib.b200fe_version.restype = c_int
+    lib.b200fe_device_available.restype = c_int
+    lib.b200fe_default_options.argtypes = [ctypes.POINTER(Options)]
+    lib.b200fe_default_options.restype = None
+    lib.b200fe_context_create.argtypes = [c_int, ctypes.POINTER(vp)]
+    lib.b200fe_context_create.restype = c_int
+    lib.b200fe_context_destroy.argtypes = [vp]
+    lib.b200fe_context_destroy.restype = None
+    lib.b200fe_last_error.argtypes = [vp]
+    lib.b200fe_last_error.restype = ctypes.c_char_p
+    lib.b200fe_context_stream.argtypes = [vp]
+    lib.b200fe_context_stream.restype = vp
+    lib.b200fe_absorb.argtypes = [vp, vp, vp, i64, c_int, c_int, pp, vp, vp,
+                                  ctypes.POINTER(Options), vp, vp, ctypes.POINTER(Result)]
+    lib.b200fe_absorb.restype = c_int
+    lib.b200fe_absorb_device.argtypes = [vp, vp, i64, c_int, c_int, pp, vp, vp,
+                                         ctypes.POINTER(Options), vp, ctypes.POINTER(Result), vp]
+    lib.b200fe_absorb_device.restype = c_int
+    lib.b200fe_demean_raw.argtypes = [vp, vp, i64, c_int, c_int, pp, vp, ctypes.c_double,
+                                      c_int, ctypes.POINTER(c_int)]
+    lib.b200fe_demean_raw.restype = c_int
+    lib.b200fe_fe_recovery_max_delta.argtypes = [vp, vp, i64, c_int, pp, vp, vp, vp,
+                                                 ctypes.POINTER(ctypes.c_double)]
+    lib.b200fe_fe_recovery_max_delta.restype = c_int
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def default_options(lib=None) -> Options:
+    o = Options()
+    (lib or load()).b200fe_default_options(ctypes.byref(o))
+    return o

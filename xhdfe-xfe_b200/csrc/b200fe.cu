@@ -1,0 +1,1329 @@
+// Host orchestration and C ABI of the B200 fixed-effects absorber.
+//
+// Entry points are declared in include/b200fe.h.  The solver (see
+// kernels.cuh for the math) runs entirely on one CUDA stream owned by the
+// context; the host only reads a handful of per-column scalars between
+// blocks of CG iterations.
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_segmented_reduce.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "b200fe.h"
+#include "kernels.cuh"
+#include "setup_kernels.cuh"
+
+using namespace b200fe;
+
+namespace {
+
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct LargeDim {
+    int dim = -1;
+    int32_t G = 0;
+    int64_t nruns = 0;
+    int64_t nchunks = 0;
+    int64_t nmulti = 0;
+    int32_t *rid = nullptr, *run_base = nullptr, *run_dest = nullptr;
+    int32_t *chunk_grp = nullptr, *chunk_beg = nullptr, *chunk_end = nullptr;
+    uint8_t* chunk_whole = nullptr;
+    int32_t *multi_grp = nullptr, *multi_c0 = nullptr, *multi_c1 = nullptr;
+};
+
+struct Structure {
+    bool valid = false;
+    int64_t n = 0;
+    int D = 0;
+    int p = 0;
+    int32_t G[B200FE_MAX_DIMS] = {0};
+    int32_t present[B200FE_MAX_DIMS] = {0};
+    int nL = 0, nS = 0;
+    LargeDim L[kMaxLarge];
+    int sdim[kMaxSmall] = {0};
+    int32_t sG[kMaxSmall] = {0};
+    int64_t lbase[kMaxLarge] = {0};
+    int64_t sbase[kMaxSmall] = {0};
+    int64_t GR = 0;
+    bool weighted = false;
+    double sum_w2 = 0.0;
+    int32_t* pord = nullptr;
+    int32_t* seg_off = nullptr;
+    double* inv_wp = nullptr;
+    double* wp64 = nullptr;
+    float* wp32 = nullptr;
+    uint32_t* sid = nullptr;
+    double* dinv64 = nullptr;
+    float* dinv32 = nullptr;
+    int32_t* gp = nullptr;  // primary ids in primary order (setup only)
+};
+
+constexpr int32_t kChunkRuns = 64;
+
+}  // namespace
+
+struct b200fe_context {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::unordered_map<std::string, Buf> bufs;
+    Structure st;
+    long long launches = 0;
+    int* h_pinned = nullptr;     // small pinned scratch
+    double* h_pinned_d = nullptr;
+};
+
+namespace {
+
+#define B_TRY(expr)                                                              \
+    do {                                                                         \
+        cudaError_t e_ = (expr);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            ctx->err = std::string(#expr) + ": " + cudaGetErrorString(e_);       \
+            return B200FE_CUDA_ERROR;                                            \
+        }                                                                        \
+    } while (0)
+
+#define B_LAUNCHED()                                                             \
+    do {                                                                         \
+        ++ctx->launches;                                                         \
+        cudaError_t e_ = cudaGetLastError();                                     \
+        if (e_ != cudaSuccess) {                                                 \
+            ctx->err = std::string("kernel launch: ") + cudaGetErrorString(e_);  \
+            return B200FE_CUDA_ERROR;                                            \
+        }                                                                        \
+    } while (0)
+
+#define B_CHECK(...)                                                             \
+    do {                                                                         \
+        int rc_ = (__VA_ARGS__);                                                        \
+        if (rc_ != B200FE_OK) return rc_;                                        \
+    } while (0)
+
+template <typename T>
+int get_buf(b200fe_context* ctx, const std::string& name, size_t count, T** out) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    bytes = (bytes + 255) & ~size_t(255);
+    Buf& b = ctx->bufs[name];
+    if (b.bytes < bytes) {
+        if (b.p) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(b.p);
+            b.p = nullptr;
+            b.bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&b.p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ctx->err = "cudaMalloc(" + name + ", " + std::to_string(bytes) + " B): " +
+                       cudaGetErrorString(e);
+            return B200FE_CUDA_ERROR;
+        }
+        b.bytes = bytes;
+    }
+    *out = static_cast<T*>(b.p);
+    return B200FE_OK;
+}
+
+int grid_for(b200fe_context* ctx, int64_t work, int threads, int per_sm = 8) {
+    int64_t g = (work + threads - 1) / threads;
+    g = std::max<int64_t>(1, std::min<int64_t>(g, static_cast<int64_t>(ctx->num_sms) * per_sm));
+    return static_cast<int>(g);
+}
+
+// ---------------------------------------------------------------------------
+// CUB helpers (setup only)
+// ---------------------------------------------------------------------------
+int cub_exclusive_sum(b200fe_context* ctx, const int32_t* in, int32_t* out, int64_t n) {
+    size_t tmp = 0;
+    B_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, ctx->stream));
+    void* t;
+    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+    B_TRY(cub::DeviceScan::ExclusiveSum(t, tmp, in, out, n, ctx->stream));
+    ++ctx->launches;
+    return B200FE_OK;
+}
+
+int cub_inclusive_sum(b200fe_context* ctx, const int32_t* in, int32_t* out, int64_t n) {
+    size_t tmp = 0;
+    B_TRY(cub::DeviceScan::InclusiveSum(nullptr, tmp, in, out, n, ctx->stream));
+    void* t;
+    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+    B_TRY(cub::DeviceScan::InclusiveSum(t, tmp, in, out, n, ctx->stream));
+    ++ctx->launches;
+    return B200FE_OK;
+}
+
+int bits_for(int32_t G) {
+    int b = 1;
+    while (b < 31 && (int64_t(1) << b) < G) ++b;
+    return b;
+}
+
+// Stable sort of (key, value) pairs by key.
+int cub_sort_pairs(b200fe_context* ctx, const int32_t* keys_in, int32_t* keys_out,
+                   const int32_t* vals_in, int32_t* vals_out, int64_t n, int32_t G) {
+    size_t tmp = 0;
+    const uint32_t* ki = reinterpret_cast<const uint32_t*>(keys_in);
+    uint32_t* ko = reinterpret_cast<uint32_t*>(keys_out);
+    const int eb = bits_for(G);
+    B_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ki, ko, vals_in, vals_out, n, 0, eb,
+                                          ctx->stream));
+    void* t;
+    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+    B_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, ki, ko, vals_in, vals_out, n, 0, eb,
+                                          ctx->stream));
+    ++ctx->launches;
+    return B200FE_OK;
+}
+
+int cub_segmented_sum(b200fe_context* ctx, const double* in, double* out, int32_t nseg,
+                      const int32_t* off) {
+    size_t tmp = 0;
+    B_TRY(cub::DeviceSegmentedReduce::Sum(nullptr, tmp, in, out, nseg, off, off + 1,
+                                          ctx->stream));
+    void* t;
+    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+    B_TRY(cub::DeviceSegmentedReduce::Sum(t, tmp, in, out, nseg, off, off + 1, ctx->stream));
+    ++ctx->launches;
+    return B200FE_OK;
+}
+
+int sync_read_int(b200fe_context* ctx, const int32_t* dptr, int count, int* host) {
+    B_TRY(cudaMemcpyAsync(ctx->h_pinned, dptr, sizeof(int) * count, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+    B_TRY(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(host, ctx->h_pinned, sizeof(int) * count);
+    return B200FE_OK;
+}
+
+int sync_read_double(b200fe_context* ctx, const double* dptr, int count, double* host) {
+    B_TRY(cudaMemcpyAsync(ctx->h_pinned_d, dptr, sizeof(double) * count,
+                          cudaMemcpyDeviceToHost, ctx->stream));
+    B_TRY(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(host, ctx->h_pinned_d, sizeof(double) * count);
+    return B200FE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Structure build
+// ---------------------------------------------------------------------------
+int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const* gids,
+                    const int32_t* G, const double* w) {
+    Structure& st = ctx->st;
+    st = Structure();
+    st.n = n;
+    st.D = D;
+    st.weighted = (w != nullptr);
+    for (int d = 0; d < D; ++d) st.G[d] = G[d];
+    // primary = most levels (first on ties)
+    int p = 0;
+    for (int d = 1; d < D; ++d)
+        if (G[d] > G[p]) p = d;
+    st.p = p;
+    const cudaStream_t s = ctx->stream;
+    const int T256 = 256;
+
+    // validate ids, detect sortedness of the primary
+    int32_t* flags;
+    B_CHECK(get_buf(ctx, "flags", 4, &flags));
+    B_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(int32_t), s));
+    for (int d = 0; d < D; ++d) {
+        validate_ids_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(gids[d], n, G[d], d == p,
+                                                                      flags);
+        B_LAUNCHED();
+    }
+    if (w) {
+        validate_weights_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(w, n, flags);
+        B_LAUNCHED();
+    }
+    int hf[4];
+    B_CHECK(sync_read_int(ctx, flags, 4, hf));
+    if (hf[0]) {
+        ctx->err = "group id outside [0, num_groups)";
+        return B200FE_INVALID_ARG;
+    }
+    if (hf[2]) {
+        ctx->err = "weights must be finite and non-negative";
+        return B200FE_INVALID_ARG;
+    }
+    const bool sorted = hf[1] == 0;
+
+    // primary order
+    int32_t* gp;
+    B_CHECK(get_buf(ctx, "gp", n, &gp));
+    if (sorted) {
+        B_TRY(cudaMemcpyAsync(gp, gids[p], sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+        st.pord = nullptr;
+    } else {
+        int32_t *iota, *pord;
+        B_CHECK(get_buf(ctx, "tmp_n_a", n, &iota));
+        B_CHECK(get_buf(ctx, "pord", n, &pord));
+        iota_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(iota, n);
+        B_LAUNCHED();
+        B_CHECK(cub_sort_pairs(ctx, gids[p], gp, iota, pord, n, G[p]));
+        st.pord = pord;
+    }
+    st.gp = gp;
+
+    // primary segments
+    int32_t *counts, *seg_off;
+    B_CHECK(get_buf(ctx, "counts_p", static_cast<size_t>(G[p]) + 1, &counts));
+    B_CHECK(get_buf(ctx, "seg_off", static_cast<size_t>(G[p]) + 1, &seg_off));
+    B_TRY(cudaMemsetAsync(counts, 0, sizeof(int32_t) * (static_cast<size_t>(G[p]) + 1), s));
+    histogram_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(gp, n, counts);
+    B_LAUNCHED();
+    B_CHECK(cub_exclusive_sum(ctx, counts, seg_off, static_cast<int64_t>(G[p]) + 1));
+    st.seg_off = seg_off;
+
+    // weights in primary order, segment weight sums
+    if (w) {
+        B_CHECK(get_buf(ctx, "wp64", n, &st.wp64));
+        B_CHECK(get_buf(ctx, "wp32", n, &st.wp32));
+        gather_kernel<double><<<grid_for(ctx, n, T256), T256, 0, s>>>(w, st.pord, n, st.wp64);
+        B_LAUNCHED();
+        to_float_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(st.wp64, n, st.wp32);
+        B_LAUNCHED();
+    }
+    B_CHECK(get_buf(ctx, "inv_wp", G[p], &st.inv_wp));
+    double* wsum_p;
+    B_CHECK(get_buf(ctx, "wsum_p", G[p], &wsum_p));
+    segment_inv_weight_kernel<<<grid_for(ctx, G[p], T256), T256, 0, s>>>(seg_off, G[p], st.wp64,
+                                                                          wsum_p, st.inv_wp);
+    B_LAUNCHED();
+
+    // classify the other dims
+    for (int d = 0; d < D; ++d) {
+        if (d == p) continue;
+        if (G[d] <= kSmallLevels && st.nS < kMaxSmall) {
+            st.sdim[st.nS] = d;
+            st.sG[st.nS] = G[d];
+            ++st.nS;
+        } else {
+            if (st.nL >= kMaxLarge) {
+                ctx->err = "more than 2 FE dimensions with over 64 levels besides the largest";
+                return B200FE_INVALID_ARG;
+            }
+            st.L[st.nL].dim = d;
+            st.L[st.nL].G = G[d];
+            ++st.nL;
+        }
+    }
+    int64_t row = 0;
+    for (int l = 0; l < st.nL; ++l) {
+        st.lbase[l] = row;
+        row += st.L[l].G;
+    }
+    for (int j = 0; j < st.nS; ++j) {
+        st.sbase[j] = row;
+        row += st.sG[j];
+    }
+    st.GR = row;
+
+    double *Wall, *Eall;
+    B_CHECK(get_buf(ctx, "diagW", std::max<int64_t>(st.GR, 1), &Wall));
+    B_CHECK(get_buf(ctx, "diagE", std::max<int64_t>(st.GR, 1), &Eall));
+
+    // large dims: ids in primary order, runs, sorted run order, chunks, diagonal
+    for (int l = 0; l < st.nL; ++l) {
+        LargeDim& L = st.L[l];
+        const std::string sfx = std::to_string(l);
+        B_CHECK(get_buf(ctx, "rid" + sfx, n, &L.rid));
+        gather_kernel<int32_t><<<grid_for(ctx, n, T256), T256, 0, s>>>(gids[L.dim], st.pord, n,
+                                                                        L.rid);
+        B_LAUNCHED();
+        int32_t *rflags, *run_id;
+        B_CHECK(get_buf(ctx, "tmp_n_a", n, &rflags));
+        B_CHECK(get_buf(ctx, "tmp_n_b", n, &run_id));
+        run_flags_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(gp, L.rid, n, rflags);
+        B_LAUNCHED();
+        B_CHECK(cub_inclusive_sum(ctx, rflags, run_id, n));
+        int nr = 0;
+        B_CHECK(sync_read_int(ctx, run_id + (n - 1), 1, &nr));
+        L.nruns = nr;
+        int32_t *run_grp, *run_start, *run_seg;
+        B_CHECK(get_buf(ctx, "run_grp", nr, &run_grp));
+        B_CHECK(get_buf(ctx, "run_start", nr, &run_start));
+        B_CHECK(get_buf(ctx, "run_seg", nr, &run_seg));
+        run_fill_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(rflags, run_id, gp, L.rid, n,
+                                                                run_grp, run_start, run_seg);
+        B_LAUNCHED();
+        B_CHECK(get_buf(ctx, "run_base" + sfx, G[p], &L.run_base));
+        run_base_kernel<<<grid_for(ctx, G[p], T256), T256, 0, s>>>(seg_off, G[p], run_id, n,
+                                                                    L.run_base);
+        B_LAUNCHED();
+        // sort runs by group (stable: primary order within a group)
+        int32_t *riota, *sorted_runs, *sorted_grp;
+        B_CHECK(get_buf(ctx, "tmp_n_a", n, &riota));  // flags no longer needed
+        B_CHECK(get_buf(ctx, "sorted_runs", nr, &sorted_runs));
+        B_CHECK(get_buf(ctx, "sorted_grp", nr, &sorted_grp));
+        iota_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(riota, nr);
+        B_LAUNCHED();
+        B_CHECK(cub_sort_pairs(ctx, run_grp, sorted_grp, riota, sorted_runs, nr, L.G));
+        // group offsets over sorted runs
+        int32_t *gcount, *grp_off;
+        B_CHECK(get_buf(ctx, "gcount", static_cast<size_t>(L.G) + 1, &gcount));
+        B_CHECK(get_buf(ctx, "grp_off" + sfx, static_cast<size_t>(L.G) + 1, &grp_off));
+        B_TRY(cudaMemsetAsync(gcount, 0, sizeof(int32_t) * (static_cast<size_t>(L.G) + 1), s));
+        histogram_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(run_grp, nr, gcount);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, gcount, grp_off, static_cast<int64_t>(L.G) + 1));
+        // run destinations and per-run diagonal terms
+        B_CHECK(get_buf(ctx, "run_dest" + sfx, nr, &L.run_dest));
+        double *cw, *ce;
+        B_CHECK(get_buf(ctx, "run_cw", nr, &cw));
+        B_CHECK(get_buf(ctx, "run_ce", nr, &ce));
+        run_weights_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(
+            sorted_runs, nr, run_start, n, run_seg, st.wp64, st.inv_wp, L.run_dest, cw, ce);
+        B_LAUNCHED();
+        B_CHECK(cub_segmented_sum(ctx, cw, Wall + st.lbase[l], L.G, grp_off));
+        B_CHECK(cub_segmented_sum(ctx, ce, Eall + st.lbase[l], L.G, grp_off));
+        // chunk list
+        int32_t *nch, *ch_off, *mflag, *midx;
+        B_CHECK(get_buf(ctx, "nch", static_cast<size_t>(L.G) + 1, &nch));
+        B_CHECK(get_buf(ctx, "ch_off", static_cast<size_t>(L.G) + 1, &ch_off));
+        B_CHECK(get_buf(ctx, "mflag", static_cast<size_t>(L.G) + 1, &mflag));
+        B_CHECK(get_buf(ctx, "midx", static_cast<size_t>(L.G) + 1, &midx));
+        B_TRY(cudaMemsetAsync(nch, 0, sizeof(int32_t) * (static_cast<size_t>(L.G) + 1), s));
+        B_TRY(cudaMemsetAsync(mflag, 0, sizeof(int32_t) * (static_cast<size_t>(L.G) + 1), s));
+        chunk_count_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(grp_off, L.G, kChunkRuns, nch);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, nch, ch_off, static_cast<int64_t>(L.G) + 1));
+        multi_flag_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(nch, L.G, mflag);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, mflag, midx, static_cast<int64_t>(L.G) + 1));
+        int hc[2];
+        B_CHECK(sync_read_int(ctx, ch_off + L.G, 1, &hc[0]));
+        B_CHECK(sync_read_int(ctx, midx + L.G, 1, &hc[1]));
+        L.nchunks = hc[0];
+        L.nmulti = hc[1];
+        B_CHECK(get_buf(ctx, "chunk_grp" + sfx, L.nchunks, &L.chunk_grp));
+        B_CHECK(get_buf(ctx, "chunk_beg" + sfx, L.nchunks, &L.chunk_beg));
+        B_CHECK(get_buf(ctx, "chunk_end" + sfx, L.nchunks, &L.chunk_end));
+        B_CHECK(get_buf(ctx, "chunk_whole" + sfx, L.nchunks, &L.chunk_whole));
+        B_CHECK(get_buf(ctx, "multi_grp" + sfx, L.nmulti, &L.multi_grp));
+        B_CHECK(get_buf(ctx, "multi_c0" + sfx, L.nmulti, &L.multi_c0));
+        B_CHECK(get_buf(ctx, "multi_c1" + sfx, L.nmulti, &L.multi_c1));
+        chunk_fill_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(
+            grp_off, L.G, kChunkRuns, ch_off, L.chunk_grp, L.chunk_beg, L.chunk_end,
+            L.chunk_whole, midx, L.multi_grp, L.multi_c0, L.multi_c1);
+        B_LAUNCHED();
+    }
+
+    // small dims: packed ids and diagonal
+    if (st.nS > 0) {
+        SmallPackArgs pa{};
+        pa.nS = st.nS;
+        for (int j = 0; j < st.nS; ++j) pa.ids[j] = gids[st.sdim[j]];
+        B_CHECK(get_buf(ctx, "sid", n, &st.sid));
+        pack_small_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(pa, st.pord, n, st.sid);
+        B_LAUNCHED();
+        const int nb = ctx->num_sms * 4;
+        double *part, *sw, *se;
+        B_CHECK(get_buf(ctx, "small_part", static_cast<size_t>(nb) * kMaxSmall * kSmallLevels * 2,
+                        &part));
+        B_CHECK(get_buf(ctx, "small_w", kMaxSmall * kSmallLevels, &sw));
+        B_CHECK(get_buf(ctx, "small_e", kMaxSmall * kSmallLevels, &se));
+        small_diag_partial_kernel<<<nb, 128, 0, s>>>(st.sid, st.nS, n, gp, st.wp64, st.inv_wp,
+                                                     part);
+        B_LAUNCHED();
+        small_diag_reduce_kernel<<<1, kMaxSmall * kSmallLevels, 0, s>>>(part, nb, st.nS, sw, se);
+        B_LAUNCHED();
+        for (int j = 0; j < st.nS; ++j) {
+            B_TRY(cudaMemcpyAsync(Wall + st.sbase[j], sw + j * kSmallLevels,
+                                  sizeof(double) * st.sG[j], cudaMemcpyDeviceToDevice, s));
+            B_TRY(cudaMemcpyAsync(Eall + st.sbase[j], se + j * kSmallLevels,
+                                  sizeof(double) * st.sG[j], cudaMemcpyDeviceToDevice, s));
+        }
+    }
+    if (st.GR > 0) {
+        B_CHECK(get_buf(ctx, "dinv64", st.GR, &st.dinv64));
+        B_CHECK(get_buf(ctx, "dinv32", st.GR, &st.dinv32));
+        dinv_kernel<<<grid_for(ctx, st.GR, T256), T256, 0, s>>>(Wall, Eall, st.GR, st.dinv64,
+                                                                 st.dinv32);
+        B_LAUNCHED();
+    }
+    // ||D'W||_F^2 = D * sum w^2
+    if (w) {
+        double *part, *outv;
+        unsigned int* ticket;
+        B_CHECK(get_buf(ctx, "dot_part_w", static_cast<size_t>(ctx->num_sms) * 8, &part));
+        B_CHECK(get_buf(ctx, "dot_out_w", 1, &outv));
+        B_CHECK(get_buf(ctx, "ticket_w", 1, &ticket));
+        B_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
+        row_dot_kernel<double, double><<<grid_for(ctx, n, kRowThreads), kRowThreads, 0, s>>>(
+            n, 1, w, w, part, ticket, outv);
+        B_LAUNCHED();
+        double sw2 = 0.0;
+        B_CHECK(sync_read_double(ctx, outv, 1, &sw2));
+        st.sum_w2 = sw2;
+    } else {
+        st.sum_w2 = static_cast<double>(n);
+    }
+    // levels present per dim (groups with positive weight): primary from
+    // segment weights; the others from the diagonal's weight sums.
+    for (int d = 0; d < D; ++d) st.present[d] = G[d];
+    B_TRY(cudaStreamSynchronize(s));
+    st.valid = true;
+    return B200FE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Solver
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Work {
+    T* R[kMaxLarge];
+    double* bins_partial;
+    double* colsq_partial;
+    double* gather_partial[kMaxLarge];
+    double* fin_partial;
+    double* chunk_partial[kMaxLarge];
+    double* dot_out;
+    unsigned int* ticket;
+    int pass_grid;
+    int pass_smem;
+    int gather_grid[kMaxLarge];
+    int fin_grid;
+};
+
+template <typename T, int CQ>
+int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const int bins_bytes = (kPassThreads / 32) * st.nS * kSmallLevels * CP * sizeof(double);
+    wk.pass_smem = std::max<int>(bins_bytes, kPassThreads * 4 * sizeof(double));
+    // occupancy-sized persistent grid for the primary pass
+    int per_sm = 1;
+    auto kfn = primary_pass_kernel<T, CQ, kMatvec>;
+    if (wk.pass_smem > 48 * 1024) {
+        B_TRY(cudaFuncSetAttribute(primary_pass_kernel<T, CQ, kMatvec>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, wk.pass_smem));
+        B_TRY(cudaFuncSetAttribute(primary_pass_kernel<T, CQ, kRhs>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, wk.pass_smem));
+        B_TRY(cudaFuncSetAttribute(primary_pass_kernel<T, CQ, kFinal>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, wk.pass_smem));
+    }
+    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kPassThreads, wk.pass_smem));
+    per_sm = std::max(1, per_sm);
+    const int64_t groups_needed = (static_cast<int64_t>(st.G[st.p]) + (32 / CQ) - 1) / (32 / CQ);
+    const int64_t blocks_needed = (groups_needed + 3) / 4;
+    wk.pass_grid = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>(blocks_needed, static_cast<int64_t>(ctx->num_sms) * per_sm)));
+    B_CHECK(get_buf(ctx, tag + "bins", static_cast<size_t>(wk.pass_grid) * std::max(st.nS, 1) *
+                                           kSmallLevels * CP, &wk.bins_partial));
+    B_CHECK(get_buf(ctx, tag + "colsq", static_cast<size_t>(wk.pass_grid) * CP, &wk.colsq_partial));
+    for (int l = 0; l < st.nL; ++l) {
+        const std::string sfx = std::to_string(l);
+        B_CHECK(get_buf(ctx, tag + "R" + sfx, static_cast<size_t>(st.L[l].nruns) * CP, &wk.R[l]));
+        wk.gather_grid[l] = grid_for(ctx, st.L[l].nchunks * CQ, kRowThreads, 8);
+        B_CHECK(get_buf(ctx, tag + "gpart" + sfx, static_cast<size_t>(wk.gather_grid[l]) * CP,
+                        &wk.gather_partial[l]));
+        B_CHECK(get_buf(ctx, tag + "cpart" + sfx, static_cast<size_t>(st.L[l].nchunks) * CP,
+                        &wk.chunk_partial[l]));
+    }
+    int64_t items = 0;
+    for (int l = 0; l < st.nL; ++l) items += st.L[l].nmulti * CP;
+    for (int j = 0; j < st.nS; ++j) items += static_cast<int64_t>(st.sG[j]) * CP;
+    wk.fin_grid = grid_for(ctx, std::max<int64_t>(items, 1), kRowThreads, 4);
+    B_CHECK(get_buf(ctx, tag + "fpart", static_cast<size_t>(wk.fin_grid) * CP, &wk.fin_partial));
+    B_CHECK(get_buf(ctx, tag + "dotout", CP, &wk.dot_out));
+    B_CHECK(get_buf(ctx, tag + "ticket", 1, &wk.ticket));
+    B_TRY(cudaMemsetAsync(wk.ticket, 0, sizeof(unsigned int), ctx->stream));
+    return B200FE_OK;
+}
+
+template <typename T>
+PassArgs<T> make_pass_args(const Structure& st, int cols, int CP, const Work<T>& wk) {
+    PassArgs<T> a{};
+    a.n = st.n;
+    a.Gp = st.G[st.p];
+    a.cols = cols;
+    a.CP = CP;
+    a.nL = st.nL;
+    a.nS = st.nS;
+    a.seg_off = st.seg_off;
+    a.inv_wp = st.inv_wp;
+    a.pord = st.pord;
+    for (int l = 0; l < st.nL; ++l) {
+        a.rid[l] = st.L[l].rid;
+        a.run_base[l] = st.L[l].run_base;
+        a.run_dest[l] = st.L[l].run_dest;
+        a.lbase[l] = st.lbase[l];
+        a.R[l] = wk.R[l];
+    }
+    a.sid = st.sid;
+    for (int j = 0; j < st.nS; ++j) a.sbase[j] = st.sbase[j];
+    a.bins_partial = wk.bins_partial;
+    a.colsq_partial = wk.colsq_partial;
+    return a;
+}
+
+// Gathers runs and bins into alpha rows `out`; dot with `dotv` into wk.dot_out.
+template <typename T, int CQ>
+int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const cudaStream_t s = ctx->stream;
+    for (int l = 0; l < st.nL; ++l) {
+        GatherArgs<T> g{};
+        g.CP = CP;
+        g.nchunks = st.L[l].nchunks;
+        g.chunk_grp = st.L[l].chunk_grp;
+        g.chunk_beg = st.L[l].chunk_beg;
+        g.chunk_end = st.L[l].chunk_end;
+        g.chunk_whole = st.L[l].chunk_whole;
+        g.R = wk.R[l];
+        g.out = out + st.lbase[l] * CP;
+        g.partial = wk.chunk_partial[l];
+        g.dotv = dotv ? dotv + st.lbase[l] * CP : nullptr;
+        g.dot_partial = wk.gather_partial[l];
+        run_gather_kernel<T, CQ><<<wk.gather_grid[l], kRowThreads, 0, s>>>(g);
+        B_LAUNCHED();
+    }
+    FinalizeArgs<T> f{};
+    f.CP = CP;
+    f.nL = st.nL;
+    f.nS = st.nS;
+    for (int l = 0; l < st.nL; ++l) {
+        f.nmulti[l] = st.L[l].nmulti;
+        f.multi_grp[l] = st.L[l].multi_grp;
+        f.multi_c0[l] = st.L[l].multi_c0;
+        f.multi_c1[l] = st.L[l].multi_c1;
+        f.partial[l] = wk.chunk_partial[l];
+        f.lbase[l] = st.lbase[l];
+        f.gather_dot_partial[l] = wk.gather_partial[l];
+        f.gather_ctas[l] = dotv ? wk.gather_grid[l] : 0;
+    }
+    for (int j = 0; j < st.nS; ++j) {
+        f.sG[j] = st.sG[j];
+        f.sbase[j] = st.sbase[j];
+    }
+    f.bins_partial = wk.bins_partial;
+    f.nbins_ctas = wk.pass_grid;
+    f.out = out;
+    f.dotv = dotv;
+    f.dot_partial = wk.fin_partial;
+    f.dot_out = dotv ? wk.dot_out : nullptr;
+    f.ticket = wk.ticket;
+    finalize_kernel<T><<<wk.fin_grid, kRowThreads, 0, s>>>(f);
+    B_LAUNCHED();
+    return B200FE_OK;
+}
+
+// q = S x ; pq = x'q (per column) into wk.dot_out
+template <typename T, int CQ>
+int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* x, T* q) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    PassArgs<T> a = make_pass_args<T>(st, 0, CP, wk);
+    a.wp = wp;
+    a.x = x;
+    primary_pass_kernel<T, CQ, kMatvec><<<wk.pass_grid, kPassThreads, wk.pass_smem, ctx->stream>>>(a);
+    B_LAUNCHED();
+    return reduce_runs<T, CQ>(ctx, wk, q, x);
+}
+
+struct ColState {
+    double* rz;
+    double* pq;
+    double* rr;
+    double* thr;
+    double* beta;
+    int* active;
+    int* iters;
+    double* partial;
+    unsigned int* ticket;
+    int* n_active;
+};
+
+// Inner PCG on S x = rhs (rows already in r), T precision.
+// thr_host[c]: stop column c when r'r <= thr (0 or negative: column inactive).
+template <typename T, int CQ>
+int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* dinv, T* x, T* r, T* z,
+        T* p, T* q, const std::vector<double>& thr_host, int max_iter, int check_interval,
+        int* iters_out) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const cudaStream_t s = ctx->stream;
+    const int64_t GR = st.GR;
+    ColState cs{};
+    B_CHECK(get_buf(ctx, "cs_rz", CP, &cs.rz));
+    B_CHECK(get_buf(ctx, "cs_pq", CP, &cs.pq));
+    B_CHECK(get_buf(ctx, "cs_rr", CP, &cs.rr));
+    B_CHECK(get_buf(ctx, "cs_thr", CP, &cs.thr));
+    B_CHECK(get_buf(ctx, "cs_beta", CP, &cs.beta));
+    B_CHECK(get_buf(ctx, "cs_active", CP, &cs.active));
+    B_CHECK(get_buf(ctx, "cs_iters", CP, &cs.iters));
+    B_CHECK(get_buf(ctx, "cs_nactive", 1, &cs.n_active));
+    B_CHECK(get_buf(ctx, "cs_ticket", 1, &cs.ticket));
+    const int rgrid = grid_for(ctx, GR * CP, kRowThreads, 8);
+    B_CHECK(get_buf(ctx, "cs_partial", static_cast<size_t>(rgrid) * 2 * CP, &cs.partial));
+    std::vector<int> act(CP, 0);
+    for (int c = 0; c < CP; ++c) act[c] = thr_host[c] > 0.0 ? 1 : 0;
+    B_TRY(cudaMemcpyAsync(cs.thr, thr_host.data(), sizeof(double) * CP, cudaMemcpyHostToDevice, s));
+    B_TRY(cudaMemcpyAsync(cs.active, act.data(), sizeof(int) * CP, cudaMemcpyHostToDevice, s));
+    B_TRY(cudaMemsetAsync(cs.rz, 0, sizeof(double) * CP, s));
+    B_TRY(cudaMemsetAsync(cs.pq, 0, sizeof(double) * CP, s));
+    B_TRY(cudaMemsetAsync(cs.iters, 0, sizeof(int) * CP, s));
+    B_TRY(cudaMemsetAsync(cs.ticket, 0, sizeof(unsigned int), s));
+    B_TRY(cudaMemsetAsync(x, 0, sizeof(T) * GR * CP, s));
+    B_TRY(cudaStreamSynchronize(s));  // act/thr host vectors are stack-owned
+
+    CgScalars sc{};
+    sc.rz = cs.rz;
+    sc.pq = cs.pq;
+    sc.rr = cs.rr;
+    sc.bb = cs.thr;
+    sc.beta = cs.beta;
+    sc.active = cs.active;
+    sc.iters = cs.iters;
+    sc.partial = cs.partial;
+    sc.ticket = cs.ticket;
+    sc.n_active = cs.n_active;
+    // z = M^-1 r, rz, rr; alpha = 0 because pq = 0
+    cg_update_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x, r, z, p, q, dinv, sc, 1.0, -1);
+    B_LAUNCHED();
+    cg_direction_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, p, z, sc, 1);
+    B_LAUNCHED();
+    int it = 0;
+    int na = 0;
+    B_CHECK(sync_read_int(ctx, cs.n_active, 1, &na));
+    while (na > 0 && it < max_iter) {
+        const int block = std::min(check_interval, max_iter - it);
+        for (int j = 0; j < block; ++j) {
+            B_CHECK(matvec<T, CQ>(ctx, wk, wp, p, q));
+            // pq is in wk.dot_out: copy into the scalar slot
+            B_TRY(cudaMemcpyAsync(cs.pq, wk.dot_out, sizeof(double) * CP, cudaMemcpyDeviceToDevice, s));
+            cg_update_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x, r, z, p, q, dinv, sc, 1.0,
+                                                             it + j);
+            B_LAUNCHED();
+            cg_direction_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, p, z, sc, 0);
+            B_LAUNCHED();
+        }
+        it += block;
+        B_CHECK(sync_read_int(ctx, cs.n_active, 1, &na));
+    }
+    *iters_out = it;
+    return B200FE_OK;
+}
+
+template <int CQ>
+int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
+                const b200fe_options& o, b200fe_result* res) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const cudaStream_t s = ctx->stream;
+    const int64_t GR = st.GR;
+    Work<double> w64{};
+    B_CHECK(prepare_work<double, CQ>(ctx, "w64_", w64));
+    const bool mixed = (o.precision == B200FE_PREC_MIXED) && GR > 0;
+    Work<float> w32{};
+    if (mixed) B_CHECK(prepare_work<float, CQ>(ctx, "w32_", w32));
+
+    double *b64, *a64, *r64, *q64, *z64 = nullptr, *p64 = nullptr, *x64 = nullptr,
+           *rin64 = nullptr;
+    B_CHECK(get_buf(ctx, "b64", GR * CP, &b64));
+    B_CHECK(get_buf(ctx, "a64", GR * CP, &a64));
+    B_CHECK(get_buf(ctx, "r64", GR * CP, &r64));
+    B_CHECK(get_buf(ctx, "q64", GR * CP, &q64));
+    float *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+    if (mixed) {
+        B_CHECK(get_buf(ctx, "x32", GR * CP, &x32));
+        B_CHECK(get_buf(ctx, "r32", GR * CP, &r32));
+        B_CHECK(get_buf(ctx, "z32", GR * CP, &z32));
+        B_CHECK(get_buf(ctx, "p32", GR * CP, &p32));
+        B_CHECK(get_buf(ctx, "q32", GR * CP, &q32));
+    } else {
+        B_CHECK(get_buf(ctx, "rin64", GR * CP, &rin64));
+        B_CHECK(get_buf(ctx, "x64", GR * CP, &x64));
+        B_CHECK(get_buf(ctx, "z64", GR * CP, &z64));
+        B_CHECK(get_buf(ctx, "p64", GR * CP, &p64));
+    }
+    double *scale_d, *inv_scale_d, *dot_part;
+    unsigned int* dot_ticket;
+    double* dot_res;
+    B_CHECK(get_buf(ctx, "scale_d", CP, &scale_d));
+    B_CHECK(get_buf(ctx, "inv_scale_d", CP, &inv_scale_d));
+    const int rgrid = grid_for(ctx, std::max<int64_t>(GR, 1) * CP, kRowThreads, 8);
+    B_CHECK(get_buf(ctx, "rowdot_part", static_cast<size_t>(rgrid) * CP, &dot_part));
+    B_CHECK(get_buf(ctx, "rowdot_ticket", 1, &dot_ticket));
+    B_CHECK(get_buf(ctx, "rowdot_res", CP, &dot_res));
+    B_TRY(cudaMemsetAsync(dot_ticket, 0, sizeof(unsigned int), s));
+
+    // 1. RHS pass: b = D_r' W (I - P_p) v ; ||v||^2 per column
+    {
+        PassArgs<double> a = make_pass_args<double>(st, cols, CP, w64);
+        a.wp = st.wp64;
+        a.v = d_v;
+        primary_pass_kernel<double, CQ, kRhs><<<w64.pass_grid, kPassThreads, w64.pass_smem, s>>>(a);
+        B_LAUNCHED();
+    }
+    std::vector<double> vnorm2(CP, 0.0);
+    {
+        std::vector<double> hp(static_cast<size_t>(w64.pass_grid) * CP);
+        B_TRY(cudaMemcpyAsync(hp.data(), w64.colsq_partial, sizeof(double) * hp.size(),
+                              cudaMemcpyDeviceToHost, s));
+        if (GR > 0) B_CHECK(reduce_runs<double, CQ>(ctx, w64, b64, nullptr));
+        B_TRY(cudaStreamSynchronize(s));
+        for (int b = 0; b < w64.pass_grid; ++b)
+            for (int c = 0; c < CP; ++c) vnorm2[c] += hp[static_cast<size_t>(b) * CP + c];
+    }
+
+    int total_iters = 0, outer = 0;
+    bool converged = true;
+    double rel_res = 0.0;
+    std::vector<double> bb(CP, 0.0), rr(CP, 0.0);
+    if (GR > 0) {
+        row_dot_kernel<double, double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, b64, b64, dot_part,
+                                                                     dot_ticket, dot_res);
+        B_LAUNCHED();
+        B_CHECK(sync_read_double(ctx, dot_res, CP, bb.data()));
+        B_TRY(cudaMemsetAsync(a64, 0, sizeof(double) * GR * CP, s));
+        B_TRY(cudaMemcpyAsync(r64, b64, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
+        rr = bb;
+        const double tol = o.tol;
+        const int max_outer = std::max(1, o.max_outer);
+        converged = false;
+        for (outer = 0; outer < max_outer; ++outer) {
+            bool all = true;
+            std::vector<double> scale(CP, 0.0), inv_scale(CP, 0.0), thr(CP, 0.0);
+            for (int c = 0; c < cols && c < CP; ++c) {
+                const bool done = !(rr[c] > tol * tol * bb[c]);
+                if (!done) {
+                    all = false;
+                    scale[c] = std::sqrt(rr[c]);
+                    inv_scale[c] = 1.0 / scale[c];
+                    // inner target relative to this round's rhs
+                    double t_in = 0.5 * tol * std::sqrt(bb[c] / rr[c]);
+                    if (mixed) t_in = std::max(t_in, o.inner_tol);
+                    t_in = std::min(t_in, 0.5);
+                    thr[c] = t_in * t_in;  // rhs is normalised to unit norm
+                }
+            }
+            if (all) {
+                converged = true;
+                break;
+            }
+            if (total_iters >= o.max_iter) break;
+            B_TRY(cudaMemcpyAsync(scale_d, scale.data(), sizeof(double) * CP, cudaMemcpyHostToDevice, s));
+            B_TRY(cudaMemcpyAsync(inv_scale_d, inv_scale.data(), sizeof(double) * CP,
+                                  cudaMemcpyHostToDevice, s));
+            int its = 0;
+            if (mixed) {
+                scale_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, r32);
+                B_LAUNCHED();
+                B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.dinv32, x32, r32, z32, p32, q32, thr,
+                                        o.max_iter - total_iters, std::max(1, o.check_interval),
+                                        &its)));
+                axpy_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x32, scale_d, a64);
+                B_LAUNCHED();
+            } else {
+                scale_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, rin64);
+                B_LAUNCHED();
+                B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.dinv64, x64, rin64, z64, p64, q64, thr,
+                                         o.max_iter - total_iters, std::max(1, o.check_interval),
+                                         &its)));
+                axpy_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x64, scale_d, a64);
+                B_LAUNCHED();
+            }
+            total_iters += its;
+            // true residual in FP64: r = b - S a
+            B_CHECK((matvec<double, CQ>(ctx, w64, st.wp64, a64, q64)));
+            sub_kernel<<<rgrid, kRowThreads, 0, s>>>(GR * CP, b64, q64, r64);
+            B_LAUNCHED();
+            row_dot_kernel<double, double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, r64, dot_part,
+                                                                         dot_ticket, dot_res);
+            B_LAUNCHED();
+            B_CHECK(sync_read_double(ctx, dot_res, CP, rr.data()));
+        }
+        if (!converged) {
+            bool all = true;
+            for (int c = 0; c < cols && c < CP; ++c)
+                if (rr[c] > tol * tol * bb[c]) all = false;
+            converged = all;
+        }
+        for (int c = 0; c < cols && c < CP; ++c)
+            if (bb[c] > 0.0) rel_res = std::max(rel_res, std::sqrt(rr[c] / bb[c]));
+    }
+
+    // final pass: out = (I - P_p)(v - D_r a); certificate scatter
+    const bool cert = o.certify != 0;
+    {
+        PassArgs<double> a = make_pass_args<double>(st, cols, CP, w64);
+        a.wp = st.wp64;
+        a.v = d_v;
+        a.out = d_out;
+        a.x = a64;
+        a.scatter = cert ? 1 : 0;
+        primary_pass_kernel<double, CQ, kFinal><<<w64.pass_grid, kPassThreads, w64.pass_smem, s>>>(a);
+        B_LAUNCHED();
+    }
+    double abs_res = 0.0, abs_rel = 0.0;
+    if (cert) {
+        std::vector<double> hp(static_cast<size_t>(w64.pass_grid) * CP);
+        B_TRY(cudaMemcpyAsync(hp.data(), w64.colsq_partial, sizeof(double) * hp.size(),
+                              cudaMemcpyDeviceToHost, s));
+        std::vector<double> res2(CP, 0.0);
+        if (GR > 0) {
+            B_CHECK(reduce_runs<double, CQ>(ctx, w64, q64, nullptr));
+            row_dot_kernel<double, double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, q64, q64, dot_part,
+                                                                         dot_ticket, dot_res);
+            B_LAUNCHED();
+            B_CHECK(sync_read_double(ctx, dot_res, CP, res2.data()));
+        }
+        B_TRY(cudaStreamSynchronize(s));
+        for (int b = 0; b < w64.pass_grid; ++b)
+            for (int c = 0; c < CP; ++c) res2[c] += hp[static_cast<size_t>(b) * CP + c];
+        const double opn = std::sqrt(static_cast<double>(st.D) * st.sum_w2);
+        for (int c = 0; c < cols; ++c) {
+            const double ab = std::sqrt(std::max(0.0, res2[c]));
+            const double sc = opn * std::sqrt(std::max(0.0, vnorm2[c]));
+            double rel = 0.0;
+            if (sc > 0.0) rel = ab / sc;
+            else if (ab > 0.0) rel = std::numeric_limits<double>::max();
+            abs_res = std::max(abs_res, ab);
+            abs_rel = std::max(abs_rel, rel);
+        }
+    }
+    B_TRY(cudaStreamSynchronize(s));
+    res->iterations += total_iters;
+    res->outer_iterations = std::max(res->outer_iterations, outer);
+    res->converged = res->converged && converged;
+    res->rel_residual = std::max(res->rel_residual, rel_res);
+    res->abs_residual = std::max(res->abs_residual, abs_res);
+    res->abs_residual_rel = std::max(res->abs_residual_rel, abs_rel);
+    return B200FE_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+namespace {
+
+int check_common(b200fe_context* ctx, int64_t n, int cols, int num_dims, const int32_t* G) {
+    if (!ctx) return B200FE_INVALID_ARG;
+    if (n <= 0 || n >= (int64_t(1) << 31) - 1) {
+        ctx->err = "n must be in [1, 2^31-2]";
+        return B200FE_INVALID_ARG;
+    }
+    if (cols <= 0) {
+        ctx->err = "need at least one column";
+        return B200FE_INVALID_ARG;
+    }
+    if (num_dims < 0 || num_dims > B200FE_MAX_DIMS) {
+        ctx->err = "num_dims must be in [0, 8]";
+        return B200FE_INVALID_ARG;
+    }
+    for (int d = 0; d < num_dims; ++d) {
+        if (!G || G[d] <= 0) {
+            ctx->err = "num_groups must be positive";
+            return B200FE_INVALID_ARG;
+        }
+    }
+    return B200FE_OK;
+}
+
+template <int CQ>
+int solve_dispatch_cq(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
+                      const b200fe_options& o, b200fe_result* res) {
+    return solve_block<CQ>(ctx, d_v, cols, d_out, o, res);
+}
+
+int solve_all(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
+              const b200fe_options& o, b200fe_result* res) {
+    const int64_t n = ctx->st.n;
+    for (int c0 = 0; c0 < cols; c0 += 32) {
+        const int cb = std::min(32, cols - c0);
+        const double* v = d_v + static_cast<int64_t>(c0) * n;
+        double* out = d_out + static_cast<int64_t>(c0) * n;
+        const int cq = (cb + 3) / 4;
+        int rc;
+        if (cq <= 1) rc = solve_dispatch_cq<1>(ctx, v, cb, out, o, res);
+        else if (cq <= 2) rc = solve_dispatch_cq<2>(ctx, v, cb, out, o, res);
+        else if (cq <= 4) rc = solve_dispatch_cq<4>(ctx, v, cb, out, o, res);
+        else rc = solve_dispatch_cq<8>(ctx, v, cb, out, o, res);
+        if (rc != B200FE_OK) return rc;
+    }
+    return B200FE_OK;
+}
+
+double tol_eff(const b200fe_options& o) {
+    if (o.tol > 0.0 && o.tolerance_mode == 1) return std::min(o.tol, 1e-9);
+    return o.tol;
+}
+
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.0f;
+    }
+    return ms;
+}
+
+int absorb_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int cols, int num_dims,
+                       const int32_t* const* d_gids, const int32_t* G, const double* d_w,
+                       const b200fe_options& o, double* d_out, b200fe_result* res) {
+    const cudaStream_t s = ctx->stream;
+    if (num_dims == 0) {
+        if (d_out != d_v)
+            B_TRY(cudaMemcpyAsync(d_out, d_v, sizeof(double) * n * cols, cudaMemcpyDeviceToDevice, s));
+        B_TRY(cudaStreamSynchronize(s));
+        res->converged = 1;
+        res->precision_certified = 1;
+        return B200FE_OK;
+    }
+    cudaEvent_t e0, e1, e2;
+    B_TRY(cudaEventCreate(&e0));
+    B_TRY(cudaEventCreate(&e1));
+    B_TRY(cudaEventCreate(&e2));
+    B_TRY(cudaEventRecord(e0, s));
+    const bool reuse = o.reuse_structure && ctx->st.valid && ctx->st.n == n &&
+                       ctx->st.D == num_dims && ctx->st.weighted == (d_w != nullptr);
+    if (!reuse) {
+        int rc = build_structure(ctx, n, num_dims, d_gids, G, d_w);
+        if (rc != B200FE_OK) {
+            ctx->st.valid = false;
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            cudaEventDestroy(e2);
+            return rc;
+        }
+    }
+    B_TRY(cudaEventRecord(e1, s));
+    res->converged = 1;
+    int rc = solve_all(ctx, d_v, cols, d_out, o, res);
+    B_TRY(cudaEventRecord(e2, s));
+    B_TRY(cudaEventSynchronize(e2));
+    res->setup_ms = reuse ? 0.0 : elapsed_ms(e0, e1);
+    res->solve_ms = elapsed_ms(e1, e2);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    if (rc != B200FE_OK) return rc;
+    res->primary_dim = ctx->st.p;
+    for (int d = 0; d < num_dims; ++d) res->num_levels_present[d] = ctx->st.present[d];
+    const double limit = std::max(8.0 * std::max(0.0, tol_eff(o)),
+                                  64.0 * std::numeric_limits<double>::epsilon());
+    res->precision_certified =
+        res->converged && (o.certify ? res->abs_residual_rel <= limit : 1);
+    return res->converged ? B200FE_OK : B200FE_NOT_CONVERGED;
+}
+
+void clear_result(b200fe_result* r) {
+    std::memset(r, 0, sizeof(*r));
+    r->primary_dim = -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200fe_version(void) { return 10000; }
+
+int b200fe_device_available(void) {
+    int count = 0;
+    const cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return count > 0 ? 1 : 0;
+}
+
+void b200fe_default_options(b200fe_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tol = 1e-8;
+    o->max_iter = 10000;
+    o->precision = B200FE_PREC_MIXED;
+    o->certify = 1;
+    o->check_interval = 4;
+    o->reuse_structure = 0;
+    o->inner_tol = 1e-5;
+    o->tolerance_mode = 1;
+    o->max_outer = 12;
+}
+
+int b200fe_context_create(int device, b200fe_context** out) {
+    if (!out) return B200FE_INVALID_ARG;
+    *out = nullptr;
+    if (!b200fe_device_available()) return B200FE_UNAVAILABLE;
+    cudaGetLastError();
+    b200fe_context* ctx = new (std::nothrow) b200fe_context();
+    if (!ctx) return B200FE_CUDA_ERROR;
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_pinned, 64 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_pinned_d, 64 * sizeof(double));
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b200fe_context_destroy(ctx);
+        return B200FE_CUDA_ERROR;
+    }
+    *out = ctx;
+    return B200FE_OK;
+}
+
+void b200fe_context_destroy(b200fe_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->bufs)
+        if (kv.second.p) cudaFree(kv.second.p);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->h_pinned_d) cudaFreeHost(ctx->h_pinned_d);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    cudaGetLastError();
+    delete ctx;
+}
+
+const char* b200fe_last_error(const b200fe_context* ctx) {
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+void* b200fe_context_stream(b200fe_context* ctx) {
+    return ctx ? static_cast<void*>(ctx->stream) : nullptr;
+}
+
+int b200fe_absorb_device(b200fe_context* ctx, const double* d_v, int64_t n, int cols,
+                         int num_dims, const int32_t* const* d_group_ids,
+                         const int32_t* num_groups, const double* d_weights,
+                         const b200fe_options* opts, double* d_out, b200fe_result* res,
+                         void* stream) {
+    b200fe_result local;
+    b200fe_result* r = res ? res : &local;
+    clear_result(r);
+    int rc = check_common(ctx, n, cols, num_dims, num_groups);
+    if (rc != B200FE_OK) return r->status = rc;
+    if (!d_v || !d_out || (num_dims > 0 && !d_group_ids)) {
+        ctx->err = "null pointer argument";
+        return r->status = B200FE_INVALID_ARG;
+    }
+    b200fe_options o;
+    if (opts) o = *opts;
+    else b200fe_default_options(&o);
+    cudaGetLastError();  // clear a stale non-sticky error from an earlier call
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return r->status = B200FE_UNAVAILABLE;
+    }
+    const cudaStream_t own = ctx->stream;
+    if (stream) ctx->stream = static_cast<cudaStream_t>(stream);
+    const long long l0 = ctx->launches;
+    rc = absorb_device_impl(ctx, d_v, n, cols, num_dims, d_group_ids, num_groups, d_weights, o,
+                            d_out, r);
+    ctx->stream = own;
+    r->kernel_launches = ctx->launches - l0;
+    return r->status = rc;
+}
+
+int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X, int64_t n, int k,
+                  int num_dims, const int32_t* const* group_ids, const int32_t* num_groups,
+                  const double* weights, const b200fe_options* opts, double* y_out,
+                  double* X_out, b200fe_result* res) {
+    b200fe_result local;
+    b200fe_result* r = res ? res : &local;
+    clear_result(r);
+    int rc = check_common(ctx, n, k + 1, num_dims, num_groups);
+    if (rc != B200FE_OK) return r->status = rc;
+    if (!y || !y_out || (k > 0 && (!X || !X_out)) || (num_dims > 0 && !group_ids)) {
+        ctx->err = "null pointer argument";
+        return r->status = B200FE_INVALID_ARG;
+    }
+    for (int d = 0; d < num_dims; ++d)
+        if (!group_ids[d]) {
+            ctx->err = "null group id array";
+            return r->status = B200FE_INVALID_ARG;
+        }
+    b200fe_options o;
+    if (opts) o = *opts;
+    else b200fe_default_options(&o);
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return r->status = B200FE_UNAVAILABLE;
+    }
+    const cudaStream_t s = ctx->stream;
+    const long long l0 = ctx->launches;
+    const int cols = k + 1;
+    auto run = [&]() -> int {
+        double *dv, *dout, *dw = nullptr;
+        B_CHECK(get_buf(ctx, "io_v", static_cast<size_t>(n) * cols, &dv));
+        B_CHECK(get_buf(ctx, "io_out", static_cast<size_t>(n) * cols, &dout));
+        int32_t* dg[B200FE_MAX_DIMS] = {nullptr};
+        for (int d = 0; d < num_dims; ++d)
+            B_CHECK(get_buf(ctx, "io_g" + std::to_string(d), n, &dg[d]));
+        if (weights) B_CHECK(get_buf(ctx, "io_w", n, &dw));
+        cudaEvent_t h0, h1, d0, d1;
+        B_TRY(cudaEventCreate(&h0));
+        B_TRY(cudaEventCreate(&h1));
+        B_TRY(cudaEventCreate(&d0));
+        B_TRY(cudaEventCreate(&d1));
+        B_TRY(cudaEventRecord(h0, s));
+        for (int d = 0; d < num_dims; ++d)
+            B_TRY(cudaMemcpyAsync(dg[d], group_ids[d], sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+        if (weights) B_TRY(cudaMemcpyAsync(dw, weights, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaMemcpyAsync(dv, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        if (k > 0)
+            B_TRY(cudaMemcpyAsync(dv + n, X, sizeof(double) * n * k, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaEventRecord(h1, s));
+        int rc2 = absorb_device_impl(ctx, dv, n, cols, num_dims, dg, num_groups, dw, o, dout, r);
+        if (rc2 != B200FE_OK && rc2 != B200FE_NOT_CONVERGED) return rc2;
+        B_TRY(cudaEventRecord(d0, s));
+        B_TRY(cudaMemcpyAsync(y_out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        if (k > 0)
+            B_TRY(cudaMemcpyAsync(X_out, dout + n, sizeof(double) * n * k, cudaMemcpyDeviceToHost, s));
+        B_TRY(cudaEventRecord(d1, s));
+        B_TRY(cudaEventSynchronize(d1));
+        r->h2d_ms = elapsed_ms(h0, h1);
+        r->d2h_ms = elapsed_ms(d0, d1);
+        cudaEventDestroy(h0);
+        cudaEventDestroy(h1);
+        cudaEventDestroy(d0);
+        cudaEventDestroy(d1);
+        return rc2;
+    };
+    rc = run();
+    r->kernel_launches = ctx->launches - l0;
+    return r->status = rc;
+}
+
+}  // extern "C"
+
+namespace {
+thread_local b200fe_context* tl_ctx = nullptr;
+
+b200fe_context* thread_context() {
+    if (!tl_ctx) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            dev = 0;
+        }
+        if (b200fe_context_create(dev, &tl_ctx) != B200FE_OK) tl_ctx = nullptr;
+    }
+    return tl_ctx;
+}
+
+int fe_recovery_impl(b200fe_context* ctx, const double* residual, int64_t n, int num_dims,
+                     const int32_t* const* group_ids, const int32_t* num_groups,
+                     const double* weights, const int32_t* sweep_order, double* out) {
+    const cudaStream_t s = ctx->stream;
+    double *dv, *dw = nullptr, *mean;
+    int32_t *dg, *iota, *sorted_keys, *ord, *counts, *off;
+    B_CHECK(get_buf(ctx, "rec_v", n, &dv));
+    B_CHECK(get_buf(ctx, "rec_g", n, &dg));
+    B_CHECK(get_buf(ctx, "rec_iota", n, &iota));
+    B_CHECK(get_buf(ctx, "rec_keys", n, &sorted_keys));
+    B_CHECK(get_buf(ctx, "rec_ord", n, &ord));
+    if (weights) {
+        B_CHECK(get_buf(ctx, "rec_w", n, &dw));
+        B_TRY(cudaMemcpyAsync(dw, weights, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    }
+    B_TRY(cudaMemcpyAsync(dv, residual, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    int32_t* flags;
+    B_CHECK(get_buf(ctx, "flags", 4, &flags));
+    double best = 0.0;
+    for (int j = 0; j < num_dims; ++j) {
+        const int d = sweep_order ? sweep_order[j] : j;
+        if (d < 0 || d >= num_dims) {
+            ctx->err = "sweep_order entry out of range";
+            return B200FE_INVALID_ARG;
+        }
+        const int32_t G = num_groups[d];
+        B_TRY(cudaMemcpyAsync(dg, group_ids[d], sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(int32_t), s));
+        validate_ids_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(dg, n, G, 0, flags);
+        B_LAUNCHED();
+        int hf[4];
+        B_CHECK(sync_read_int(ctx, flags, 4, hf));
+        if (hf[0]) {
+            ctx->err = "group id outside [0, num_groups)";
+            return B200FE_INVALID_ARG;
+        }
+        iota_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(iota, n);
+        B_LAUNCHED();
+        B_CHECK(cub_sort_pairs(ctx, dg, sorted_keys, iota, ord, n, G));
+        B_CHECK(get_buf(ctx, "rec_counts", static_cast<size_t>(G) + 1, &counts));
+        B_CHECK(get_buf(ctx, "rec_off", static_cast<size_t>(G) + 1, &off));
+        B_CHECK(get_buf(ctx, "rec_mean", G, &mean));
+        B_TRY(cudaMemsetAsync(counts, 0, sizeof(int32_t) * (static_cast<size_t>(G) + 1), s));
+        histogram_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(dg, n, counts);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, counts, off, static_cast<int64_t>(G) + 1));
+        const int gg = grid_for(ctx, G, 256, 4);
+        double* part;
+        B_CHECK(get_buf(ctx, "rec_part", gg, &part));
+        group_mean_csr_kernel<<<gg, 256, 0, s>>>(off, ord, G, dv, dw, mean, part);
+        B_LAUNCHED();
+        std::vector<double> hp(gg);
+        B_TRY(cudaMemcpyAsync(hp.data(), part, sizeof(double) * gg, cudaMemcpyDeviceToHost, s));
+        subtract_mean_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(dv, dg, mean, n);
+        B_LAUNCHED();
+        B_TRY(cudaStreamSynchronize(s));
+        for (double v : hp) best = std::max(best, v);
+    }
+    *out = best;
+    return B200FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200fe_demean_raw(double* Y, double* X, int64_t n, int k, int num_dims,
+                      const int32_t* const* fe, const int32_t* nlev, double tol, int max_iter,
+                      int* iters_out) {
+    b200fe_context* ctx = thread_context();
+    if (!ctx) return B200FE_UNAVAILABLE;
+    b200fe_options o;
+    b200fe_default_options(&o);
+    if (tol > 0.0) o.tol = tol;
+    if (max_iter > 0) o.max_iter = max_iter;
+    o.certify = 0;
+    b200fe_result r;
+    const int rc = b200fe_absorb(ctx, Y, X, n, k, num_dims, fe, nlev, nullptr, &o, Y, X, &r);
+    if (iters_out) *iters_out = r.iterations;
+    return rc;
+}
+
+int b200fe_fe_recovery_max_delta(b200fe_context* ctx, const double* residual, int64_t n,
+                                 int num_dims, const int32_t* const* group_ids,
+                                 const int32_t* num_groups, const double* weights,
+                                 const int32_t* sweep_order, double* out_max_delta) {
+    if (!ctx || !residual || !out_max_delta || n <= 0 || num_dims < 0 ||
+        num_dims > B200FE_MAX_DIMS || (num_dims > 0 && (!group_ids || !num_groups)))
+        return B200FE_INVALID_ARG;
+    *out_max_delta = 0.0;
+    if (num_dims == 0) return B200FE_OK;
+    for (int d = 0; d < num_dims; ++d)
+        if (num_groups[d] <= 0 || !group_ids[d]) return B200FE_INVALID_ARG;
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return B200FE_UNAVAILABLE;
+    }
+    return fe_recovery_impl(ctx, residual, n, num_dims, group_ids, num_groups, weights,
+                            sweep_order, out_max_delta);
+}
+
+}  // extern "C"

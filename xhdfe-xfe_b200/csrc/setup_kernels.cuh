@@ -1,0 +1,388 @@
+// Setup kernels: build the device-resident FE structure once per call (or
+// once per structure when the caller reuses it).  They replace the host-side
+// indexer work the reference does before every GPU absorption
+// (build_indexer / compute_weight_sums, src/fe_absorption.cpp:845-942, and
+// the CSR offsets of finalize_contiguous_groups, :547-590).
+
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace b200fe {
+
+// flags[0] |= 1 if some id is out of [0, G); flags[1] |= 1 if ids are not
+// non-decreasing (only checked when check_sorted).
+__global__ void validate_ids_kernel(const int32_t* __restrict__ g, int64_t n, int32_t G,
+                                    int check_sorted, int* flags) {
+    int bad = 0, unsorted = 0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t v = g[i];
+        bad |= (v < 0 || v >= G);
+        if (check_sorted && i > 0) unsorted |= (v < g[i - 1]);
+    }
+    bad = __syncthreads_or(bad);
+    unsorted = __syncthreads_or(unsorted);
+    if (threadIdx.x == 0) {
+        if (bad) atomicOr(flags, 1);
+        if (unsorted) atomicOr(flags + 1, 1);
+    }
+}
+
+// flags[2] |= 1 if a weight is negative or not finite.
+__global__ void validate_weights_kernel(const double* __restrict__ w, int64_t n, int* flags) {
+    int bad = 0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double v = w[i];
+        bad |= !(v >= 0.0) || !(v <= 1.7976931348623157e308);
+    }
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0 && bad) atomicOr(flags + 2, 1);
+}
+
+__global__ void iota_kernel(int32_t* __restrict__ out, int64_t n) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<int32_t>(i);
+}
+
+// Integer histogram (exact, order independent).
+__global__ void histogram_kernel(const int32_t* __restrict__ ids, int64_t n,
+                                 int32_t* __restrict__ counts) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        atomicAdd(counts + ids[i], 1);
+}
+
+// Gather a dense id array (or weights) into primary order.
+template <typename V>
+__global__ void gather_kernel(const V* __restrict__ src, const int32_t* __restrict__ ord,
+                              int64_t n, V* __restrict__ dst) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = ord ? src[ord[i]] : src[i];
+}
+
+__global__ void to_float_kernel(const double* __restrict__ src, int64_t n, float* __restrict__ dst) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = static_cast<float>(src[i]);
+}
+
+// Pack the small dims' ids (< 64 levels each) into 8-bit fields.
+struct SmallPackArgs {
+    int nS;
+    const int32_t* ids[kMaxSmall];
+};
+__global__ void pack_small_kernel(SmallPackArgs a, const int32_t* __restrict__ ord, int64_t n,
+                                  uint32_t* __restrict__ sid) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t o = ord ? ord[i] : i;
+        uint32_t p = 0;
+        for (int s = 0; s < a.nS; ++s) p |= (static_cast<uint32_t>(a.ids[s][o]) & 0xffu) << (8 * s);
+        sid[i] = p;
+    }
+}
+
+// Segment weight sums, serial in primary order per segment (deterministic).
+// Unit weights: the count.  Writes 1/W (0 for empty or zero-weight segments).
+__global__ void segment_inv_weight_kernel(const int32_t* __restrict__ seg_off, int32_t G,
+                                          const double* __restrict__ wp,
+                                          double* __restrict__ wsum,
+                                          double* __restrict__ inv_w) {
+    for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < G;
+         s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t b = seg_off[s], e = seg_off[s + 1];
+        double W = 0.0;
+        if (wp) {
+            for (int32_t k = b; k < e; ++k) W += wp[k];
+        } else {
+            W = static_cast<double>(e - b);
+        }
+        if (wsum) wsum[s] = W;
+        inv_w[s] = W > 0.0 ? 1.0 / W : 0.0;
+    }
+}
+
+// Run-start flags of a large dim in primary order: obs k starts a run when it
+// starts its primary segment or its id differs from obs k-1.
+__global__ void run_flags_kernel(const int32_t* __restrict__ gp, const int32_t* __restrict__ rid,
+                                 int64_t n, int32_t* __restrict__ flags) {
+    for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        flags[k] = (k == 0 || gp[k] != gp[k - 1] || rid[k] != rid[k - 1]) ? 1 : 0;
+}
+
+// For run starts: run_grp, run_start, run_seg.  run_id is the inclusive scan.
+__global__ void run_fill_kernel(const int32_t* __restrict__ flags, const int32_t* __restrict__ run_id,
+                                const int32_t* __restrict__ gp, const int32_t* __restrict__ rid,
+                                int64_t n, int32_t* __restrict__ run_grp,
+                                int32_t* __restrict__ run_start, int32_t* __restrict__ run_seg) {
+    for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (flags[k]) {
+            const int32_t m = run_id[k] - 1;
+            run_grp[m] = rid[k];
+            run_start[m] = static_cast<int32_t>(k);
+            run_seg[m] = gp[k];
+        }
+    }
+}
+
+// run_base[s] = index of the first run of segment s.
+__global__ void run_base_kernel(const int32_t* __restrict__ seg_off, int32_t G,
+                                const int32_t* __restrict__ run_id, int64_t n,
+                                int32_t* __restrict__ run_base) {
+    for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < G;
+         s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t b = seg_off[s];
+        run_base[s] = (b < n && seg_off[s + 1] > b) ? run_id[b] - 1 : 0;
+    }
+}
+
+// Per run: weight c_m and its diagonal term c_m^2 / W_seg, written at the
+// run's sorted position.  Also run_dest (inverse of the sorted order).
+__global__ void run_weights_kernel(const int32_t* __restrict__ sorted_runs, int64_t nruns,
+                                   const int32_t* __restrict__ run_start, int64_t n,
+                                   const int32_t* __restrict__ run_seg,
+                                   const double* __restrict__ wp, const double* __restrict__ inv_wp,
+                                   int32_t* __restrict__ run_dest, double* __restrict__ cw_sorted,
+                                   double* __restrict__ ce_sorted) {
+    for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nruns;
+         j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t m = sorted_runs[j];
+        run_dest[m] = static_cast<int32_t>(j);
+        const int32_t b = run_start[m];
+        const int32_t e = (m + 1 < nruns) ? run_start[m + 1] : static_cast<int32_t>(n);
+        double c = 0.0;
+        if (wp) {
+            for (int32_t k = b; k < e; ++k) c += wp[k];
+        } else {
+            c = static_cast<double>(e - b);
+        }
+        cw_sorted[j] = c;
+        ce_sorted[j] = c * c * inv_wp[run_seg[m]];
+    }
+}
+
+// Chunk list of a large dim: group g owns runs [grp_off[g], grp_off[g+1]),
+// split into ceil(len/CH) chunks (one chunk for an empty group).
+__global__ void chunk_count_kernel(const int32_t* __restrict__ grp_off, int32_t G, int32_t CH,
+                                   int32_t* __restrict__ nch) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t len = grp_off[g + 1] - grp_off[g];
+        nch[g] = len <= CH ? 1 : (len + CH - 1) / CH;
+    }
+}
+
+__global__ void chunk_fill_kernel(const int32_t* __restrict__ grp_off, int32_t G, int32_t CH,
+                                  const int32_t* __restrict__ ch_off,
+                                  int32_t* __restrict__ chunk_grp, int32_t* __restrict__ chunk_beg,
+                                  int32_t* __restrict__ chunk_end, uint8_t* __restrict__ chunk_whole,
+                                  const int32_t* __restrict__ multi_idx,
+                                  int32_t* __restrict__ multi_grp, int32_t* __restrict__ multi_c0,
+                                  int32_t* __restrict__ multi_c1) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t b = grp_off[g], e = grp_off[g + 1];
+        const int32_t c0 = ch_off[g], c1 = ch_off[g + 1];
+        const bool whole = (c1 - c0) == 1;
+        for (int32_t c = c0; c < c1; ++c) {
+            const int32_t cb = b + (c - c0) * CH;
+            chunk_grp[c] = static_cast<int32_t>(g);
+            chunk_beg[c] = cb;
+            chunk_end[c] = min(e, cb + CH);
+            chunk_whole[c] = whole ? 1 : 0;
+        }
+        if (!whole) {
+            const int32_t mi = multi_idx[g];
+            multi_grp[mi] = static_cast<int32_t>(g);
+            multi_c0[mi] = c0;
+            multi_c1[mi] = c1;
+        }
+    }
+}
+
+__global__ void multi_flag_kernel(const int32_t* __restrict__ nch, int32_t G, int32_t* __restrict__ f) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        f[g] = nch[g] > 1 ? 1 : 0;
+}
+
+// Small dims: per-level weight sum and diagonal correction, deterministic:
+// each warp owns a contiguous range, lanes update the warp's bins one at a
+// time, CTA partials are summed in a fixed order by small_diag_reduce_kernel.
+__global__ void __launch_bounds__(128)
+small_diag_partial_kernel(const uint32_t* __restrict__ sid, int nS, int64_t n,
+                          const int32_t* __restrict__ gp, const double* __restrict__ wp,
+                          const double* __restrict__ inv_wp, double* __restrict__ partial) {
+    __shared__ double bins[4][kMaxSmall * kSmallLevels * 2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < 4 * kMaxSmall * kSmallLevels * 2; i += 128)
+        (&bins[0][0])[i] = 0.0;
+    __syncthreads();
+    const int64_t per_block = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t b0 = static_cast<int64_t>(blockIdx.x) * per_block;
+    const int64_t b1 = min(n, b0 + per_block);
+    const int64_t per_warp = (max(b1 - b0, int64_t(0)) + 3) / 4;
+    const int64_t w0 = b0 + warp * per_warp, w1 = min(b1, w0 + per_warp);
+    for (int64_t base = w0; base < w1; base += 32) {
+        const int64_t k = base + lane;
+        const bool valid = k < w1;
+        uint32_t packed = 0;
+        double w = 0.0, e = 0.0;
+        if (valid) {
+            packed = sid[k];
+            w = wp ? wp[k] : 1.0;
+            e = w * w * inv_wp[gp[k]];
+        }
+        for (int j = 0; j < 32; ++j) {
+            __syncwarp();
+            if (lane == j && valid) {
+                for (int s = 0; s < nS; ++s) {
+                    const uint32_t h = (packed >> (8 * s)) & 0xffu;
+                    bins[warp][(s * kSmallLevels + h) * 2 + 0] += w;
+                    bins[warp][(s * kSmallLevels + h) * 2 + 1] += e;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nS * kSmallLevels * 2; i += 128)
+        partial[static_cast<int64_t>(blockIdx.x) * kMaxSmall * kSmallLevels * 2 + i] =
+            ((bins[0][i] + bins[1][i]) + bins[2][i]) + bins[3][i];
+}
+
+__global__ void small_diag_reduce_kernel(const double* __restrict__ partial, int nblocks, int nS,
+                                         double* __restrict__ wsum_out, double* __restrict__ e_out) {
+    const int i = threadIdx.x;  // over nS * 64
+    if (i >= nS * kSmallLevels) return;
+    double W = 0.0, E = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        W += partial[static_cast<int64_t>(b) * kMaxSmall * kSmallLevels * 2 + 2 * i];
+        E += partial[static_cast<int64_t>(b) * kMaxSmall * kSmallLevels * 2 + 2 * i + 1];
+    }
+    wsum_out[i] = W;
+    e_out[i] = E;
+}
+
+// dinv = 1/(W - E) for identified unknowns, 0 for levels without weight or in
+// the null space of S (diagonal below 1e-11 of the level weight).
+__global__ void dinv_kernel(const double* __restrict__ W, const double* __restrict__ E, int64_t G,
+                            double* __restrict__ dinv64, float* __restrict__ dinv32) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double d = W[g] - E[g];
+        const double v = (W[g] > 0.0 && d > 1e-11 * W[g]) ? 1.0 / d : 0.0;
+        dinv64[g] = v;
+        dinv32[g] = static_cast<float>(v);
+    }
+}
+
+// Column-wise dot of two alpha-row arrays with a last-CTA fixed-order reduce.
+template <typename A, typename B>
+__global__ void __launch_bounds__(kRowThreads)
+row_dot_kernel(int64_t GR, int CP, const A* __restrict__ a, const B* __restrict__ b,
+               double* __restrict__ partial, unsigned int* ticket, double* __restrict__ out) {
+    __shared__ double red[kRowThreads];
+    __shared__ bool last;
+    const int64_t total = GR * CP;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kRowThreads;
+    double s = 0.0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * kRowThreads + threadIdx.x; i < total;
+         i += stride)
+        s = fma(static_cast<double>(a[i]), static_cast<double>(b[i]), s);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x < CP) {
+        double t = 0.0;
+        for (int k = threadIdx.x; k < kRowThreads; k += CP) t += red[k];
+        partial[static_cast<int64_t>(blockIdx.x) * CP + threadIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < CP) {
+        double t = 0.0;
+        for (int bb = 0; bb < static_cast<int>(gridDim.x); ++bb)
+            t += __ldcg(partial + static_cast<int64_t>(bb) * CP + threadIdx.x);
+        out[threadIdx.x] = t;
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// Elementwise helpers over alpha rows.
+// dst = src64 * inv_scale[c]   (per-column scaling of an inner right-hand side)
+template <typename T>
+__global__ void scale_rows_kernel(int64_t GR, int CP, const double* __restrict__ src,
+                                  const double* __restrict__ inv_scale, T* __restrict__ dst) {
+    const int64_t total = GR * CP;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = static_cast<T>(src[i] * inv_scale[i % CP]);
+}
+// a64 += scale[c] * x
+template <typename T>
+__global__ void axpy_rows_kernel(int64_t GR, int CP, const T* __restrict__ x,
+                                 const double* __restrict__ scale, double* __restrict__ a) {
+    const int64_t total = GR * CP;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        a[i] += scale[i % CP] * static_cast<double>(x[i]);
+}
+// r = b - q
+__global__ void sub_kernel(int64_t total, const double* __restrict__ b, const double* __restrict__ q,
+                           double* __restrict__ r) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        r[i] = b[i] - q[i];
+}
+
+// Gauss-Seidel max-delta (FE recovery check): means of dim d over the
+// residual, then subtract.  Deterministic per-group serial sums over a CSR.
+__global__ void group_mean_csr_kernel(const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
+                                      int32_t G, const double* __restrict__ v,
+                                      const double* __restrict__ w, double* __restrict__ mean,
+                                      double* __restrict__ absmax_partial) {
+    double mx = 0.0;
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double s = 0.0, W = 0.0;
+        for (int32_t j = off[g]; j < off[g + 1]; ++j) {
+            const int32_t i = ord[j];
+            const double wi = w ? w[i] : 1.0;
+            s += wi * v[i];
+            W += wi;
+        }
+        const double m = W > 0.0 ? s / W : 0.0;
+        mean[g] = m;
+        mx = fmax(mx, fabs(m));
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = mx;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + st]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) absmax_partial[blockIdx.x] = red[0];
+}
+
+__global__ void subtract_mean_kernel(double* __restrict__ v, const int32_t* __restrict__ gid,
+                                     const double* __restrict__ mean, int64_t n) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        v[i] -= mean[gid[i]];
+}
+
+}  // namespace b200fe
