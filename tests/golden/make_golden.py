@@ -1,0 +1,141 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own CPU core.
+
+Run in a container where oracle/_ref/libxhdfe_ref.so was built from the
+reference sources (oracle/Makefile, target ``ref``):
+
+    python tests/golden/make_golden.py
+
+For each case it stores, in <case>.npz:
+  * sha256 digests of the generated inputs (the generators are re-run by the
+    tests, which check the digests first);
+  * the reference's near-exact within transform (absorb_fixed_effects_v6,
+    strict-residual mode, tol 1e-14) on a fixed subset of rows, plus the
+    per-column norms of the full transform;
+  * the reference's result at tol 1e-8 (reghdfe-comparable): iterations,
+    converged, abs_residual_rel;
+  * the reference's HdfeRegressorV11::fit coefficients and standard errors.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+import __graft_entry__ as ge  # noqa: E402
+import oracle  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def digest(*arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        a = np.ascontiguousarray(a)
+        h.update(str(a.dtype).encode())
+        h.update(str(a.shape).encode())
+        h.update(a.tobytes())
+    return h.hexdigest()
+
+
+def case_packed120():
+    i = np.arange(120)
+    f1 = (i % 20).astype(np.int32)
+    f2 = ((i * 7 + i // 20) % 20).astype(np.int32)
+    y = 0.7 * np.sin(i / 3) + 0.2 * (f1 - 9.5) + 0.1 * (f2 - 9.5)
+    X = np.cos(i / 5)[:, None]
+    return dict(y=y, X=X, fes=[f1, f2], weights=None, cluster=None)
+
+
+def case_soa40():
+    i = np.arange(40)
+    f1 = (i // 2).astype(np.int32)
+    f2 = ((i + 1) // 2).astype(np.int32)
+    y = np.sin(i / 3) + 0.2 * f1 - 0.1 * f2
+    X = np.cos(i / 5)[:, None]
+    return dict(y=y, X=X, fes=[f1, f2], weights=np.ones(40), cluster=None)
+
+
+def case_validate50k():
+    rng = np.random.default_rng(20260605)
+    n = 50000
+    fe1 = (np.arange(n) % 1000).astype(np.int32)
+    fe2 = (np.arange(n) % 97).astype(np.int32)
+    x1 = rng.normal(size=n)
+    x2 = rng.normal(size=n)
+    X = np.column_stack([x1, x2])
+    y = 1.25 * x1 - 0.70 * x2 + 0.01 * fe1 - 0.02 * fe2 + rng.normal(scale=0.01, size=n)
+    return dict(y=y, X=X, fes=[fe1, fe2], weights=None, cluster=None)
+
+
+def _akm(n, three_way, seed, weighted=False):
+    panels = ge.load_module("panels")
+    p = panels.akm_two_way(n, n_firms=2000, n_years=10, seed=seed, three_way=three_way)
+    p = panels.subset(p, panels.drop_singletons(p.fes))
+    w = None
+    if weighted:
+        w = np.random.default_rng(seed + 1000).lognormal(0.0, 0.5, size=p.n)
+    return dict(y=p.y, X=np.asarray(p.X), fes=p.fes, weights=w, cluster=p.cluster)
+
+
+CASES = {
+    "packed120": case_packed120,
+    "soa40": case_soa40,
+    "validate50k": case_validate50k,
+    "akm2_20k": lambda: _akm(20_000, False, 101),
+    "akm3_20k": lambda: _akm(20_000, True, 102),
+    "akm3w_20k": lambda: _akm(20_000, True, 103, weighted=True),
+}
+
+
+def subset_rows(n: int) -> np.ndarray:
+    step = max(1, n // 400)
+    rows = np.unique(np.concatenate([np.arange(0, n, step), np.arange(max(0, n - 5), n)]))
+    return rows.astype(np.int64)
+
+
+def make(name: str) -> dict:
+    c = CASES[name]()
+    y, X, fes, w, cl = c["y"], np.asarray(c["X"]), c["fes"], c["weights"], c["cluster"]
+    n = y.shape[0]
+    exact = oracle.ref_absorb(y, X, fes, w, tol=1e-14, tolerance_mode="strict-residual",
+                              method="gauss-seidel", threads=1, max_iter=1_000_000)
+    comp = oracle.ref_absorb(y, X, fes, w, tol=1e-8, tolerance_mode="reghdfe-comparable",
+                             method="auto", threads=1)
+    fit = oracle.ref_fit(y, X, fes, w, cl, tol=1e-12, tolerance_mode="strict-residual",
+                         threads=1, fit_intercept=False, drop_singletons=False)
+    rows = subset_rows(n)
+    levels = [int(np.asarray(f).max()) + 1 for f in fes]
+    meta = {
+        "case": name, "n": n, "k": int(X.shape[1]), "levels": levels,
+        "weighted": w is not None, "clustered": cl is not None,
+        "exact_iterations": exact["iterations"], "exact_converged": exact["converged"],
+        "exact_abs_residual_rel": exact["abs_residual_rel"],
+        "comparable_iterations": comp["iterations"], "comparable_converged": comp["converged"],
+        "comparable_abs_residual_rel": comp["abs_residual_rel"],
+        "comparable_precision_certified": comp["precision_certified"],
+        "fit_iterations": fit["iterations"], "fit_nobs": fit["nobs"],
+        "input_digest": digest(y, X, *[np.asarray(f, dtype=np.int32) for f in fes],
+                               *( [w] if w is not None else [])),
+    }
+    np.savez_compressed(
+        OUT / f"{name}.npz", rows=rows, exact_rows=exact["V"][rows],
+        exact_colnorm=np.linalg.norm(exact["V"], axis=0),
+        comparable_rows=comp["V"][rows], coef=fit["coef"], se=fit["se"],
+        meta=np.array(json.dumps(meta)))
+    return meta
+
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or list(CASES)
+    for nm in names:
+        m = make(nm)
+        print(json.dumps({k: m[k] for k in ("case", "n", "exact_iterations",
+                                            "exact_abs_residual_rel",
+                                            "comparable_iterations")}))
