@@ -1,0 +1,376 @@
+"""Benchmark: demeaning time to 1e-8, AKM three-way panel, 50M observations.
+
+Workload: the seeded AKM generator at N = 50,000,000 observations (about 5M
+workers, 800k firms with Zipf(1.1) sizes, 36 years), the outcome plus 12
+regressors (13 columns), singletons dropped, three FE dimensions absorbed to a
+relative tolerance of 1e-8.  A step is one complete absorption call: FE
+structure build, right-hand side, preconditioned CG with FP64 refinement,
+within transform and device certificate.
+
+Lines printed by rank 0 (one JSON line):
+  value    seconds per absorption with inputs resident in HBM (max over ranks)
+  e2e      same call through the C ABI with pinned host buffers, the host to
+           device copy of y, X and the ids and the copy back of the within
+           transform inside the timed region
+  roofline the dominant kernel's algorithmic bytes / its CUDA-event time
+  cpu_baseline  the reference's own CPU core (oracle/_ref) on a bounded
+           sample of the same workload, scaled linearly in N to 50M rows
+
+--impl reference runs the reference's own CPU core instead (rank 0 only).
+With --gpus N > 1 every rank absorbs its own replica panel (no collective in
+the data path; replicas only), launched by torch.distributed.run.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import __graft_entry__ as ge  # noqa: E402
+
+METRIC = "demeaning time to 1e-8 tol, AKM 3-way 50M obs (13 columns, one absorption call)"
+UNIT = "s"
+N_OBS = 50_000_000
+N_FIRMS = 800_000
+N_YEARS = 36
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_OBS)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    return ap.parse_args()
+
+
+def make_panel(n: int, seed: int):
+    panels = ge.load_module("panels")
+    firms = max(1000, int(N_FIRMS * n / N_OBS))
+    p = panels.akm_batched(n, n_firms=firms, n_years=N_YEARS, seed=seed)
+    keep = panels.drop_singletons(p.fes)
+    return panels.subset(p, keep)
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()), "measured"
+        except ValueError:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the hot kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except ValueError:
+            return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU core on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_baseline(sample_n: int, threads: int):
+    import oracle
+    if not oracle.ref_available():
+        return None
+    p = make_panel(sample_n, seed=12345)
+    t0 = time.perf_counter()
+    r = oracle.ref_absorb(p.y, p.X, p.fes, None, tol=1e-8, tolerance_mode="reghdfe-comparable",
+                          method="auto", threads=threads)
+    dt = time.perf_counter() - t0
+    return {
+        "value": dt * (N_OBS / p.n), "unit": UNIT, "cores": threads, "kind": "reference",
+        "sample": (f"reference CPU core (absorb_fixed_effects_v6, reghdfe-comparable tol 1e-8, "
+                   f"{threads} threads) on a {p.n}-row panel of the same generator "
+                   f"({p.levels} levels, 13 columns): {dt:.3f} s, scaled linearly to 50M rows"),
+        "sample_seconds": dt, "sample_rows": p.n, "iterations": r["iterations"],
+        "converged": r["converged"],
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = cpu_baseline(args.cpu_sample, threads)
+        if info is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "reference CPU core (oracle/_ref/libxhdfe_ref.so) was not built"}))
+            return 0
+        if i >= args.warmup:
+            vals.append(info["value"])
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000.0,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded AKM generator)",
+        "config": {"workload": "akm_3way_50M_13col_demean", "n_obs": N_OBS, "columns": 13,
+                   "fe_dims": ["worker", "firm", "year"], "tol": 1e-8,
+                   "sample_rows": info["sample_rows"]},
+        "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    pkg = ge.load_package()
+    t0 = time.perf_counter()
+    panel = make_panel(args.n, seed=rank)
+    gen_s = time.perf_counter() - t0
+    n, k = panel.n, panel.k
+    cols = k + 1
+    dev = torch.device("cuda", local)
+    v = torch.empty((cols, n), dtype=torch.float64, device=dev)
+    v[0].copy_(torch.from_numpy(panel.y))
+    v[1:].copy_(torch.from_numpy(np.ascontiguousarray(panel.X.T)))
+    gids = [torch.from_numpy(f).to(dev) for f in panel.fes]
+    out = torch.empty_like(v)
+    absorber = pkg.Absorber(local)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    def step(opts):
+        return absorber.absorb_device(v, gids, panel.levels, None, opts, out=out, stream=sh)[1]
+
+    opts = pkg.make_options(tol=1e-8, precision=args.precision, profile=True)
+    for _ in range(args.warmup):
+        step(opts)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    results = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        results.append(step(opts))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    r_last = results[-1]
+    launches = int(sum(r.kernel_launches for r in results))
+    lib_calls = int(sum(r.library_calls for r in results))
+
+    # per-category profile over the timed steps
+    libm = ge.load_module("_lib")
+    prof = {}
+    for ci, name in enumerate(libm.PROF_NAMES):
+        tms = sum(r.prof_ms[ci] for r in results)
+        tb = sum(r.prof_bytes[ci] for r in results)
+        nl = sum(r.prof_launches[ci] for r in results)
+        if nl:
+            prof[name] = {"ms_total": tms, "launches": int(nl), "bytes_total": tb,
+                          "gbs": (tb / (tms * 1e-3) / 1e9) if tms > 0 else None,
+                          "share": tms / (ms * args.steps)}
+    hot = max((k2 for k2 in prof if k2 != "setup"), key=lambda k2: prof[k2]["ms_total"])
+    peaks, peak_kind = measured_peaks()
+    hp = prof[hot]
+    achieved = hp["bytes_total"] / (hp["ms_total"] * 1e-3) / 1e9
+    traffic = committed_traffic()
+    roofline = {
+        "kernel": hot, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+        "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_kind": peak_kind,
+        "bytes_per_launch": hp["bytes_total"] / hp["launches"],
+        "ms_per_launch": hp["ms_total"] / hp["launches"],
+        "traffic": (traffic or {}).get(hot, {}).get("dram_bytes_per_launch") if traffic else None,
+    }
+
+    # plain FP64 on the same GPU (the comparison the metric names)
+    fp64 = None
+    if not args.no_fp64_compare and args.precision != "fp64":
+        o64 = pkg.make_options(tol=1e-8, precision="fp64")
+        step(o64)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r64 = [step(o64) for _ in range(2)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fp64 = {"ms_per_step": e0.elapsed_time(e1) / 2, "iterations": r64[-1].iterations,
+                "rel_residual": r64[-1].rel_residual}
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        y_h = torch.from_numpy(panel.y).pin_memory().numpy()
+        X_h = torch.from_numpy(np.ascontiguousarray(panel.X.T)).pin_memory().numpy().T
+        g_h = [torch.from_numpy(f).pin_memory().numpy() for f in panel.fes]
+        yo = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        Xo = torch.empty((k, n), dtype=torch.float64).pin_memory().numpy().T
+        o_e = pkg.make_options(tol=1e-8, precision=args.precision)
+        absorber.absorb(y_h, X_h, g_h, panel.levels, None, o_e, y_out=yo, X_out=Xo)
+        times = []
+        for _ in range(args.e2e_steps):
+            if dist:
+                dist.barrier()
+            t1 = time.perf_counter()
+            re = absorber.absorb(y_h, X_h, g_h, panel.levels, None, o_e, y_out=yo, X_out=Xo)
+            times.append(time.perf_counter() - t1)
+        et = statistics.median(times)
+        if dist:
+            t = torch.tensor([et], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            et = float(t.item())
+        e2e = {"value": et, "unit": UNIT,
+               "h2d_bytes_per_step": int(n * cols * 8 + n * 4 * len(panel.fes)),
+               "d2h_bytes_per_step": int(n * cols * 8),
+               "h2d_ms": re.h2d_ms, "d2h_ms": re.d2h_ms, "converged": re.converged}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_sample, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms / 1000.0, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner CG + f64 refinement" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded AKM generator, per-rank replica seed = rank)",
+            "config": {"workload": "akm_3way_50M_13col_demean", "n_obs_generated": args.n,
+                       "n_obs_after_singleton_drop": n, "columns": cols,
+                       "fe_dims": ["worker", "firm", "year"], "levels": panel.levels,
+                       "tol": 1e-8, "precision": args.precision,
+                       "l2_policy": "inputs larger than L2 (5.2 GB of columns per step)",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": launches, "library_calls": lib_calls,
+            "iterations": r_last.iterations, "outer_iterations": r_last.outer_iterations,
+            "converged": bool(r_last.converged), "rel_residual": r_last.rel_residual,
+            "abs_residual_rel": r_last.abs_residual_rel,
+            "precision_certified": bool(r_last.precision_certified),
+            "setup_ms": r_last.setup_ms, "solve_ms": r_last.solve_ms,
+            "roofline": roofline, "profile": prof, "clocks": clocks,
+            "fp64_plain": fp64,
+            "e2e": e2e, "cpu_baseline": cpu, "generate_s": gen_s,
+        }
+        print(json.dumps(line))
+    absorber.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -58,7 +58,18 @@ typedef struct b200fe_options {
     int tolerance_mode;    /* certificate limit as the reference: 0 xhdfe-fast,
                               1 reghdfe-comparable (tol_eff = min(tol, 1e-9)), 2 strict (1)  */
     int max_outer;         /* MIXED: cap on refinement rounds (default 12)                    */
+    int profile;           /* 1: time every kernel category with CUDA events (default 0)      */
 } b200fe_options;
+
+/* Kernel categories of the profile arrays in b200fe_result. */
+#define B200FE_PROF_PASS 0      /* alpha-space primary-segment pass (S x), the CG hot kernel */
+#define B200FE_PROF_GATHER 1    /* run gather-sum per large FE dimension                    */
+#define B200FE_PROF_FINALIZE 2  /* multi-chunk groups, small-dim bins, dot reduction        */
+#define B200FE_PROF_VECTOR 3    /* CG vector updates and column dots                        */
+#define B200FE_PROF_RHS 4       /* data pass forming the projected right-hand side          */
+#define B200FE_PROF_FINAL 5     /* data pass writing the within transform (+ certificate)   */
+#define B200FE_PROF_SETUP 6     /* FE structure build                                        */
+#define B200FE_PROF_CATEGORIES 8
 
 typedef struct b200fe_result {
     int status;
@@ -75,7 +86,13 @@ typedef struct b200fe_result {
     double solve_ms;         /* RHS pass + PCG + output pass (+ certificate)                */
     double h2d_ms;
     double d2h_ms;
-    long long kernel_launches;
+    long long kernel_launches;   /* this library's own kernels launched by the call     */
+    long long library_calls;     /* CUB device-primitive calls (setup sorts and scans)   */
+    /* profile == 1: per category, summed CUDA-event time, launches, and the
+       algorithmic bytes those launches had to move (HBM roofline numerator). */
+    double prof_ms[B200FE_PROF_CATEGORIES];
+    double prof_bytes[B200FE_PROF_CATEGORIES];
+    long long prof_launches[B200FE_PROF_CATEGORIES];
 } b200fe_result;
 
 /* Library version, e.g. 10000 for 1.0.0. */

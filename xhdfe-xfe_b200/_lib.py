@@ -16,6 +16,8 @@ LIB_PATH = HERE / "libb200fe.so"
 OK, NOT_CONVERGED, UNAVAILABLE, CUDA_ERROR, INVALID_ARG = 0, 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
 MAX_DIMS = 8
+PROF_CATEGORIES = 8
+PROF_NAMES = ("pass", "gather", "finalize", "vector", "rhs", "final", "setup", "spare")
 
 STATUS_NAMES = {
     OK: "ok",
@@ -52,6 +54,7 @@ class Options(ctypes.Structure):
         ("inner_tol", ctypes.c_double),
         ("tolerance_mode", ctypes.c_int),
         ("max_outer", ctypes.c_int),
+        ("profile", ctypes.c_int),
     ]
 
 
@@ -72,6 +75,10 @@ class Result(ctypes.Structure):
         ("h2d_ms", ctypes.c_double),
         ("d2h_ms", ctypes.c_double),
         ("kernel_launches", ctypes.c_longlong),
+        ("library_calls", ctypes.c_longlong),
+        ("prof_ms", ctypes.c_double * PROF_CATEGORIES),
+        ("prof_bytes", ctypes.c_double * PROF_CATEGORIES),
+        ("prof_launches", ctypes.c_longlong * PROF_CATEGORIES),
     ]
 
 

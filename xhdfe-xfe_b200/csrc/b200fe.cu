@@ -82,8 +82,19 @@ struct b200fe_context {
     std::unordered_map<std::string, Buf> bufs;
     Structure st;
     long long launches = 0;
+    long long lib_calls = 0;
     int* h_pinned = nullptr;     // small pinned scratch
     double* h_pinned_d = nullptr;
+    // opt-in event profiler (b200fe_options.profile)
+    struct ProfRec {
+        cudaEvent_t a, b;
+        int cat;
+        double bytes;
+    };
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<ProfRec> prof;
 };
 
 namespace {
@@ -144,6 +155,41 @@ int grid_for(b200fe_context* ctx, int64_t work, int threads, int per_sm = 8) {
     return static_cast<int>(g);
 }
 
+// Records a CUDA-event interval on the context stream around a scope when
+// profiling is on; the bytes are the launches' algorithmic traffic.
+struct ProfScope {
+    b200fe_context* ctx;
+    int cat;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    static cudaEvent_t event(b200fe_context* c) {
+        if (c->ev_used < c->ev_pool.size()) return c->ev_pool[c->ev_used++];
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        c->ev_pool.push_back(e);
+        ++c->ev_used;
+        return e;
+    }
+    ProfScope(b200fe_context* c, int category, double b) : ctx(c), cat(category), bytes(b) {
+        if (ctx->profiling) {
+            a = event(ctx);
+            if (a) cudaEventRecord(a, ctx->stream);
+        }
+    }
+    ~ProfScope() {
+        if (ctx->profiling && a) {
+            cudaEvent_t b = event(ctx);
+            if (b) {
+                cudaEventRecord(b, ctx->stream);
+                ctx->prof.push_back({a, b, cat, bytes});
+            }
+        }
+    }
+};
+
 // ---------------------------------------------------------------------------
 // CUB helpers (setup only)
 // ---------------------------------------------------------------------------
@@ -153,7 +199,7 @@ int cub_exclusive_sum(b200fe_context* ctx, const int32_t* in, int32_t* out, int6
     void* t;
     B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
     B_TRY(cub::DeviceScan::ExclusiveSum(t, tmp, in, out, n, ctx->stream));
-    ++ctx->launches;
+    ++ctx->lib_calls;
     return B200FE_OK;
 }
 
@@ -163,7 +209,7 @@ int cub_inclusive_sum(b200fe_context* ctx, const int32_t* in, int32_t* out, int6
     void* t;
     B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
     B_TRY(cub::DeviceScan::InclusiveSum(t, tmp, in, out, n, ctx->stream));
-    ++ctx->launches;
+    ++ctx->lib_calls;
     return B200FE_OK;
 }
 
@@ -186,7 +232,7 @@ int cub_sort_pairs(b200fe_context* ctx, const int32_t* keys_in, int32_t* keys_ou
     B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
     B_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, ki, ko, vals_in, vals_out, n, 0, eb,
                                           ctx->stream));
-    ++ctx->launches;
+    ++ctx->lib_calls;
     return B200FE_OK;
 }
 
@@ -198,7 +244,7 @@ int cub_segmented_sum(b200fe_context* ctx, const double* in, double* out, int32_
     void* t;
     B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
     B_TRY(cub::DeviceSegmentedReduce::Sum(t, tmp, in, out, nseg, off, off + 1, ctx->stream));
-    ++ctx->launches;
+    ++ctx->lib_calls;
     return B200FE_OK;
 }
 
@@ -572,9 +618,29 @@ PassArgs<T> make_pass_args(const Structure& st, int cols, int CP, const Work<T>&
     return a;
 }
 
+// Algorithmic bytes of one launch (what the launch must read or write at
+// least once from HBM); alpha vectors of the large dims are counted once.
+double struct_obs_bytes(const Structure& st, size_t wsize) {
+    return static_cast<double>(st.n) *
+               (4.0 * st.nL + (st.nS ? 4.0 : 0.0) + (st.weighted ? double(wsize) : 0.0)) +
+           static_cast<double>(st.G[st.p]) * (4.0 + 8.0 + 4.0 * st.nL);
+}
+double runs_write_bytes(const Structure& st, int CP, size_t tsize) {
+    double b = 0.0;
+    for (int l = 0; l < st.nL; ++l)
+        b += static_cast<double>(st.L[l].nruns) * (4.0 + CP * double(tsize));
+    return b;
+}
+double gather_bytes(const Structure& st, int l, int CP, size_t tsize, bool dot) {
+    return static_cast<double>(st.L[l].nchunks) * 13.0 +
+           static_cast<double>(st.L[l].nruns) * CP * double(tsize) +
+           static_cast<double>(st.L[l].G) * CP * double(tsize) * (dot ? 2.0 : 1.0);
+}
+
 // Gathers runs and bins into alpha rows `out`; dot with `dotv` into wk.dot_out.
 template <typename T, int CQ>
-int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv) {
+int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
+                int cat_gather = B200FE_PROF_GATHER, int cat_fin = B200FE_PROF_FINALIZE) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
     const cudaStream_t s = ctx->stream;
@@ -591,6 +657,7 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv) {
         g.partial = wk.chunk_partial[l];
         g.dotv = dotv ? dotv + st.lbase[l] * CP : nullptr;
         g.dot_partial = wk.gather_partial[l];
+        ProfScope ps(ctx, cat_gather, gather_bytes(st, l, CP, sizeof(T), dotv != nullptr));
         run_gather_kernel<T, CQ><<<wk.gather_grid[l], kRowThreads, 0, s>>>(g);
         B_LAUNCHED();
     }
@@ -619,6 +686,10 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv) {
     f.dot_partial = wk.fin_partial;
     f.dot_out = dotv ? wk.dot_out : nullptr;
     f.ticket = wk.ticket;
+    double fb = static_cast<double>(wk.pass_grid) * st.nS * kSmallLevels * CP * 8.0;
+    for (int l = 0; l < st.nL; ++l) fb += static_cast<double>(st.L[l].nmulti) * CP * (8.0 + sizeof(T));
+    for (int j = 0; j < st.nS; ++j) fb += static_cast<double>(st.sG[j]) * CP * sizeof(T);
+    ProfScope ps(ctx, cat_fin, fb);
     finalize_kernel<T><<<wk.fin_grid, kRowThreads, 0, s>>>(f);
     B_LAUNCHED();
     return B200FE_OK;
@@ -632,8 +703,13 @@ int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* x, T* q
     PassArgs<T> a = make_pass_args<T>(st, 0, CP, wk);
     a.wp = wp;
     a.x = x;
-    primary_pass_kernel<T, CQ, kMatvec><<<wk.pass_grid, kPassThreads, wk.pass_smem, ctx->stream>>>(a);
-    B_LAUNCHED();
+    {
+        ProfScope ps(ctx, B200FE_PROF_PASS,
+                     struct_obs_bytes(st, sizeof(T)) + runs_write_bytes(st, CP, sizeof(T)) +
+                         static_cast<double>(st.GR) * CP * sizeof(T));
+        primary_pass_kernel<T, CQ, kMatvec><<<wk.pass_grid, kPassThreads, wk.pass_smem, ctx->stream>>>(a);
+        B_LAUNCHED();
+    }
     return reduce_runs<T, CQ>(ctx, wk, q, x);
 }
 
@@ -708,11 +784,15 @@ int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* dinv, T* x
             B_CHECK(matvec<T, CQ>(ctx, wk, wp, p, q));
             // pq is in wk.dot_out: copy into the scalar slot
             B_TRY(cudaMemcpyAsync(cs.pq, wk.dot_out, sizeof(double) * CP, cudaMemcpyDeviceToDevice, s));
-            cg_update_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x, r, z, p, q, dinv, sc, 1.0,
-                                                             it + j);
-            B_LAUNCHED();
-            cg_direction_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, p, z, sc, 0);
-            B_LAUNCHED();
+            {
+                ProfScope ps(ctx, B200FE_PROF_VECTOR,
+                             static_cast<double>(GR) * (CP * 10.0 + 1.0) * sizeof(T));
+                cg_update_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x, r, z, p, q, dinv, sc,
+                                                                 1.0, it + j);
+                B_LAUNCHED();
+                cg_direction_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, p, z, sc, 0);
+                B_LAUNCHED();
+            }
         }
         it += block;
         B_CHECK(sync_read_int(ctx, cs.n_active, 1, &na));
@@ -769,6 +849,9 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         PassArgs<double> a = make_pass_args<double>(st, cols, CP, w64);
         a.wp = st.wp64;
         a.v = d_v;
+        ProfScope ps(ctx, B200FE_PROF_RHS,
+                     static_cast<double>(st.n) * cols * 8.0 + struct_obs_bytes(st, 8) +
+                         runs_write_bytes(st, CP, 8));
         primary_pass_kernel<double, CQ, kRhs><<<w64.pass_grid, kPassThreads, w64.pass_smem, s>>>(a);
         B_LAUNCHED();
     }
@@ -777,7 +860,8 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         std::vector<double> hp(static_cast<size_t>(w64.pass_grid) * CP);
         B_TRY(cudaMemcpyAsync(hp.data(), w64.colsq_partial, sizeof(double) * hp.size(),
                               cudaMemcpyDeviceToHost, s));
-        if (GR > 0) B_CHECK(reduce_runs<double, CQ>(ctx, w64, b64, nullptr));
+        if (GR > 0)
+            B_CHECK(reduce_runs<double, CQ>(ctx, w64, b64, nullptr, B200FE_PROF_RHS, B200FE_PROF_RHS));
         B_TRY(cudaStreamSynchronize(s));
         for (int b = 0; b < w64.pass_grid; ++b)
             for (int c = 0; c < CP; ++c) vnorm2[c] += hp[static_cast<size_t>(b) * CP + c];
@@ -869,6 +953,10 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         a.out = d_out;
         a.x = a64;
         a.scatter = cert ? 1 : 0;
+        ProfScope ps(ctx, B200FE_PROF_FINAL,
+                     static_cast<double>(st.n) * cols * 16.0 + struct_obs_bytes(st, 8) +
+                         static_cast<double>(GR) * CP * 8.0 +
+                         (cert ? runs_write_bytes(st, CP, 8) : 0.0));
         primary_pass_kernel<double, CQ, kFinal><<<w64.pass_grid, kPassThreads, w64.pass_smem, s>>>(a);
         B_LAUNCHED();
     }
@@ -879,7 +967,8 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                               cudaMemcpyDeviceToHost, s));
         std::vector<double> res2(CP, 0.0);
         if (GR > 0) {
-            B_CHECK(reduce_runs<double, CQ>(ctx, w64, q64, nullptr));
+            B_CHECK(reduce_runs<double, CQ>(ctx, w64, q64, nullptr, B200FE_PROF_FINAL,
+                                            B200FE_PROF_FINAL));
             row_dot_kernel<double, double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, q64, q64, dot_part,
                                                                          dot_ticket, dot_res);
             B_LAUNCHED();
@@ -996,8 +1085,15 @@ int absorb_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int co
     B_TRY(cudaEventRecord(e0, s));
     const bool reuse = o.reuse_structure && ctx->st.valid && ctx->st.n == n &&
                        ctx->st.D == num_dims && ctx->st.weighted == (d_w != nullptr);
+    ctx->profiling = o.profile != 0;
+    ctx->prof.clear();
+    ctx->ev_used = 0;
     if (!reuse) {
-        int rc = build_structure(ctx, n, num_dims, d_gids, G, d_w);
+        int rc;
+        {
+            ProfScope ps(ctx, B200FE_PROF_SETUP, 0.0);
+            rc = build_structure(ctx, n, num_dims, d_gids, G, d_w);
+        }
         if (rc != B200FE_OK) {
             ctx->st.valid = false;
             cudaEventDestroy(e0);
@@ -1013,6 +1109,16 @@ int absorb_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int co
     B_TRY(cudaEventSynchronize(e2));
     res->setup_ms = reuse ? 0.0 : elapsed_ms(e0, e1);
     res->solve_ms = elapsed_ms(e1, e2);
+    if (ctx->profiling) {
+        for (const auto& pr : ctx->prof) {
+            if (pr.cat < 0 || pr.cat >= B200FE_PROF_CATEGORIES) continue;
+            res->prof_ms[pr.cat] += elapsed_ms(pr.a, pr.b);
+            res->prof_bytes[pr.cat] += pr.bytes;
+            res->prof_launches[pr.cat] += 1;
+        }
+        ctx->prof.clear();
+        ctx->profiling = false;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
@@ -1059,6 +1165,7 @@ void b200fe_default_options(b200fe_options* o) {
     o->inner_tol = 1e-5;
     o->tolerance_mode = 1;
     o->max_outer = 12;
+    o->profile = 0;
 }
 
 int b200fe_context_create(int device, b200fe_context** out) {
@@ -1089,6 +1196,7 @@ void b200fe_context_destroy(b200fe_context* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& kv : ctx->bufs)
         if (kv.second.p) cudaFree(kv.second.p);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->h_pinned_d) cudaFreeHost(ctx->h_pinned_d);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1128,11 +1236,12 @@ int b200fe_absorb_device(b200fe_context* ctx, const double* d_v, int64_t n, int 
     }
     const cudaStream_t own = ctx->stream;
     if (stream) ctx->stream = static_cast<cudaStream_t>(stream);
-    const long long l0 = ctx->launches;
+    const long long l0 = ctx->launches, c0 = ctx->lib_calls;
     rc = absorb_device_impl(ctx, d_v, n, cols, num_dims, d_group_ids, num_groups, d_weights, o,
                             d_out, r);
     ctx->stream = own;
     r->kernel_launches = ctx->launches - l0;
+    r->library_calls = ctx->lib_calls - c0;
     return r->status = rc;
 }
 
@@ -1163,7 +1272,7 @@ int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X, int64_t
         return r->status = B200FE_UNAVAILABLE;
     }
     const cudaStream_t s = ctx->stream;
-    const long long l0 = ctx->launches;
+    const long long l0 = ctx->launches, c0 = ctx->lib_calls;
     const int cols = k + 1;
     auto run = [&]() -> int {
         double *dv, *dout, *dw = nullptr;
@@ -1204,6 +1313,7 @@ int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X, int64_t
     };
     rc = run();
     r->kernel_launches = ctx->launches - l0;
+    r->library_calls = ctx->lib_calls - c0;
     return r->status = rc;
 }
 
