@@ -135,3 +135,35 @@ def test_bitwise_deterministic(absorber, pkg, panels):
     assert np.array_equal(r1.y_tilde, r2.y_tilde)
     assert np.array_equal(r1.X_tilde, r2.X_tilde)
     assert r1.iterations == r2.iterations
+
+
+def test_no_large_dimension(absorber, pkg, oracle_mod, panels):
+    # worker (primary) + year (small): no run structure, bins only
+    p = _akm(panels, 20_000, True, seed=23)
+    fes = [p.fes[0], p.fes[2]]
+    keep = panels.drop_singletons(fes)
+    fes = [pkg.dense_ids(f[keep])[0] for f in fes]
+    G = [int(f.max()) + 1 for f in fes]
+    _check(absorber, pkg, oracle_mod, p.y[keep], p.X[keep], fes, G)
+
+
+def test_all_segments_long(absorber, pkg, oracle_mod):
+    # primary groups of ~515 observations: every segment takes the long path
+    rng = np.random.default_rng(29)
+    n = 50000
+    fe1 = (np.arange(n) % 50).astype(np.int32)
+    fe2 = (np.arange(n) % 97).astype(np.int32)
+    X = rng.normal(size=(n, 3))
+    y = X @ np.array([0.5, -0.2, 0.1]) + 0.01 * fe1 + rng.normal(size=n)
+    _check(absorber, pkg, oracle_mod, y, X, [fe1, fe2], [50, 97])
+
+
+def test_zipf_primary_mixed_long_and_tiles(absorber, pkg, oracle_mod, panels):
+    # firm (Zipf sizes) as the largest dim with year: big firms are long segments
+    p = _akm(panels, 30_000, True, seed=31, firms=3000)
+    fes = [p.fes[1], p.fes[2]]
+    keep = panels.drop_singletons(fes)
+    fes = [pkg.dense_ids(f[keep])[0] for f in fes]
+    G = [int(f.max()) + 1 for f in fes]
+    w = np.random.default_rng(3).lognormal(0.0, 0.5, size=int(keep.sum()))
+    _check(absorber, pkg, oracle_mod, p.y[keep], p.X[keep], fes, G, w=w)

@@ -55,6 +55,7 @@ class Options(ctypes.Structure):
         ("tolerance_mode", ctypes.c_int),
         ("max_outer", ctypes.c_int),
         ("profile", ctypes.c_int),
+        ("pass_kernel", ctypes.c_int),
     ]
 
 

@@ -75,7 +75,8 @@ def cuda_backend_available() -> bool:
 
 def make_options(*, tol=1e-8, tolerance_mode="reghdfe-comparable", precision="mixed",
                  max_iter=10000, certify=True, check_interval=4, reuse_structure=False,
-                 inner_tol=1e-5, max_outer=12, profile=False) -> _lib.Options:
+                 inner_tol=1e-5, max_outer=12, profile=False,
+                 pass_kernel=0) -> _lib.Options:
     o = _lib.default_options()
     o.tol = float(tol)
     o.tolerance_mode = TOLERANCE_MODES[tolerance_mode] if isinstance(tolerance_mode, str) \
@@ -88,6 +89,7 @@ def make_options(*, tol=1e-8, tolerance_mode="reghdfe-comparable", precision="mi
     o.inner_tol = float(inner_tol)
     o.max_outer = int(max_outer)
     o.profile = 1 if profile else 0
+    o.pass_kernel = int(pass_kernel)
     return o
 
 

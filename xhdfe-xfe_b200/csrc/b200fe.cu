@@ -13,7 +13,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <limits>
+#include <type_traits>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -37,7 +39,7 @@ struct LargeDim {
     int64_t nruns = 0;
     int64_t nchunks = 0;
     int64_t nmulti = 0;
-    int32_t *rid = nullptr, *run_base = nullptr, *run_dest = nullptr;
+    int32_t *rid = nullptr, *run_base = nullptr, *run_dest = nullptr, *run_start = nullptr;
     int32_t *chunk_grp = nullptr, *chunk_beg = nullptr, *chunk_end = nullptr;
     uint8_t* chunk_whole = nullptr;
     int32_t *multi_grp = nullptr, *multi_c0 = nullptr, *multi_c1 = nullptr;
@@ -68,6 +70,18 @@ struct Structure {
     double* dinv64 = nullptr;
     float* dinv32 = nullptr;
     int32_t* gp = nullptr;  // primary ids in primary order (setup only)
+    int SG = 0;             // bin rows over all small dims
+    int sgoff[kMaxSmall] = {0};
+    int32_t* tile_seg = nullptr;
+    uint8_t* tile_long = nullptr;
+    int64_t ntiles = 0;
+    int32_t* long_segs = nullptr;
+    int64_t nlong = 0;
+    // run-level pass metadata (at most one large dim)
+    int2* seg_meta = nullptr;
+    int4* run_meta = nullptr;
+    double* run_w64 = nullptr;
+    float* run_w32 = nullptr;
 };
 
 constexpr int32_t kChunkRuns = 64;
@@ -92,6 +106,7 @@ struct b200fe_context {
         double bytes;
     };
     bool profiling = false;
+    int pass_kernel = 0;
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<ProfRec> prof;
@@ -124,6 +139,15 @@ namespace {
         if (rc_ != B200FE_OK) return rc_;                                        \
     } while (0)
 
+// Debug aid: B200FE_POISON=<substring> fills newly allocated floating-point
+// workspace whose name contains the substring ("*" for all) with NaN bytes,
+// so a read before the first write shows up as a NaN.  Index arrays are never
+// poisoned.
+const char* poison_filter() {
+    static const char* f = std::getenv("B200FE_POISON");
+    return f;
+}
+
 template <typename T>
 int get_buf(b200fe_context* ctx, const std::string& name, size_t count, T** out) {
     size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
@@ -144,6 +168,12 @@ int get_buf(b200fe_context* ctx, const std::string& name, size_t count, T** out)
             return B200FE_CUDA_ERROR;
         }
         b.bytes = bytes;
+        const char* pf = poison_filter();
+        if (pf && (std::is_same<T, double>::value || std::is_same<T, float>::value) &&
+            (std::strcmp(pf, "*") == 0 || name.find(pf) != std::string::npos)) {
+            cudaMemsetAsync(b.p, 0xff, bytes, ctx->stream);
+            cudaStreamSynchronize(ctx->stream);
+        }
     }
     *out = static_cast<T*>(b.p);
     return B200FE_OK;
@@ -351,10 +381,37 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
                                                                           wsum_p, st.inv_wp);
     B_LAUNCHED();
 
+    // tiles of whole segments and the list of long segments
+    {
+        int32_t *tflag, *tidx, *lflag, *lidx;
+        const size_t g1 = static_cast<size_t>(G[p]) + 1;
+        B_CHECK(get_buf(ctx, "tflag", g1, &tflag));
+        B_CHECK(get_buf(ctx, "tidx", g1, &tidx));
+        B_CHECK(get_buf(ctx, "lflag", g1, &lflag));
+        B_CHECK(get_buf(ctx, "lidx", g1, &lidx));
+        tile_flag_kernel<<<grid_for(ctx, g1, T256), T256, 0, s>>>(seg_off, G[p], tflag, lflag);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, tflag, tidx, g1));
+        B_CHECK(cub_exclusive_sum(ctx, lflag, lidx, g1));
+        int cnt[2];
+        B_CHECK(sync_read_int(ctx, tidx + G[p], 1, &cnt[0]));
+        B_CHECK(sync_read_int(ctx, lidx + G[p], 1, &cnt[1]));
+        st.ntiles = cnt[0];
+        st.nlong = cnt[1];
+        B_CHECK(get_buf(ctx, "tile_seg", static_cast<size_t>(st.ntiles) + 1, &st.tile_seg));
+        B_CHECK(get_buf(ctx, "tile_long", static_cast<size_t>(st.ntiles) + 1, &st.tile_long));
+        B_CHECK(get_buf(ctx, "long_segs", static_cast<size_t>(st.nlong) + 1, &st.long_segs));
+        tile_fill_kernel<<<grid_for(ctx, g1, T256), T256, 0, s>>>(
+            seg_off, G[p], tflag, tidx, lflag, lidx, st.tile_seg, st.tile_long, st.long_segs);
+        B_LAUNCHED();
+    }
+
     // classify the other dims
     for (int d = 0; d < D; ++d) {
         if (d == p) continue;
-        if (G[d] <= kSmallLevels && st.nS < kMaxSmall) {
+        int sg_total = 0;
+        for (int j = 0; j < st.nS; ++j) sg_total += st.sG[j];
+        if (G[d] <= kSmallLevels && st.nS < kMaxSmall && sg_total + G[d] <= kMaxSmallRows) {
             st.sdim[st.nS] = d;
             st.sG[st.nS] = G[d];
             ++st.nS;
@@ -373,9 +430,12 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         st.lbase[l] = row;
         row += st.L[l].G;
     }
+    st.SG = 0;
     for (int j = 0; j < st.nS; ++j) {
         st.sbase[j] = row;
+        st.sgoff[j] = st.SG;
         row += st.sG[j];
+        st.SG += st.sG[j];
     }
     st.GR = row;
 
@@ -402,14 +462,20 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         L.nruns = nr;
         int32_t *run_grp, *run_start, *run_seg;
         B_CHECK(get_buf(ctx, "run_grp", nr, &run_grp));
-        B_CHECK(get_buf(ctx, "run_start", nr, &run_start));
+        B_CHECK(get_buf(ctx, "run_start" + sfx, static_cast<size_t>(nr) + 1, &run_start));
         B_CHECK(get_buf(ctx, "run_seg", nr, &run_seg));
+        L.run_start = run_start;
         run_fill_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(rflags, run_id, gp, L.rid, n,
                                                                 run_grp, run_start, run_seg);
         B_LAUNCHED();
-        B_CHECK(get_buf(ctx, "run_base" + sfx, G[p], &L.run_base));
-        run_base_kernel<<<grid_for(ctx, G[p], T256), T256, 0, s>>>(seg_off, G[p], run_id, n,
-                                                                    L.run_base);
+        {
+            const int32_t n32 = static_cast<int32_t>(n);
+            B_TRY(cudaMemcpyAsync(run_start + nr, &n32, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+            B_TRY(cudaStreamSynchronize(s));  // n32 lives on this stack frame
+        }
+        B_CHECK(get_buf(ctx, "run_base" + sfx, static_cast<size_t>(G[p]) + 1, &L.run_base));
+        run_base_kernel<<<grid_for(ctx, static_cast<int64_t>(G[p]) + 1, T256), T256, 0, s>>>(
+            seg_off, G[p], run_id, n, nr, L.run_base);
         B_LAUNCHED();
         // sort runs by group (stable: primary order within a group)
         int32_t *riota, *sorted_runs, *sorted_grp;
@@ -429,12 +495,24 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         B_CHECK(cub_exclusive_sum(ctx, gcount, grp_off, static_cast<int64_t>(L.G) + 1));
         // run destinations and per-run diagonal terms
         B_CHECK(get_buf(ctx, "run_dest" + sfx, nr, &L.run_dest));
-        double *cw, *ce;
+        double *cw, *ce, *cw_run;
         B_CHECK(get_buf(ctx, "run_cw", nr, &cw));
         B_CHECK(get_buf(ctx, "run_ce", nr, &ce));
+        B_CHECK(get_buf(ctx, "run_cw_run", nr, &cw_run));
         run_weights_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(
-            sorted_runs, nr, run_start, n, run_seg, st.wp64, st.inv_wp, L.run_dest, cw, ce);
+            sorted_runs, nr, run_start, n, run_seg, st.wp64, st.inv_wp, L.run_dest, cw, ce,
+            cw_run);
         B_LAUNCHED();
+        if (st.nL == 1) {
+            B_CHECK(get_buf(ctx, "seg_meta", static_cast<size_t>(G[p]) + 1, &st.seg_meta));
+            B_CHECK(get_buf(ctx, "run_meta", nr, &st.run_meta));
+            B_CHECK(get_buf(ctx, "run_w64", nr, &st.run_w64));
+            B_CHECK(get_buf(ctx, "run_w32", nr, &st.run_w32));
+            pack_meta_kernel<<<grid_for(ctx, std::max<int64_t>(nr, G[p] + 1), T256), T256, 0, s>>>(
+                seg_off, L.run_base, G[p], run_grp, L.run_dest, run_start, nr, cw_run,
+                st.seg_meta, st.run_meta, st.run_w64, st.run_w32);
+            B_LAUNCHED();
+        }
         B_CHECK(cub_segmented_sum(ctx, cw, Wall + st.lbase[l], L.G, grp_off));
         B_CHECK(cub_segmented_sum(ctx, ce, Eall + st.lbase[l], L.G, grp_off));
         // chunk list
@@ -466,6 +544,14 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         chunk_fill_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(
             grp_off, L.G, kChunkRuns, ch_off, L.chunk_grp, L.chunk_beg, L.chunk_end,
             L.chunk_whole, midx, L.multi_grp, L.multi_c0, L.multi_c1);
+        B_LAUNCHED();
+    }
+
+    if (st.nL == 0 && st.GR > 0) {
+        B_CHECK(get_buf(ctx, "seg_meta", static_cast<size_t>(G[p]) + 1, &st.seg_meta));
+        pack_meta_kernel<<<grid_for(ctx, static_cast<int64_t>(G[p]) + 1, T256), T256, 0, s>>>(
+            seg_off, nullptr, G[p], nullptr, nullptr, nullptr, 0, nullptr, st.seg_meta, nullptr,
+            nullptr, nullptr);
         B_LAUNCHED();
     }
 
@@ -533,45 +619,70 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
 template <typename T>
 struct Work {
     T* R[kMaxLarge];
-    double* bins_partial;
-    double* colsq_partial;
+    double* bins_partial;   // [nbins_ctas][SG][CP]
+    double* colsq_partial;  // [nbins_ctas][CP]
     double* gather_partial[kMaxLarge];
     double* fin_partial;
     double* chunk_partial[kMaxLarge];
     double* dot_out;
     unsigned int* ticket;
-    int pass_grid;
-    int pass_smem;
+    int tile_grid, tile_smem;
+    int run_grid, run_smem;  // run-level matvec (nL <= 1), 0 otherwise
+    int long_grid, long_smem;
+    int nbins_ctas;
     int gather_grid[kMaxLarge];
     int fin_grid;
+    int64_t fin_rows;
 };
+
+template <typename T, int CQ, int MODE>
+int set_pass_smem(b200fe_context* ctx, int tile_smem, int long_smem) {
+    B_TRY(cudaFuncSetAttribute(tile_pass_kernel<T, CQ, MODE>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
+    B_TRY(cudaFuncSetAttribute(segment_pass_kernel<T, CQ, MODE>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, long_smem));
+    return B200FE_OK;
+}
 
 template <typename T, int CQ>
 int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
-    const int bins_bytes = (kPassThreads / 32) * st.nS * kSmallLevels * CP * sizeof(double);
-    wk.pass_smem = std::max<int>(bins_bytes, kPassThreads * 4 * sizeof(double));
-    // occupancy-sized persistent grid for the primary pass
+    wk.tile_smem = static_cast<int>(tile_smem_bytes<T>(CP, st.SG));
+    wk.long_smem = std::max<int>((kPassThreads / 32) * st.SG * CP * sizeof(double),
+                                 kPassThreads * 4 * sizeof(double));
+    B_CHECK((set_pass_smem<T, CQ, kMatvec>(ctx, wk.tile_smem, wk.long_smem)));
+    B_CHECK((set_pass_smem<T, CQ, kRhs>(ctx, wk.tile_smem, wk.long_smem)));
+    B_CHECK((set_pass_smem<T, CQ, kFinal>(ctx, wk.tile_smem, wk.long_smem)));
     int per_sm = 1;
-    auto kfn = primary_pass_kernel<T, CQ, kMatvec>;
-    if (wk.pass_smem > 48 * 1024) {
-        B_TRY(cudaFuncSetAttribute(primary_pass_kernel<T, CQ, kMatvec>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, wk.pass_smem));
-        B_TRY(cudaFuncSetAttribute(primary_pass_kernel<T, CQ, kRhs>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, wk.pass_smem));
-        B_TRY(cudaFuncSetAttribute(primary_pass_kernel<T, CQ, kFinal>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, wk.pass_smem));
-    }
-    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kPassThreads, wk.pass_smem));
+    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_pass_kernel<T, CQ, kMatvec>,
+                                                        kTileThreads, wk.tile_smem));
     per_sm = std::max(1, per_sm);
-    const int64_t groups_needed = (static_cast<int64_t>(st.G[st.p]) + (32 / CQ) - 1) / (32 / CQ);
-    const int64_t blocks_needed = (groups_needed + 3) / 4;
-    wk.pass_grid = static_cast<int>(std::max<int64_t>(
-        1, std::min<int64_t>(blocks_needed, static_cast<int64_t>(ctx->num_sms) * per_sm)));
-    B_CHECK(get_buf(ctx, tag + "bins", static_cast<size_t>(wk.pass_grid) * std::max(st.nS, 1) *
-                                           kSmallLevels * CP, &wk.bins_partial));
-    B_CHECK(get_buf(ctx, tag + "colsq", static_cast<size_t>(wk.pass_grid) * CP, &wk.colsq_partial));
+    wk.tile_grid = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>(st.ntiles, static_cast<int64_t>(ctx->num_sms) * per_sm)));
+    wk.run_grid = 0;
+    wk.run_smem = 0;
+    if (st.nL <= 1 && st.GR > 0 && ctx->pass_kernel == 0) {
+        wk.run_smem = static_cast<int>(run_smem_bytes<T>(CP, st.SG));
+        B_TRY(cudaFuncSetAttribute(run_pass_kernel<T, CQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   wk.run_smem));
+        int rps = 1;
+        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rps, run_pass_kernel<T, CQ>, kRunThreads,
+                                                            wk.run_smem));
+        rps = std::max(1, rps);
+        const int64_t warps = (static_cast<int64_t>(st.G[st.p]) + (32 / CQ) - 1) / (32 / CQ);
+        wk.run_grid = static_cast<int>(std::max<int64_t>(
+            1, std::min<int64_t>((warps + 3) / 4, static_cast<int64_t>(ctx->num_sms) * rps)));
+    }
+    wk.long_grid = 0;
+    if (st.nlong > 0) {
+        const int64_t groups = (st.nlong + (32 / CQ) - 1) / (32 / CQ);
+        wk.long_grid = grid_for(ctx, groups * 32, kPassThreads, 4);
+    }
+    wk.nbins_ctas = std::max(wk.tile_grid, wk.run_grid) + wk.long_grid;
+    B_CHECK(get_buf(ctx, tag + "bins", static_cast<size_t>(wk.nbins_ctas) * std::max(st.SG, 1) * CP,
+                    &wk.bins_partial));
+    B_CHECK(get_buf(ctx, tag + "colsq", static_cast<size_t>(wk.nbins_ctas) * CP, &wk.colsq_partial));
     for (int l = 0; l < st.nL; ++l) {
         const std::string sfx = std::to_string(l);
         B_CHECK(get_buf(ctx, tag + "R" + sfx, static_cast<size_t>(st.L[l].nruns) * CP, &wk.R[l]));
@@ -581,11 +692,12 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
         B_CHECK(get_buf(ctx, tag + "cpart" + sfx, static_cast<size_t>(st.L[l].nchunks) * CP,
                         &wk.chunk_partial[l]));
     }
-    int64_t items = 0;
-    for (int l = 0; l < st.nL; ++l) items += st.L[l].nmulti * CP;
-    for (int j = 0; j < st.nS; ++j) items += static_cast<int64_t>(st.sG[j]) * CP;
-    wk.fin_grid = grid_for(ctx, std::max<int64_t>(items, 1), kRowThreads, 4);
-    B_CHECK(get_buf(ctx, tag + "fpart", static_cast<size_t>(wk.fin_grid) * CP, &wk.fin_partial));
+    wk.fin_rows = st.SG;
+    for (int l = 0; l < st.nL; ++l) wk.fin_rows += st.L[l].nmulti;
+    wk.fin_grid = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>(wk.fin_rows, static_cast<int64_t>(ctx->num_sms) * 8)));
+    B_CHECK(get_buf(ctx, tag + "fpart", static_cast<size_t>(std::max<int64_t>(wk.fin_rows, 1)) * CP,
+                    &wk.fin_partial));
     B_CHECK(get_buf(ctx, tag + "dotout", CP, &wk.dot_out));
     B_CHECK(get_buf(ctx, tag + "ticket", 1, &wk.ticket));
     B_TRY(cudaMemsetAsync(wk.ticket, 0, sizeof(unsigned int), ctx->stream));
@@ -607,15 +719,102 @@ PassArgs<T> make_pass_args(const Structure& st, int cols, int CP, const Work<T>&
     for (int l = 0; l < st.nL; ++l) {
         a.rid[l] = st.L[l].rid;
         a.run_base[l] = st.L[l].run_base;
+        a.run_start[l] = st.L[l].run_start;
         a.run_dest[l] = st.L[l].run_dest;
         a.lbase[l] = st.lbase[l];
         a.R[l] = wk.R[l];
     }
     a.sid = st.sid;
-    for (int j = 0; j < st.nS; ++j) a.sbase[j] = st.sbase[j];
+    for (int j = 0; j < st.nS; ++j) {
+        a.sbase[j] = st.sbase[j];
+        a.sgoff[j] = st.sgoff[j];
+    }
+    a.SG = st.SG;
     a.bins_partial = wk.bins_partial;
     a.colsq_partial = wk.colsq_partial;
+    a.tile_seg = st.tile_seg;
+    a.tile_long = st.tile_long;
+    a.ntiles = st.ntiles;
+    a.long_segs = st.long_segs;
+    a.nlong = st.nlong;
     return a;
+}
+
+// Tile pass over the regular tiles, then the long segments (if any).
+template <typename T, int CQ, int MODE>
+int launch_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a) {
+    a.bins_cta0 = 0;
+    tile_pass_kernel<T, CQ, MODE><<<wk.tile_grid, kTileThreads, wk.tile_smem, ctx->stream>>>(a);
+    B_LAUNCHED();
+    {
+        const Structure& st = ctx->st;
+        const int slots = std::max(wk.tile_grid, wk.run_grid);
+        const int CP = a.CP;
+        if (st.nS > 0 && wk.tile_grid < slots) {
+            B_TRY(cudaMemsetAsync(wk.bins_partial + static_cast<int64_t>(wk.tile_grid) * st.SG * CP, 0,
+                                  sizeof(double) * (slots - wk.tile_grid) * st.SG * CP, ctx->stream));
+            B_TRY(cudaMemsetAsync(wk.colsq_partial + static_cast<int64_t>(wk.tile_grid) * CP, 0,
+                                  sizeof(double) * (slots - wk.tile_grid) * CP, ctx->stream));
+        } else if (wk.tile_grid < slots) {
+            B_TRY(cudaMemsetAsync(wk.colsq_partial + static_cast<int64_t>(wk.tile_grid) * CP, 0,
+                                  sizeof(double) * (slots - wk.tile_grid) * CP, ctx->stream));
+        }
+    }
+    if (wk.long_grid > 0) {
+        a.bins_cta0 = std::max(wk.tile_grid, wk.run_grid);
+        segment_pass_kernel<T, CQ, MODE><<<wk.long_grid, kPassThreads, wk.long_smem, ctx->stream>>>(a);
+        B_LAUNCHED();
+    }
+    return B200FE_OK;
+}
+
+// Matvec pass: run-level kernel when there is at most one large dim, else
+// the tile kernel; then the long segments.  Bin partials of CTAs beyond the
+// launched grid are zeroed so finalize can sum a fixed number of slots.
+template <typename T, int CQ>
+int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, const T* run_w) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const int slots = std::max(wk.tile_grid, wk.run_grid);
+    if (wk.run_grid > 0) {
+        RunArgs<T> r{};
+        r.Gp = st.G[st.p];
+        r.CP = CP;
+        r.nS = st.nS;
+        r.has_large = st.nL == 1;
+        r.seg_meta = st.seg_meta;
+        r.inv_wp = st.inv_wp;
+        r.wp = a.wp;
+        r.sid = st.sid;
+        r.sbase0 = st.nS > 0 ? st.sbase[0] : 0;
+        for (int j = 0; j < st.nS; ++j) r.sgoff[j] = st.sgoff[j];
+        r.SG = st.SG;
+        r.lbase = st.nL == 1 ? st.lbase[0] : 0;
+        r.run_meta = st.run_meta;
+        r.run_w = run_w;
+        r.x = a.x;
+        r.R = st.nL == 1 ? wk.R[0] : nullptr;
+        r.bins_partial = wk.bins_partial;
+        r.bins_cta0 = 0;
+        run_pass_kernel<T, CQ><<<wk.run_grid, kRunThreads, wk.run_smem, ctx->stream>>>(r);
+        B_LAUNCHED();
+        if (st.nS > 0 && wk.run_grid < slots)
+            B_TRY(cudaMemsetAsync(wk.bins_partial + static_cast<int64_t>(wk.run_grid) * st.SG * CP, 0,
+                                  sizeof(double) * (slots - wk.run_grid) * st.SG * CP, ctx->stream));
+    } else {
+        a.bins_cta0 = 0;
+        tile_pass_kernel<T, CQ, kMatvec><<<wk.tile_grid, kTileThreads, wk.tile_smem, ctx->stream>>>(a);
+        B_LAUNCHED();
+        if (st.nS > 0 && wk.tile_grid < slots)
+            B_TRY(cudaMemsetAsync(wk.bins_partial + static_cast<int64_t>(wk.tile_grid) * st.SG * CP, 0,
+                                  sizeof(double) * (slots - wk.tile_grid) * st.SG * CP, ctx->stream));
+    }
+    if (wk.long_grid > 0) {
+        a.bins_cta0 = slots;
+        segment_pass_kernel<T, CQ, kMatvec><<<wk.long_grid, kPassThreads, wk.long_smem, ctx->stream>>>(a);
+        B_LAUNCHED();
+    }
+    return B200FE_OK;
 }
 
 // Algorithmic bytes of one launch (what the launch must read or write at
@@ -675,20 +874,19 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
         f.gather_dot_partial[l] = wk.gather_partial[l];
         f.gather_ctas[l] = dotv ? wk.gather_grid[l] : 0;
     }
-    for (int j = 0; j < st.nS; ++j) {
-        f.sG[j] = st.sG[j];
-        f.sbase[j] = st.sbase[j];
-    }
+    f.SG = st.SG;
+    f.sgbase = st.nS > 0 ? st.sbase[0] : 0;
     f.bins_partial = wk.bins_partial;
-    f.nbins_ctas = wk.pass_grid;
+    f.nbins_ctas = wk.nbins_ctas;
+    f.nrows = wk.fin_rows;
     f.out = out;
     f.dotv = dotv;
     f.dot_partial = wk.fin_partial;
     f.dot_out = dotv ? wk.dot_out : nullptr;
     f.ticket = wk.ticket;
-    double fb = static_cast<double>(wk.pass_grid) * st.nS * kSmallLevels * CP * 8.0;
+    double fb = static_cast<double>(wk.nbins_ctas) * st.SG * CP * 8.0;
     for (int l = 0; l < st.nL; ++l) fb += static_cast<double>(st.L[l].nmulti) * CP * (8.0 + sizeof(T));
-    for (int j = 0; j < st.nS; ++j) fb += static_cast<double>(st.sG[j]) * CP * sizeof(T);
+    fb += static_cast<double>(st.SG) * CP * sizeof(T);
     ProfScope ps(ctx, cat_fin, fb);
     finalize_kernel<T><<<wk.fin_grid, kRowThreads, 0, s>>>(f);
     B_LAUNCHED();
@@ -697,7 +895,8 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
 
 // q = S x ; pq = x'q (per column) into wk.dot_out
 template <typename T, int CQ>
-int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* x, T* q) {
+int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, const T* x,
+           T* q) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
     PassArgs<T> a = make_pass_args<T>(st, 0, CP, wk);
@@ -707,8 +906,7 @@ int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* x, T* q
         ProfScope ps(ctx, B200FE_PROF_PASS,
                      struct_obs_bytes(st, sizeof(T)) + runs_write_bytes(st, CP, sizeof(T)) +
                          static_cast<double>(st.GR) * CP * sizeof(T));
-        primary_pass_kernel<T, CQ, kMatvec><<<wk.pass_grid, kPassThreads, wk.pass_smem, ctx->stream>>>(a);
-        B_LAUNCHED();
+        B_CHECK((launch_matvec_pass<T, CQ>(ctx, wk, a, run_w)));
     }
     return reduce_runs<T, CQ>(ctx, wk, q, x);
 }
@@ -729,7 +927,8 @@ struct ColState {
 // Inner PCG on S x = rhs (rows already in r), T precision.
 // thr_host[c]: stop column c when r'r <= thr (0 or negative: column inactive).
 template <typename T, int CQ>
-int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* dinv, T* x, T* r, T* z,
+int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, const T* dinv, T* x,
+        T* r, T* z,
         T* p, T* q, const std::vector<double>& thr_host, int max_iter, int check_interval,
         int* iters_out) {
     const Structure& st = ctx->st;
@@ -781,7 +980,7 @@ int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* dinv, T* x
     while (na > 0 && it < max_iter) {
         const int block = std::min(check_interval, max_iter - it);
         for (int j = 0; j < block; ++j) {
-            B_CHECK(matvec<T, CQ>(ctx, wk, wp, p, q));
+            B_CHECK((matvec<T, CQ>(ctx, wk, wp, run_w, p, q)));
             // pq is in wk.dot_out: copy into the scalar slot
             B_TRY(cudaMemcpyAsync(cs.pq, wk.dot_out, sizeof(double) * CP, cudaMemcpyDeviceToDevice, s));
             {
@@ -852,18 +1051,17 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         ProfScope ps(ctx, B200FE_PROF_RHS,
                      static_cast<double>(st.n) * cols * 8.0 + struct_obs_bytes(st, 8) +
                          runs_write_bytes(st, CP, 8));
-        primary_pass_kernel<double, CQ, kRhs><<<w64.pass_grid, kPassThreads, w64.pass_smem, s>>>(a);
-        B_LAUNCHED();
+        B_CHECK((launch_pass<double, CQ, kRhs>(ctx, w64, a)));
     }
     std::vector<double> vnorm2(CP, 0.0);
     {
-        std::vector<double> hp(static_cast<size_t>(w64.pass_grid) * CP);
+        std::vector<double> hp(static_cast<size_t>(w64.nbins_ctas) * CP);
         B_TRY(cudaMemcpyAsync(hp.data(), w64.colsq_partial, sizeof(double) * hp.size(),
                               cudaMemcpyDeviceToHost, s));
         if (GR > 0)
             B_CHECK(reduce_runs<double, CQ>(ctx, w64, b64, nullptr, B200FE_PROF_RHS, B200FE_PROF_RHS));
         B_TRY(cudaStreamSynchronize(s));
-        for (int b = 0; b < w64.pass_grid; ++b)
+        for (int b = 0; b < w64.nbins_ctas; ++b)
             for (int c = 0; c < CP; ++c) vnorm2[c] += hp[static_cast<size_t>(b) * CP + c];
     }
 
@@ -880,19 +1078,31 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         B_TRY(cudaMemcpyAsync(r64, b64, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
         rr = bb;
         const double tol = o.tol;
+        // Stop column c when ||r_c||^2 <= thr_c = max(tol^2 ||b_c||^2, floor_c^2).
+        // The floor, 1e3 eps ||D'W||_F ||v_c||, sits four orders of magnitude
+        // below the certificate limit; it only binds for a column (almost) in
+        // the span of the FEs, whose b_c is rounding noise that partly lies in
+        // the null space of S and cannot be reduced relative to itself.
+        std::vector<double> thr64(CP, 0.0);
+        {
+            const double fl = 1e3 * std::numeric_limits<double>::epsilon();
+            const double opn2 = static_cast<double>(st.D) * st.sum_w2;
+            for (int c = 0; c < cols && c < CP; ++c)
+                thr64[c] = std::max(tol * tol * bb[c], fl * fl * opn2 * vnorm2[c]);
+        }
         const int max_outer = std::max(1, o.max_outer);
         converged = false;
         for (outer = 0; outer < max_outer; ++outer) {
             bool all = true;
             std::vector<double> scale(CP, 0.0), inv_scale(CP, 0.0), thr(CP, 0.0);
             for (int c = 0; c < cols && c < CP; ++c) {
-                const bool done = !(rr[c] > tol * tol * bb[c]);
+                const bool done = !(rr[c] > thr64[c]);
                 if (!done) {
                     all = false;
                     scale[c] = std::sqrt(rr[c]);
                     inv_scale[c] = 1.0 / scale[c];
                     // inner target relative to this round's rhs
-                    double t_in = 0.5 * tol * std::sqrt(bb[c] / rr[c]);
+                    double t_in = 0.5 * std::sqrt(thr64[c] / rr[c]);
                     if (mixed) t_in = std::max(t_in, o.inner_tol);
                     t_in = std::min(t_in, 0.5);
                     thr[c] = t_in * t_in;  // rhs is normalised to unit norm
@@ -910,7 +1120,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             if (mixed) {
                 scale_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, r32);
                 B_LAUNCHED();
-                B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.dinv32, x32, r32, z32, p32, q32, thr,
+                B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.run_w32, st.dinv32, x32, r32, z32, p32, q32, thr,
                                         o.max_iter - total_iters, std::max(1, o.check_interval),
                                         &its)));
                 axpy_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x32, scale_d, a64);
@@ -918,7 +1128,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             } else {
                 scale_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, rin64);
                 B_LAUNCHED();
-                B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.dinv64, x64, rin64, z64, p64, q64, thr,
+                B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
                                          o.max_iter - total_iters, std::max(1, o.check_interval),
                                          &its)));
                 axpy_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x64, scale_d, a64);
@@ -926,7 +1136,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             }
             total_iters += its;
             // true residual in FP64: r = b - S a
-            B_CHECK((matvec<double, CQ>(ctx, w64, st.wp64, a64, q64)));
+            B_CHECK((matvec<double, CQ>(ctx, w64, st.wp64, st.run_w64, a64, q64)));
             sub_kernel<<<rgrid, kRowThreads, 0, s>>>(GR * CP, b64, q64, r64);
             B_LAUNCHED();
             row_dot_kernel<double, double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, r64, dot_part,
@@ -937,11 +1147,12 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         if (!converged) {
             bool all = true;
             for (int c = 0; c < cols && c < CP; ++c)
-                if (rr[c] > tol * tol * bb[c]) all = false;
+                if (rr[c] > thr64[c]) all = false;
             converged = all;
         }
+        // residual relative to the scale the stop rule uses (||b_c|| or the floor)
         for (int c = 0; c < cols && c < CP; ++c)
-            if (bb[c] > 0.0) rel_res = std::max(rel_res, std::sqrt(rr[c] / bb[c]));
+            if (thr64[c] > 0.0) rel_res = std::max(rel_res, tol * std::sqrt(rr[c] / thr64[c]));
     }
 
     // final pass: out = (I - P_p)(v - D_r a); certificate scatter
@@ -957,12 +1168,11 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                      static_cast<double>(st.n) * cols * 16.0 + struct_obs_bytes(st, 8) +
                          static_cast<double>(GR) * CP * 8.0 +
                          (cert ? runs_write_bytes(st, CP, 8) : 0.0));
-        primary_pass_kernel<double, CQ, kFinal><<<w64.pass_grid, kPassThreads, w64.pass_smem, s>>>(a);
-        B_LAUNCHED();
+        B_CHECK((launch_pass<double, CQ, kFinal>(ctx, w64, a)));
     }
     double abs_res = 0.0, abs_rel = 0.0;
     if (cert) {
-        std::vector<double> hp(static_cast<size_t>(w64.pass_grid) * CP);
+        std::vector<double> hp(static_cast<size_t>(w64.nbins_ctas) * CP);
         B_TRY(cudaMemcpyAsync(hp.data(), w64.colsq_partial, sizeof(double) * hp.size(),
                               cudaMemcpyDeviceToHost, s));
         std::vector<double> res2(CP, 0.0);
@@ -975,7 +1185,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             B_CHECK(sync_read_double(ctx, dot_res, CP, res2.data()));
         }
         B_TRY(cudaStreamSynchronize(s));
-        for (int b = 0; b < w64.pass_grid; ++b)
+        for (int b = 0; b < w64.nbins_ctas; ++b)
             for (int c = 0; c < CP; ++c) res2[c] += hp[static_cast<size_t>(b) * CP + c];
         const double opn = std::sqrt(static_cast<double>(st.D) * st.sum_w2);
         for (int c = 0; c < cols; ++c) {
@@ -1037,16 +1247,16 @@ int solve_dispatch_cq(b200fe_context* ctx, const double* d_v, int cols, double* 
 int solve_all(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
               const b200fe_options& o, b200fe_result* res) {
     const int64_t n = ctx->st.n;
-    for (int c0 = 0; c0 < cols; c0 += 32) {
-        const int cb = std::min(32, cols - c0);
+    // column blocks of at most 16 (CP <= 16 bounds the staged tile in shared memory)
+    for (int c0 = 0; c0 < cols; c0 += 16) {
+        const int cb = std::min(16, cols - c0);
         const double* v = d_v + static_cast<int64_t>(c0) * n;
         double* out = d_out + static_cast<int64_t>(c0) * n;
         const int cq = (cb + 3) / 4;
         int rc;
         if (cq <= 1) rc = solve_dispatch_cq<1>(ctx, v, cb, out, o, res);
         else if (cq <= 2) rc = solve_dispatch_cq<2>(ctx, v, cb, out, o, res);
-        else if (cq <= 4) rc = solve_dispatch_cq<4>(ctx, v, cb, out, o, res);
-        else rc = solve_dispatch_cq<8>(ctx, v, cb, out, o, res);
+        else rc = solve_dispatch_cq<4>(ctx, v, cb, out, o, res);
         if (rc != B200FE_OK) return rc;
     }
     return B200FE_OK;
@@ -1086,6 +1296,7 @@ int absorb_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int co
     const bool reuse = o.reuse_structure && ctx->st.valid && ctx->st.n == n &&
                        ctx->st.D == num_dims && ctx->st.weighted == (d_w != nullptr);
     ctx->profiling = o.profile != 0;
+    ctx->pass_kernel = o.pass_kernel;
     ctx->prof.clear();
     ctx->ev_used = 0;
     if (!reuse) {
@@ -1166,6 +1377,7 @@ void b200fe_default_options(b200fe_options* o) {
     o->tolerance_mode = 1;
     o->max_outer = 12;
     o->profile = 0;
+    o->pass_kernel = 0;
 }
 
 int b200fe_context_create(int device, b200fe_context** out) {

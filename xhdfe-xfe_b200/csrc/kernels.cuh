@@ -40,9 +40,14 @@ namespace b200fe {
 constexpr int kMaxDims = 8;
 constexpr int kMaxLarge = 2;
 constexpr int kMaxSmall = 4;
-constexpr int kSmallLevels = 64;
-constexpr int kPassThreads = 128;  // primary pass CTA size (4 warps)
+constexpr int kSmallLevels = 64;   // a non-primary dim with <= 64 levels is "small"
+constexpr int kMaxSmallRows = 128; // total levels over all small dims
+constexpr int kPassThreads = 128;  // long-segment pass CTA size (4 warps)
+constexpr int kTileThreads = 256;  // tile pass CTA size (8 warps)
 constexpr int kRowThreads = 256;   // alpha-space row kernels
+constexpr int kTileObs = 512;      // observations staged per tile
+constexpr int kTileStride = 384;   // tiles start within windows of this many obs
+constexpr int kLongSeg = kTileObs - kTileStride;  // longer segments take the long path
 
 // ---------------------------------------------------------------------------
 // 4-wide column quads.  A lane owns columns 4q..4q+3 of an alpha row.
@@ -103,19 +108,25 @@ __device__ __forceinline__ void store_quad_stream(double* p, const Acc4& a) {
     __stcs(reinterpret_cast<double2*>(p) + 1, make_double2(a.v[2], a.v[3]));
 }
 
+
 // ---------------------------------------------------------------------------
-// Primary-segment pass.
+// Primary-segment passes.
 //
-// One group of CQ lanes owns one primary segment s at a time.  For each obs
-// k in s it forms a value val_k (per mode), then
-//     mean_s = sum_k w_k val_k / W_s                          (loop 1)
-//     z_k    = w_k (val_k - mean_s)                           (loop 2)
-// and scatters z_k into the runs of every large dim and the per-warp bins of
-// every small dim.  Modes:
+// For every primary segment s (one value of the eliminated dim) and every
+// observation k in s, with a per-mode value val_k:
+//     mean_s = sum_k w_k val_k / W_s
+//     z_k    = w_k (val_k - mean_s)
+// z_k is scattered into the runs of every large dim and the bins of every
+// small dim.  Modes:
 //   kMatvec : val_k = (D_r x)_k           -> runs/bins give S x
 //   kRhs    : val_k = v_k (data columns)  -> runs/bins give b = D_r'W(I-P_p)v
 //   kFinal  : val_k = v_k - (D_r a)_k     -> writes v~_k = val_k - mean_s, and
 //             (certify) runs/bins of z_k give D_r' W v~ for the certificate
+//
+// tile_pass_kernel handles tiles of whole segments (<= kTileObs obs): all
+// loads of a tile are issued at once into shared memory, then segment means,
+// runs and bins are reduced from shared memory.  Segments longer than
+// kLongSeg form their own tiles and go through segment_pass_kernel.
 // ---------------------------------------------------------------------------
 enum PassMode { kMatvec = 0, kRhs = 1, kFinal = 2 };
 
@@ -131,23 +142,519 @@ struct PassArgs {
     const T* wp;              // [n] weights in primary order, or null (unit)
     const int32_t* pord;      // [n] primary order -> input row, or null (identity)
     const int32_t* rid[kMaxLarge];
-    const int32_t* run_base[kMaxLarge];
-    const int32_t* run_dest[kMaxLarge];
+    const int32_t* run_base[kMaxLarge];   // [Gp+1] first run of each segment
+    const int32_t* run_start[kMaxLarge];  // [nruns+1] first obs of each run
+    const int32_t* run_dest[kMaxLarge];   // [nruns] row of each run in R (group order)
     int64_t lbase[kMaxLarge];  // alpha row offset of each large dim
     const uint32_t* sid;       // [n] packed small-dim ids (8 bits each) or null
     int64_t sbase[kMaxSmall];  // alpha row offset of each small dim
+    int sgoff[kMaxSmall];      // bin row offset of each small dim
+    int SG;                    // bin rows (levels over all small dims)
     const T* x;                // alpha-space input [GR][CP] (kMatvec, kFinal)
     const double* v;           // data, column-major n x cols (kRhs, kFinal)
     double* out;               // output, column-major n x cols (kFinal)
     T* R[kMaxLarge];           // run rows [nruns][CP]
-    double* bins_partial;      // [gridDim][nS][64][CP]
-    double* colsq_partial;     // [gridDim][CP]: kRhs sum v^2; kFinal sum_s (sum_k z_k)^2
+    double* bins_partial;      // [ctas][SG][CP]; this launch writes from bins_cta0
+    double* colsq_partial;     // [ctas][CP]: kRhs sum v^2; kFinal sum_s (sum_k z_k)^2
+    int bins_cta0;             // first CTA slot of this launch in the partial arrays
     int scatter;               // kFinal: 1 to scatter z for the certificate
+    // tiles
+    const int32_t* tile_seg;   // [ntiles+1] first segment of each tile
+    const uint8_t* tile_long;  // [ntiles] 1 for a single long segment
+    int64_t ntiles;
+    // long segments (segment_pass_kernel)
+    const int32_t* long_segs;
+    int64_t nlong;
 };
 
+// (D_r x)_k for the 4 columns of lane quad q
+template <typename T>
+__device__ __forceinline__ void gather_u(const PassArgs<T>& a, int64_t k, int q, Acc4& u) {
+    acc_zero(u);
+#pragma unroll
+    for (int l = 0; l < kMaxLarge; ++l) {
+        if (l < a.nL) {
+            const int32_t g = __ldg(a.rid[l] + k);
+            add_quad(a.x + (a.lbase[l] + g) * a.CP + 4 * q, u);
+        }
+    }
+    if (a.nS > 0) {
+        const uint32_t packed = __ldg(a.sid + k);
+        for (int s = 0; s < a.nS; ++s) {
+            const uint32_t h = (packed >> (8 * s)) & 0xffu;
+            add_quad(a.x + (a.sbase[s] + h) * a.CP + 4 * q, u);
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void smem_load4(const T* p, Acc4& o);
+template <>
+__device__ __forceinline__ void smem_load4<float>(const float* p, Acc4& o) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    o.v[0] = t.x; o.v[1] = t.y; o.v[2] = t.z; o.v[3] = t.w;
+}
+template <>
+__device__ __forceinline__ void smem_load4<double>(const double* p, Acc4& o) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    o.v[0] = a.x; o.v[1] = a.y; o.v[2] = b.x; o.v[3] = b.y;
+}
+template <typename T>
+__device__ __forceinline__ void smem_store4(T* p, const Acc4& o);
+template <>
+__device__ __forceinline__ void smem_store4<float>(float* p, const Acc4& o) {
+    *reinterpret_cast<float4*>(p) = make_float4(static_cast<float>(o.v[0]), static_cast<float>(o.v[1]),
+                                                static_cast<float>(o.v[2]), static_cast<float>(o.v[3]));
+}
+template <>
+__device__ __forceinline__ void smem_store4<double>(double* p, const Acc4& o) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(o.v[0], o.v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(o.v[2], o.v[3]);
+}
+
+// Dynamic shared memory of tile_pass_kernel, in bytes.
+template <typename T>
+__host__ __device__ constexpr size_t tile_smem_bytes(int CP, int SG) {
+    return static_cast<size_t>(kTileObs + 1) * CP * sizeof(T)  // staged values
+           + static_cast<size_t>(kTileObs) * sizeof(T)         // weights
+           + static_cast<size_t>(kTileThreads / 32) * SG * (CP + 1) * sizeof(double)  // bins
+           + static_cast<size_t>(kTileThreads) * 4 * sizeof(double);                 // colsq red
+}
+
+// Staged tile values: kMatvec keeps rows [kl][CP] (16-byte quads, gathered
+// per observation); the data modes keep columns [c][kTileObs + 1] so the
+// coalesced column loads and stores are free of bank conflicts.
+template <typename T, int CP, int MODE>
+struct Stage {
+    static constexpr int LD = kTileObs + 1;
+    __device__ static __forceinline__ void load4(const T* u, int kl, int q, Acc4& o) {
+        if (MODE == kMatvec) {
+            smem_load4<T>(u + kl * CP + 4 * q, o);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) o.v[j] = static_cast<double>(u[(4 * q + j) * LD + kl]);
+        }
+    }
+    __device__ static __forceinline__ void store4(T* u, int kl, int q, const Acc4& o) {
+        if (MODE == kMatvec) {
+            smem_store4<T>(u + kl * CP + 4 * q, o);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) u[(4 * q + j) * LD + kl] = static_cast<T>(o.v[j]);
+        }
+    }
+    __device__ static __forceinline__ T& at(T* u, int kl, int c) {
+        return MODE == kMatvec ? u[kl * CP + c] : u[c * LD + kl];
+    }
+};
+
+template <typename T, int CQ, int MODE>
+__global__ void __launch_bounds__(kTileThreads)
+tile_pass_kernel(const PassArgs<T> a) {
+    constexpr int CP = 4 * CQ;
+    using St = Stage<T, CP, MODE>;
+    constexpr int GPB = kTileThreads / CQ;  // lane groups per block
+    constexpr int BROW = CP + 1;            // padded bin row (doubles)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* ubuf = reinterpret_cast<T*>(smem_raw);
+    T* wbuf = ubuf + (kTileObs + 1) * CP;
+    double* bins = reinterpret_cast<double*>(wbuf + kTileObs);
+    double* red = bins + (kTileThreads / 32) * a.SG * BROW;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int g = tid / CQ;  // lane group
+    const int q = tid % CQ;
+    const bool scatter = (MODE != kFinal) || a.scatter;
+    double* my_bins = bins + warp * a.SG * BROW;
+    for (int i = tid; i < (kTileThreads / 32) * a.SG * BROW; i += kTileThreads) bins[i] = 0.0;
+    double colsq[4] = {0.0, 0.0, 0.0, 0.0};
+
+    for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        if (a.tile_long[t]) continue;
+        const int32_t s0 = a.tile_seg[t], s1 = a.tile_seg[t + 1];
+        const int64_t k0 = a.seg_off[s0];
+        const int nk = static_cast<int>(a.seg_off[s1] - k0);
+        __syncthreads();  // previous tile fully consumed
+        // ---- phase A: stage values and weights --------------------------
+        if (MODE == kMatvec) {
+            for (int kl = g; kl < nk; kl += GPB) {
+                Acc4 u;
+                gather_u(a, k0 + kl, q, u);
+                St::store4(ubuf, kl, q, u);
+            }
+        } else {
+            const int total = CP * nk;
+            for (int idx = tid; idx < total; idx += kTileThreads) {
+                const int c = idx / nk;
+                const int kl = idx - c * nk;
+                double val = 0.0;
+                if (c < a.cols) {
+                    const int64_t k = k0 + kl;
+                    const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
+                    val = __ldcs(a.v + static_cast<int64_t>(c) * a.n + o);
+                }
+                St::at(ubuf, kl, c) = static_cast<T>(val);
+            }
+        }
+        for (int kl = tid; kl < nk; kl += kTileThreads)
+            wbuf[kl] = a.wp ? a.wp[k0 + kl] : static_cast<T>(1);
+        if (MODE == kFinal) {
+            __syncthreads();
+            for (int kl = g; kl < nk; kl += GPB) {
+                Acc4 u, val;
+                gather_u(a, k0 + kl, q, u);
+                St::load4(ubuf, kl, q, val);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) val.v[j] -= u.v[j];
+                St::store4(ubuf, kl, q, val);
+            }
+        }
+        __syncthreads();
+        // ---- phase B: segment means; ubuf <- z (kMatvec/kRhs) or d (kFinal)
+        for (int32_t s = s0 + g; s < s1; s += GPB) {
+            const int b = static_cast<int>(a.seg_off[s] - k0);
+            const int e = static_cast<int>(a.seg_off[s + 1] - k0);
+            Acc4 acc;
+            acc_zero(acc);
+            for (int kl = b; kl < e; ++kl) {
+                Acc4 val;
+                St::load4(ubuf, kl, q, val);
+                const double w = static_cast<double>(wbuf[kl]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    acc.v[j] = fma(w, val.v[j], acc.v[j]);
+                    if (MODE == kRhs) colsq[j] = fma(val.v[j], val.v[j], colsq[j]);
+                }
+            }
+            const double iw = a.inv_wp[s];
+            Acc4 zs;
+            acc_zero(zs);
+            for (int kl = b; kl < e; ++kl) {
+                Acc4 val;
+                St::load4(ubuf, kl, q, val);
+                const double w = static_cast<double>(wbuf[kl]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const double d = val.v[j] - acc.v[j] * iw;
+                    val.v[j] = (MODE == kFinal) ? d : w * d;
+                    if (MODE == kFinal) zs.v[j] = fma(w, d, zs.v[j]);
+                }
+                St::store4(ubuf, kl, q, val);
+            }
+            if (MODE == kFinal) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) colsq[j] = fma(zs.v[j], zs.v[j], colsq[j]);
+            }
+        }
+        __syncthreads();
+        // ---- phase C: runs of the large dims -----------------------------
+        if (scatter) {
+#pragma unroll
+            for (int l = 0; l < kMaxLarge; ++l) {
+                if (l >= a.nL) continue;
+                const int32_t rb = a.run_base[l][s0], re = a.run_base[l][s1];
+                for (int32_t m = rb + g; m < re; m += GPB) {
+                    const int b = static_cast<int>(a.run_start[l][m] - k0);
+                    const int e = static_cast<int>(a.run_start[l][m + 1] - k0);
+                    Acc4 acc;
+                    acc_zero(acc);
+                    for (int kl = b; kl < e; ++kl) {
+                        Acc4 z;
+                        St::load4(ubuf, kl, q, z);
+                        const double w = (MODE == kFinal) ? static_cast<double>(wbuf[kl]) : 1.0;
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc.v[j] = fma(w, z.v[j], acc.v[j]);
+                    }
+                    store_quad_stream(a.R[l] + static_cast<int64_t>(a.run_dest[l][m]) * CP + 4 * q,
+                                      acc);
+                }
+            }
+            // ---- phase C': small-dim bins, warp-private, fixed order ------
+            // A warp step covers 32/CP consecutive observations, one per
+            // group of CP lanes (lane = column).  Groups with the same level
+            // are summed in group order by the first of them, which then
+            // updates the warp's bin row once.
+            if (a.nS > 0) {
+                constexpr int G = 32 / CP;
+                const int gi = lane / CP;
+                const int c = lane % CP;
+                const int per_warp = (nk + (kTileThreads / 32) - 1) / (kTileThreads / 32);
+                const int wb = warp * per_warp;
+                const int we = min(nk, wb + per_warp);
+                for (int base = wb; base < we; base += G) {
+                    const int kl = base + gi;
+                    const bool valid = kl < we;
+                    const uint32_t packed = valid ? __ldg(a.sid + k0 + kl) : 0u;
+                    for (int s = 0; s < a.nS; ++s) {
+                        const uint32_t key = valid ? ((packed >> (8 * s)) & 0xffu) : 0x100u + gi;
+                        const unsigned int match = __match_any_sync(0xffffffffu, key);
+                        if (valid && (__ffs(match) - 1) / CP == gi) {
+                            double acc = 0.0;
+#pragma unroll
+                            for (int g2 = 0; g2 < G; ++g2) {
+                                if (match & (1u << (g2 * CP))) {
+                                    const int kj = base + g2;
+                                    const double w =
+                                        (MODE == kFinal) ? static_cast<double>(wbuf[kj]) : 1.0;
+                                    acc = fma(w, static_cast<double>(St::at(ubuf, kj, c)), acc);
+                                }
+                            }
+                            my_bins[(a.sgoff[s] + static_cast<int>(key)) * BROW + c] += acc;
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+        }
+        // ---- phase D: write the within transform -------------------------
+        if (MODE == kFinal) {
+            const int total = a.cols * nk;
+            for (int idx = tid; idx < total; idx += kTileThreads) {
+                const int c = idx / nk;
+                const int kl = idx - c * nk;
+                const int64_t k = k0 + kl;
+                const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
+                __stcs(a.out + static_cast<int64_t>(c) * a.n + o,
+                       static_cast<double>(St::at(ubuf, kl, c)));
+            }
+        }
+    }
+    __syncthreads();
+    const int cta = a.bins_cta0 + blockIdx.x;
+    if (a.nS > 0 && scatter) {
+        double* dst = a.bins_partial + static_cast<int64_t>(cta) * a.SG * CP;
+        for (int i = tid; i < a.SG * CP; i += kTileThreads) {
+            const int r = i / CP, c = i - r * CP;
+            double s = 0.0;
+            for (int w = 0; w < kTileThreads / 32; ++w) s += bins[(w * a.SG + r) * BROW + c];
+            dst[i] = s;
+        }
+    }
+    if (MODE == kRhs || MODE == kFinal) {
+        for (int j = 0; j < 4; ++j) red[tid * 4 + j] = colsq[j];
+        __syncthreads();
+        if (tid < CQ) {
+            double s4[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int t = tid; t < kTileThreads; t += CQ)
+                for (int j = 0; j < 4; ++j) s4[j] += red[t * 4 + j];
+            for (int j = 0; j < 4; ++j)
+                a.colsq_partial[static_cast<int64_t>(cta) * CP + 4 * tid + j] = s4[j];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Run-level matvec (at most one large non-primary dim).
+//
+// Within a run (obs of one primary segment with the same large-dim group f)
+// the large-dim part of u_k = x_f[f] + sum_small x_s[h_s(k)] is constant, so
+//     U_m   = c_m x_f[f_m] + sum_{k in m} w_k ys_k      (ys_k: small-dim part)
+//     t_s   = sum_{m in s} U_m / W_s
+//     R_m   = U_m - c_m t_s                              (run row of S x)
+//     z_k   = w_k (x_f[f_m] + ys_k - t_s)                (small-dim bins)
+// One x_f gather per run, small-dim rows of x from shared memory.  A group of
+// CQ lanes owns one segment; bins are per warp, updated in warp-synchronous
+// steps in which only groups that hit the same bin row are serialized (in
+// group order), so the sums are deterministic.
+// ---------------------------------------------------------------------------
+constexpr int kRunThreads = 128;
+
+template <typename T>
+struct RunArgs {
+    int32_t Gp;
+    int CP;
+    int nS;
+    int has_large;
+    const int2* seg_meta;   // [Gp+1] {first obs, first run}
+    const double* inv_wp;   // [Gp]
+    const T* wp;            // [n] or null
+    const uint32_t* sid;    // [n] or null
+    int64_t sbase0;         // alpha row of the first small-dim level
+    int sgoff[kMaxSmall];
+    int SG;
+    int64_t lbase;          // alpha row of the large dim
+    const int4* run_meta;   // [nruns] {group, dest row, first obs, end obs}
+    const T* run_w;         // [nruns] run weights c_m
+    const T* x;             // alpha [GR][CP]
+    T* R;                   // [nruns][CP]
+    double* bins_partial;   // [ctas][SG][CP]
+    int bins_cta0;
+};
+
+template <typename T>
+__host__ __device__ constexpr size_t run_smem_bytes(int CP, int SG) {
+    return static_cast<size_t>(SG) * CP * sizeof(T) +
+           static_cast<size_t>(kRunThreads / 32) * SG * CP * sizeof(double) + 16;
+}
+
+template <typename T>
+__device__ __forceinline__ void small_part(const RunArgs<T>& a, const T* xs, uint32_t packed,
+                                           int q, Acc4& ys) {
+    acc_zero(ys);
+    for (int s = 0; s < a.nS; ++s) {
+        const int h = static_cast<int>((packed >> (8 * s)) & 0xffu);
+        Acc4 v;
+        smem_load4<T>(xs + (a.sgoff[s] + h) * a.CP + 4 * q, v);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) ys.v[j] += v.v[j];
+    }
+}
+
+template <typename T, int CQ>
+__global__ void __launch_bounds__(kRunThreads)
+run_pass_kernel(const RunArgs<T> a) {
+    constexpr int CP = 4 * CQ;
+    constexpr int GPW = 32 / CQ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* xs = reinterpret_cast<T*>(smem_raw);
+    double* bins = reinterpret_cast<double*>(
+        smem_raw + ((static_cast<size_t>(a.SG) * CP * sizeof(T) + 15) & ~size_t(15)));
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int gw = lane / CQ;
+    const int q = lane % CQ;
+    for (int i = tid; i < a.SG * CP; i += kRunThreads) xs[i] = a.x[a.sbase0 * CP + i];
+    for (int i = tid; i < (kRunThreads / 32) * a.SG * CP; i += kRunThreads) bins[i] = 0.0;
+    __syncthreads();
+    double* wbins = bins + warp * a.SG * CP;
+    const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (kRunThreads / 32);
+    const int64_t wid = static_cast<int64_t>(blockIdx.x) * (kRunThreads / 32) + warp;
+
+    for (int64_t s0 = wid * GPW; s0 < a.Gp; s0 += nwarps * GPW) {
+        const int64_t s = s0 + gw;
+        int k0 = 0, k1 = 0, rb = 0, re = 0;
+        double iw = 0.0;
+        if (s < a.Gp) {
+            const int2 m0 = a.seg_meta[s], m1 = a.seg_meta[s + 1];
+            k0 = m0.x;
+            k1 = m1.x;
+            rb = m0.y;
+            re = m1.y;
+            iw = a.inv_wp[s];
+            if (k1 - k0 > kLongSeg) k1 = k0;  // long segments take the long path
+        }
+        const int len = k1 - k0;
+        // pass 1: t = (sum_m c_m x_f[f_m] + sum_k w_k ys_k) / W_s
+        Acc4 tsum;
+        acc_zero(tsum);
+        if (a.has_large && len > 0) {
+            for (int m = rb; m < re; ++m) {
+                const int4 rm = a.run_meta[m];
+                const double cm = static_cast<double>(a.run_w[m]);
+                Acc4 xf;
+                load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) tsum.v[j] = fma(cm, xf.v[j], tsum.v[j]);
+            }
+        }
+        if (a.nS > 0) {
+            for (int k = k0; k < k1; ++k) {
+                Acc4 ys;
+                small_part(a, xs, __ldg(a.sid + k), q, ys);
+                const double w = a.wp ? static_cast<double>(a.wp[k]) : 1.0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) tsum.v[j] = fma(w, ys.v[j], tsum.v[j]);
+            }
+        }
+        Acc4 t;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) t.v[j] = tsum.v[j] * iw;
+
+        // pass 2: run rows and small-dim bins, warp-synchronous over obs
+        int steps = len;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) steps = max(steps, __shfl_xor_sync(0xffffffffu, steps, off));
+        int m = rb;
+        int run_end = k1;
+        double cm = 0.0;
+        Acc4 xf, Y;
+        acc_zero(xf);
+        acc_zero(Y);
+        if (a.has_large && len > 0) {
+            const int4 rm = a.run_meta[m];
+            cm = static_cast<double>(a.run_w[m]);
+            load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+            run_end = rm.w;
+        }
+        for (int step = 0; step < steps; ++step) {
+            const bool active = step < len;
+            const int k = k0 + step;
+            Acc4 z;
+            acc_zero(z);
+            uint32_t packed = 0;
+            if (active) {
+                if (a.has_large && k == run_end) {
+                    const int4 rp = a.run_meta[m];
+                    Acc4 r;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) r.v[j] = fma(cm, xf.v[j] - t.v[j], Y.v[j]);
+                    store_quad_stream(a.R + static_cast<int64_t>(rp.y) * CP + 4 * q, r);
+                    ++m;
+                    const int4 rm = a.run_meta[m];
+                    cm = static_cast<double>(a.run_w[m]);
+                    load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+                    run_end = rm.w;
+                    acc_zero(Y);
+                }
+                const double w = a.wp ? static_cast<double>(a.wp[k]) : 1.0;
+                Acc4 ys;
+                acc_zero(ys);
+                if (a.nS > 0) {
+                    packed = __ldg(a.sid + k);
+                    small_part(a, xs, packed, q, ys);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    Y.v[j] = fma(w, ys.v[j], Y.v[j]);
+                    z.v[j] = w * (xf.v[j] + ys.v[j] - t.v[j]);
+                }
+            }
+            for (int sd = 0; sd < a.nS; ++sd) {
+                const uint32_t key = active ? ((packed >> (8 * sd)) & 0xffu) : 0x100u + gw;
+                const unsigned int match = __match_any_sync(0xffffffffu, key);
+                const int rank = __popc(match & ((1u << lane) - 1u)) / CQ;
+                int msize = __popc(match) / CQ;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1)
+                    msize = max(msize, __shfl_xor_sync(0xffffffffu, msize, off));
+                double* brow = wbins + (a.sgoff[sd] + static_cast<int>(key & 0xffu)) * CP + 4 * q;
+                for (int r = 0; r < msize; ++r) {
+                    if (active && rank == r) {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) brow[j] += z.v[j];
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        if (a.has_large && len > 0) {
+            const int4 rp = a.run_meta[m];
+            Acc4 r;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) r.v[j] = fma(cm, xf.v[j] - t.v[j], Y.v[j]);
+            store_quad_stream(a.R + static_cast<int64_t>(rp.y) * CP + 4 * q, r);
+        }
+    }
+    __syncthreads();
+    if (a.nS > 0) {
+        double* dst = a.bins_partial + static_cast<int64_t>(a.bins_cta0 + blockIdx.x) * a.SG * CP;
+        for (int i = tid; i < a.SG * CP; i += kRunThreads) {
+            double sum = 0.0;
+            for (int w = 0; w < kRunThreads / 32; ++w) sum += bins[w * a.SG * CP + i];
+            dst[i] = sum;
+        }
+    }
+}
+
+// Long segments: one group of CQ lanes walks one listed segment serially.
+// Correct for any length; used only for the few segments longer than
+// kLongSeg, which do not fit a tile.
 template <typename T, int MODE>
-__device__ __forceinline__ void pass_value(const PassArgs<T>& a, int64_t k, int q,
-                                           Acc4& val) {
+__device__ __forceinline__ void seg_value(const PassArgs<T>& a, int64_t k, int q, Acc4& val) {
     acc_zero(val);
     if (MODE == kRhs || MODE == kFinal) {
         const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
@@ -159,21 +666,7 @@ __device__ __forceinline__ void pass_value(const PassArgs<T>& a, int64_t k, int 
     }
     if (MODE == kMatvec || MODE == kFinal) {
         Acc4 u;
-        acc_zero(u);
-#pragma unroll
-        for (int l = 0; l < kMaxLarge; ++l) {
-            if (l < a.nL) {
-                const int32_t g = __ldg(a.rid[l] + k);
-                add_quad(a.x + (a.lbase[l] + g) * a.CP + 4 * q, u);
-            }
-        }
-        if (a.nS > 0) {
-            const uint32_t packed = __ldg(a.sid + k);
-            for (int s = 0; s < a.nS; ++s) {
-                const uint32_t h = (packed >> (8 * s)) & 0xffu;
-                add_quad(a.x + (a.sbase[s] + h) * a.CP + 4 * q, u);
-            }
-        }
+        gather_u(a, k, q, u);
         if (MODE == kMatvec) {
             val = u;
         } else {
@@ -185,29 +678,27 @@ __device__ __forceinline__ void pass_value(const PassArgs<T>& a, int64_t k, int 
 
 template <typename T, int CQ, int MODE>
 __global__ void __launch_bounds__(kPassThreads)
-primary_pass_kernel(const PassArgs<T> a) {
-    extern __shared__ double smem_bins[];  // [warps][nS][64][CP]
-    constexpr int GPW = 32 / CQ;           // segment groups per warp
+segment_pass_kernel(const PassArgs<T> a) {
+    extern __shared__ double smem_bins[];  // [warps][SG][CP], then colsq red
+    constexpr int GPW = 32 / CQ;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int gw = lane / CQ;              // group within warp
+    const int gw = lane / CQ;
     const int q = lane % CQ;
     const int warps_per_block = kPassThreads / 32;
-    const int bin_stride = a.nS * kSmallLevels * a.CP;  // doubles per warp
+    const int bin_stride = a.SG * a.CP;
     double* my_bins = smem_bins + warp * bin_stride;
     const bool scatter = (MODE != kFinal) || a.scatter;
-
     for (int i = threadIdx.x; i < warps_per_block * bin_stride; i += kPassThreads)
         smem_bins[i] = 0.0;
     __syncthreads();
-
     double colsq[4] = {0.0, 0.0, 0.0, 0.0};
     const int64_t total_warps = static_cast<int64_t>(gridDim.x) * warps_per_block;
     const int64_t warp_id = static_cast<int64_t>(blockIdx.x) * warps_per_block + warp;
-
-    for (int64_t s0 = warp_id * GPW; s0 < a.Gp; s0 += total_warps * GPW) {
-        const int64_t s = s0 + gw;
-        const bool valid = s < a.Gp;
+    for (int64_t i0 = warp_id * GPW; i0 < a.nlong; i0 += total_warps * GPW) {
+        const int64_t li = i0 + gw;
+        const bool valid = li < a.nlong;
+        const int32_t s = valid ? a.long_segs[li] : 0;
         int64_t beg = 0, len = 0;
         double inv_w = 0.0;
         if (valid) {
@@ -215,32 +706,27 @@ primary_pass_kernel(const PassArgs<T> a) {
             len = a.seg_off[s + 1] - beg;
             inv_w = a.inv_wp[s];
         }
-        // loop 1: weighted segment mean of the value
         Acc4 acc;
         acc_zero(acc);
         for (int64_t t = 0; t < len; ++t) {
             const int64_t k = beg + t;
             Acc4 val;
-            pass_value<T, MODE>(a, k, q, val);
+            seg_value<T, MODE>(a, k, q, val);
             const double w = a.wp ? static_cast<double>(a.wp[k]) : 1.0;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc.v[j] = fma(w, val.v[j], acc.v[j]);
-            if (MODE == kRhs) {
-#pragma unroll
-                for (int j = 0; j < 4; ++j) colsq[j] = fma(val.v[j], val.v[j], colsq[j]);
+            for (int j = 0; j < 4; ++j) {
+                acc.v[j] = fma(w, val.v[j], acc.v[j]);
+                if (MODE == kRhs) colsq[j] = fma(val.v[j], val.v[j], colsq[j]);
             }
         }
         Acc4 mean;
 #pragma unroll
         for (int j = 0; j < 4; ++j) mean.v[j] = acc.v[j] * inv_w;
-
-        // loop 2: z_k = w_k (val_k - mean); outputs, runs and bins
         int64_t steps = len;
         if (a.nS > 0 && scatter) {
             int64_t m = len;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1)
-                m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+            for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
             steps = m;
         }
         int32_t cur[kMaxLarge];
@@ -262,7 +748,7 @@ primary_pass_kernel(const PassArgs<T> a) {
             uint32_t packed = 0;
             if (active) {
                 Acc4 val;
-                pass_value<T, MODE>(a, k, q, val);
+                seg_value<T, MODE>(a, k, q, val);
                 const double w = a.wp ? static_cast<double>(a.wp[k]) : 1.0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -284,14 +770,14 @@ primary_pass_kernel(const PassArgs<T> a) {
 #pragma unroll
                     for (int l = 0; l < kMaxLarge; ++l) {
                         if (l >= a.nL) continue;
-                        const int32_t g = __ldg(a.rid[l] + k);
-                        if (t > 0 && g != prev[l]) {
+                        const int32_t gid = __ldg(a.rid[l] + k);
+                        if (t > 0 && gid != prev[l]) {
                             store_quad_stream(a.R[l] + static_cast<int64_t>(a.run_dest[l][cur[l]]) * a.CP + 4 * q,
                                               racc[l]);
                             ++cur[l];
                             acc_zero(racc[l]);
                         }
-                        prev[l] = g;
+                        prev[l] = gid;
 #pragma unroll
                         for (int j = 0; j < 4; ++j) racc[l].v[j] += z.v[j];
                     }
@@ -299,13 +785,12 @@ primary_pass_kernel(const PassArgs<T> a) {
                 }
             }
             if (a.nS > 0 && scatter) {
-                // fixed-order, race-free bin update: one segment group at a time
                 for (int j = 0; j < GPW; ++j) {
                     __syncwarp();
                     if (gw == j && active) {
                         for (int s2 = 0; s2 < a.nS; ++s2) {
                             const uint32_t h = (packed >> (8 * s2)) & 0xffu;
-                            double* b = my_bins + (s2 * kSmallLevels + h) * a.CP + 4 * q;
+                            double* b = my_bins + (a.sgoff[s2] + h) * a.CP + 4 * q;
 #pragma unroll
                             for (int c = 0; c < 4; ++c) b[c] += z.v[c];
                         }
@@ -317,19 +802,19 @@ primary_pass_kernel(const PassArgs<T> a) {
         if (scatter && valid && len > 0) {
 #pragma unroll
             for (int l = 0; l < kMaxLarge; ++l)
-                if (l < a.nL) store_quad_stream(a.R[l] + static_cast<int64_t>(a.run_dest[l][cur[l]]) * a.CP + 4 * q,
-                                  racc[l]);
+                if (l < a.nL)
+                    store_quad_stream(a.R[l] + static_cast<int64_t>(a.run_dest[l][cur[l]]) * a.CP + 4 * q,
+                                      racc[l]);
         }
         if (MODE == kFinal && valid) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) colsq[j] = fma(zsum.v[j], zsum.v[j], colsq[j]);
         }
     }
-
-    // per-CTA bins: warps summed in fixed order
     __syncthreads();
+    const int cta = a.bins_cta0 + blockIdx.x;
     if (a.nS > 0 && scatter) {
-        double* dst = a.bins_partial + static_cast<int64_t>(blockIdx.x) * bin_stride;
+        double* dst = a.bins_partial + static_cast<int64_t>(cta) * bin_stride;
         for (int i = threadIdx.x; i < bin_stride; i += kPassThreads) {
             double s = 0.0;
             for (int w = 0; w < warps_per_block; ++w) s += smem_bins[w * bin_stride + i];
@@ -337,11 +822,8 @@ primary_pass_kernel(const PassArgs<T> a) {
         }
     }
     if (MODE == kRhs || MODE == kFinal) {
-        // per-CTA column sums of colsq: lanes with the same q hold the same columns
         __syncthreads();
-        double* red = smem_bins;  // reuse: [kPassThreads][4]
-        // make sure there is room: bins area may be empty (nS == 0) -> caller
-        // sizes dynamic smem to at least kPassThreads*4 doubles.
+        double* red = smem_bins;
         for (int j = 0; j < 4; ++j) red[threadIdx.x * 4 + j] = colsq[j];
         __syncthreads();
         if (threadIdx.x < CQ) {
@@ -349,13 +831,36 @@ primary_pass_kernel(const PassArgs<T> a) {
             for (int t = threadIdx.x; t < kPassThreads; t += CQ)
                 for (int j = 0; j < 4; ++j) s4[j] += red[t * 4 + j];
             for (int j = 0; j < 4; ++j)
-                a.colsq_partial[static_cast<int64_t>(blockIdx.x) * a.CP + 4 * threadIdx.x + j] = s4[j];
+                a.colsq_partial[static_cast<int64_t>(cta) * a.CP + 4 * threadIdx.x + j] = s4[j];
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Run gather-sum (large dims): out row of group g = sum of its runs' rows.
+// Deterministic block reduction of per-column partials: out[c] = sum over
+// parts p in [0, nparts) of part[p * stride + c], c < CP.  Thread t sums the
+// parts p == t / CP (mod blockDim / CP) in order; a fixed tree finishes.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double block_column_sum(const double* part, int64_t nparts,
+                                                   int64_t stride, int CP, double* red) {
+    const int t = threadIdx.x;
+    const int J = blockDim.x / CP;
+    const int c = t % CP;
+    const int j = t / CP;
+    double s = 0.0;
+    if (j < J)
+        for (int64_t p = j; p < nparts; p += J) s += __ldcg(part + p * stride + c);
+    red[t] = s;
+    __syncthreads();
+    for (int h = J / 2; h > 0; h >>= 1) {
+        if (j < h) red[t] += red[t + h * CP];
+        __syncthreads();
+    }
+    return red[c];  // valid for every thread after the tree
+}
+
+// ---------------------------------------------------------------------------
+// Run gather-sum (large dims): row of group g = sum of its runs' rows.
 // Chunks (group, begin, end) with end-begin <= chunk size; groups with one
 // chunk are written directly, multi-chunk groups leave a partial per chunk.
 // Also accumulates, per CTA, the dot of the written rows with `dotv`.
@@ -421,33 +926,32 @@ run_gather_kernel(const GatherArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// Finalize: multi-chunk large groups and small-dim bins; then the last CTA
-// reduces every dot partial (run_gather CTAs and this kernel's) in a fixed
-// order into dot_out[CP].
+// Finalize: one CTA per output row that needs a second reduction level
+// (multi-chunk large groups, then small-dim levels); each sums its partials
+// with block_column_sum.  The last CTA then reduces every dot partial
+// (run_gather CTAs, then this kernel's rows) into dot_out[CP].
 // ---------------------------------------------------------------------------
 template <typename T>
 struct FinalizeArgs {
     int CP;
     int nL, nS;
-    // multi-chunk groups of each large dim
     int64_t nmulti[kMaxLarge];
     const int32_t* multi_grp[kMaxLarge];
     const int32_t* multi_c0[kMaxLarge];
     const int32_t* multi_c1[kMaxLarge];
     const double* partial[kMaxLarge];
     int64_t lbase[kMaxLarge];
-    // small dims
-    int32_t sG[kMaxSmall];
-    int64_t sbase[kMaxSmall];
-    const double* bins_partial;  // [nbins_ctas][nS][64][CP]
+    int SG;                      // small-dim levels (bin rows)
+    int64_t sgbase;              // alpha row of bin row 0 (small dims are contiguous)
+    const double* bins_partial;  // [nbins_ctas][SG][CP]
     int nbins_ctas;
+    int64_t nrows;               // sum nmulti + SG
     T* out;                      // alpha rows [GR][CP]
     const T* dotv;               // or null
-    // dot reduction
-    double* dot_partial;         // this kernel's [gridDim][CP]
-    const double* gather_dot_partial[kMaxLarge];  // run_gather's partials
+    double* dot_partial;         // this kernel's [nrows][CP]
+    const double* gather_dot_partial[kMaxLarge];
     int gather_ctas[kMaxLarge];
-    double* dot_out;             // [CP]
+    double* dot_out;             // [CP] or null
     unsigned int* ticket;
 };
 
@@ -456,80 +960,54 @@ __global__ void __launch_bounds__(kRowThreads)
 finalize_kernel(const FinalizeArgs<T> a) {
     __shared__ double red[kRowThreads];
     __shared__ bool last;
-    // item space: (multi groups of each large dim) then (small bins), per column
-    double dot = 0.0;
-    int mycol = -1;
-    int64_t items = 0;
-    for (int l = 0; l < a.nL; ++l) items += a.nmulti[l] * a.CP;
-    for (int s = 0; s < a.nS; ++s) items += static_cast<int64_t>(a.sG[s]) * a.CP;
-    // stride is a multiple of CP so each thread keeps one column
-    const int64_t stride = static_cast<int64_t>(gridDim.x) * kRowThreads;
-    const int64_t start = static_cast<int64_t>(blockIdx.x) * kRowThreads + threadIdx.x;
-    for (int64_t it = start; it < items; it += stride) {
-        int64_t r = it;
-        const int c = static_cast<int>(r % a.CP);
-        int64_t rowi = r / a.CP;
-        mycol = c;
-        double sum = 0.0;
+    const int CP = a.CP;
+    for (int64_t r = blockIdx.x; r < a.nrows; r += gridDim.x) {
+        int64_t ri = r;
         int64_t orow = -1;
-        bool done = false;
-        for (int l = 0; l < a.nL && !done; ++l) {
-            if (rowi < a.nmulti[l]) {
-                const int32_t g = a.multi_grp[l][rowi];
-                for (int32_t ch = a.multi_c0[l][rowi]; ch < a.multi_c1[l][rowi]; ++ch)
-                    sum += a.partial[l][static_cast<int64_t>(ch) * a.CP + c];
-                orow = a.lbase[l] + g;
-                done = true;
+        const double* part = nullptr;
+        int64_t np = 0, stride = CP;
+        for (int l = 0; l < a.nL && orow < 0; ++l) {
+            if (ri < a.nmulti[l]) {
+                const int32_t c0 = a.multi_c0[l][ri], c1 = a.multi_c1[l][ri];
+                part = a.partial[l] + static_cast<int64_t>(c0) * CP;
+                np = c1 - c0;
+                orow = a.lbase[l] + a.multi_grp[l][ri];
             } else {
-                rowi -= a.nmulti[l];
+                ri -= a.nmulti[l];
             }
         }
-        for (int s = 0; s < a.nS && !done; ++s) {
-            if (rowi < a.sG[s]) {
-                const int64_t off = (static_cast<int64_t>(s) * kSmallLevels + rowi) * a.CP + c;
-                const int64_t stride_cta = static_cast<int64_t>(a.nS) * kSmallLevels * a.CP;
-                for (int b = 0; b < a.nbins_ctas; ++b) sum += a.bins_partial[b * stride_cta + off];
-                orow = a.sbase[s] + rowi;
-                done = true;
-            } else {
-                rowi -= a.sG[s];
-            }
+        if (orow < 0) {  // small-dim level ri
+            part = a.bins_partial + ri * CP;
+            np = a.nbins_ctas;
+            stride = static_cast<int64_t>(a.SG) * CP;
+            orow = a.sgbase + ri;
         }
-        const T stored = static_cast<T>(sum);
-        a.out[orow * a.CP + c] = stored;
-        if (a.dotv) dot = fma(static_cast<double>(a.dotv[orow * a.CP + c]),
-                              static_cast<double>(stored), dot);
+        const double sum = block_column_sum(part, np, stride, CP, red);
+        if (threadIdx.x < CP) {
+            const T stored = static_cast<T>(sum);
+            a.out[orow * CP + threadIdx.x] = stored;
+            if (a.dot_out)
+                a.dot_partial[r * CP + threadIdx.x] =
+                    a.dotv ? static_cast<double>(a.dotv[orow * CP + threadIdx.x]) *
+                                 static_cast<double>(stored)
+                           : 0.0;
+        }
+        __syncthreads();
     }
     if (!a.dot_out) return;
-    // per-CTA per-column partials: thread t always handles column (start % CP)
-    // because stride % CP == 0 is guaranteed by the launcher.
-    red[threadIdx.x] = dot;
-    (void)mycol;
-    __syncthreads();
-    if (threadIdx.x < a.CP) {
-        double s = 0.0;
-        for (int t = threadIdx.x; t < kRowThreads; t += a.CP) s += red[t];
-        a.dot_partial[static_cast<int64_t>(blockIdx.x) * a.CP + threadIdx.x] = s;
-    }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned int t = atomicAdd(a.ticket, 1u);
-        last = (t == gridDim.x - 1);
-    }
+    if (threadIdx.x == 0) last = (atomicAdd(a.ticket, 1u) == gridDim.x - 1);
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (threadIdx.x < a.CP) {
-        const int c = threadIdx.x;
-        double s = 0.0;
-        for (int l = 0; l < a.nL; ++l)
-            for (int b = 0; b < a.gather_ctas[l]; ++b)
-                s += __ldcg(a.gather_dot_partial[l] + static_cast<int64_t>(b) * a.CP + c);
-        for (int b = 0; b < static_cast<int>(gridDim.x); ++b)
-            s += __ldcg(a.dot_partial + static_cast<int64_t>(b) * a.CP + c);
-        a.dot_out[c] = s;
+    double total = 0.0;
+    for (int l = 0; l < a.nL; ++l) {
+        total += block_column_sum(a.gather_dot_partial[l], a.gather_ctas[l], CP, CP, red);
+        __syncthreads();
     }
+    total += block_column_sum(a.dot_partial, a.nrows, CP, CP, red);
+    if (threadIdx.x < CP) a.dot_out[threadIdx.x] = total;
     if (threadIdx.x == 0) *a.ticket = 0u;
 }
 
@@ -537,11 +1015,10 @@ finalize_kernel(const FinalizeArgs<T> a) {
 // PCG vector kernels over the alpha rows (GR x CP), per-column scalars.
 // ---------------------------------------------------------------------------
 struct CgScalars {
-    // per column (CP entries each)
     double* rz;      // r'z
     double* pq;      // p'Sp
     double* rr;      // r'r
-    double* bb;      // b'b (fixed per solve)
+    double* bb;      // per-column stop threshold on r'r
     double* beta;
     double* alpha;
     int* active;     // 1 while the column iterates
@@ -559,6 +1036,7 @@ cg_update_kernel(int64_t GR, int CP, T* __restrict__ x, T* __restrict__ r,
                  T* __restrict__ z, const T* __restrict__ p, const T* __restrict__ qv,
                  const T* __restrict__ dinv, CgScalars sc, double tol2, int iter) {
     __shared__ double red[kRowThreads][2];
+    __shared__ double red1[kRowThreads];
     __shared__ bool last;
     const int64_t total = GR * CP;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * kRowThreads;  // multiple of CP
@@ -600,13 +1078,11 @@ cg_update_kernel(int64_t GR, int CP, T* __restrict__ x, T* __restrict__ r,
     __syncthreads();
     if (!last) return;
     __threadfence();
+    const double s0 = block_column_sum(sc.partial, gridDim.x, 2 * CP, CP, red1);
+    __syncthreads();
+    const double s1 = block_column_sum(sc.partial + CP, gridDim.x, 2 * CP, CP, red1);
     if (threadIdx.x < CP) {
         const int cc = threadIdx.x;
-        double s0 = 0.0, s1 = 0.0;
-        for (int b = 0; b < static_cast<int>(gridDim.x); ++b) {
-            s0 += __ldcg(sc.partial + static_cast<int64_t>(b) * 2 * CP + cc);
-            s1 += __ldcg(sc.partial + static_cast<int64_t>(b) * 2 * CP + CP + cc);
-        }
         const int was_active = sc.active[cc];
         if (was_active) {
             const double old = sc.rz[cc];
@@ -638,6 +1114,10 @@ cg_direction_kernel(int64_t GR, int CP, T* __restrict__ p, const T* __restrict__
     const bool act = sc.active[c] != 0;
     const double be = first ? 0.0 : sc.beta[c];
     if (!act && !first) return;
+    if (first) {  // p is not read: its memory is uninitialised before the first step
+        for (int64_t i = start; i < total; i += stride) p[i] = z[i];
+        return;
+    }
     for (int64_t i = start; i < total; i += stride)
         p[i] = static_cast<T>(static_cast<double>(z[i]) + be * static_cast<double>(p[i]));
 }

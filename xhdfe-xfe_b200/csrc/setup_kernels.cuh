@@ -134,14 +134,61 @@ __global__ void run_fill_kernel(const int32_t* __restrict__ flags, const int32_t
     }
 }
 
-// run_base[s] = index of the first run of segment s.
+// run_base[s] = index of the first run at or after segment s's first obs
+// (so run_base is non-decreasing and empty segments own no run);
+// run_base[G] = nruns.
 __global__ void run_base_kernel(const int32_t* __restrict__ seg_off, int32_t G,
-                                const int32_t* __restrict__ run_id, int64_t n,
+                                const int32_t* __restrict__ run_id, int64_t n, int64_t nruns,
                                 int32_t* __restrict__ run_base) {
-    for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < G;
+    for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s <= G;
          s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int32_t b = seg_off[s];
-        run_base[s] = (b < n && seg_off[s + 1] > b) ? run_id[b] - 1 : 0;
+        run_base[s] = (s < G && b < n) ? run_id[b] - 1 : static_cast<int32_t>(nruns);
+    }
+}
+
+// Tiles of whole primary segments.  A tile starts at segment s when s is the
+// first segment, s or s-1 is long (> kLongSeg obs), or s starts in a later
+// window of kTileStride observations than s-1.  A regular tile then holds at
+// most kTileStride + kLongSeg = kTileObs observations; a long segment is a
+// tile of its own.
+__global__ void tile_flag_kernel(const int32_t* __restrict__ seg_off, int32_t G,
+                                 int32_t* __restrict__ tflag, int32_t* __restrict__ lflag) {
+    for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s <= G;
+         s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (s == G) {
+            tflag[s] = 0;
+            lflag[s] = 0;
+            continue;
+        }
+        const int32_t b = seg_off[s];
+        const bool lng = seg_off[s + 1] - b > kLongSeg;
+        bool start = (s == 0) || lng;
+        if (!start) {
+            const int32_t pb = seg_off[s - 1];
+            start = (b - pb > kLongSeg) || (b / kTileStride != pb / kTileStride);
+        }
+        tflag[s] = start ? 1 : 0;
+        lflag[s] = lng ? 1 : 0;
+    }
+}
+
+__global__ void tile_fill_kernel(const int32_t* __restrict__ seg_off, int32_t G,
+                                 const int32_t* __restrict__ tflag, const int32_t* __restrict__ tidx,
+                                 const int32_t* __restrict__ lflag, const int32_t* __restrict__ lidx,
+                                 int32_t* __restrict__ tile_seg, uint8_t* __restrict__ tile_long,
+                                 int32_t* __restrict__ long_segs) {
+    for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s <= G;
+         s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (s == G) {
+            tile_seg[tidx[G]] = G;  // sentinel
+            continue;
+        }
+        if (tflag[s]) {
+            tile_seg[tidx[s]] = static_cast<int32_t>(s);
+            tile_long[tidx[s]] = lflag[s] ? 1 : 0;
+        }
+        if (lflag[s]) long_segs[lidx[s]] = static_cast<int32_t>(s);
     }
 }
 
@@ -152,7 +199,7 @@ __global__ void run_weights_kernel(const int32_t* __restrict__ sorted_runs, int6
                                    const int32_t* __restrict__ run_seg,
                                    const double* __restrict__ wp, const double* __restrict__ inv_wp,
                                    int32_t* __restrict__ run_dest, double* __restrict__ cw_sorted,
-                                   double* __restrict__ ce_sorted) {
+                                   double* __restrict__ ce_sorted, double* __restrict__ cw_run) {
     for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nruns;
          j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int32_t m = sorted_runs[j];
@@ -167,6 +214,30 @@ __global__ void run_weights_kernel(const int32_t* __restrict__ sorted_runs, int6
         }
         cw_sorted[j] = c;
         ce_sorted[j] = c * c * inv_wp[run_seg[m]];
+        cw_run[m] = c;
+    }
+}
+
+// Packed metadata of the run-level pass: seg_meta[s] = {first obs, first
+// run} (s <= G, with the sentinels), run_meta[m] = {group, dest row, first
+// obs, end obs}, run weights in run order as float and double.
+__global__ void pack_meta_kernel(const int32_t* __restrict__ seg_off,
+                                 const int32_t* __restrict__ run_base, int32_t G,
+                                 const int32_t* __restrict__ run_grp,
+                                 const int32_t* __restrict__ run_dest,
+                                 const int32_t* __restrict__ run_start, int64_t nruns,
+                                 const double* __restrict__ cw_run, int2* __restrict__ seg_meta,
+                                 int4* __restrict__ run_meta, double* __restrict__ rw64,
+                                 float* __restrict__ rw32) {
+    const int64_t total = max(static_cast<int64_t>(G) + 1, nruns);
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (i <= G) seg_meta[i] = make_int2(seg_off[i], run_base ? run_base[i] : 0);
+        if (i < nruns) {
+            run_meta[i] = make_int4(run_grp[i], run_dest[i], run_start[i], run_start[i + 1]);
+            rw64[i] = cw_run[i];
+            rw32[i] = static_cast<float>(cw_run[i]);
+        }
     }
 }
 
