@@ -167,3 +167,18 @@ def test_zipf_primary_mixed_long_and_tiles(absorber, pkg, oracle_mod, panels):
     G = [int(f.max()) + 1 for f in fes]
     w = np.random.default_rng(3).lognormal(0.0, 0.5, size=int(keep.sum()))
     _check(absorber, pkg, oracle_mod, p.y[keep], p.X[keep], fes, G, w=w)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_block_and_tile_matvec_agree(absorber, pkg, oracle_mod, panels, weighted):
+    # the block-level CG matvec and the general tile matvec solve the same system
+    p = _akm(panels, 30_000, True, seed=37)
+    w = np.random.default_rng(5).lognormal(0.0, 0.5, size=p.n) if weighted else None
+    outs = []
+    for pk in (0, 1):
+        o = pkg.make_options(tol=1e-10, precision="fp64", pass_kernel=pk)
+        r = absorber.absorb(p.y, p.X, p.fes, p.levels, w, o)
+        assert r.converged
+        outs.append(np.column_stack([r.y_tilde, r.X_tilde]))
+    scale = np.linalg.norm(np.column_stack([p.y, p.X]), axis=0)
+    assert (np.linalg.norm(outs[0] - outs[1], axis=0) / scale).max() <= 1e-9

@@ -40,6 +40,8 @@ struct LargeDim {
     int64_t nchunks = 0;
     int64_t nmulti = 0;
     int32_t *rid = nullptr, *run_base = nullptr, *run_dest = nullptr, *run_start = nullptr;
+    int32_t* run_grp = nullptr;
+    double* cw_run = nullptr;
     int32_t *chunk_grp = nullptr, *chunk_beg = nullptr, *chunk_end = nullptr;
     uint8_t* chunk_whole = nullptr;
     int32_t *multi_grp = nullptr, *multi_c0 = nullptr, *multi_c1 = nullptr;
@@ -77,11 +79,17 @@ struct Structure {
     int64_t ntiles = 0;
     int32_t* long_segs = nullptr;
     int64_t nlong = 0;
-    // run-level pass metadata (at most one large dim)
+    // block-level pass metadata (at most one large and one small dim)
+    bool block_ok = false;
     int2* seg_meta = nullptr;
     int4* run_meta = nullptr;
     double* run_w64 = nullptr;
     float* run_w32 = nullptr;
+    int2* block_meta = nullptr;
+    double* block_w64 = nullptr;
+    float* block_w32 = nullptr;
+    int64_t nblocks = 0;
+    double* small_w = nullptr;  // [SG] level weights of the small dim
 };
 
 constexpr int32_t kChunkRuns = 64;
@@ -461,7 +469,8 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         B_CHECK(sync_read_int(ctx, run_id + (n - 1), 1, &nr));
         L.nruns = nr;
         int32_t *run_grp, *run_start, *run_seg;
-        B_CHECK(get_buf(ctx, "run_grp", nr, &run_grp));
+        B_CHECK(get_buf(ctx, "run_grp" + sfx, nr, &run_grp));
+        L.run_grp = run_grp;
         B_CHECK(get_buf(ctx, "run_start" + sfx, static_cast<size_t>(nr) + 1, &run_start));
         B_CHECK(get_buf(ctx, "run_seg", nr, &run_seg));
         L.run_start = run_start;
@@ -498,21 +507,12 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         double *cw, *ce, *cw_run;
         B_CHECK(get_buf(ctx, "run_cw", nr, &cw));
         B_CHECK(get_buf(ctx, "run_ce", nr, &ce));
-        B_CHECK(get_buf(ctx, "run_cw_run", nr, &cw_run));
+        B_CHECK(get_buf(ctx, "run_cw_run" + sfx, nr, &cw_run));
+        L.cw_run = cw_run;
         run_weights_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(
             sorted_runs, nr, run_start, n, run_seg, st.wp64, st.inv_wp, L.run_dest, cw, ce,
             cw_run);
         B_LAUNCHED();
-        if (st.nL == 1) {
-            B_CHECK(get_buf(ctx, "seg_meta", static_cast<size_t>(G[p]) + 1, &st.seg_meta));
-            B_CHECK(get_buf(ctx, "run_meta", nr, &st.run_meta));
-            B_CHECK(get_buf(ctx, "run_w64", nr, &st.run_w64));
-            B_CHECK(get_buf(ctx, "run_w32", nr, &st.run_w32));
-            pack_meta_kernel<<<grid_for(ctx, std::max<int64_t>(nr, G[p] + 1), T256), T256, 0, s>>>(
-                seg_off, L.run_base, G[p], run_grp, L.run_dest, run_start, nr, cw_run,
-                st.seg_meta, st.run_meta, st.run_w64, st.run_w32);
-            B_LAUNCHED();
-        }
         B_CHECK(cub_segmented_sum(ctx, cw, Wall + st.lbase[l], L.G, grp_off));
         B_CHECK(cub_segmented_sum(ctx, ce, Eall + st.lbase[l], L.G, grp_off));
         // chunk list
@@ -547,14 +547,6 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         B_LAUNCHED();
     }
 
-    if (st.nL == 0 && st.GR > 0) {
-        B_CHECK(get_buf(ctx, "seg_meta", static_cast<size_t>(G[p]) + 1, &st.seg_meta));
-        pack_meta_kernel<<<grid_for(ctx, static_cast<int64_t>(G[p]) + 1, T256), T256, 0, s>>>(
-            seg_off, nullptr, G[p], nullptr, nullptr, nullptr, 0, nullptr, st.seg_meta, nullptr,
-            nullptr, nullptr);
-        B_LAUNCHED();
-    }
-
     // small dims: packed ids and diagonal
     if (st.nS > 0) {
         SmallPackArgs pa{};
@@ -581,6 +573,48 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
                                   sizeof(double) * st.sG[j], cudaMemcpyDeviceToDevice, s));
         }
     }
+    if (st.nS > 0) st.small_w = Wall + st.sbase[0];
+
+    // blocks and packed metadata of the block-level pass
+    st.block_ok = st.GR > 0 && st.nL <= 1 && st.nS <= 1;
+    if (st.block_ok) {
+        int32_t *bflags, *bid, *bstart;
+        B_CHECK(get_buf(ctx, "tmp_n_a", n, &bflags));
+        B_CHECK(get_buf(ctx, "tmp_n_b", n, &bid));
+        block_flags_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(
+            gp, st.nL == 1 ? st.L[0].rid : nullptr, st.nS == 1 ? st.sid : nullptr, st.wp64, n, bflags);
+        B_LAUNCHED();
+        B_CHECK(cub_inclusive_sum(ctx, bflags, bid, n));
+        int nb = 0;
+        B_CHECK(sync_read_int(ctx, bid + (n - 1), 1, &nb));
+        st.nblocks = nb;
+        B_CHECK(get_buf(ctx, "block_start", nb, &bstart));
+        block_start_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(bflags, bid, n, bstart);
+        B_LAUNCHED();
+        B_CHECK(get_buf(ctx, "block_meta", nb, &st.block_meta));
+        if (w) {
+            B_CHECK(get_buf(ctx, "block_w64", nb, &st.block_w64));
+            B_CHECK(get_buf(ctx, "block_w32", nb, &st.block_w32));
+        }
+        block_meta_kernel<<<grid_for(ctx, nb, T256), T256, 0, s>>>(
+            bstart, nb, n, st.nS == 1 ? st.sid : nullptr, st.wp64, st.block_meta, st.block_w64,
+            st.block_w32);
+        B_LAUNCHED();
+        const int64_t npr = st.nL == 1 ? st.L[0].nruns : static_cast<int64_t>(G[p]);
+        B_CHECK(get_buf(ctx, "seg_meta", static_cast<size_t>(G[p]) + 1, &st.seg_meta));
+        B_CHECK(get_buf(ctx, "run_meta", npr, &st.run_meta));
+        B_CHECK(get_buf(ctx, "run_w64", npr, &st.run_w64));
+        B_CHECK(get_buf(ctx, "run_w32", npr, &st.run_w32));
+        const bool lg = st.nL == 1;
+        pack_meta_kernel<<<grid_for(ctx, std::max<int64_t>(npr, static_cast<int64_t>(G[p]) + 1), T256),
+                           T256, 0, s>>>(
+            seg_off, lg ? st.L[0].run_base : nullptr, G[p], lg ? st.L[0].run_grp : nullptr,
+            lg ? st.L[0].run_dest : nullptr, lg ? st.L[0].run_start : nullptr,
+            lg ? st.L[0].nruns : 0, lg ? st.L[0].cw_run : nullptr, bid, nb, n, st.seg_meta,
+            st.run_meta, st.run_w64, st.run_w32);
+        B_LAUNCHED();
+    }
+
     if (st.GR > 0) {
         B_CHECK(get_buf(ctx, "dinv64", st.GR, &st.dinv64));
         B_CHECK(get_buf(ctx, "dinv32", st.GR, &st.dinv32));
@@ -627,7 +661,7 @@ struct Work {
     double* dot_out;
     unsigned int* ticket;
     int tile_grid, tile_smem;
-    int run_grid, run_smem;  // run-level matvec (nL <= 1), 0 otherwise
+    int run_grid, run_smem;  // block-level matvec grid/smem (0 when it does not apply)
     int long_grid, long_smem;
     int nbins_ctas;
     int gather_grid[kMaxLarge];
@@ -662,12 +696,12 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
         1, std::min<int64_t>(st.ntiles, static_cast<int64_t>(ctx->num_sms) * per_sm)));
     wk.run_grid = 0;
     wk.run_smem = 0;
-    if (st.nL <= 1 && st.GR > 0 && ctx->pass_kernel == 0) {
-        wk.run_smem = static_cast<int>(run_smem_bytes<T>(CP, st.SG));
-        B_TRY(cudaFuncSetAttribute(run_pass_kernel<T, CQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (st.block_ok && ctx->pass_kernel == 0) {
+        wk.run_smem = static_cast<int>(block_smem_bytes<T>(CP, st.SG));
+        B_TRY(cudaFuncSetAttribute(block_pass_kernel<T, CQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    wk.run_smem));
         int rps = 1;
-        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rps, run_pass_kernel<T, CQ>, kRunThreads,
+        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rps, block_pass_kernel<T, CQ>, kBlockThreads,
                                                             wk.run_smem));
         rps = std::max(1, rps);
         const int64_t warps = (static_cast<int64_t>(st.G[st.p]) + (32 / CQ) - 1) / (32 / CQ);
@@ -696,8 +730,7 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     for (int l = 0; l < st.nL; ++l) wk.fin_rows += st.L[l].nmulti;
     wk.fin_grid = static_cast<int>(std::max<int64_t>(
         1, std::min<int64_t>(wk.fin_rows, static_cast<int64_t>(ctx->num_sms) * 8)));
-    B_CHECK(get_buf(ctx, tag + "fpart", static_cast<size_t>(std::max<int64_t>(wk.fin_rows, 1)) * CP,
-                    &wk.fin_partial));
+    B_CHECK(get_buf(ctx, tag + "fpart", static_cast<size_t>(wk.fin_grid) * CP, &wk.fin_partial));
     B_CHECK(get_buf(ctx, tag + "dotout", CP, &wk.dot_out));
     B_CHECK(get_buf(ctx, tag + "ticket", 1, &wk.ticket));
     B_TRY(cudaMemsetAsync(wk.ticket, 0, sizeof(unsigned int), ctx->stream));
@@ -772,31 +805,31 @@ int launch_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a) {
 // the tile kernel; then the long segments.  Bin partials of CTAs beyond the
 // launched grid are zeroed so finalize can sum a fixed number of slots.
 template <typename T, int CQ>
-int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, const T* run_w) {
+int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, const T* run_w,
+                       const T* block_w) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
     const int slots = std::max(wk.tile_grid, wk.run_grid);
     if (wk.run_grid > 0) {
-        RunArgs<T> r{};
+        BlockArgs<T> r{};
         r.Gp = st.G[st.p];
         r.CP = CP;
-        r.nS = st.nS;
         r.has_large = st.nL == 1;
+        r.has_small = st.nS == 1;
+        r.SG = st.SG;
         r.seg_meta = st.seg_meta;
         r.inv_wp = st.inv_wp;
-        r.wp = a.wp;
-        r.sid = st.sid;
-        r.sbase0 = st.nS > 0 ? st.sbase[0] : 0;
-        for (int j = 0; j < st.nS; ++j) r.sgoff[j] = st.sgoff[j];
-        r.SG = st.SG;
-        r.lbase = st.nL == 1 ? st.lbase[0] : 0;
         r.run_meta = st.run_meta;
         r.run_w = run_w;
+        r.block_meta = st.block_meta;
+        r.block_w = block_w;
+        r.lbase = st.nL == 1 ? st.lbase[0] : 0;
+        r.sbase = st.nS == 1 ? st.sbase[0] : 0;
         r.x = a.x;
         r.R = st.nL == 1 ? wk.R[0] : nullptr;
         r.bins_partial = wk.bins_partial;
         r.bins_cta0 = 0;
-        run_pass_kernel<T, CQ><<<wk.run_grid, kRunThreads, wk.run_smem, ctx->stream>>>(r);
+        block_pass_kernel<T, CQ><<<wk.run_grid, kBlockThreads, wk.run_smem, ctx->stream>>>(r);
         B_LAUNCHED();
         if (st.nS > 0 && wk.run_grid < slots)
             B_TRY(cudaMemsetAsync(wk.bins_partial + static_cast<int64_t>(wk.run_grid) * st.SG * CP, 0,
@@ -811,6 +844,7 @@ int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, co
     }
     if (wk.long_grid > 0) {
         a.bins_cta0 = slots;
+        a.bins_no_diag = wk.run_grid > 0 ? 1 : 0;
         segment_pass_kernel<T, CQ, kMatvec><<<wk.long_grid, kPassThreads, wk.long_smem, ctx->stream>>>(a);
         B_LAUNCHED();
     }
@@ -839,7 +873,8 @@ double gather_bytes(const Structure& st, int l, int CP, size_t tsize, bool dot) 
 // Gathers runs and bins into alpha rows `out`; dot with `dotv` into wk.dot_out.
 template <typename T, int CQ>
 int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
-                int cat_gather = B200FE_PROF_GATHER, int cat_fin = B200FE_PROF_FINALIZE) {
+                int cat_gather = B200FE_PROF_GATHER, int cat_fin = B200FE_PROF_FINALIZE,
+                bool small_diag = false) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
     const cudaStream_t s = ctx->stream;
@@ -878,6 +913,8 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
     f.sgbase = st.nS > 0 ? st.sbase[0] : 0;
     f.bins_partial = wk.bins_partial;
     f.nbins_ctas = wk.nbins_ctas;
+    f.small_diag = (small_diag && st.nS > 0) ? st.small_w : nullptr;
+    f.x = dotv;
     f.nrows = wk.fin_rows;
     f.out = out;
     f.dotv = dotv;
@@ -895,20 +932,30 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
 
 // q = S x ; pq = x'q (per column) into wk.dot_out
 template <typename T, int CQ>
-int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, const T* x,
-           T* q) {
+int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w,
+           const T* block_w, const T* x, T* q) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
     PassArgs<T> a = make_pass_args<T>(st, 0, CP, wk);
     a.wp = wp;
     a.x = x;
     {
-        ProfScope ps(ctx, B200FE_PROF_PASS,
-                     struct_obs_bytes(st, sizeof(T)) + runs_write_bytes(st, CP, sizeof(T)) +
-                         static_cast<double>(st.GR) * CP * sizeof(T));
-        B_CHECK((launch_matvec_pass<T, CQ>(ctx, wk, a, run_w)));
+        double pb;
+        if (wk.run_grid > 0) {  // block-level pass: per segment, run and block
+            pb = static_cast<double>(st.G[st.p]) * 16.0 + static_cast<double>(st.GR) * CP * sizeof(T) +
+                 static_cast<double>(st.nblocks) * (8.0 + (st.weighted ? sizeof(T) : 0.0));
+            const int64_t npr = st.nL == 1 ? st.L[0].nruns : st.G[st.p];
+            pb += static_cast<double>(npr) * (16.0 + sizeof(T));
+            if (st.nL == 1) pb += static_cast<double>(st.L[0].nruns) * CP * double(sizeof(T));
+        } else {
+            pb = struct_obs_bytes(st, sizeof(T)) + runs_write_bytes(st, CP, sizeof(T)) +
+                 static_cast<double>(st.GR) * CP * sizeof(T);
+        }
+        ProfScope ps(ctx, B200FE_PROF_PASS, pb);
+        B_CHECK((launch_matvec_pass<T, CQ>(ctx, wk, a, run_w, block_w)));
     }
-    return reduce_runs<T, CQ>(ctx, wk, q, x);
+    return reduce_runs<T, CQ>(ctx, wk, q, x, B200FE_PROF_GATHER, B200FE_PROF_FINALIZE,
+                              wk.run_grid > 0);
 }
 
 struct ColState {
@@ -927,8 +974,8 @@ struct ColState {
 // Inner PCG on S x = rhs (rows already in r), T precision.
 // thr_host[c]: stop column c when r'r <= thr (0 or negative: column inactive).
 template <typename T, int CQ>
-int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, const T* dinv, T* x,
-        T* r, T* z,
+int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, const T* block_w,
+        const T* dinv, T* x, T* r, T* z,
         T* p, T* q, const std::vector<double>& thr_host, int max_iter, int check_interval,
         int* iters_out) {
     const Structure& st = ctx->st;
@@ -980,7 +1027,7 @@ int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, con
     while (na > 0 && it < max_iter) {
         const int block = std::min(check_interval, max_iter - it);
         for (int j = 0; j < block; ++j) {
-            B_CHECK((matvec<T, CQ>(ctx, wk, wp, run_w, p, q)));
+            B_CHECK((matvec<T, CQ>(ctx, wk, wp, run_w, block_w, p, q)));
             // pq is in wk.dot_out: copy into the scalar slot
             B_TRY(cudaMemcpyAsync(cs.pq, wk.dot_out, sizeof(double) * CP, cudaMemcpyDeviceToDevice, s));
             {
@@ -1120,7 +1167,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             if (mixed) {
                 scale_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, r32);
                 B_LAUNCHED();
-                B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.run_w32, st.dinv32, x32, r32, z32, p32, q32, thr,
+                B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.run_w32, st.block_w32, st.dinv32, x32, r32, z32, p32, q32, thr,
                                         o.max_iter - total_iters, std::max(1, o.check_interval),
                                         &its)));
                 axpy_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x32, scale_d, a64);
@@ -1128,7 +1175,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             } else {
                 scale_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, rin64);
                 B_LAUNCHED();
-                B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
+                B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
                                          o.max_iter - total_iters, std::max(1, o.check_interval),
                                          &its)));
                 axpy_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x64, scale_d, a64);
@@ -1136,7 +1183,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             }
             total_iters += its;
             // true residual in FP64: r = b - S a
-            B_CHECK((matvec<double, CQ>(ctx, w64, st.wp64, st.run_w64, a64, q64)));
+            B_CHECK((matvec<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, a64, q64)));
             sub_kernel<<<rgrid, kRowThreads, 0, s>>>(GR * CP, b64, q64, r64);
             B_LAUNCHED();
             row_dot_kernel<double, double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, r64, dot_part,

@@ -158,6 +158,7 @@ struct PassArgs {
     double* colsq_partial;     // [ctas][CP]: kRhs sum v^2; kFinal sum_s (sum_k z_k)^2
     int bins_cta0;             // first CTA slot of this launch in the partial arrays
     int scatter;               // kFinal: 1 to scatter z for the certificate
+    int bins_no_diag;          // kMatvec: bins get z_k - w_k x_s[h_k] (finalize adds W_h x_s[h])
     // tiles
     const int32_t* tile_seg;   // [ntiles+1] first segment of each tile
     const uint8_t* tile_long;  // [ntiles] 1 for a single long segment
@@ -447,37 +448,40 @@ tile_pass_kernel(const PassArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// Run-level matvec (at most one large non-primary dim).
+// Block-level matvec (at most one large and one small non-primary dim).
 //
-// Within a run (obs of one primary segment with the same large-dim group f)
-// the large-dim part of u_k = x_f[f] + sum_small x_s[h_s(k)] is constant, so
-//     U_m   = c_m x_f[f_m] + sum_{k in m} w_k ys_k      (ys_k: small-dim part)
-//     t_s   = sum_{m in s} U_m / W_s
-//     R_m   = U_m - c_m t_s                              (run row of S x)
-//     z_k   = w_k (x_f[f_m] + ys_k - t_s)                (small-dim bins)
-// One x_f gather per run, small-dim rows of x from shared memory.  A group of
-// CQ lanes owns one segment; bins are per warp, updated in warp-synchronous
-// steps in which only groups that hit the same bin row are serialized (in
-// group order), so the sums are deterministic.
+// A run is a maximal block of obs of one primary segment s with the same
+// large-dim group f; a run is cut into blocks of obs whose small-dim levels
+// are consecutive (h0, h0+1, ..., h0+len-1) and whose weights are equal (w_b).
+// With P the prefix sums of the small-dim rows of x (P[h] = sum_{h'<h} x_y[h']):
+//     U_m  = c_m x_f[f_m] + sum_{b in m} w_b (P[h0_b + len_b] - P[h0_b])
+//     t_s  = sum_{m in s} U_m / W_s
+//     R_m  = U_m - c_m t_s                               (run row of S x)
+// and each block adds w_b (x_f[f_m] - t_s) to the small-dim bins of levels
+// h0_b .. h0_b + len_b - 1 (a difference-array update at two points); the
+// diagonal part W_h x_y[h] of the small rows is added by finalize.  Work is
+// per run and per block, not per observation.  A matched panel observed in
+// consecutive years has about one block per run.
 // ---------------------------------------------------------------------------
-constexpr int kRunThreads = 128;
+constexpr int kBlockThreads = 128;
+
+__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 
 template <typename T>
-struct RunArgs {
+struct BlockArgs {
     int32_t Gp;
     int CP;
-    int nS;
-    int has_large;
+    int has_large;          // one large dim: runs carry x_f and write R rows
+    int has_small;          // one small dim
+    int SG;                 // its levels
     const int2* seg_meta;   // [Gp+1] {first obs, first run}
     const double* inv_wp;   // [Gp]
-    const T* wp;            // [n] or null
-    const uint32_t* sid;    // [n] or null
-    int64_t sbase0;         // alpha row of the first small-dim level
-    int sgoff[kMaxSmall];
-    int SG;
-    int64_t lbase;          // alpha row of the large dim
-    const int4* run_meta;   // [nruns] {group, dest row, first obs, end obs}
+    const int4* run_meta;   // [nruns] {group, dest row, first block, end block}
     const T* run_w;         // [nruns] run weights c_m
+    const int2* block_meta; // [nblocks] {first small level, length}
+    const T* block_w;       // [nblocks] or null (unit weights)
+    int64_t lbase;          // alpha row of the large dim
+    int64_t sbase;          // alpha row of small level 0
     const T* x;             // alpha [GR][CP]
     T* R;                   // [nruns][CP]
     double* bins_partial;   // [ctas][SG][CP]
@@ -485,167 +489,193 @@ struct RunArgs {
 };
 
 template <typename T>
-__host__ __device__ constexpr size_t run_smem_bytes(int CP, int SG) {
-    return static_cast<size_t>(SG) * CP * sizeof(T) +
-           static_cast<size_t>(kRunThreads / 32) * SG * CP * sizeof(double) + 16;
-}
-
-template <typename T>
-__device__ __forceinline__ void small_part(const RunArgs<T>& a, const T* xs, uint32_t packed,
-                                           int q, Acc4& ys) {
-    acc_zero(ys);
-    for (int s = 0; s < a.nS; ++s) {
-        const int h = static_cast<int>((packed >> (8 * s)) & 0xffu);
-        Acc4 v;
-        smem_load4<T>(xs + (a.sgoff[s] + h) * a.CP + 4 * q, v);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) ys.v[j] += v.v[j];
-    }
+__host__ __device__ size_t block_smem_bytes(int CP, int SG) {
+    return align16(static_cast<size_t>(SG + 1) * CP * sizeof(T)) +
+           static_cast<size_t>(kBlockThreads / 32) * (SG + 1) * CP * sizeof(double);
 }
 
 template <typename T, int CQ>
-__global__ void __launch_bounds__(kRunThreads)
-run_pass_kernel(const RunArgs<T> a) {
+__global__ void __launch_bounds__(kBlockThreads)
+block_pass_kernel(const BlockArgs<T> a) {
     constexpr int CP = 4 * CQ;
     constexpr int GPW = 32 / CQ;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* xs = reinterpret_cast<T*>(smem_raw);
-    double* bins = reinterpret_cast<double*>(
-        smem_raw + ((static_cast<size_t>(a.SG) * CP * sizeof(T) + 15) & ~size_t(15)));
+    const int SG1 = a.SG + 1;
+    T* P = reinterpret_cast<T*>(smem_raw);
+    double* D = reinterpret_cast<double*>(smem_raw + align16(static_cast<size_t>(SG1) * CP * sizeof(T)));
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const int gw = lane / CQ;
     const int q = lane % CQ;
-    for (int i = tid; i < a.SG * CP; i += kRunThreads) xs[i] = a.x[a.sbase0 * CP + i];
-    for (int i = tid; i < (kRunThreads / 32) * a.SG * CP; i += kRunThreads) bins[i] = 0.0;
+    if (a.has_small) {
+        // prefix sums of the small-dim rows of x, one column per thread
+        for (int c = tid; c < CP; c += kBlockThreads) {
+            double acc = 0.0;
+            P[c] = static_cast<T>(0);
+            for (int h = 0; h < a.SG; ++h) {
+                acc += static_cast<double>(a.x[(a.sbase + h) * CP + c]);
+                P[(h + 1) * CP + c] = static_cast<T>(acc);
+            }
+        }
+        for (int i = tid; i < (kBlockThreads / 32) * SG1 * CP; i += kBlockThreads) D[i] = 0.0;
+    }
     __syncthreads();
-    double* wbins = bins + warp * a.SG * CP;
-    const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (kRunThreads / 32);
-    const int64_t wid = static_cast<int64_t>(blockIdx.x) * (kRunThreads / 32) + warp;
+    double* wD = D + warp * SG1 * CP;
+    const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (kBlockThreads / 32);
+    const int64_t wid = static_cast<int64_t>(blockIdx.x) * (kBlockThreads / 32) + warp;
 
     for (int64_t s0 = wid * GPW; s0 < a.Gp; s0 += nwarps * GPW) {
         const int64_t s = s0 + gw;
-        int k0 = 0, k1 = 0, rb = 0, re = 0;
+        int rb = 0, re = 0;
         double iw = 0.0;
         if (s < a.Gp) {
             const int2 m0 = a.seg_meta[s], m1 = a.seg_meta[s + 1];
-            k0 = m0.x;
-            k1 = m1.x;
-            rb = m0.y;
-            re = m1.y;
+            if (m1.x - m0.x <= kLongSeg) {  // long segments take the long path
+                rb = m0.y;
+                re = m1.y;
+            }
             iw = a.inv_wp[s];
-            if (k1 - k0 > kLongSeg) k1 = k0;  // long segments take the long path
         }
-        const int len = k1 - k0;
-        // pass 1: t = (sum_m c_m x_f[f_m] + sum_k w_k ys_k) / W_s
+        // pass 1 (per group): t = sum_m U_m / W_s
         Acc4 tsum;
         acc_zero(tsum);
-        if (a.has_large && len > 0) {
-            for (int m = rb; m < re; ++m) {
-                const int4 rm = a.run_meta[m];
+        int bfirst = 0, bend = 0;
+        for (int m = rb; m < re; ++m) {
+            const int4 rm = a.run_meta[m];
+            if (m == rb) bfirst = rm.z;
+            bend = rm.w;
+            if (a.has_large) {
                 const double cm = static_cast<double>(a.run_w[m]);
                 Acc4 xf;
                 load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
 #pragma unroll
-                for (int j = 0; j < 4; ++j) tsum.v[j] = fma(cm, xf.v[j], tsum.v[j]);
+                for (int i = 0; i < 4; ++i) tsum.v[i] = fma(cm, xf.v[i], tsum.v[i]);
             }
-        }
-        if (a.nS > 0) {
-            for (int k = k0; k < k1; ++k) {
-                Acc4 ys;
-                small_part(a, xs, __ldg(a.sid + k), q, ys);
-                const double w = a.wp ? static_cast<double>(a.wp[k]) : 1.0;
+            if (a.has_small) {
+                for (int b = rm.z; b < rm.w; ++b) {
+                    const int2 bm = a.block_meta[b];
+                    const double wb = a.block_w ? static_cast<double>(a.block_w[b]) : 1.0;
+                    Acc4 p0, p1;
+                    smem_load4<T>(P + bm.x * CP + 4 * q, p0);
+                    smem_load4<T>(P + (bm.x + bm.y) * CP + 4 * q, p1);
 #pragma unroll
-                for (int j = 0; j < 4; ++j) tsum.v[j] = fma(w, ys.v[j], tsum.v[j]);
+                    for (int i = 0; i < 4; ++i) tsum.v[i] = fma(wb, p1.v[i] - p0.v[i], tsum.v[i]);
+                }
             }
         }
         Acc4 t;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) t.v[j] = tsum.v[j] * iw;
+        for (int i = 0; i < 4; ++i) t.v[i] = tsum.v[i] * iw;
 
-        // pass 2: run rows and small-dim bins, warp-synchronous over obs
-        int steps = len;
+        // pass 2: warp-synchronous over this segment's blocks
+        const int nb = bend - bfirst;
+        const int steps = a.has_small ? static_cast<int>(__reduce_max_sync(0xffffffffu, static_cast<unsigned>(nb)))
+                                      : 0;
+        if (!a.has_small) {
+            // no small dim: one R row per run, U_m = c_m x_f
+            for (int m = rb; m < re && a.has_large; ++m) {
+                const int4 rm = a.run_meta[m];
+                const double cm = static_cast<double>(a.run_w[m]);
+                Acc4 xf, r;
+                load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) steps = max(steps, __shfl_xor_sync(0xffffffffu, steps, off));
+                for (int i = 0; i < 4; ++i) r.v[i] = cm * (xf.v[i] - t.v[i]);
+                store_quad_stream(a.R + static_cast<int64_t>(rm.y) * CP + 4 * q, r);
+            }
+            continue;
+        }
         int m = rb;
-        int run_end = k1;
+        int run_bend = 0;
         double cm = 0.0;
-        Acc4 xf, Y;
+        int rdest = 0;
+        Acc4 xf, U;
         acc_zero(xf);
-        acc_zero(Y);
-        if (a.has_large && len > 0) {
+        acc_zero(U);
+        if (nb > 0) {
             const int4 rm = a.run_meta[m];
-            cm = static_cast<double>(a.run_w[m]);
-            load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
-            run_end = rm.w;
+            run_bend = rm.w;
+            rdest = rm.y;
+            if (a.has_large) {
+                cm = static_cast<double>(a.run_w[m]);
+                load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+            }
         }
         for (int step = 0; step < steps; ++step) {
-            const bool active = step < len;
-            const int k = k0 + step;
-            Acc4 z;
-            acc_zero(z);
-            uint32_t packed = 0;
+            const bool active = step < nb;
+            const int b = bfirst + step;
+            int h0 = 0, h1 = 0;
+            Acc4 delta;
+            acc_zero(delta);
             if (active) {
-                if (a.has_large && k == run_end) {
-                    const int4 rp = a.run_meta[m];
-                    Acc4 r;
+                if (b == run_bend) {  // the current run is complete
+                    if (a.has_large) {
+                        Acc4 r;
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) r.v[j] = fma(cm, xf.v[j] - t.v[j], Y.v[j]);
-                    store_quad_stream(a.R + static_cast<int64_t>(rp.y) * CP + 4 * q, r);
+                        for (int i = 0; i < 4; ++i) r.v[i] = fma(cm, xf.v[i] - t.v[i], U.v[i]);
+                        store_quad_stream(a.R + static_cast<int64_t>(rdest) * CP + 4 * q, r);
+                    }
                     ++m;
                     const int4 rm = a.run_meta[m];
-                    cm = static_cast<double>(a.run_w[m]);
-                    load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
-                    run_end = rm.w;
-                    acc_zero(Y);
+                    run_bend = rm.w;
+                    rdest = rm.y;
+                    if (a.has_large) {
+                        cm = static_cast<double>(a.run_w[m]);
+                        load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+                    }
+                    acc_zero(U);
                 }
-                const double w = a.wp ? static_cast<double>(a.wp[k]) : 1.0;
-                Acc4 ys;
-                acc_zero(ys);
-                if (a.nS > 0) {
-                    packed = __ldg(a.sid + k);
-                    small_part(a, xs, packed, q, ys);
-                }
+                const int2 bm = a.block_meta[b];
+                const double wb = a.block_w ? static_cast<double>(a.block_w[b]) : 1.0;
+                h0 = bm.x;
+                h1 = bm.x + bm.y;
+                Acc4 p0, p1;
+                smem_load4<T>(P + h0 * CP + 4 * q, p0);
+                smem_load4<T>(P + h1 * CP + 4 * q, p1);
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    Y.v[j] = fma(w, ys.v[j], Y.v[j]);
-                    z.v[j] = w * (xf.v[j] + ys.v[j] - t.v[j]);
+                for (int i = 0; i < 4; ++i) {
+                    U.v[i] = fma(wb, p1.v[i] - p0.v[i], U.v[i]);
+                    delta.v[i] = wb * (xf.v[i] - t.v[i]);
                 }
             }
-            for (int sd = 0; sd < a.nS; ++sd) {
-                const uint32_t key = active ? ((packed >> (8 * sd)) & 0xffu) : 0x100u + gw;
+            // difference-array updates D[h0] += delta, D[h1] -= delta
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const int hh = side == 0 ? h0 : h1;
+                const uint32_t key = active ? static_cast<uint32_t>(hh) : 0x10000u + gw;
                 const unsigned int match = __match_any_sync(0xffffffffu, key);
                 const int rank = __popc(match & ((1u << lane) - 1u)) / CQ;
-                int msize = __popc(match) / CQ;
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1)
-                    msize = max(msize, __shfl_xor_sync(0xffffffffu, msize, off));
-                double* brow = wbins + (a.sgoff[sd] + static_cast<int>(key & 0xffu)) * CP + 4 * q;
+                const int msize = static_cast<int>(
+                    __reduce_max_sync(0xffffffffu, static_cast<unsigned>(__popc(match) / CQ)));
+                double* drow = wD + hh * CP + 4 * q;
                 for (int r = 0; r < msize; ++r) {
                     if (active && rank == r) {
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) brow[j] += z.v[j];
+                        for (int i = 0; i < 4; ++i) drow[i] += side == 0 ? delta.v[i] : -delta.v[i];
                     }
                     __syncwarp();
                 }
             }
         }
-        if (a.has_large && len > 0) {
-            const int4 rp = a.run_meta[m];
+        if (nb > 0 && a.has_large) {
             Acc4 r;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) r.v[j] = fma(cm, xf.v[j] - t.v[j], Y.v[j]);
-            store_quad_stream(a.R + static_cast<int64_t>(rp.y) * CP + 4 * q, r);
+            for (int i = 0; i < 4; ++i) r.v[i] = fma(cm, xf.v[i] - t.v[i], U.v[i]);
+            store_quad_stream(a.R + static_cast<int64_t>(rdest) * CP + 4 * q, r);
         }
     }
     __syncthreads();
-    if (a.nS > 0) {
+    if (a.has_small) {
+        // bins = prefix sums of the difference arrays, warps summed in order
         double* dst = a.bins_partial + static_cast<int64_t>(a.bins_cta0 + blockIdx.x) * a.SG * CP;
-        for (int i = tid; i < a.SG * CP; i += kRunThreads) {
-            double sum = 0.0;
-            for (int w = 0; w < kRunThreads / 32; ++w) sum += bins[w * a.SG * CP + i];
-            dst[i] = sum;
+        for (int c = tid; c < CP; c += kBlockThreads) {
+            double run = 0.0;
+            for (int h = 0; h < a.SG; ++h) {
+                double d = 0.0;
+                for (int w = 0; w < kBlockThreads / 32; ++w) d += D[(w * SG1 + h) * CP + c];
+                run += d;
+                dst[h * CP + c] = run;
+            }
         }
     }
 }
@@ -791,8 +821,16 @@ segment_pass_kernel(const PassArgs<T> a) {
                         for (int s2 = 0; s2 < a.nS; ++s2) {
                             const uint32_t h = (packed >> (8 * s2)) & 0xffu;
                             double* b = my_bins + (a.sgoff[s2] + h) * a.CP + 4 * q;
+                            Acc4 zb = z;
+                            if (MODE == kMatvec && a.bins_no_diag) {
+                                Acc4 xh;
+                                load_quad(a.x + (a.sbase[s2] + h) * a.CP + 4 * q, xh);
+                                const double w = a.wp ? static_cast<double>(a.wp[k]) : 1.0;
 #pragma unroll
-                            for (int c = 0; c < 4; ++c) b[c] += z.v[c];
+                                for (int c = 0; c < 4; ++c) zb.v[c] -= w * xh.v[c];
+                            }
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) b[c] += zb.v[c];
                         }
                     }
                 }
@@ -945,10 +983,12 @@ struct FinalizeArgs {
     int64_t sgbase;              // alpha row of bin row 0 (small dims are contiguous)
     const double* bins_partial;  // [nbins_ctas][SG][CP]
     int nbins_ctas;
+    const double* small_diag;    // [SG] level weights W_h to add W_h x[h] (block pass), or null
+    const T* x;                  // the matvec input (for small_diag)
     int64_t nrows;               // sum nmulti + SG
     T* out;                      // alpha rows [GR][CP]
     const T* dotv;               // or null
-    double* dot_partial;         // this kernel's [nrows][CP]
+    double* dot_partial;         // this kernel's [gridDim][CP]
     const double* gather_dot_partial[kMaxLarge];
     int gather_ctas[kMaxLarge];
     double* dot_out;             // [CP] or null
@@ -961,6 +1001,7 @@ finalize_kernel(const FinalizeArgs<T> a) {
     __shared__ double red[kRowThreads];
     __shared__ bool last;
     const int CP = a.CP;
+    double dotc = 0.0;  // thread c < CP: this CTA's dot contribution of column c
     for (int64_t r = blockIdx.x; r < a.nrows; r += gridDim.x) {
         int64_t ri = r;
         int64_t orow = -1;
@@ -982,19 +1023,21 @@ finalize_kernel(const FinalizeArgs<T> a) {
             stride = static_cast<int64_t>(a.SG) * CP;
             orow = a.sgbase + ri;
         }
-        const double sum = block_column_sum(part, np, stride, CP, red);
+        double sum = block_column_sum(part, np, stride, CP, red);
         if (threadIdx.x < CP) {
+            if (a.small_diag && r >= a.nrows - a.SG)
+                sum = fma(a.small_diag[r - (a.nrows - a.SG)],
+                          static_cast<double>(a.x[orow * CP + threadIdx.x]), sum);
             const T stored = static_cast<T>(sum);
             a.out[orow * CP + threadIdx.x] = stored;
-            if (a.dot_out)
-                a.dot_partial[r * CP + threadIdx.x] =
-                    a.dotv ? static_cast<double>(a.dotv[orow * CP + threadIdx.x]) *
-                                 static_cast<double>(stored)
-                           : 0.0;
+            if (a.dotv)
+                dotc = fma(static_cast<double>(a.dotv[orow * CP + threadIdx.x]),
+                           static_cast<double>(stored), dotc);
         }
         __syncthreads();
     }
     if (!a.dot_out) return;
+    if (threadIdx.x < CP) a.dot_partial[static_cast<int64_t>(blockIdx.x) * CP + threadIdx.x] = dotc;
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last = (atomicAdd(a.ticket, 1u) == gridDim.x - 1);
@@ -1006,7 +1049,7 @@ finalize_kernel(const FinalizeArgs<T> a) {
         total += block_column_sum(a.gather_dot_partial[l], a.gather_ctas[l], CP, CP, red);
         __syncthreads();
     }
-    total += block_column_sum(a.dot_partial, a.nrows, CP, CP, red);
+    total += block_column_sum(a.dot_partial, gridDim.x, CP, CP, red);
     if (threadIdx.x < CP) a.dot_out[threadIdx.x] = total;
     if (threadIdx.x == 0) *a.ticket = 0u;
 }

@@ -218,25 +218,73 @@ __global__ void run_weights_kernel(const int32_t* __restrict__ sorted_runs, int6
     }
 }
 
-// Packed metadata of the run-level pass: seg_meta[s] = {first obs, first
-// run} (s <= G, with the sentinels), run_meta[m] = {group, dest row, first
-// obs, end obs}, run weights in run order as float and double.
+// Blocks of the block-level pass, in primary order: obs k starts a block when
+// it starts its primary segment or its large-dim run, when its small-dim
+// level is not the previous obs's level + 1, or when its weight differs.
+__global__ void block_flags_kernel(const int32_t* __restrict__ gp, const int32_t* __restrict__ rid,
+                                   const uint32_t* __restrict__ sid, const double* __restrict__ wp,
+                                   int64_t n, int32_t* __restrict__ flags) {
+    for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        bool st = (k == 0) || gp[k] != gp[k - 1];
+        if (!st && rid) st = rid[k] != rid[k - 1];
+        if (!st && sid) st = (sid[k] & 0xffu) != (sid[k - 1] & 0xffu) + 1u;
+        if (!st && wp) st = wp[k] != wp[k - 1];
+        flags[k] = st ? 1 : 0;
+    }
+}
+
+__global__ void block_start_kernel(const int32_t* __restrict__ flags, const int32_t* __restrict__ bid,
+                                   int64_t n, int32_t* __restrict__ block_start) {
+    for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        if (flags[k]) block_start[bid[k] - 1] = static_cast<int32_t>(k);
+}
+
+__global__ void block_meta_kernel(const int32_t* __restrict__ block_start, int64_t nblocks, int64_t n,
+                                  const uint32_t* __restrict__ sid, const double* __restrict__ wp,
+                                  int2* __restrict__ block_meta, double* __restrict__ bw64,
+                                  float* __restrict__ bw32) {
+    for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < nblocks;
+         b += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t k = block_start[b];
+        const int32_t e = (b + 1 < nblocks) ? block_start[b + 1] : static_cast<int32_t>(n);
+        block_meta[b] = make_int2(sid ? static_cast<int>(sid[k] & 0xffu) : 0, e - k);
+        if (wp) {
+            bw64[b] = wp[k];
+            bw32[b] = static_cast<float>(wp[k]);
+        }
+    }
+}
+
+// Packed metadata of the block-level pass.  With a large dim:
+// seg_meta[s] = {first obs, first run}, run_meta[m] = {group, dest row, first
+// block, end block}, run weights as float and double.  Without one, each
+// segment is a pseudo-run: seg_meta[s] = {first obs, s} and run_meta[s] =
+// {0, 0, first block, end block}.
 __global__ void pack_meta_kernel(const int32_t* __restrict__ seg_off,
                                  const int32_t* __restrict__ run_base, int32_t G,
                                  const int32_t* __restrict__ run_grp,
                                  const int32_t* __restrict__ run_dest,
                                  const int32_t* __restrict__ run_start, int64_t nruns,
-                                 const double* __restrict__ cw_run, int2* __restrict__ seg_meta,
+                                 const double* __restrict__ cw_run, const int32_t* __restrict__ bid,
+                                 int64_t nblocks, int64_t n, int2* __restrict__ seg_meta,
                                  int4* __restrict__ run_meta, double* __restrict__ rw64,
                                  float* __restrict__ rw32) {
-    const int64_t total = max(static_cast<int64_t>(G) + 1, nruns);
+    const int64_t npr = run_base ? nruns : static_cast<int64_t>(G);  // (pseudo-)runs
+    const int64_t total = max(static_cast<int64_t>(G) + 1, npr);
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        if (i <= G) seg_meta[i] = make_int2(seg_off[i], run_base ? run_base[i] : 0);
-        if (i < nruns) {
-            run_meta[i] = make_int4(run_grp[i], run_dest[i], run_start[i], run_start[i + 1]);
-            rw64[i] = cw_run[i];
-            rw32[i] = static_cast<float>(cw_run[i]);
+        if (i <= G) seg_meta[i] = make_int2(seg_off[i], run_base ? run_base[i] : static_cast<int>(i));
+        if (i < npr) {
+            const int64_t k0 = run_base ? run_start[i] : seg_off[i];
+            const int64_t k1 = run_base ? run_start[i + 1] : seg_off[i + 1];
+            const int32_t b0 = k0 < n ? bid[k0] - 1 : static_cast<int32_t>(nblocks);
+            const int32_t b1 = k1 < n ? bid[k1] - 1 : static_cast<int32_t>(nblocks);
+            run_meta[i] = make_int4(run_base ? run_grp[i] : 0, run_base ? run_dest[i] : 0, b0, b1);
+            const double c = run_base ? cw_run[i] : 0.0;
+            rw64[i] = c;
+            rw32[i] = static_cast<float>(c);
         }
     }
 }
