@@ -661,6 +661,7 @@ struct Work {
     double* dot_out;
     unsigned int* ticket;
     int tile_grid, tile_smem;
+    int data_grid, data_smem;  // FP64 data passes (double Work only)
     int run_grid, run_smem;  // block-level matvec grid/smem (0 when it does not apply)
     int long_grid, long_smem;
     int nbins_ctas;
@@ -694,6 +695,21 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     per_sm = std::max(1, per_sm);
     wk.tile_grid = static_cast<int>(std::max<int64_t>(
         1, std::min<int64_t>(st.ntiles, static_cast<int64_t>(ctx->num_sms) * per_sm)));
+    wk.data_grid = 0;
+    wk.data_smem = 0;
+    if (std::is_same<T, double>::value) {
+        wk.data_smem = static_cast<int>(data_smem_bytes(CP, st.SG));
+        B_TRY(cudaFuncSetAttribute(data_pass_kernel<CP, kRhs>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   wk.data_smem));
+        B_TRY(cudaFuncSetAttribute(data_pass_kernel<CP, kFinal>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, wk.data_smem));
+        int dps = 1;
+        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dps, data_pass_kernel<CP, kRhs>, kDataThreads,
+                                                            wk.data_smem));
+        dps = std::max(1, dps);
+        wk.data_grid = static_cast<int>(std::max<int64_t>(
+            1, std::min<int64_t>(st.ntiles, static_cast<int64_t>(ctx->num_sms) * dps)));
+    }
     wk.run_grid = 0;
     wk.run_smem = 0;
     if (st.block_ok && ctx->pass_kernel == 0) {
@@ -713,7 +729,7 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
         const int64_t groups = (st.nlong + (32 / CQ) - 1) / (32 / CQ);
         wk.long_grid = grid_for(ctx, groups * 32, kPassThreads, 4);
     }
-    wk.nbins_ctas = std::max(wk.tile_grid, wk.run_grid) + wk.long_grid;
+    wk.nbins_ctas = std::max(std::max(wk.tile_grid, wk.run_grid), wk.data_grid) + wk.long_grid;
     B_CHECK(get_buf(ctx, tag + "bins", static_cast<size_t>(wk.nbins_ctas) * std::max(st.SG, 1) * CP,
                     &wk.bins_partial));
     B_CHECK(get_buf(ctx, tag + "colsq", static_cast<size_t>(wk.nbins_ctas) * CP, &wk.colsq_partial));
@@ -773,28 +789,33 @@ PassArgs<T> make_pass_args(const Structure& st, int cols, int CP, const Work<T>&
     return a;
 }
 
-// Tile pass over the regular tiles, then the long segments (if any).
+// Data pass (FP64, lane = column) or tile pass over the regular tiles, then
+// the long segments (if any).  Partial slots beyond the launched grid are
+// zeroed so finalize and the host sum a fixed number of slots.
 template <typename T, int CQ, int MODE>
 int launch_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const int slots = std::max(std::max(wk.tile_grid, wk.run_grid), wk.data_grid);
+    int used;
     a.bins_cta0 = 0;
-    tile_pass_kernel<T, CQ, MODE><<<wk.tile_grid, kTileThreads, wk.tile_smem, ctx->stream>>>(a);
+    if constexpr (std::is_same<T, double>::value && MODE != kMatvec) {
+        data_pass_kernel<CP, MODE><<<wk.data_grid, kDataThreads, wk.data_smem, ctx->stream>>>(a);
+        used = wk.data_grid;
+    } else {
+        tile_pass_kernel<T, CQ, MODE><<<wk.tile_grid, kTileThreads, wk.tile_smem, ctx->stream>>>(a);
+        used = wk.tile_grid;
+    }
     B_LAUNCHED();
-    {
-        const Structure& st = ctx->st;
-        const int slots = std::max(wk.tile_grid, wk.run_grid);
-        const int CP = a.CP;
-        if (st.nS > 0 && wk.tile_grid < slots) {
-            B_TRY(cudaMemsetAsync(wk.bins_partial + static_cast<int64_t>(wk.tile_grid) * st.SG * CP, 0,
-                                  sizeof(double) * (slots - wk.tile_grid) * st.SG * CP, ctx->stream));
-            B_TRY(cudaMemsetAsync(wk.colsq_partial + static_cast<int64_t>(wk.tile_grid) * CP, 0,
-                                  sizeof(double) * (slots - wk.tile_grid) * CP, ctx->stream));
-        } else if (wk.tile_grid < slots) {
-            B_TRY(cudaMemsetAsync(wk.colsq_partial + static_cast<int64_t>(wk.tile_grid) * CP, 0,
-                                  sizeof(double) * (slots - wk.tile_grid) * CP, ctx->stream));
-        }
+    if (used < slots) {
+        if (st.nS > 0)
+            B_TRY(cudaMemsetAsync(wk.bins_partial + static_cast<int64_t>(used) * st.SG * CP, 0,
+                                  sizeof(double) * (slots - used) * st.SG * CP, ctx->stream));
+        B_TRY(cudaMemsetAsync(wk.colsq_partial + static_cast<int64_t>(used) * CP, 0,
+                              sizeof(double) * (slots - used) * CP, ctx->stream));
     }
     if (wk.long_grid > 0) {
-        a.bins_cta0 = std::max(wk.tile_grid, wk.run_grid);
+        a.bins_cta0 = slots;
         segment_pass_kernel<T, CQ, MODE><<<wk.long_grid, kPassThreads, wk.long_smem, ctx->stream>>>(a);
         B_LAUNCHED();
     }
@@ -809,7 +830,7 @@ int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, co
                        const T* block_w) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
-    const int slots = std::max(wk.tile_grid, wk.run_grid);
+    const int slots = std::max(std::max(wk.tile_grid, wk.run_grid), wk.data_grid);
     if (wk.run_grid > 0) {
         BlockArgs<T> r{};
         r.Gp = st.G[st.p];

@@ -494,6 +494,73 @@ __host__ __device__ size_t block_smem_bytes(int CP, int SG) {
            static_cast<size_t>(kBlockThreads / 32) * (SG + 1) * CP * sizeof(double);
 }
 
+// 4-wide vector in the solve's own precision (float math for the FP32 inner
+// solve, double for the FP64 refinement).
+template <typename T>
+struct V4 {
+    T v[4];
+};
+template <typename T>
+__device__ __forceinline__ void v4_zero(V4<T>& a) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) a.v[j] = static_cast<T>(0);
+}
+__device__ __forceinline__ void v4_load(const float* p, V4<float>& o) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    o.v[0] = t.x; o.v[1] = t.y; o.v[2] = t.z; o.v[3] = t.w;
+}
+__device__ __forceinline__ void v4_load(const double* p, V4<double>& o) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    o.v[0] = a.x; o.v[1] = a.y; o.v[2] = b.x; o.v[3] = b.y;
+}
+__device__ __forceinline__ void v4_lds(const float* p, V4<float>& o) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    o.v[0] = t.x; o.v[1] = t.y; o.v[2] = t.z; o.v[3] = t.w;
+}
+__device__ __forceinline__ void v4_lds(const double* p, V4<double>& o) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    o.v[0] = a.x; o.v[1] = a.y; o.v[2] = b.x; o.v[3] = b.y;
+}
+__device__ __forceinline__ void v4_store_stream(float* p, const V4<float>& a) {
+    __stcs(reinterpret_cast<float4*>(p), make_float4(a.v[0], a.v[1], a.v[2], a.v[3]));
+}
+__device__ __forceinline__ void v4_store_stream(double* p, const V4<double>& a) {
+    __stcs(reinterpret_cast<double2*>(p), make_double2(a.v[0], a.v[1]));
+    __stcs(reinterpret_cast<double2*>(p) + 1, make_double2(a.v[2], a.v[3]));
+}
+
+// Adds +delta (side 0) or -delta (side 1) to row `key` of the warp's
+// difference array.  Groups with distinct keys update in parallel; groups
+// sharing a key update one after another in group order (deterministic).
+template <typename T, int CQ>
+__device__ __forceinline__ void diff_update(double* wD, int CP, int key, bool active, int gw,
+                                            int lane, int q, const V4<T>& delta, bool negate) {
+    const uint32_t k = active ? static_cast<uint32_t>(key) : 0x10000u + gw;
+    const unsigned int match = __match_any_sync(0xffffffffu, k);
+    double* row = wD + key * CP + 4 * q;
+    if (__all_sync(0xffffffffu, __popc(match) == CQ)) {
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) row[i] += negate ? -static_cast<double>(delta.v[i])
+                                                         : static_cast<double>(delta.v[i]);
+        }
+        return;
+    }
+    const int rank = __popc(match & ((1u << lane) - 1u)) / CQ;
+    const int msize = static_cast<int>(
+        __reduce_max_sync(0xffffffffu, static_cast<unsigned>(__popc(match) / CQ)));
+    for (int r = 0; r < msize; ++r) {
+        if (active && rank == r) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) row[i] += negate ? -static_cast<double>(delta.v[i])
+                                                         : static_cast<double>(delta.v[i]);
+        }
+        __syncwarp();
+    }
+}
+
 template <typename T, int CQ>
 __global__ void __launch_bounds__(kBlockThreads)
 block_pass_kernel(const BlockArgs<T> a) {
@@ -528,140 +595,124 @@ block_pass_kernel(const BlockArgs<T> a) {
     for (int64_t s0 = wid * GPW; s0 < a.Gp; s0 += nwarps * GPW) {
         const int64_t s = s0 + gw;
         int rb = 0, re = 0;
-        double iw = 0.0;
+        T iw = static_cast<T>(0);
         if (s < a.Gp) {
             const int2 m0 = a.seg_meta[s], m1 = a.seg_meta[s + 1];
             if (m1.x - m0.x <= kLongSeg) {  // long segments take the long path
                 rb = m0.y;
                 re = m1.y;
             }
-            iw = a.inv_wp[s];
+            iw = static_cast<T>(a.inv_wp[s]);
         }
         // pass 1 (per group): t = sum_m U_m / W_s
-        Acc4 tsum;
-        acc_zero(tsum);
+        V4<T> tsum;
+        v4_zero(tsum);
         int bfirst = 0, bend = 0;
-        for (int m = rb; m < re; ++m) {
-            const int4 rm = a.run_meta[m];
-            if (m == rb) bfirst = rm.z;
-            bend = rm.w;
-            if (a.has_large) {
-                const double cm = static_cast<double>(a.run_w[m]);
-                Acc4 xf;
-                load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+        if (re > rb) {
+            bfirst = a.run_meta[rb].z;
+            bend = a.run_meta[re - 1].w;
+        }
+        if (a.has_large) {
+            for (int m = rb; m < re; ++m) {
+                const int f = a.run_meta[m].x;
+                const T cm = a.run_w[m];
+                V4<T> xf;
+                v4_load(a.x + (a.lbase + f) * CP + 4 * q, xf);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) tsum.v[i] = fma(cm, xf.v[i], tsum.v[i]);
             }
-            if (a.has_small) {
-                for (int b = rm.z; b < rm.w; ++b) {
-                    const int2 bm = a.block_meta[b];
-                    const double wb = a.block_w ? static_cast<double>(a.block_w[b]) : 1.0;
-                    Acc4 p0, p1;
-                    smem_load4<T>(P + bm.x * CP + 4 * q, p0);
-                    smem_load4<T>(P + (bm.x + bm.y) * CP + 4 * q, p1);
+        }
+        if (a.has_small) {
+            for (int b = bfirst; b < bend; ++b) {
+                const int2 bm = a.block_meta[b];
+                const T wb = a.block_w ? a.block_w[b] : static_cast<T>(1);
+                V4<T> p0, p1;
+                v4_lds(P + bm.x * CP + 4 * q, p0);
+                v4_lds(P + (bm.x + bm.y) * CP + 4 * q, p1);
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) tsum.v[i] = fma(wb, p1.v[i] - p0.v[i], tsum.v[i]);
-                }
+                for (int i = 0; i < 4; ++i) tsum.v[i] = fma(wb, p1.v[i] - p0.v[i], tsum.v[i]);
             }
         }
-        Acc4 t;
+        V4<T> t;
 #pragma unroll
         for (int i = 0; i < 4; ++i) t.v[i] = tsum.v[i] * iw;
 
-        // pass 2: warp-synchronous over this segment's blocks
-        const int nb = bend - bfirst;
-        const int steps = a.has_small ? static_cast<int>(__reduce_max_sync(0xffffffffu, static_cast<unsigned>(nb)))
-                                      : 0;
         if (!a.has_small) {
-            // no small dim: one R row per run, U_m = c_m x_f
+            // no small dim: one R row per run, R_m = c_m (x_f - t)
             for (int m = rb; m < re && a.has_large; ++m) {
                 const int4 rm = a.run_meta[m];
-                const double cm = static_cast<double>(a.run_w[m]);
-                Acc4 xf, r;
-                load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+                const T cm = a.run_w[m];
+                V4<T> xf, r;
+                v4_load(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) r.v[i] = cm * (xf.v[i] - t.v[i]);
-                store_quad_stream(a.R + static_cast<int64_t>(rm.y) * CP + 4 * q, r);
+                v4_store_stream(a.R + static_cast<int64_t>(rm.y) * CP + 4 * q, r);
             }
             continue;
         }
+        // pass 2: warp-synchronous over this segment's blocks
+        const int nb = bend - bfirst;
+        const int steps = static_cast<int>(__reduce_max_sync(0xffffffffu, static_cast<unsigned>(nb)));
         int m = rb;
-        int run_bend = 0;
-        double cm = 0.0;
-        int rdest = 0;
-        Acc4 xf, U;
-        acc_zero(xf);
-        acc_zero(U);
+        int run_bend = 0, rdest = 0;
+        T cm = static_cast<T>(0);
+        V4<T> xf, U;
+        v4_zero(xf);
+        v4_zero(U);
         if (nb > 0) {
             const int4 rm = a.run_meta[m];
             run_bend = rm.w;
             rdest = rm.y;
             if (a.has_large) {
-                cm = static_cast<double>(a.run_w[m]);
-                load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+                cm = a.run_w[m];
+                v4_load(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
             }
         }
         for (int step = 0; step < steps; ++step) {
             const bool active = step < nb;
             const int b = bfirst + step;
             int h0 = 0, h1 = 0;
-            Acc4 delta;
-            acc_zero(delta);
+            V4<T> delta;
+            v4_zero(delta);
             if (active) {
                 if (b == run_bend) {  // the current run is complete
                     if (a.has_large) {
-                        Acc4 r;
+                        V4<T> r;
 #pragma unroll
                         for (int i = 0; i < 4; ++i) r.v[i] = fma(cm, xf.v[i] - t.v[i], U.v[i]);
-                        store_quad_stream(a.R + static_cast<int64_t>(rdest) * CP + 4 * q, r);
+                        v4_store_stream(a.R + static_cast<int64_t>(rdest) * CP + 4 * q, r);
                     }
                     ++m;
                     const int4 rm = a.run_meta[m];
                     run_bend = rm.w;
                     rdest = rm.y;
                     if (a.has_large) {
-                        cm = static_cast<double>(a.run_w[m]);
-                        load_quad(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+                        cm = a.run_w[m];
+                        v4_load(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
                     }
-                    acc_zero(U);
+                    v4_zero(U);
                 }
                 const int2 bm = a.block_meta[b];
-                const double wb = a.block_w ? static_cast<double>(a.block_w[b]) : 1.0;
+                const T wb = a.block_w ? a.block_w[b] : static_cast<T>(1);
                 h0 = bm.x;
                 h1 = bm.x + bm.y;
-                Acc4 p0, p1;
-                smem_load4<T>(P + h0 * CP + 4 * q, p0);
-                smem_load4<T>(P + h1 * CP + 4 * q, p1);
+                V4<T> p0, p1;
+                v4_lds(P + h0 * CP + 4 * q, p0);
+                v4_lds(P + h1 * CP + 4 * q, p1);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     U.v[i] = fma(wb, p1.v[i] - p0.v[i], U.v[i]);
                     delta.v[i] = wb * (xf.v[i] - t.v[i]);
                 }
             }
-            // difference-array updates D[h0] += delta, D[h1] -= delta
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const int hh = side == 0 ? h0 : h1;
-                const uint32_t key = active ? static_cast<uint32_t>(hh) : 0x10000u + gw;
-                const unsigned int match = __match_any_sync(0xffffffffu, key);
-                const int rank = __popc(match & ((1u << lane) - 1u)) / CQ;
-                const int msize = static_cast<int>(
-                    __reduce_max_sync(0xffffffffu, static_cast<unsigned>(__popc(match) / CQ)));
-                double* drow = wD + hh * CP + 4 * q;
-                for (int r = 0; r < msize; ++r) {
-                    if (active && rank == r) {
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) drow[i] += side == 0 ? delta.v[i] : -delta.v[i];
-                    }
-                    __syncwarp();
-                }
-            }
+            diff_update<T, CQ>(wD, CP, h0, active, gw, lane, q, delta, false);
+            diff_update<T, CQ>(wD, CP, h1, active, gw, lane, q, delta, true);
         }
         if (nb > 0 && a.has_large) {
-            Acc4 r;
+            V4<T> r;
 #pragma unroll
             for (int i = 0; i < 4; ++i) r.v[i] = fma(cm, xf.v[i] - t.v[i], U.v[i]);
-            store_quad_stream(a.R + static_cast<int64_t>(rdest) * CP + 4 * q, r);
+            v4_store_stream(a.R + static_cast<int64_t>(rdest) * CP + 4 * q, r);
         }
     }
     __syncthreads();
@@ -677,6 +728,176 @@ block_pass_kernel(const BlockArgs<T> a) {
                 dst[h * CP + c] = run;
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 data passes (kRhs, kFinal) over tiles of whole segments, lane = column.
+//
+// A group of CP lanes (one per column) owns one segment, run or observation at
+// a time; the tile's columns are staged column-major in shared memory, so the
+// coalesced column loads/stores and the per-column reductions are free of
+// bank conflicts.  Same outputs as tile_pass_kernel in these modes.
+// ---------------------------------------------------------------------------
+constexpr int kDataThreads = 256;
+
+__host__ __device__ constexpr size_t data_smem_bytes(int CP, int SG) {
+    return static_cast<size_t>(CP) * (kTileObs + 1) * sizeof(double)     // staged columns
+           + static_cast<size_t>(kTileObs) * sizeof(double)              // weights
+           + static_cast<size_t>(kDataThreads / 32) * SG * CP * sizeof(double)  // bins
+           + static_cast<size_t>(kDataThreads) * sizeof(double);         // colsq reduction
+}
+
+template <int CP, int MODE>
+__global__ void __launch_bounds__(kDataThreads)
+data_pass_kernel(const PassArgs<double> a) {
+    constexpr int LD = kTileObs + 1;
+    constexpr int GPB = kDataThreads / CP;  // lane groups per block
+    constexpr int G = 32 / CP;              // lane groups per warp
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* ubuf = reinterpret_cast<double*>(smem_raw);
+    double* wbuf = ubuf + CP * LD;
+    double* bins = wbuf + kTileObs;
+    double* red = bins + (kDataThreads / 32) * a.SG * CP;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int g = tid / CP;   // group in block
+    const int gi = lane / CP; // group in warp
+    const int c = tid % CP;   // column of this lane
+    const bool scatter = (MODE != kFinal) || a.scatter;
+    double* my_bins = bins + warp * a.SG * CP;
+    for (int i = tid; i < (kDataThreads / 32) * a.SG * CP; i += kDataThreads) bins[i] = 0.0;
+    double colsq = 0.0;
+
+    for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        if (a.tile_long[t]) continue;
+        const int32_t s0 = a.tile_seg[t], s1 = a.tile_seg[t + 1];
+        const int64_t k0 = a.seg_off[s0];
+        const int nk = static_cast<int>(a.seg_off[s1] - k0);
+        __syncthreads();
+        // ---- stage the columns (coalesced) and weights ---------------------
+        for (int kl = tid; kl < kTileObs; kl += kDataThreads) {
+            if (kl >= nk) break;
+            const int64_t k = k0 + kl;
+            const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
+#pragma unroll
+            for (int cc = 0; cc < CP; ++cc)
+                ubuf[cc * LD + kl] = cc < a.cols ? __ldcs(a.v + static_cast<int64_t>(cc) * a.n + o) : 0.0;
+        }
+        for (int kl = tid; kl < nk; kl += kDataThreads)
+            wbuf[kl] = a.wp ? a.wp[k0 + kl] : 1.0;
+        if (MODE == kFinal) {
+            __syncthreads();
+            for (int kl = g; kl < nk; kl += GPB) {  // v - D_r a, a row per lane group
+                const int64_t k = k0 + kl;
+                double u = 0.0;
+#pragma unroll
+                for (int l = 0; l < kMaxLarge; ++l)
+                    if (l < a.nL) u += __ldg(a.x + (a.lbase[l] + __ldg(a.rid[l] + k)) * CP + c);
+                if (a.nS > 0) {
+                    const uint32_t packed = __ldg(a.sid + k);
+                    for (int s = 0; s < a.nS; ++s)
+                        u += __ldg(a.x + (a.sbase[s] + ((packed >> (8 * s)) & 0xffu)) * CP + c);
+                }
+                ubuf[c * LD + kl] -= u;
+            }
+        }
+        __syncthreads();
+        // ---- segment means; ubuf <- z (kRhs) or d (kFinal) -----------------
+        for (int32_t s = s0 + g; s < s1; s += GPB) {
+            const int b = static_cast<int>(a.seg_off[s] - k0);
+            const int e = static_cast<int>(a.seg_off[s + 1] - k0);
+            double acc = 0.0;
+            for (int kl = b; kl < e; ++kl) {
+                const double val = ubuf[c * LD + kl];
+                acc = fma(wbuf[kl], val, acc);
+                if (MODE == kRhs) colsq = fma(val, val, colsq);
+            }
+            const double mean = acc * a.inv_wp[s];
+            double zs = 0.0;
+            for (int kl = b; kl < e; ++kl) {
+                const double d = ubuf[c * LD + kl] - mean;
+                const double w = wbuf[kl];
+                ubuf[c * LD + kl] = (MODE == kFinal) ? d : w * d;
+                if (MODE == kFinal) zs = fma(w, d, zs);
+            }
+            if (MODE == kFinal) colsq = fma(zs, zs, colsq);
+        }
+        __syncthreads();
+        if (scatter) {
+            // ---- runs of the large dims ---------------------------------------
+#pragma unroll
+            for (int l = 0; l < kMaxLarge; ++l) {
+                if (l >= a.nL) continue;
+                const int32_t rb = a.run_base[l][s0], re = a.run_base[l][s1];
+                for (int32_t m = rb + g; m < re; m += GPB) {
+                    const int b = static_cast<int>(a.run_start[l][m] - k0);
+                    const int e = static_cast<int>(a.run_start[l][m + 1] - k0);
+                    double acc = 0.0;
+                    for (int kl = b; kl < e; ++kl)
+                        acc = fma((MODE == kFinal) ? wbuf[kl] : 1.0, ubuf[c * LD + kl], acc);
+                    __stcs(a.R[l] + static_cast<int64_t>(a.run_dest[l][m]) * CP + c,
+                           static_cast<double>(acc));
+                }
+            }
+            // ---- small-dim bins (warp-private, groups with equal levels summed
+            //      in group order by the first of them) ---------------------------
+            if (a.nS > 0) {
+                const int per_warp = (nk + (kDataThreads / 32) - 1) / (kDataThreads / 32);
+                const int wb = warp * per_warp;
+                const int we = min(nk, wb + per_warp);
+                for (int base = wb; base < we; base += G) {
+                    const int kl = base + gi;
+                    const bool valid = kl < we;
+                    const uint32_t packed = valid ? __ldg(a.sid + k0 + kl) : 0u;
+                    for (int s = 0; s < a.nS; ++s) {
+                        const uint32_t key = valid ? ((packed >> (8 * s)) & 0xffu) : 0x100u + gi;
+                        const unsigned int match = __match_any_sync(0xffffffffu, key);
+                        if (valid && (__ffs(match) - 1) / CP == gi) {
+                            double acc = 0.0;
+#pragma unroll
+                            for (int g2 = 0; g2 < G; ++g2) {
+                                if (match & (1u << (g2 * CP))) {
+                                    const int kj = base + g2;
+                                    acc = fma((MODE == kFinal) ? wbuf[kj] : 1.0, ubuf[c * LD + kj], acc);
+                                }
+                            }
+                            my_bins[(a.sgoff[s] + static_cast<int>(key)) * CP + c] += acc;
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+        }
+        // ---- write the within transform (coalesced) ---------------------------
+        if (MODE == kFinal) {
+            for (int kl = tid; kl < kTileObs; kl += kDataThreads) {
+                if (kl >= nk) break;
+                const int64_t k = k0 + kl;
+                const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
+#pragma unroll
+                for (int cc = 0; cc < CP; ++cc)
+                    if (cc < a.cols) __stcs(a.out + static_cast<int64_t>(cc) * a.n + o, ubuf[cc * LD + kl]);
+            }
+        }
+    }
+    __syncthreads();
+    const int cta = a.bins_cta0 + blockIdx.x;
+    if (a.nS > 0 && scatter) {
+        double* dst = a.bins_partial + static_cast<int64_t>(cta) * a.SG * CP;
+        for (int i = tid; i < a.SG * CP; i += kDataThreads) {
+            double sum = 0.0;
+            for (int w = 0; w < kDataThreads / 32; ++w) sum += bins[w * a.SG * CP + i];
+            dst[i] = sum;
+        }
+    }
+    red[tid] = colsq;
+    __syncthreads();
+    if (tid < CP) {
+        double sum = 0.0;
+        for (int j = 0; j < GPB; ++j) sum += red[j * CP + tid];
+        a.colsq_partial[static_cast<int64_t>(cta) * CP + tid] = sum;
     }
 }
 
@@ -886,8 +1107,18 @@ __device__ __forceinline__ double block_column_sum(const double* part, int64_t n
     const int c = t % CP;
     const int j = t / CP;
     double s = 0.0;
-    if (j < J)
-        for (int64_t p = j; p < nparts; p += J) s += __ldcg(part + p * stride + c);
+    if (j < J) {
+        // eight independent accumulators keep eight loads in flight; their
+        // fixed combination order keeps the sum deterministic
+        double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int64_t p = j;
+        for (; p + 7 * J < nparts; p += 8 * J) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc[u] += __ldcg(part + (p + u * J) * stride + c);
+        }
+        for (; p < nparts; p += J) acc[0] += __ldcg(part + p * stride + c);
+        s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    }
     red[t] = s;
     __syncthreads();
     for (int h = J / 2; h > 0; h >>= 1) {
