@@ -23,10 +23,12 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libxhdfe_ref.so"
+# the reference core built with -DHDFE_USE_CUDA over the B200 library (drop-in check)
+REF_B200_SO = HERE / "_ref" / "libxhdfe_ref_b200.so"
 
 _vp, _i64, _int, _dbl = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double
 _olib = None
-_rlib = None
+_rlib = {}
 
 
 def build_oracle() -> Path:
@@ -105,7 +107,7 @@ def certify(V_orig, V_tilde, fes, G, weights=None):
 class XrefOptions(ctypes.Structure):
     _fields_ = [("tol", _dbl), ("tolerance_mode", _int), ("absorption_method", _int),
                 ("num_threads", _int), ("max_iter", _int), ("drop_singletons", _int),
-                ("se_type", _int), ("fit_intercept", _int)]
+                ("se_type", _int), ("fit_intercept", _int), ("gpu_backend", _int)]
 
 
 TOLERANCE_MODES = {"xhdfe-fast": 0, "reghdfe-comparable": 1, "strict-residual": 2}
@@ -117,12 +119,11 @@ def ref_available() -> bool:
     return REF_SO.exists()
 
 
-def rlib() -> ctypes.CDLL:
-    global _rlib
-    if _rlib is None:
-        if not REF_SO.exists():
-            raise FileNotFoundError(f"{REF_SO} not built (oracle/Makefile target 'ref')")
-        lib = ctypes.CDLL(str(REF_SO))
+def rlib(path: Path = REF_SO) -> ctypes.CDLL:
+    if path not in _rlib:
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (oracle/Makefile targets 'ref', 'ref_b200')")
+        lib = ctypes.CDLL(str(path))
         P = ctypes.POINTER
         lib.xref_absorb.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, P(XrefOptions), _vp, _vp,
                                     P(_int), P(_dbl), ctypes.c_char_p, _int]
@@ -133,12 +134,15 @@ def rlib() -> ctypes.CDLL:
         lib.xref_fit.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, _vp, P(XrefOptions), _vp,
                                  _vp, P(_int), P(_dbl), ctypes.c_char_p, _int]
         lib.xref_fit.restype = _int
-        _rlib = lib
-    return _rlib
+        _rlib[path] = lib
+    return _rlib[path]
+
+
+GPU_BACKENDS = {"default": 0, "cpu": 1, "cuda": 2}
 
 
 def _xopts(tol, tolerance_mode, method, threads, max_iter=0, drop_singletons=True,
-           se_type="unadjusted", fit_intercept=True):
+           se_type="unadjusted", fit_intercept=True, gpu_backend="default"):
     o = XrefOptions()
     o.tol = tol
     o.tolerance_mode = TOLERANCE_MODES[tolerance_mode]
@@ -148,41 +152,42 @@ def _xopts(tol, tolerance_mode, method, threads, max_iter=0, drop_singletons=Tru
     o.drop_singletons = 1 if drop_singletons else 0
     o.se_type = SE_TYPES[se_type]
     o.fit_intercept = 1 if fit_intercept else 0
+    o.gpu_backend = GPU_BACKENDS[gpu_backend]
     return o
 
 
 def ref_absorb(y, X, fes, weights=None, *, tol=1e-8, tolerance_mode="reghdfe-comparable",
-               method="auto", threads=1, max_iter=0):
+               method="auto", threads=1, max_iter=0, gpu_backend="default", lib_path=REF_SO):
     """Reference absorb_fixed_effects_v6 (raw ids, no singleton drop)."""
     V, g, _, w = _pack(y, X, fes, [1] * len(fes), weights)
     n, C = V.shape
     Vo = np.empty_like(V, order="F")
-    info = (_int * 4)()
+    info = (_int * 8)()
     dinfo = (_dbl * 2)()
     err = ctypes.create_string_buffer(512)
-    o = _xopts(tol, tolerance_mode, method, threads, max_iter)
-    rc = rlib().xref_absorb(V[:, 0].ctypes.data, V[:, 1:].ctypes.data if C > 1 else None, n, C - 1,
+    o = _xopts(tol, tolerance_mode, method, threads, max_iter, gpu_backend=gpu_backend)
+    rc = rlib(lib_path).xref_absorb(V[:, 0].ctypes.data, V[:, 1:].ctypes.data if C > 1 else None, n, C - 1,
                             g.ctypes.data, len(fes), None if w is None else w.ctypes.data,
                             ctypes.byref(o), Vo[:, 0].ctypes.data,
                             Vo[:, 1:].ctypes.data if C > 1 else None, info, dinfo, err, 512)
     if rc != 0:
         raise RuntimeError(err.value.decode())
     return {"V": Vo, "iterations": info[0], "converged": bool(info[1]),
-            "precision_certified": bool(info[2]), "abs_residual": dinfo[0],
-            "abs_residual_rel": dinfo[1]}
+            "precision_certified": bool(info[2]), "gpu_status_code": info[3],
+            "abs_residual": dinfo[0], "abs_residual_rel": dinfo[1]}
 
 
 def ref_partial_out(y, X, fes, weights=None, *, tol=1e-8, tolerance_mode="reghdfe-comparable",
-                    threads=1, drop_singletons=True):
+                    threads=1, drop_singletons=True, gpu_backend="default", lib_path=REF_SO):
     V, g, _, w = _pack(y, X, fes, [1] * len(fes), weights)
     n, C = V.shape
     Vo = np.zeros_like(V, order="F")
     idx = np.zeros(n, dtype=np.int32)
-    info = (_int * 4)()
+    info = (_int * 8)()
     dinfo = (_dbl * 2)()
     err = ctypes.create_string_buffer(512)
-    o = _xopts(tol, tolerance_mode, "auto", threads, 0, drop_singletons)
-    rc = rlib().xref_partial_out(V[:, 0].ctypes.data, V[:, 1:].ctypes.data if C > 1 else None, n,
+    o = _xopts(tol, tolerance_mode, "auto", threads, 0, drop_singletons, gpu_backend=gpu_backend)
+    rc = rlib(lib_path).xref_partial_out(V[:, 0].ctypes.data, V[:, 1:].ctypes.data if C > 1 else None, n,
                                  C - 1, g.ctypes.data, len(fes),
                                  None if w is None else w.ctypes.data, ctypes.byref(o),
                                  Vo[:, 0].ctypes.data, Vo[:, 1:].ctypes.data if C > 1 else None,
@@ -198,24 +203,26 @@ def ref_partial_out(y, X, fes, weights=None, *, tol=1e-8, tolerance_mode="reghdf
         Vk[:, 1:] = flat.reshape((kept, C - 1), order="F")
     return {"V": Vk, "sample_index": idx[:kept].copy(), "iterations": info[0],
             "converged": bool(info[1]), "precision_certified": bool(info[2]),
+            "gpu_status_code": info[4],
             "abs_residual": dinfo[0], "abs_residual_rel": dinfo[1]}
 
 
 def ref_fit(y, X, fes, weights=None, cluster=None, *, tol=1e-8,
             tolerance_mode="reghdfe-comparable", threads=1, se_type=None, fit_intercept=False,
-            drop_singletons=True):
+            drop_singletons=True, gpu_backend="default", lib_path=REF_SO):
     V, g, _, w = _pack(y, X, fes, [1] * len(fes), weights)
     n, C = V.shape
     k = C - 1
     coef = np.zeros(k + 2)
     se = np.zeros(k + 2)
-    info = (_int * 6)()
+    info = (_int * 8)()
     dinfo = (_dbl * 4)()
     err = ctypes.create_string_buffer(512)
     st = se_type or ("cluster" if cluster is not None else "unadjusted")
-    o = _xopts(tol, tolerance_mode, "auto", threads, 0, drop_singletons, st, fit_intercept)
+    o = _xopts(tol, tolerance_mode, "auto", threads, 0, drop_singletons, st, fit_intercept,
+               gpu_backend)
     cl = None if cluster is None else np.ascontiguousarray(cluster, dtype=np.int32)
-    rc = rlib().xref_fit(V[:, 0].ctypes.data, V[:, 1:].ctypes.data, n, k, g.ctypes.data, len(fes),
+    rc = rlib(lib_path).xref_fit(V[:, 0].ctypes.data, V[:, 1:].ctypes.data, n, k, g.ctypes.data, len(fes),
                          None if w is None else w.ctypes.data,
                          None if cl is None else cl.ctypes.data, ctypes.byref(o),
                          coef.ctypes.data, se.ctypes.data, info, dinfo, err, 512)
@@ -224,5 +231,6 @@ def ref_fit(y, X, fes, weights=None, cluster=None, *, tol=1e-8,
     p = info[5]
     return {"coef": coef[:p].copy(), "se": se[:p].copy(), "iterations": info[0],
             "converged": bool(info[1]), "precision_certified": bool(info[2]), "nobs": info[3],
-            "num_singletons": info[4], "abs_residual_rel": dinfo[0], "rss": dinfo[1],
+            "num_singletons": info[4], "gpu_status_code": info[6],
+            "abs_residual_rel": dinfo[0], "rss": dinfo[1],
             "r2_within": dinfo[2], "df_a": dinfo[3]}

@@ -18,10 +18,12 @@
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "fe_absorption.hpp"
+#include "fe_absorption_cuda.hpp"
 #include "hdfe/hdfe_regressor.hpp"
 #include "hdfe/hdfe_regressor_v11.hpp"
 
@@ -41,7 +43,18 @@ struct XrefOptions {
     int drop_singletons;
     int se_type;          // 0 homoskedastic, 1 robust, 2 cluster
     int fit_intercept;
+    int gpu_backend;      // 0 library default, 1 force CPU, 2 force CUDA
 };
+
+// Thread-local backend selection through the reference's own override
+// (include/fe_absorption_cuda.hpp:108-122).
+std::unique_ptr<hdfe::detail::ScopedGpuBackendOverride> backend_guard(const XrefOptions* o) {
+    if (o->gpu_backend == 1)
+        return std::make_unique<hdfe::detail::ScopedGpuBackendOverride>(hdfe::detail::GpuBackend::Cpu);
+    if (o->gpu_backend == 2)
+        return std::make_unique<hdfe::detail::ScopedGpuBackendOverride>(hdfe::detail::GpuBackend::Cuda);
+    return nullptr;
+}
 
 hdfe::HdfeOptions to_options(const XrefOptions* o) {
     hdfe::HdfeOptions opts;
@@ -84,7 +97,7 @@ extern "C" {
 
 // Demean y (n) and X (n x k, column-major) on all FE dims, no singleton drop.
 // info[0]=iterations info[1]=converged info[2]=precision_certified
-// dinfo[0]=abs_residual dinfo[1]=abs_residual_rel
+// info[3]=gpu_status_code dinfo[0]=abs_residual dinfo[1]=abs_residual_rel
 int xref_absorb(const double* y, const double* X, int64_t n, int k,
                 const int32_t* fe_flat, int dims, const double* w,
                 const XrefOptions* o, double* y_out, double* X_out,
@@ -98,6 +111,7 @@ int xref_absorb(const double* y, const double* X, int64_t n, int k,
             wv = Map<const VectorXd>(w, n);
         }
         hdfe::HdfeOptions opts = to_options(o);
+        auto guard = backend_guard(o);
         hdfe::detail::AbsorptionResult r = hdfe::detail::absorb_fixed_effects_v6(
             ym, Xm, fes, w ? &wv : nullptr, opts, opts.absorption_method);
         std::memcpy(y_out, r.y_tilde.data(), sizeof(double) * static_cast<std::size_t>(n));
@@ -108,6 +122,7 @@ int xref_absorb(const double* y, const double* X, int64_t n, int k,
         info[0] = r.iterations;
         info[1] = r.converged ? 1 : 0;
         info[2] = r.precision_certified ? 1 : 0;
+        info[3] = r.gpu_status_code;
         dinfo[0] = r.abs_residual;
         dinfo[1] = r.abs_residual_rel;
         return 0;
@@ -137,6 +152,7 @@ int xref_partial_out(const double* y, const double* X, int64_t n, int k,
             wv = Map<const VectorXd>(w, n);
         }
         hdfe::HdfeOptions opts = to_options(o);
+        auto guard = backend_guard(o);
         hdfe::v11::HdfeRegressorV11 reg(opts);
         hdfe::detail::AbsorptionResult r =
             reg.partial_out(ym, Xm, fes, w ? &wv : nullptr, nullptr, nullptr);
@@ -154,6 +170,7 @@ int xref_partial_out(const double* y, const double* X, int64_t n, int k,
         info[1] = r.converged ? 1 : 0;
         info[2] = r.precision_certified ? 1 : 0;
         info[3] = static_cast<int>(kept);
+        info[4] = reg.gpu_status_code();
         dinfo[0] = r.abs_residual;
         dinfo[1] = r.abs_residual_rel;
         return 0;
@@ -188,6 +205,7 @@ int xref_fit(const double* y, const double* X, int64_t n, int k,
             clusters = to_fes(cluster, n, 1);
         }
         hdfe::HdfeOptions opts = to_options(o);
+        auto guard = backend_guard(o);
         hdfe::v11::HdfeRegressorV11 reg(opts);
         reg.fit(ym, Xm, fes, w ? &wv : nullptr, cluster ? &clusters : nullptr);
         const hdfe::HdfeResults& res = reg.results();
@@ -202,6 +220,7 @@ int xref_fit(const double* y, const double* X, int64_t n, int k,
         info[3] = res.nobs;
         info[4] = res.num_singletons;
         info[5] = p;
+        info[6] = reg.gpu_status_code();
         dinfo[0] = res.abs_residual_rel;
         dinfo[1] = res.rss;
         dinfo[2] = res.r2_within;

@@ -1,0 +1,205 @@
+// Reference-side binding: the C++ symbols that reisportela/xhdfe-xfe's core
+// calls when it is built with -DHDFE_USE_CUDA, implemented over the C ABI of
+// libb200fe.so (include/b200fe.h).  Compile this file with the reference's
+// headers in place of src/fe_absorption_cuda.cu and src/akm_kss_cuda.cu and
+// link libb200fe.so; src/fe_absorption.cpp, the pybind11 module, the R package
+// and the Stata plugin then reach the B200 absorber unchanged.
+//
+// Symbols (signatures from include/fe_absorption_cuda.hpp and
+// include/hdfe/akm_kss_cuda.hpp of the reference):
+//   cuda_backend_available                     (fe_absorption_cuda.hpp:125)
+//   absorb_fixed_effects_cuda                  (fe_absorption_cuda.hpp:127-134)
+//   absorb_fixed_effects_group_individual_cuda (fe_absorption_cuda.hpp:136-145)
+//   fe_recovery_max_delta_cuda(_cached)        (fe_absorption_cuda.hpp:152-162)
+//   cuda_cert_shadow_begin/finish/abort        (fe_absorption_cuda.hpp:74-99)
+//   akm_cuda_*                                 (akm_kss_cuda.hpp:17-74)
+// The host certificate certify_cuda_absorption_result stays the reference's
+// own src/fe_absorption_cuda_certificate.cpp.
+//
+// Contract kept from the reference (src/fe_absorption_cuda.cu:2294-4738):
+// return false on any failure (the caller reports status 4 and fails closed
+// when the GPU backend was requested, src/fe_absorption.cpp:9227-9237);
+// return true with converged=false on non-convergence; never throw.  Features
+// this library does not provide yet return false, so the reference fails
+// closed rather than silently using another path: heterogeneous slopes, saved
+// fixed effects (retain_fixed_effects), group/individual FEs, and the AKM/KSS
+// GPU solver (akm_cuda_available() is false, so AKM stays on the CPU).
+
+#include <Eigen/Dense>
+
+#include <cstdint>
+#include <vector>
+
+#include "b200fe.h"
+#include "fe_absorption_cuda.hpp"
+#include "hdfe/akm_kss_cuda.hpp"
+
+namespace {
+
+// One context per host thread, like the reference's thread_local workspace
+// (src/fe_absorption_cuda.cu:1536).
+b200fe_context* thread_ctx() {
+    thread_local b200fe_context* ctx = nullptr;
+    thread_local bool tried = false;
+    if (!tried) {
+        tried = true;
+        if (b200fe_context_create(0, &ctx) != B200FE_OK) ctx = nullptr;
+    }
+    return ctx;
+}
+
+}  // namespace
+
+namespace hdfe {
+namespace detail {
+
+bool cuda_backend_available() { return b200fe_device_available() != 0; }
+
+bool absorb_fixed_effects_cuda(const Eigen::Ref<const Eigen::VectorXd>& y,
+                               const Eigen::Ref<const Eigen::MatrixXd>& X,
+                               const std::vector<GpuFeInput>& fe_inputs,
+                               const Eigen::VectorXd* weights,
+                               const std::vector<std::size_t>& sweep_order,
+                               const HdfeOptions& options, AbsorptionMethod /*method*/,
+                               AbsorptionResult& result) {
+    try {
+        const int64_t n = y.size();
+        const int k = static_cast<int>(X.cols());
+        if (X.rows() != n) return false;  // the reference requires ld == n
+        if (fe_inputs.empty()) {
+            result.y_tilde = y;
+            result.X_tilde = X;
+            result.iterations = 0;
+            result.converged = true;
+            return true;
+        }
+        if (fe_inputs.size() > B200FE_MAX_DIMS || options.retain_fixed_effects) return false;
+        std::vector<const int32_t*> gids;
+        std::vector<int32_t> levels;
+        for (const GpuFeInput& fe : fe_inputs) {
+            if (fe.is_slope || !fe.group_ids) return false;
+            gids.push_back(fe.group_ids);
+            levels.push_back(fe.num_groups);
+        }
+        b200fe_context* ctx = thread_ctx();
+        if (!ctx) return false;
+        b200fe_options o;
+        b200fe_default_options(&o);
+        o.tol = options.tol > 0.0 ? options.tol : 1e-8;
+        o.tolerance_mode = static_cast<int>(options.tolerance_mode);
+        if (options.max_iter > 0) o.max_iter = options.max_iter;
+        // contiguous copies: Eigen::Ref may have an inner stride
+        const Eigen::VectorXd yc = y;
+        const Eigen::MatrixXd Xc = X;
+        result.y_tilde.resize(n);
+        result.X_tilde.resize(n, k);
+        b200fe_result r;
+        const int rc = b200fe_absorb(ctx, yc.data(), k ? Xc.data() : nullptr, n, k,
+                                     static_cast<int>(gids.size()), gids.data(), levels.data(),
+                                     weights ? weights->data() : nullptr, &o,
+                                     result.y_tilde.data(), k ? result.X_tilde.data() : nullptr, &r);
+        if (rc != B200FE_OK && rc != B200FE_NOT_CONVERGED) return false;
+        result.iterations = r.iterations;
+        result.converged = rc == B200FE_OK;
+        result.fe_levels.clear();
+        for (std::size_t d = 0; d < fe_inputs.size(); ++d)
+            result.fe_levels.push_back(fe_inputs[d].num_levels_present > 0
+                                           ? fe_inputs[d].num_levels_present
+                                           : fe_inputs[d].num_groups);
+        result.sweep_order_used.assign(sweep_order.begin(), sweep_order.end());
+        return true;
+    } catch (...) {
+        return false;
+    }
+}
+
+bool absorb_fixed_effects_group_individual_cuda(
+    const Eigen::Ref<const Eigen::VectorXd>&, const Eigen::Ref<const Eigen::MatrixXd>&,
+    const std::vector<GpuFeInput>&, const GroupIndividualStructure&, const Eigen::VectorXd*,
+    const std::vector<std::size_t>&, const HdfeOptions&, AbsorptionMethod, AbsorptionResult&) {
+    return false;  // not provided: the caller fails closed
+}
+
+static bool recovery_max_delta(const Eigen::Ref<const Eigen::VectorXd>& residual,
+                               const std::vector<GpuFeInput>& fe_inputs,
+                               const Eigen::VectorXd* weights,
+                               const std::vector<std::size_t>& sweep_order, double& out) {
+    try {
+        b200fe_context* ctx = thread_ctx();
+        if (!ctx || fe_inputs.size() > B200FE_MAX_DIMS) return false;
+        std::vector<const int32_t*> gids;
+        std::vector<int32_t> levels;
+        for (const GpuFeInput& fe : fe_inputs) {
+            if (fe.is_slope || !fe.group_ids) return false;
+            gids.push_back(fe.group_ids);
+            levels.push_back(fe.num_groups);
+        }
+        std::vector<int32_t> order(sweep_order.begin(), sweep_order.end());
+        const Eigen::VectorXd rc = residual;
+        return b200fe_fe_recovery_max_delta(ctx, rc.data(), rc.size(),
+                                            static_cast<int>(gids.size()), gids.data(),
+                                            levels.data(), weights ? weights->data() : nullptr,
+                                            order.empty() ? nullptr : order.data(),
+                                            &out) == B200FE_OK;
+    } catch (...) {
+        return false;
+    }
+}
+
+bool fe_recovery_max_delta_cuda(const Eigen::Ref<const Eigen::VectorXd>& residual,
+                                const std::vector<GpuFeInput>& fe_inputs,
+                                const Eigen::VectorXd* weights,
+                                const std::vector<std::size_t>& sweep_order,
+                                double& out_max_delta) {
+    return recovery_max_delta(residual, fe_inputs, weights, sweep_order, out_max_delta);
+}
+
+bool fe_recovery_max_delta_cuda_cached(const Eigen::Ref<const Eigen::VectorXd>& residual,
+                                       const std::vector<GpuFeInput>& fe_inputs,
+                                       const Eigen::VectorXd* weights,
+                                       const std::vector<std::size_t>& sweep_order,
+                                       double& out_max_delta) {
+    return recovery_max_delta(residual, fe_inputs, weights, sweep_order, out_max_delta);
+}
+
+// The device shadow certificate is an optional cross-check the reference runs
+// only when XHDFE_GPU_CERT_SHADOW=1; here it reports ERROR and the host
+// certificate stays authoritative, as in the reference.
+CudaCertShadowHandle* cuda_cert_shadow_begin(const double*, const double*, int, int, int,
+                                             const double*, const int* const*,
+                                             const double* const*, const int*, int,
+                                             const double* const*, const unsigned char*) {
+    return nullptr;
+}
+
+bool cuda_cert_shadow_finish(CudaCertShadowHandle*, const double*, const double*, double,
+                             CudaCertShadowResult* out) {
+    if (out) out->verdict = 3;
+    return false;
+}
+
+void cuda_cert_shadow_abort(CudaCertShadowHandle*) {}
+
+}  // namespace detail
+
+namespace akm {
+
+// The KSS leverage solver is not provided by this library yet: the AKM code
+// checks akm_cuda_available() first and then stays on its CPU solver.
+bool akm_cuda_available() { return false; }
+bool akm_cuda_stable_sort_u64(const std::uint64_t*, std::int64_t*, std::size_t) { return false; }
+AkmCudaContext* akm_cuda_create(int, int, const int*, const int*, const double*, std::size_t,
+                                const std::int64_t*, const std::int64_t*, const std::int64_t*,
+                                const double*, const double*, const double*) {
+    return nullptr;
+}
+void akm_cuda_destroy(AkmCudaContext*) {}
+int akm_cuda_solve_S(AkmCudaContext*, const double*, double*, double, int) { return -1; }
+int akm_cuda_solve_S_multi(AkmCudaContext*, const double*, double*, int, double, int, int*) {
+    return -1;
+}
+int akm_cuda_max_lanes() { return 0; }
+double* akm_cuda_pack_buffer(AkmCudaContext*, int) { return nullptr; }
+
+}  // namespace akm
+}  // namespace hdfe
