@@ -163,6 +163,28 @@ int b200fe_fe_recovery_max_delta(b200fe_context* ctx, const double* residual,
                                  const int32_t* sweep_order,
                                  double* out_max_delta);
 
+/* One-way within transform that allocates no device memory, for callers that
+ * cannot call cudaMalloc while they use this library: a host application that
+ * keeps all device memory in its own pool, or a plugin that must not grow its
+ * CUDA footprint in the middle of a session.  The caller passes every input
+ * and output as a device pointer: d_v column-major n x cols, d_group_ids dense
+ * ids in [0, num_groups) sorted non-decreasing (data ordered by the FE, e.g. a
+ * panel sorted by worker), d_weights n doubles or NULL, d_out n x cols (not
+ * aliasing d_v).  d_out receives v minus the weighted group mean of v, per
+ * column.  The only scratch is a fixed array inside the library: at most 2^20
+ * groups (a larger num_groups returns B200FE_INVALID_ARG before any GPU work),
+ * kept by every GPU that loads the library until the process exits.  All calls
+ * on one device share that array, so calls whose GPU work overlaps race on it.
+ * The first call on a device looks up the array's address with that device
+ * current; make it before any stream capture.  Unsorted or out-of-range ids
+ * return B200FE_INVALID_ARG.  stream: a cudaStream_t as void*, or NULL.
+ * This entry point has no counterpart in the reference, which always
+ * allocates its device workspace. */
+int b200fe_demean_sorted_noalloc(const double* d_v, int64_t n, int cols,
+                                 const int32_t* d_group_ids, int32_t num_groups,
+                                 const double* d_weights, double* d_out,
+                                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = (
     "b200fe_absorb_device",
     "b200fe_demean_raw",
     "b200fe_fe_recovery_max_delta",
+    "b200fe_demean_sorted_noalloc",
 )
 
 
@@ -123,6 +124,8 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.b200fe_fe_recovery_max_delta.argtypes = [vp, vp, i64, c_int, pp, vp, vp, vp,
                                                  ctypes.POINTER(ctypes.c_double)]
     lib.b200fe_fe_recovery_max_delta.restype = c_int
+    lib.b200fe_demean_sorted_noalloc.argtypes = [vp, i64, c_int, vp, ctypes.c_int32, vp, vp, vp]
+    lib.b200fe_demean_sorted_noalloc.restype = c_int
     if path is None:
         _LIB = lib
     return lib
