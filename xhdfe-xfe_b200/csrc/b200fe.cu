@@ -698,7 +698,7 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     wk.data_grid = 0;
     wk.data_smem = 0;
     if (std::is_same<T, double>::value) {
-        wk.data_smem = static_cast<int>(data_smem_bytes(CP, st.SG));
+        wk.data_smem = static_cast<int>(data_smem_bytes(CP, st.SG, st.nL));
         B_TRY(cudaFuncSetAttribute(data_pass_kernel<CP, kRhs>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    wk.data_smem));
         B_TRY(cudaFuncSetAttribute(data_pass_kernel<CP, kFinal>,

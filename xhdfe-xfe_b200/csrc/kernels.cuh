@@ -737,15 +737,23 @@ block_pass_kernel(const BlockArgs<T> a) {
 // A group of CP lanes (one per column) owns one segment, run or observation at
 // a time; the tile's columns are staged column-major in shared memory, so the
 // coalesced column loads/stores and the per-column reductions are free of
-// bank conflicts.  Same outputs as tile_pass_kernel in these modes.
+// bank conflicts.  Everything a later phase indexes by observation or run
+// (large-dim ids, packed small-dim ids, run offsets and destination rows) is
+// staged in the same coalesced first phase, so the serial per-group loops
+// after it touch only shared memory and the gathered alpha rows (L2), and no
+// global load waits on another.  Same outputs as tile_pass_kernel in these
+// modes.
 // ---------------------------------------------------------------------------
 constexpr int kDataThreads = 256;
 
-__host__ __device__ constexpr size_t data_smem_bytes(int CP, int SG) {
+__host__ __device__ constexpr size_t data_smem_bytes(int CP, int SG, int nL) {
     return static_cast<size_t>(CP) * (kTileObs + 1) * sizeof(double)     // staged columns
            + static_cast<size_t>(kTileObs) * sizeof(double)              // weights
            + static_cast<size_t>(kDataThreads / 32) * SG * CP * sizeof(double)  // bins
-           + static_cast<size_t>(kDataThreads) * sizeof(double);         // colsq reduction
+           + static_cast<size_t>(kTileObs) * sizeof(uint32_t)            // packed small ids
+           + static_cast<size_t>(nL) * kTileObs * sizeof(int32_t)        // large-dim ids
+           + static_cast<size_t>(nL) * kTileObs * sizeof(int32_t)        // run rows in R
+           + static_cast<size_t>(nL) * (kTileObs + 2) * sizeof(uint16_t);  // run offsets
 }
 
 template <int CP, int MODE>
@@ -758,7 +766,11 @@ data_pass_kernel(const PassArgs<double> a) {
     double* ubuf = reinterpret_cast<double*>(smem_raw);
     double* wbuf = ubuf + CP * LD;
     double* bins = wbuf + kTileObs;
-    double* red = bins + (kDataThreads / 32) * a.SG * CP;
+    uint32_t* sidbuf = reinterpret_cast<uint32_t*>(bins + (kDataThreads / 32) * a.SG * CP);
+    int32_t* ridbuf = reinterpret_cast<int32_t*>(sidbuf + kTileObs);  // [nL][kTileObs]
+    int32_t* dstbuf = ridbuf + a.nL * kTileObs;                        // [nL][kTileObs]
+    uint16_t* offbuf = reinterpret_cast<uint16_t*>(dstbuf + a.nL * kTileObs);  // [nL][kTileObs+2]
+    double* red = ubuf;  // colsq reduction, after the tile loop
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -775,28 +787,49 @@ data_pass_kernel(const PassArgs<double> a) {
         const int32_t s0 = a.tile_seg[t], s1 = a.tile_seg[t + 1];
         const int64_t k0 = a.seg_off[s0];
         const int nk = static_cast<int>(a.seg_off[s1] - k0);
+        int32_t rb[kMaxLarge], nr[kMaxLarge];
+#pragma unroll
+        for (int l = 0; l < kMaxLarge; ++l) {
+            rb[l] = (l < a.nL && scatter) ? a.run_base[l][s0] : 0;
+            nr[l] = (l < a.nL && scatter) ? a.run_base[l][s1] - rb[l] : 0;
+        }
         __syncthreads();
-        // ---- stage the columns (coalesced) and weights ---------------------
-        for (int kl = tid; kl < kTileObs; kl += kDataThreads) {
-            if (kl >= nk) break;
+        // ---- stage columns, weights, ids and run tables (coalesced) -----------
+        for (int kl = tid; kl < nk; kl += kDataThreads) {
             const int64_t k = k0 + kl;
             const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
 #pragma unroll
             for (int cc = 0; cc < CP; ++cc)
                 ubuf[cc * LD + kl] = cc < a.cols ? __ldcs(a.v + static_cast<int64_t>(cc) * a.n + o) : 0.0;
+            wbuf[kl] = a.wp ? a.wp[k] : 1.0;
+            if (a.nS > 0 && (scatter || MODE == kFinal)) sidbuf[kl] = __ldg(a.sid + k);
+            if (MODE == kFinal) {
+#pragma unroll
+                for (int l = 0; l < kMaxLarge; ++l)
+                    if (l < a.nL) ridbuf[l * kTileObs + kl] = __ldg(a.rid[l] + k);
+            }
         }
-        for (int kl = tid; kl < nk; kl += kDataThreads)
-            wbuf[kl] = a.wp ? a.wp[k0 + kl] : 1.0;
+#pragma unroll
+        for (int l = 0; l < kMaxLarge; ++l) {
+            if (l >= a.nL || !scatter) continue;
+            for (int j = tid; j <= nr[l]; j += kDataThreads) {
+                offbuf[l * (kTileObs + 2) + j] =
+                    static_cast<uint16_t>(__ldg(a.run_start[l] + rb[l] + j) - k0);
+                if (j < nr[l]) dstbuf[l * kTileObs + j] = __ldg(a.run_dest[l] + rb[l] + j);
+            }
+        }
         if (MODE == kFinal) {
             __syncthreads();
-            for (int kl = g; kl < nk; kl += GPB) {  // v - D_r a, a row per lane group
-                const int64_t k = k0 + kl;
+            // v - D_r a: one alpha row per lane group; the ids come from shared
+            // memory, so the unrolled loads of several observations overlap
+#pragma unroll 4
+            for (int kl = g; kl < nk; kl += GPB) {
                 double u = 0.0;
 #pragma unroll
                 for (int l = 0; l < kMaxLarge; ++l)
-                    if (l < a.nL) u += __ldg(a.x + (a.lbase[l] + __ldg(a.rid[l] + k)) * CP + c);
+                    if (l < a.nL) u += __ldg(a.x + (a.lbase[l] + ridbuf[l * kTileObs + kl]) * CP + c);
                 if (a.nS > 0) {
-                    const uint32_t packed = __ldg(a.sid + k);
+                    const uint32_t packed = sidbuf[kl];
                     for (int s = 0; s < a.nS; ++s)
                         u += __ldg(a.x + (a.sbase[s] + ((packed >> (8 * s)) & 0xffu)) * CP + c);
                 }
@@ -830,15 +863,14 @@ data_pass_kernel(const PassArgs<double> a) {
 #pragma unroll
             for (int l = 0; l < kMaxLarge; ++l) {
                 if (l >= a.nL) continue;
-                const int32_t rb = a.run_base[l][s0], re = a.run_base[l][s1];
-                for (int32_t m = rb + g; m < re; m += GPB) {
-                    const int b = static_cast<int>(a.run_start[l][m] - k0);
-                    const int e = static_cast<int>(a.run_start[l][m + 1] - k0);
+                const uint16_t* off = offbuf + l * (kTileObs + 2);
+                const int32_t* dst = dstbuf + l * kTileObs;
+                for (int j = g; j < nr[l]; j += GPB) {
+                    const int b = off[j], e = off[j + 1];
                     double acc = 0.0;
                     for (int kl = b; kl < e; ++kl)
                         acc = fma((MODE == kFinal) ? wbuf[kl] : 1.0, ubuf[c * LD + kl], acc);
-                    __stcs(a.R[l] + static_cast<int64_t>(a.run_dest[l][m]) * CP + c,
-                           static_cast<double>(acc));
+                    __stcs(a.R[l] + static_cast<int64_t>(dst[j]) * CP + c, acc);
                 }
             }
             // ---- small-dim bins (warp-private, groups with equal levels summed
@@ -850,7 +882,7 @@ data_pass_kernel(const PassArgs<double> a) {
                 for (int base = wb; base < we; base += G) {
                     const int kl = base + gi;
                     const bool valid = kl < we;
-                    const uint32_t packed = valid ? __ldg(a.sid + k0 + kl) : 0u;
+                    const uint32_t packed = valid ? sidbuf[kl] : 0u;
                     for (int s = 0; s < a.nS; ++s) {
                         const uint32_t key = valid ? ((packed >> (8 * s)) & 0xffu) : 0x100u + gi;
                         const unsigned int match = __match_any_sync(0xffffffffu, key);
@@ -872,8 +904,7 @@ data_pass_kernel(const PassArgs<double> a) {
         }
         // ---- write the within transform (coalesced) ---------------------------
         if (MODE == kFinal) {
-            for (int kl = tid; kl < kTileObs; kl += kDataThreads) {
-                if (kl >= nk) break;
+            for (int kl = tid; kl < nk; kl += kDataThreads) {
                 const int64_t k = k0 + kl;
                 const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
 #pragma unroll
