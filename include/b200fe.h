@@ -185,6 +185,62 @@ int b200fe_demean_sorted_noalloc(const double* d_v, int64_t n, int cols,
                                  const double* d_weights, double* d_out,
                                  void* stream);
 
+/* ---------------------------------------------------------------------------
+ * AKM/KSS two-way solver: Jacobi-PCG on the grounded worker-partialled firm
+ * Laplacian S = Df - B' Dw^{-1} B over the match (worker-firm pair) structure,
+ * the firm-side system of the leave-out (KSS) variance decomposition.  The
+ * ground firm is the last one (J - 1): its rhs entry is ignored and its
+ * solution entry is zero.  FP64 throughout; reductions have a fixed order, so
+ * results are bitwise reproducible on a device.
+ * ------------------------------------------------------------------------- */
+typedef struct b200fe_kss b200fe_kss;
+
+/* Builds a solver context on the current device from host arrays: matches
+ * m = 0..n_matches-1 sorted by worker (m_w non-decreasing) with firms m_f and
+ * weights m_c; w_ptr[N+1] / f_ptr[J+1] the worker and firm CSR offsets;
+ * f_matches[n_matches] the match ids in firm order; Dw[N], Df[J] the worker
+ * and firm weight sums; inv_diagS[J] the Jacobi preconditioner (0 at the
+ * ground).  The arrays are copied; the caller may free them on return.
+ * Replaces hdfe::akm::akm_cuda_create (include/hdfe/akm_kss_cuda.hpp:30-36,
+ * src/akm_kss_cuda.cu:330-380). */
+int b200fe_kss_create(int n_workers, int n_firms, const int32_t* m_w,
+                      const int32_t* m_f, const double* m_c, int64_t n_matches,
+                      const int64_t* w_ptr, const int64_t* f_ptr,
+                      const int64_t* f_matches, const double* Dw,
+                      const double* Df, const double* inv_diagS,
+                      b200fe_kss** out);
+/* Replaces akm_cuda_destroy (akm_kss_cuda.hpp:38). */
+void b200fe_kss_destroy(b200fe_kss* kss);
+const char* b200fe_kss_last_error(const b200fe_kss* kss);
+/* Largest nb of b200fe_kss_solve_multi.  Replaces akm_cuda_max_lanes
+ * (akm_kss_cuda.hpp:62-64). */
+int b200fe_kss_max_lanes(void);
+/* Page-locked host buffer of nb * J doubles owned by the context (NULL if
+ * pinned memory is unavailable); valid until a larger nb is requested or the
+ * context is destroyed.  It may serve as both rhs_pack and z_pack.
+ * Replaces akm_cuda_pack_buffer (akm_kss_cuda.hpp:66-76). */
+double* b200fe_kss_pack_buffer(b200fe_kss* kss, int nb);
+/* nb independent grounded solves S z_l = rhs_l, lane-major packs (lane l at
+ * offset l*J); x0 = 0; lane l stops when ||r_l||^2 <= tol^2 ||rhs_l||^2
+ * (rhs with its ground entry zeroed) and iters_out[l] receives its
+ * iteration count, or -1 (its z zeroed) when it does not converge within
+ * max_iter or its curvature p'Sp is not positive and finite.  Returns
+ * B200FE_OK (individual lane failures are reported per lane) or an error
+ * status.  rhs_pack and z_pack may be the same buffer.
+ * Replaces akm_cuda_solve_S_multi (akm_kss_cuda.hpp:49-60,
+ * src/akm_kss_cuda.cu:530-650). */
+int b200fe_kss_solve_multi(b200fe_kss* kss, const double* rhs_pack, double* z_pack,
+                           int nb, double tol, int max_iter, int* iters_out);
+/* One solve; *iterations receives the count.  Returns B200FE_OK,
+ * B200FE_NOT_CONVERGED (z zeroed) or an error status.
+ * Replaces akm_cuda_solve_S (akm_kss_cuda.hpp:40-44, src/akm_kss_cuda.cu:655-700). */
+int b200fe_kss_solve(b200fe_kss* kss, const double* rhs, double* z, double tol,
+                     int max_iter, int* iterations);
+/* Stable ascending sort of host uint64 keys: order_out[i] is the input row of
+ * the i-th smallest key, equal keys in input order.
+ * Replaces akm_cuda_stable_sort_u64 (akm_kss_cuda.hpp:21-28). */
+int b200fe_stable_sort_u64(const uint64_t* keys, int64_t* order_out, int64_t n);
+
 #ifdef __cplusplus
 }
 #endif

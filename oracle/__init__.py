@@ -134,6 +134,10 @@ def rlib(path: Path = REF_SO) -> ctypes.CDLL:
         lib.xref_fit.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, _vp, P(XrefOptions), _vp,
                                  _vp, P(_int), P(_dbl), ctypes.c_char_p, _int]
         lib.xref_fit.restype = _int
+        if hasattr(lib, "xref_akm_kss"):
+            lib.xref_akm_kss.argtypes = [_vp, _vp, _vp, _i64, _vp, ctypes.c_uint64, _dbl, _vp, P(_int),
+                                         P(ctypes.c_longlong), ctypes.c_char_p, _int]
+            lib.xref_akm_kss.restype = _int
         _rlib[path] = lib
     return _rlib[path]
 
@@ -234,3 +238,35 @@ def ref_fit(y, X, fes, weights=None, cluster=None, *, tol=1e-8,
             "num_singletons": info[4], "gpu_status_code": info[6],
             "abs_residual_rel": dinfo[0], "rss": dinfo[1],
             "r2_within": dinfo[2], "df_a": dinfo[3]}
+
+
+LEVERAGE = {"auto": 0, "exact": 1, "jla": 2}
+
+
+def ref_akm_kss(y, worker, firm, *, leverages="auto", jla_draws=0, seed=20260705, cg_tol=1e-10,
+                direct_max_firms=-1, use_gpu=False, threads=0, cg_max_iter=0, lib_path=REF_SO):
+    """The reference's hdfe::akm::akm_kss_decompose (include/hdfe/akm_kss.hpp:227-233)
+    on raw worker/firm ids, no controls.  use_gpu routes its PCG solves to the
+    CUDA backend the library was linked with (only the ref_b200 build has one)."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    w = np.ascontiguousarray(worker, dtype=np.int32)
+    f = np.ascontiguousarray(firm, dtype=np.int32)
+    opts = np.array([LEVERAGE[leverages], jla_draws, direct_max_firms, int(use_gpu), threads,
+                     cg_max_iter], dtype=np.int32)
+    out = np.zeros(16)
+    info = (_int * 8)()
+    iters = ctypes.c_longlong(0)
+    err = ctypes.create_string_buffer(512)
+    rc = rlib(lib_path).xref_akm_kss(y.ctypes.data, w.ctypes.data, f.ctypes.data, len(y),
+                                    opts.ctypes.data, seed, cg_tol, out.ctypes.data, info,
+                                    ctypes.byref(iters), err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    names = ["var_alpha", "var_psi", "cov_alpha_psi"]
+    return {"plugin": dict(zip(names, out[0:3])), "agsu": dict(zip(names, out[3:6])),
+            "kss": dict(zip(names, out[6:9])), "var_y": out[9], "sigma2_ho": out[10],
+            "mean_pii": out[11], "max_pii": out[12], "n_obs": int(out[13]),
+            "n_workers": info[0], "n_firms": info[1], "n_matches": info[2],
+            "gpu_used": bool(info[3]), "gpu_status_code": info[4], "solver_direct": bool(info[5]),
+            "converged": bool(info[6]), "jla_draws_used": info[7],
+            "solver_iterations": int(iters.value)}

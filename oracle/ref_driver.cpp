@@ -10,6 +10,7 @@
 //   xref_absorb       -> hdfe::detail::absorb_fixed_effects_v6  (src/fe_absorption.cpp:8750)
 //   xref_partial_out  -> hdfe::v11::HdfeRegressorV11::partial_out (src/hdfe_regressor_v11.cpp:10275)
 //   xref_fit          -> hdfe::v11::HdfeRegressorV11::fit         (src/hdfe_regressor_v11.cpp:7522)
+//   xref_akm_kss      -> hdfe::akm::akm_kss_decompose              (include/hdfe/akm_kss.hpp:227-233)
 // Every entry point catches all exceptions and returns a nonzero status with
 // the message copied into err (the reference's own fail-closed contract).
 
@@ -25,6 +26,7 @@
 #include "fe_absorption.hpp"
 #include "fe_absorption_cuda.hpp"
 #include "hdfe/hdfe_regressor.hpp"
+#include "hdfe/akm_kss.hpp"
 #include "hdfe/hdfe_regressor_v11.hpp"
 
 namespace {
@@ -225,6 +227,61 @@ int xref_fit(const double* y, const double* X, int64_t n, int k,
         dinfo[1] = res.rss;
         dinfo[2] = res.r2_within;
         dinfo[3] = res.df_a;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+// AKM + leave-out decomposition.  opts (ints): [0] leverage method (0 auto,
+// 1 exact, 2 jla), [1] jla_draws, [2] direct_max_firms (-1: library default),
+// [3] use_gpu, [4] num_threads, [5] cg_max_iter; seed and cg_tol as given.
+// out (doubles, 16): plugin var_alpha, var_psi, cov; agsu (3); kss (3); var_y;
+// sigma2_ho; mean_pii; max_pii; n_obs of the leave-out sample.
+// info (ints, 8): [0] workers, [1] firms, [2] matches, [3] gpu_used,
+// [4] gpu_status_code, [5] solver_direct, [6] converged, [7] jla_draws_used.
+// iters_out: total PCG iterations.
+int xref_akm_kss(const double* y, const int32_t* worker, const int32_t* firm, int64_t n,
+                 const int* opts, uint64_t seed, double cg_tol, double* out, int* info,
+                 long long* iters_out, char* err, int err_len) {
+    try {
+        const VectorXd yv = Map<const VectorXd>(y, n);
+        VectorXi wv(n), fv(n);
+        for (int64_t i = 0; i < n; ++i) {
+            wv[i] = worker[i];
+            fv[i] = firm[i];
+        }
+        hdfe::akm::AkmOptions o;
+        o.leverage_method = opts[0] == 1   ? hdfe::akm::LeverageMethod::Exact
+                            : opts[0] == 2 ? hdfe::akm::LeverageMethod::Jla
+                                           : hdfe::akm::LeverageMethod::Auto;
+        if (opts[1] > 0) o.jla_draws = opts[1];
+        if (opts[2] >= 0) o.direct_max_firms = opts[2];
+        o.use_gpu = opts[3] != 0;
+        o.num_threads = opts[4];
+        o.cg_max_iter = opts[5];
+        o.seed = seed;
+        if (cg_tol > 0.0) o.cg_tol = cg_tol;
+        const hdfe::akm::AkmKssResult r = hdfe::akm::akm_kss_decompose(yv, wv, fv, nullptr, o);
+        const double vals[16] = {r.plugin.var_alpha, r.plugin.var_psi, r.plugin.cov_alpha_psi,
+                                 r.agsu.var_alpha,   r.agsu.var_psi,   r.agsu.cov_alpha_psi,
+                                 r.kss.var_alpha,    r.kss.var_psi,    r.kss.cov_alpha_psi,
+                                 r.var_y,            r.sigma2_ho,      r.mean_pii,
+                                 r.max_pii,          static_cast<double>(r.sample.n_obs), 0.0, 0.0};
+        std::memcpy(out, vals, sizeof(vals));
+        info[0] = r.sample.n_workers;
+        info[1] = r.sample.n_firms;
+        info[2] = static_cast<int>(r.sample.n_matches);
+        info[3] = r.gpu_used ? 1 : 0;
+        info[4] = r.gpu_status_code;
+        info[5] = r.solver_direct ? 1 : 0;
+        info[6] = r.converged ? 1 : 0;
+        info[7] = r.jla_draws_used;
+        *iters_out = r.solver_iterations;
         return 0;
     } catch (const std::exception& e) {
         set_err(err, err_len, e.what());

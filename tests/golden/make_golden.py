@@ -14,6 +14,16 @@ For each case it stores, in <case>.npz:
   * the reference's result at tol 1e-8 (reghdfe-comparable): iterations,
     converged, abs_residual_rel;
   * the reference's HdfeRegressorV11::fit coefficients and standard errors.
+
+KSS cases (kss_<case>.npz) hold the inputs of an AKM leave-out decomposition
+and the reference's hdfe::akm::akm_kss_decompose results on them:
+  * kss_felsdvsimul: the reference's own example data (data/felsdvsimul.dta,
+    read from the reference tree; y, worker i, firm j), exact and JLA
+    (150 draws, seed 42) leverages; the reference documents these numbers
+    (docs/akm-kss.md:19-27) and the fixture records the values its CPU core
+    produces here;
+  * kss_akm20k: a seeded two-way AKM panel of this repository's generator,
+    JLA leverages (200 draws) on the reference's matrix-free PCG path.
 """
 
 from __future__ import annotations
@@ -132,7 +142,56 @@ def make(name: str) -> dict:
     return meta
 
 
+REF_DATA = Path("/root/reference/data/felsdvsimul.dta")
+KSS_KEYS = ("plugin", "agsu", "kss")
+
+
+def _kss_vec(r) -> np.ndarray:
+    return np.array([r[k][c] for k in KSS_KEYS for c in ("var_alpha", "var_psi", "cov_alpha_psi")])
+
+
+def kss_inputs(name: str):
+    if name == "felsdvsimul":
+        import pandas as pd
+        d = pd.read_stata(REF_DATA)
+        return (d["y"].to_numpy(np.float64), d["i"].to_numpy(np.int32), d["j"].to_numpy(np.int32))
+    if name == "akm20k":
+        p = ge.load_module("panels").akm_two_way(20_000, n_firms=300, n_years=10, seed=11,
+                                                  move_prob=0.15)
+        return p.y, p.fes[0].astype(np.int32), p.fes[1].astype(np.int32)
+    raise KeyError(name)
+
+
+def make_kss(name: str) -> dict:
+    y, w, f = kss_inputs(name)
+    runs = {}
+    if name == "felsdvsimul":
+        runs["exact"] = oracle.ref_akm_kss(y, w, f, leverages="exact", threads=1)
+        runs["jla"] = oracle.ref_akm_kss(y, w, f, leverages="jla", jla_draws=150, seed=42, threads=1)
+        runs["jla_pcg"] = oracle.ref_akm_kss(y, w, f, leverages="jla", jla_draws=150, seed=42,
+                                             direct_max_firms=0, threads=1)
+    else:
+        runs["jla_pcg"] = oracle.ref_akm_kss(y, w, f, leverages="jla", jla_draws=200, seed=20260705,
+                                             direct_max_firms=0, threads=1)
+    meta = {k: {"n_obs": r["n_obs"], "n_workers": r["n_workers"], "n_firms": r["n_firms"],
+                "n_matches": r["n_matches"], "solver_direct": r["solver_direct"],
+                "solver_iterations": r["solver_iterations"]} for k, r in runs.items()}
+    np.savez_compressed(OUT / f"kss_{name}.npz", y=y, worker=w, firm=f,
+                        **{f"{k}_components": _kss_vec(r) for k, r in runs.items()},
+                        **{f"{k}_pii": np.array([r["mean_pii"], r["max_pii"], r["sigma2_ho"]])
+                           for k, r in runs.items()},
+                        meta=np.array(json.dumps(meta)))
+    return meta
+
+
+KSS_CASES = ("felsdvsimul", "akm20k")
+
+
 if __name__ == "__main__":
+    if sys.argv[1:2] == ["kss"]:
+        for nm in sys.argv[2:] or KSS_CASES:
+            print(nm, json.dumps(make_kss(nm)))
+        sys.exit(0)
     names = sys.argv[1:] or list(CASES)
     for nm in names:
         m = make(nm)

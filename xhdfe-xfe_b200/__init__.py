@@ -16,5 +16,6 @@ from .absorber import (  # noqa: F401
     make_options,
     partial_out,
 )
+from .kss import KssSolver, kss_system, max_lanes, stable_sort_u64  # noqa: F401
 
 __version__ = "1.0.0"

@@ -41,6 +41,14 @@ EXPORTED_SYMBOLS = (
     "b200fe_demean_raw",
     "b200fe_fe_recovery_max_delta",
     "b200fe_demean_sorted_noalloc",
+    "b200fe_kss_create",
+    "b200fe_kss_destroy",
+    "b200fe_kss_last_error",
+    "b200fe_kss_max_lanes",
+    "b200fe_kss_pack_buffer",
+    "b200fe_kss_solve_multi",
+    "b200fe_kss_solve",
+    "b200fe_stable_sort_u64",
 )
 
 
@@ -126,6 +134,23 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.b200fe_fe_recovery_max_delta.restype = c_int
     lib.b200fe_demean_sorted_noalloc.argtypes = [vp, i64, c_int, vp, ctypes.c_int32, vp, vp, vp]
     lib.b200fe_demean_sorted_noalloc.restype = c_int
+    lib.b200fe_kss_create.argtypes = [c_int, c_int, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp,
+                                      ctypes.POINTER(vp)]
+    lib.b200fe_kss_create.restype = c_int
+    lib.b200fe_kss_destroy.argtypes = [vp]
+    lib.b200fe_kss_destroy.restype = None
+    lib.b200fe_kss_last_error.argtypes = [vp]
+    lib.b200fe_kss_last_error.restype = ctypes.c_char_p
+    lib.b200fe_kss_max_lanes.argtypes = []
+    lib.b200fe_kss_max_lanes.restype = c_int
+    lib.b200fe_kss_pack_buffer.argtypes = [vp, c_int]
+    lib.b200fe_kss_pack_buffer.restype = vp
+    lib.b200fe_kss_solve_multi.argtypes = [vp, vp, vp, c_int, ctypes.c_double, c_int, vp]
+    lib.b200fe_kss_solve_multi.restype = c_int
+    lib.b200fe_kss_solve.argtypes = [vp, vp, vp, ctypes.c_double, c_int, ctypes.POINTER(c_int)]
+    lib.b200fe_kss_solve.restype = c_int
+    lib.b200fe_stable_sort_u64.argtypes = [vp, vp, i64]
+    lib.b200fe_stable_sort_u64.restype = c_int
     if path is None:
         _LIB = lib
     return lib

@@ -10,7 +10,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
-SOURCES = ["b200fe.cu", "noalloc.cu"]
+SOURCES = ["b200fe.cu", "noalloc.cu", "kss.cu"]
 HEADERS = ["kernels.cuh", "setup_kernels.cuh"]
 OUT = HERE / "libb200fe.so"
 

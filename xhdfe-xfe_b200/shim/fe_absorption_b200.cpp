@@ -22,11 +22,12 @@
 // return true with converged=false on non-convergence; never throw.  Features
 // this library does not provide yet return false, so the reference fails
 // closed rather than silently using another path: heterogeneous slopes, saved
-// fixed effects (retain_fixed_effects), group/individual FEs, and the AKM/KSS
-// GPU solver (akm_cuda_available() is false, so AKM stays on the CPU).
+// fixed effects (retain_fixed_effects) and group/individual FEs.  The AKM/KSS
+// solver (akm_cuda_*) runs on the library's batched PCG (b200fe_kss_*).
 
 #include <Eigen/Dense>
 
+#include <climits>
 #include <cstdint>
 #include <vector>
 
@@ -184,22 +185,64 @@ void cuda_cert_shadow_abort(CudaCertShadowHandle*) {}
 
 namespace akm {
 
-// The KSS leverage solver is not provided by this library yet: the AKM code
-// checks akm_cuda_available() first and then stays on its CPU solver.
-bool akm_cuda_available() { return false; }
-bool akm_cuda_stable_sort_u64(const std::uint64_t*, std::int64_t*, std::size_t) { return false; }
-AkmCudaContext* akm_cuda_create(int, int, const int*, const int*, const double*, std::size_t,
-                                const std::int64_t*, const std::int64_t*, const std::int64_t*,
-                                const double*, const double*, const double*) {
-    return nullptr;
+// The AKM/KSS firm-system solver (akm_kss_cuda.hpp:17-74) over the B200
+// batched Jacobi-PCG (b200fe_kss_*): the same grounded system, stopping rule,
+// per-lane iteration counts and failure reporting.
+struct AkmCudaContext {
+    b200fe_kss* kss = nullptr;
+};
+
+bool akm_cuda_available() { return b200fe_device_available() != 0; }
+
+bool akm_cuda_stable_sort_u64(const std::uint64_t* keys, std::int64_t* order_out, std::size_t n) {
+    if (n > static_cast<std::size_t>(INT32_MAX)) return false;
+    return b200fe_stable_sort_u64(keys, order_out, static_cast<int64_t>(n)) == B200FE_OK;
 }
-void akm_cuda_destroy(AkmCudaContext*) {}
-int akm_cuda_solve_S(AkmCudaContext*, const double*, double*, double, int) { return -1; }
-int akm_cuda_solve_S_multi(AkmCudaContext*, const double*, double*, int, double, int, int*) {
-    return -1;
+
+AkmCudaContext* akm_cuda_create(int n_workers, int n_firms, const int* m_w, const int* m_f,
+                                const double* m_c, std::size_t n_matches,
+                                const std::int64_t* w_ptr, const std::int64_t* f_ptr,
+                                const std::int64_t* f_matches, const double* Dw,
+                                const double* Df, const double* inv_diagS) {
+    try {
+        b200fe_kss* k = nullptr;
+        if (b200fe_kss_create(n_workers, n_firms, m_w, m_f, m_c, static_cast<int64_t>(n_matches),
+                              w_ptr, f_ptr, f_matches, Dw, Df, inv_diagS, &k) != B200FE_OK)
+            return nullptr;
+        AkmCudaContext* c = new AkmCudaContext;
+        c->kss = k;
+        return c;
+    } catch (...) {
+        return nullptr;
+    }
 }
-int akm_cuda_max_lanes() { return 0; }
-double* akm_cuda_pack_buffer(AkmCudaContext*, int) { return nullptr; }
+
+void akm_cuda_destroy(AkmCudaContext* ctx) {
+    if (!ctx) return;
+    b200fe_kss_destroy(ctx->kss);
+    delete ctx;
+}
+
+int akm_cuda_solve_S(AkmCudaContext* ctx, const double* rhs, double* z, double tol, int max_iter) {
+    if (!ctx) return -1;
+    int it = -1;
+    return b200fe_kss_solve(ctx->kss, rhs, z, tol, max_iter, &it) == B200FE_OK ? it : -1;
+}
+
+int akm_cuda_solve_S_multi(AkmCudaContext* ctx, const double* rhs_pack, double* z_pack, int nb,
+                           double tol, int max_iter, int* iters_out) {
+    if (!ctx) return -1;
+    return b200fe_kss_solve_multi(ctx->kss, rhs_pack, z_pack, nb, tol, max_iter, iters_out) ==
+                   B200FE_OK
+               ? 0
+               : -1;
+}
+
+int akm_cuda_max_lanes() { return b200fe_kss_max_lanes(); }
+
+double* akm_cuda_pack_buffer(AkmCudaContext* ctx, int nb) {
+    return ctx ? b200fe_kss_pack_buffer(ctx->kss, nb) : nullptr;
+}
 
 }  // namespace akm
 }  // namespace hdfe
