@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     return ap.parse_args()
 
@@ -166,6 +168,25 @@ def cpu_baseline(sample_n: int, threads: int):
         "sample_seconds": dt, "sample_rows": p.n, "iterations": r["iterations"],
         "converged": r["converged"],
     }
+
+
+def reference_gpu(panel, threads: int):
+    """The reference's own CUDA backend (src/fe_absorption_cuda.cu, built for
+    sm_100a by oracle/Makefile target ref_cuda) on the same panel, through the
+    reference's absorb_fixed_effects_v6 with host arrays (its H2D/D2H inside):
+    comparable to this arm's e2e number."""
+    import oracle
+    if not oracle.REF_CUDA_SO.exists():
+        return None
+    t0 = time.perf_counter()
+    r = oracle.ref_absorb(panel.y, panel.X, panel.fes, None, tol=1e-8,
+                          tolerance_mode="reghdfe-comparable", method="auto", threads=threads,
+                          gpu_backend="cuda", lib_path=oracle.REF_CUDA_SO)
+    dt = time.perf_counter() - t0
+    return {"value": dt, "unit": UNIT, "kind": "reference CUDA backend built for sm_100a, host arrays",
+            "iterations": r["iterations"], "converged": r["converged"],
+            "precision_certified": r["precision_certified"],
+            "abs_residual_rel": r["abs_residual_rel"], "gpu_status_code": r["gpu_status_code"]}
 
 
 def run_reference(args):
@@ -333,6 +354,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_sample, os.cpu_count() or 1)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu(panel, os.cpu_count() or 1)
 
     if rank == 0:
         line = {
@@ -345,7 +369,7 @@ def run_ours(args):
                        "n_obs_after_singleton_drop": n, "columns": cols,
                        "fe_dims": ["worker", "firm", "year"], "levels": panel.levels,
                        "tol": 1e-8, "precision": args.precision,
-                       "l2_policy": "inputs larger than L2 (5.2 GB of columns per step)",
+                       "l2_policy": f"inputs larger than L2 ({n * cols * 8 / 1e9:.1f} GB of columns per step)",
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": launches, "library_calls": lib_calls,
             "iterations": r_last.iterations, "outer_iterations": r_last.outer_iterations,
@@ -355,7 +379,7 @@ def run_ours(args):
             "setup_ms": r_last.setup_ms, "solve_ms": r_last.solve_ms,
             "roofline": roofline, "profile": prof, "clocks": clocks,
             "fp64_plain": fp64,
-            "e2e": e2e, "cpu_baseline": cpu, "generate_s": gen_s,
+            "e2e": e2e, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "generate_s": gen_s,
         }
         print(json.dumps(line))
     absorber.close()

@@ -59,8 +59,10 @@ typedef struct b200fe_options {
                               1 reghdfe-comparable (tol_eff = min(tol, 1e-9)), 2 strict (1)  */
     int max_outer;         /* MIXED: cap on refinement rounds (default 12)                    */
     int profile;           /* 1: time every kernel category with CUDA events (default 0)      */
-    int pass_kernel;       /* CG matvec pass: 0 auto (run-level when at most one FE dim
-                              besides the largest has over 64 levels), 1 general tile pass  */
+    int pass_kernel;       /* CG matvec pass: 0 auto (block level when at most one large and
+                              one small FE dim besides the largest; with a small dim, its
+                              dense coupling rows when they are small), 1 general tile pass,
+                              2 block level without the dense coupling                        */
 } b200fe_options;
 
 /* Kernel categories of the profile arrays in b200fe_result. */

@@ -6,7 +6,11 @@ Python front of the two checkers built by oracle/Makefile:
   absorber (demean_oracle.c): Irons-Tuck MAP with the honest stop, a tight
   projection for pinning, and the normal-equation certificate;
 * ``_ref/libxhdfe_ref.so``  -- the reference's own CPU core compiled from its
-  unmodified sources, behind ref_driver.cpp.
+  unmodified sources, behind ref_driver.cpp;
+* ``_ref/libxhdfe_ref_cuda.so`` -- the same core with the reference's own CUDA
+  backend compiled for sm_100a (target ``ref_cuda``), timed as the GPU bar;
+* ``_ref/libxhdfe_ref_b200.so`` -- the same core over this repository's
+  reference-side binding (the drop-in check).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this package, and only as the checker (never as the measured or shipped path).
@@ -25,6 +29,8 @@ ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libxhdfe_ref.so"
 # the reference core built with -DHDFE_USE_CUDA over the B200 library (drop-in check)
 REF_B200_SO = HERE / "_ref" / "libxhdfe_ref_b200.so"
+# the reference core with its own CUDA backend built for sm_100a (GPU bar)
+REF_CUDA_SO = HERE / "_ref" / "libxhdfe_ref_cuda.so"
 
 _vp, _i64, _int, _dbl = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double
 _olib = None

@@ -45,6 +45,11 @@ struct LargeDim {
     int32_t *chunk_grp = nullptr, *chunk_beg = nullptr, *chunk_end = nullptr;
     uint8_t* chunk_whole = nullptr;
     int32_t *multi_grp = nullptr, *multi_c0 = nullptr, *multi_c1 = nullptr;
+    // second reduction level for groups of more than kFinFewParts chunks:
+    // super-chunks of at most kSuperParts chunk partials
+    int64_t nsup = 0;
+    int32_t *multi_s0 = nullptr, *multi_s1 = nullptr;  // [nmulti] super range (empty: none)
+    int32_t *sup_c0 = nullptr, *sup_c1 = nullptr;      // [nsup] chunk range of each super-chunk
 };
 
 struct Structure {
@@ -90,6 +95,14 @@ struct Structure {
     float* block_w32 = nullptr;
     int64_t nblocks = 0;
     double* small_w = nullptr;  // [SG] level weights of the small dim
+    // dense coupling of the small dim (block level, one small dim): the CG
+    // matvec then runs the block pass over the large dim only and adds
+    // C_fy x_small, C_fy' x_f and C_yy x_small
+    bool coupled = false;
+    int SGP = 0;              // row stride of cfy: SG rounded up to 4 (padding zero)
+    double* cfy64 = nullptr;  // [G_f][SGP]
+    float* cfy32 = nullptr;
+    double* cyy = nullptr;    // [SG][SG]
 };
 
 constexpr int32_t kChunkRuns = 64;
@@ -274,18 +287,6 @@ int cub_sort_pairs(b200fe_context* ctx, const int32_t* keys_in, int32_t* keys_ou
     return B200FE_OK;
 }
 
-int cub_segmented_sum(b200fe_context* ctx, const double* in, double* out, int32_t nseg,
-                      const int32_t* off) {
-    size_t tmp = 0;
-    B_TRY(cub::DeviceSegmentedReduce::Sum(nullptr, tmp, in, out, nseg, off, off + 1,
-                                          ctx->stream));
-    void* t;
-    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
-    B_TRY(cub::DeviceSegmentedReduce::Sum(t, tmp, in, out, nseg, off, off + 1, ctx->stream));
-    ++ctx->lib_calls;
-    return B200FE_OK;
-}
-
 int sync_read_int(b200fe_context* ctx, const int32_t* dptr, int count, int* host) {
     B_TRY(cudaMemcpyAsync(ctx->h_pinned, dptr, sizeof(int) * count, cudaMemcpyDeviceToHost,
                           ctx->stream));
@@ -364,13 +365,10 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
     st.gp = gp;
 
     // primary segments
-    int32_t *counts, *seg_off;
-    B_CHECK(get_buf(ctx, "counts_p", static_cast<size_t>(G[p]) + 1, &counts));
+    int32_t* seg_off;
     B_CHECK(get_buf(ctx, "seg_off", static_cast<size_t>(G[p]) + 1, &seg_off));
-    B_TRY(cudaMemsetAsync(counts, 0, sizeof(int32_t) * (static_cast<size_t>(G[p]) + 1), s));
-    histogram_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(gp, n, counts);
+    segment_offsets_kernel<<<grid_for(ctx, n + 1, T256), T256, 0, s>>>(gp, n, G[p], seg_off);
     B_LAUNCHED();
-    B_CHECK(cub_exclusive_sum(ctx, counts, seg_off, static_cast<int64_t>(G[p]) + 1));
     st.seg_off = seg_off;
 
     // weights in primary order, segment weight sums
@@ -495,13 +493,11 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         B_LAUNCHED();
         B_CHECK(cub_sort_pairs(ctx, run_grp, sorted_grp, riota, sorted_runs, nr, L.G));
         // group offsets over sorted runs
-        int32_t *gcount, *grp_off;
-        B_CHECK(get_buf(ctx, "gcount", static_cast<size_t>(L.G) + 1, &gcount));
+        int32_t* grp_off;
         B_CHECK(get_buf(ctx, "grp_off" + sfx, static_cast<size_t>(L.G) + 1, &grp_off));
-        B_TRY(cudaMemsetAsync(gcount, 0, sizeof(int32_t) * (static_cast<size_t>(L.G) + 1), s));
-        histogram_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(run_grp, nr, gcount);
+        segment_offsets_kernel<<<grid_for(ctx, static_cast<int64_t>(nr) + 1, T256), T256, 0, s>>>(
+            sorted_grp, nr, L.G, grp_off);
         B_LAUNCHED();
-        B_CHECK(cub_exclusive_sum(ctx, gcount, grp_off, static_cast<int64_t>(L.G) + 1));
         // run destinations and per-run diagonal terms
         B_CHECK(get_buf(ctx, "run_dest" + sfx, nr, &L.run_dest));
         double *cw, *ce, *cw_run;
@@ -513,8 +509,6 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
             sorted_runs, nr, run_start, n, run_seg, st.wp64, st.inv_wp, L.run_dest, cw, ce,
             cw_run);
         B_LAUNCHED();
-        B_CHECK(cub_segmented_sum(ctx, cw, Wall + st.lbase[l], L.G, grp_off));
-        B_CHECK(cub_segmented_sum(ctx, ce, Eall + st.lbase[l], L.G, grp_off));
         // chunk list
         int32_t *nch, *ch_off, *mflag, *midx;
         B_CHECK(get_buf(ctx, "nch", static_cast<size_t>(L.G) + 1, &nch));
@@ -545,7 +539,64 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
             grp_off, L.G, kChunkRuns, ch_off, L.chunk_grp, L.chunk_beg, L.chunk_end,
             L.chunk_whole, midx, L.multi_grp, L.multi_c0, L.multi_c1);
         B_LAUNCHED();
+        // diagonal terms W_g, E_g of the groups over the chunk list (balanced
+        // however skewed the group sizes are)
+        {
+            double* part2;
+            B_CHECK(get_buf(ctx, "wsum_part", static_cast<size_t>(L.nchunks) * 2, &part2));
+            chunk_wsum_kernel<<<grid_for(ctx, L.nchunks, T256), T256, 0, s>>>(
+                L.nchunks, L.chunk_grp, L.chunk_beg, L.chunk_end, L.chunk_whole, cw, ce,
+                Wall + st.lbase[l], Eall + st.lbase[l], part2);
+            B_LAUNCHED();
+            if (L.nmulti > 0) {
+                multi_wsum_kernel<<<static_cast<int>(std::min<int64_t>(
+                                        L.nmulti, static_cast<int64_t>(ctx->num_sms) * 8)),
+                                    256, 0, s>>>(L.nmulti, L.multi_grp, L.multi_c0, L.multi_c1, part2,
+                                                 Wall + st.lbase[l], Eall + st.lbase[l]);
+                B_LAUNCHED();
+            }
+        }
+        // super-chunks: a group with many chunks (Zipf sizes: one firm may own
+        // 10%+ of the runs) has its chunk partials summed in slices of
+        // kSuperParts by many lane groups before finalize adds the slices
+        L.nsup = 0;
+        if (L.nmulti > 0) {
+            std::vector<int32_t> c0(L.nmulti), c1(L.nmulti);
+            B_TRY(cudaMemcpyAsync(c0.data(), L.multi_c0, sizeof(int32_t) * L.nmulti, cudaMemcpyDeviceToHost, s));
+            B_TRY(cudaMemcpyAsync(c1.data(), L.multi_c1, sizeof(int32_t) * L.nmulti, cudaMemcpyDeviceToHost, s));
+            B_TRY(cudaStreamSynchronize(s));
+            std::vector<int32_t> s0(L.nmulti), s1(L.nmulti), sb, se;
+            for (int64_t r = 0; r < L.nmulti; ++r) {
+                s0[r] = s1[r] = static_cast<int32_t>(sb.size());
+                if (c1[r] - c0[r] <= kFinFewParts) continue;
+                for (int32_t c = c0[r]; c < c1[r]; c += kSuperParts) {
+                    sb.push_back(c);
+                    se.push_back(std::min(c1[r], c + kSuperParts));
+                }
+                s1[r] = static_cast<int32_t>(sb.size());
+            }
+            L.nsup = static_cast<int64_t>(sb.size());
+            B_CHECK(get_buf(ctx, "multi_s0" + sfx, L.nmulti, &L.multi_s0));
+            B_CHECK(get_buf(ctx, "multi_s1" + sfx, L.nmulti, &L.multi_s1));
+            B_CHECK(get_buf(ctx, "sup_c0" + sfx, std::max<int64_t>(L.nsup, 1), &L.sup_c0));
+            B_CHECK(get_buf(ctx, "sup_c1" + sfx, std::max<int64_t>(L.nsup, 1), &L.sup_c1));
+            B_TRY(cudaMemcpyAsync(L.multi_s0, s0.data(), sizeof(int32_t) * L.nmulti, cudaMemcpyHostToDevice, s));
+            B_TRY(cudaMemcpyAsync(L.multi_s1, s1.data(), sizeof(int32_t) * L.nmulti, cudaMemcpyHostToDevice, s));
+            if (L.nsup > 0) {
+                B_TRY(cudaMemcpyAsync(L.sup_c0, sb.data(), sizeof(int32_t) * L.nsup, cudaMemcpyHostToDevice, s));
+                B_TRY(cudaMemcpyAsync(L.sup_c1, se.data(), sizeof(int32_t) * L.nsup, cudaMemcpyHostToDevice, s));
+            }
+            B_TRY(cudaStreamSynchronize(s));  // the host vectors leave scope
+        }
     }
+
+    // the dense small-dim coupling of the CG matvec (block level, one small
+    // dim with at most kCoupleMaxSG levels, coupling rows no larger than the
+    // run rows): its setup also yields the exact small-dim diagonal
+    const bool block_ok = st.GR > 0 && st.nL <= 1 && st.nS <= 1;
+    const bool will_couple =
+        block_ok && ctx->pass_kernel == 0 && st.nS == 1 && st.SG <= kCoupleMaxSG &&
+        (st.nL == 0 || static_cast<int64_t>(st.L[0].G) * st.SG <= st.L[0].nruns * 16);
 
     // small dims: packed ids and diagonal
     if (st.nS > 0) {
@@ -555,6 +606,8 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         B_CHECK(get_buf(ctx, "sid", n, &st.sid));
         pack_small_kernel<<<grid_for(ctx, n, T256), T256, 0, s>>>(pa, st.pord, n, st.sid);
         B_LAUNCHED();
+    }
+    if (st.nS > 0 && !will_couple) {
         const int nb = ctx->num_sms * 4;
         double *part, *sw, *se;
         B_CHECK(get_buf(ctx, "small_part", static_cast<size_t>(nb) * kMaxSmall * kSmallLevels * 2,
@@ -576,7 +629,7 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
     if (st.nS > 0) st.small_w = Wall + st.sbase[0];
 
     // blocks and packed metadata of the block-level pass
-    st.block_ok = st.GR > 0 && st.nL <= 1 && st.nS <= 1;
+    st.block_ok = block_ok;
     if (st.block_ok) {
         int32_t *bflags, *bid, *bstart;
         B_CHECK(get_buf(ctx, "tmp_n_a", n, &bflags));
@@ -613,6 +666,68 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
             lg ? st.L[0].nruns : 0, lg ? st.L[0].cw_run : nullptr, bid, nb, n, st.seg_meta,
             st.run_meta, st.run_w64, st.run_w32);
         B_LAUNCHED();
+        // dense coupling of the small dim, when its rows are cheaper to stream
+        // than one more pass over the runs
+        const int64_t SG = st.SG;
+        st.coupled = will_couple;
+        if (st.coupled) {
+            st.SGP = static_cast<int>((SG + 3) & ~int64_t(3));
+            const int64_t SGP = st.SGP;
+            if (lg) {
+                const LargeDim& L = st.L[0];
+                int32_t *sorted_runs, *run_seg;
+                B_CHECK(get_buf(ctx, "sorted_runs", L.nruns, &sorted_runs));
+                B_CHECK(get_buf(ctx, "run_seg", L.nruns, &run_seg));
+                double* cpart;
+                B_CHECK(get_buf(ctx, "cfy64", static_cast<size_t>(L.G) * SGP, &st.cfy64));
+                B_CHECK(get_buf(ctx, "cfy32", static_cast<size_t>(L.G) * SGP, &st.cfy32));
+                B_CHECK(get_buf(ctx, "cfy_part", static_cast<size_t>(L.nchunks) * SGP, &cpart));
+                const size_t fsmem = static_cast<size_t>(kCoupleWarps) * 32 * SG * sizeof(double);
+                B_TRY(cudaFuncSetAttribute(coupling_fy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(fsmem)));
+                int fps = 1;
+                B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fps, coupling_fy_kernel,
+                                                                    kCoupleWarps * 32, fsmem));
+                const int fgrid = static_cast<int>(std::max<int64_t>(
+                    1, std::min<int64_t>((L.nchunks + kCoupleWarps - 1) / kCoupleWarps,
+                                         static_cast<int64_t>(ctx->num_sms) * std::max(fps, 1))));
+                coupling_fy_kernel<<<fgrid, kCoupleWarps * 32, fsmem, s>>>(
+                    L.nchunks, L.chunk_grp, L.chunk_beg, L.chunk_end, L.chunk_whole, sorted_runs,
+                    run_seg, st.run_meta, st.seg_meta, st.block_meta, st.block_w64, L.cw_run,
+                    st.inv_wp, st.SG, st.SGP, st.cfy64, cpart);
+                B_LAUNCHED();
+                if (L.nmulti > 0) {
+                    coupling_fy_combine_kernel<<<static_cast<int>(std::min<int64_t>(
+                                                     L.nmulti, static_cast<int64_t>(ctx->num_sms) * 8)),
+                                                 256, 0, s>>>(L.nmulti, L.multi_grp, L.multi_c0,
+                                                              L.multi_c1, cpart, st.SGP, st.cfy64);
+                    B_LAUNCHED();
+                }
+                to_float_kernel<<<grid_for(ctx, static_cast<int64_t>(L.G) * SGP, T256), T256, 0, s>>>(
+                    st.cfy64, static_cast<int64_t>(L.G) * SGP, st.cfy32);
+                B_LAUNCHED();
+            }
+            const size_t ysmem = static_cast<size_t>(kCoupleYyWarps) * (SG * SG + SG + 32 * SG) * sizeof(double);
+            B_TRY(cudaFuncSetAttribute(coupling_yy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(ysmem)));
+            int yps = 1;
+            B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&yps, coupling_yy_kernel,
+                                                                kCoupleYyWarps * 32, ysmem));
+            const int ny = static_cast<int>(std::max<int64_t>(
+                1, std::min<int64_t>((static_cast<int64_t>(G[p]) + 32 * kCoupleYyWarps - 1) /
+                                         (32 * kCoupleYyWarps),
+                                     static_cast<int64_t>(ctx->num_sms) * std::max(yps, 1))));
+            double* ypart;
+            B_CHECK(get_buf(ctx, "cyy_part", static_cast<size_t>(ny) * (SG * SG + SG), &ypart));
+            B_CHECK(get_buf(ctx, "cyy", static_cast<size_t>(SG) * SG, &st.cyy));
+            coupling_yy_kernel<<<ny, kCoupleYyWarps * 32, ysmem, s>>>(G[p], st.seg_meta, st.run_meta,
+                                                                      st.block_meta, st.block_w64,
+                                                                      st.inv_wp, st.SG, ypart);
+            B_LAUNCHED();
+            coupling_yy_reduce_kernel<<<grid_for(ctx, SG * SG, T256), T256, 0, s>>>(
+                ypart, ny, st.SG, st.cyy, Wall + st.sbase[0], Eall + st.sbase[0]);
+            B_LAUNCHED();
+        }
     }
 
     if (st.GR > 0) {
@@ -650,6 +765,15 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
 // ---------------------------------------------------------------------------
 // Solver
 // ---------------------------------------------------------------------------
+constexpr int kRunBatch = 2;  // runs per load batch of run_pass_kernel
+
+template <typename T>
+const T* pick_prec(const float* f32, const double* f64);
+template <>
+const float* pick_prec<float>(const float* f32, const double*) { return f32; }
+template <>
+const double* pick_prec<double>(const float*, const double* f64) { return f64; }
+
 template <typename T>
 struct Work {
     T* R[kMaxLarge];
@@ -658,6 +782,7 @@ struct Work {
     double* gather_partial[kMaxLarge];
     double* fin_partial;
     double* chunk_partial[kMaxLarge];
+    double* super_partial[kMaxLarge];
     double* dot_out;
     unsigned int* ticket;
     int tile_grid, tile_smem;
@@ -665,6 +790,7 @@ struct Work {
     int run_grid, run_smem;  // block-level matvec grid/smem (0 when it does not apply)
     int long_grid, long_smem;
     int nbins_ctas;
+    int couple_grid;  // CTAs of coupling_xf_kernel (coupled matvec), <= nbins_ctas
     int gather_grid[kMaxLarge];
     int fin_grid;
     int64_t fin_rows;
@@ -712,8 +838,9 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     }
     wk.run_grid = 0;
     wk.run_smem = 0;
-    if (st.block_ok && ctx->pass_kernel == 0) {
-        wk.run_smem = static_cast<int>(block_smem_bytes<T>(CP, st.SG));
+    if (st.block_ok && (ctx->pass_kernel == 0 || ctx->pass_kernel == 2)) {
+        // the coupled matvec runs the pass without the small dim: no shared memory
+        wk.run_smem = st.coupled ? 0 : static_cast<int>(block_smem_bytes<T>(CP, st.SG));
         B_TRY(cudaFuncSetAttribute(block_pass_kernel<T, CQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    wk.run_smem));
         int rps = 1;
@@ -730,6 +857,11 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
         wk.long_grid = grid_for(ctx, groups * 32, kPassThreads, 4);
     }
     wk.nbins_ctas = std::max(std::max(wk.tile_grid, wk.run_grid), wk.data_grid) + wk.long_grid;
+    wk.couple_grid = 0;
+    if (st.coupled && wk.run_grid > 0 && st.nL == 1)
+        wk.couple_grid = static_cast<int>(std::max<int64_t>(
+            1, std::min<int64_t>({static_cast<int64_t>(wk.nbins_ctas),
+                                  static_cast<int64_t>(ctx->num_sms) * 4, st.L[0].G})));
     B_CHECK(get_buf(ctx, tag + "bins", static_cast<size_t>(wk.nbins_ctas) * std::max(st.SG, 1) * CP,
                     &wk.bins_partial));
     B_CHECK(get_buf(ctx, tag + "colsq", static_cast<size_t>(wk.nbins_ctas) * CP, &wk.colsq_partial));
@@ -741,6 +873,8 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
                         &wk.gather_partial[l]));
         B_CHECK(get_buf(ctx, tag + "cpart" + sfx, static_cast<size_t>(st.L[l].nchunks) * CP,
                         &wk.chunk_partial[l]));
+        B_CHECK(get_buf(ctx, tag + "spart" + sfx, static_cast<size_t>(std::max<int64_t>(st.L[l].nsup, 1)) * CP,
+                        &wk.super_partial[l]));
     }
     wk.fin_rows = st.SG;
     for (int l = 0; l < st.nL; ++l) wk.fin_rows += st.L[l].nmulti;
@@ -831,6 +965,37 @@ int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, co
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
     const int slots = std::max(std::max(wk.tile_grid, wk.run_grid), wk.data_grid);
+    if (wk.run_grid > 0 && st.coupled) {
+        // large dim only over every segment, then C_fy' x_f into the bin partials
+        if (st.nL == 1) {
+            BlockArgs<T> r{};
+            r.Gp = st.G[st.p];
+            r.CP = CP;
+            r.has_large = 1;
+            r.has_small = 0;
+            r.SG = st.SG;
+            r.seg_meta = st.seg_meta;
+            r.inv_wp = st.inv_wp;
+            r.run_meta = st.run_meta;
+            r.run_w = run_w;
+            r.block_meta = st.block_meta;
+            r.block_w = block_w;
+            r.lbase = st.lbase[0];
+            r.sbase = st.sbase[0];
+            r.x = a.x;
+            r.R = wk.R[0];
+            r.bins_partial = wk.bins_partial;
+            r.bins_cta0 = 0;
+            r.all_segs = 1;
+            run_pass_kernel<T, CQ, kRunBatch><<<wk.run_grid, kBlockThreads, 0, ctx->stream>>>(r);
+            B_LAUNCHED();
+            coupling_xf_kernel<T, CQ><<<wk.couple_grid, 256, 0, ctx->stream>>>(
+                st.L[0].G, st.SG, st.SGP, pick_prec<T>(st.cfy32, st.cfy64), a.x + st.lbase[0] * CP,
+                wk.bins_partial);
+            B_LAUNCHED();
+        }
+        return B200FE_OK;
+    }
     if (wk.run_grid > 0) {
         BlockArgs<T> r{};
         r.Gp = st.G[st.p];
@@ -850,7 +1015,11 @@ int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, co
         r.R = st.nL == 1 ? wk.R[0] : nullptr;
         r.bins_partial = wk.bins_partial;
         r.bins_cta0 = 0;
-        block_pass_kernel<T, CQ><<<wk.run_grid, kBlockThreads, wk.run_smem, ctx->stream>>>(r);
+        r.all_segs = 0;
+        if (st.nL == 1 && st.nS == 0)  // runs only (two-way)
+            run_pass_kernel<T, CQ, kRunBatch><<<wk.run_grid, kBlockThreads, 0, ctx->stream>>>(r);
+        else
+            block_pass_kernel<T, CQ><<<wk.run_grid, kBlockThreads, wk.run_smem, ctx->stream>>>(r);
         B_LAUNCHED();
         if (st.nS > 0 && wk.run_grid < slots)
             B_TRY(cudaMemsetAsync(wk.bins_partial + static_cast<int64_t>(wk.run_grid) * st.SG * CP, 0,
@@ -895,7 +1064,7 @@ double gather_bytes(const Structure& st, int l, int CP, size_t tsize, bool dot) 
 template <typename T, int CQ>
 int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
                 int cat_gather = B200FE_PROF_GATHER, int cat_fin = B200FE_PROF_FINALIZE,
-                bool small_diag = false) {
+                bool small_diag = false, bool coupled = false) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
     const cudaStream_t s = ctx->stream;
@@ -912,9 +1081,22 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
         g.partial = wk.chunk_partial[l];
         g.dotv = dotv ? dotv + st.lbase[l] * CP : nullptr;
         g.dot_partial = wk.gather_partial[l];
+        if (coupled && l == 0) {  // + C_fy x_small (x is the matvec input, dotv)
+            g.cfy = pick_prec<T>(st.cfy32, st.cfy64);
+            g.xs = dotv + st.sbase[0] * CP;
+            g.SG = st.SG;
+            g.SGP = st.SGP;
+        }
         ProfScope ps(ctx, cat_gather, gather_bytes(st, l, CP, sizeof(T), dotv != nullptr));
-        run_gather_kernel<T, CQ><<<wk.gather_grid[l], kRowThreads, 0, s>>>(g);
+        const size_t gsmem = g.cfy ? static_cast<size_t>(st.SGP) * CP * sizeof(T) : 0;
+        run_gather_kernel<T, CQ><<<wk.gather_grid[l], kRowThreads, gsmem, s>>>(g);
         B_LAUNCHED();
+        if (st.L[l].nsup > 0) {
+            multi_super_kernel<<<grid_for(ctx, st.L[l].nsup * CP, kRowThreads), kRowThreads, 0, s>>>(
+                st.L[l].nsup, st.L[l].sup_c0, st.L[l].sup_c1, wk.chunk_partial[l], CP,
+                wk.super_partial[l]);
+            B_LAUNCHED();
+        }
     }
     FinalizeArgs<T> f{};
     f.CP = CP;
@@ -926,6 +1108,9 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
         f.multi_c0[l] = st.L[l].multi_c0;
         f.multi_c1[l] = st.L[l].multi_c1;
         f.partial[l] = wk.chunk_partial[l];
+        f.multi_s0[l] = st.L[l].multi_s0;
+        f.multi_s1[l] = st.L[l].multi_s1;
+        f.super_partial[l] = wk.super_partial[l];
         f.lbase[l] = st.lbase[l];
         f.gather_dot_partial[l] = wk.gather_partial[l];
         f.gather_ctas[l] = dotv ? wk.gather_grid[l] : 0;
@@ -933,8 +1118,11 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
     f.SG = st.SG;
     f.sgbase = st.nS > 0 ? st.sbase[0] : 0;
     f.bins_partial = wk.bins_partial;
-    f.nbins_ctas = wk.nbins_ctas;
-    f.small_diag = (small_diag && st.nS > 0) ? st.small_w : nullptr;
+    f.nbins_ctas = coupled ? wk.couple_grid : wk.nbins_ctas;
+    f.small_diag = (small_diag && st.nS > 0 && !coupled) ? st.small_w : nullptr;
+    f.small_dense = coupled ? st.cyy : nullptr;
+    f.cfy = (coupled && st.nL == 1) ? pick_prec<T>(st.cfy32, st.cfy64) : nullptr;
+    f.SGP = st.SGP;
     f.x = dotv;
     f.nrows = wk.fin_rows;
     f.out = out;
@@ -942,7 +1130,7 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
     f.dot_partial = wk.fin_partial;
     f.dot_out = dotv ? wk.dot_out : nullptr;
     f.ticket = wk.ticket;
-    double fb = static_cast<double>(wk.nbins_ctas) * st.SG * CP * 8.0;
+    double fb = static_cast<double>(f.nbins_ctas) * st.SG * CP * 8.0;
     for (int l = 0; l < st.nL; ++l) fb += static_cast<double>(st.L[l].nmulti) * CP * (8.0 + sizeof(T));
     fb += static_cast<double>(st.SG) * CP * sizeof(T);
     ProfScope ps(ctx, cat_fin, fb);
@@ -962,7 +1150,12 @@ int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w,
     a.x = x;
     {
         double pb;
-        if (wk.run_grid > 0) {  // block-level pass: per segment, run and block
+        if (wk.run_grid > 0 && st.coupled) {  // large-dim runs + dense coupling rows
+            pb = static_cast<double>(st.G[st.p]) * 16.0;
+            if (st.nL == 1)
+                pb += static_cast<double>(st.L[0].nruns) * (16.0 + sizeof(T) + CP * double(sizeof(T))) +
+                      static_cast<double>(st.L[0].G) * (CP + st.SG) * double(sizeof(T));
+        } else if (wk.run_grid > 0) {  // block-level pass: per segment, run and block
             pb = static_cast<double>(st.G[st.p]) * 16.0 + static_cast<double>(st.GR) * CP * sizeof(T) +
                  static_cast<double>(st.nblocks) * (8.0 + (st.weighted ? sizeof(T) : 0.0));
             const int64_t npr = st.nL == 1 ? st.L[0].nruns : st.G[st.p];
@@ -976,7 +1169,7 @@ int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w,
         B_CHECK((launch_matvec_pass<T, CQ>(ctx, wk, a, run_w, block_w)));
     }
     return reduce_runs<T, CQ>(ctx, wk, q, x, B200FE_PROF_GATHER, B200FE_PROF_FINALIZE,
-                              wk.run_grid > 0);
+                              wk.run_grid > 0, wk.run_grid > 0 && st.coupled);
 }
 
 struct ColState {

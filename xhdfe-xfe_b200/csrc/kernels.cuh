@@ -486,6 +486,7 @@ struct BlockArgs {
     T* R;                   // [nruns][CP]
     double* bins_partial;   // [ctas][SG][CP]
     int bins_cta0;
+    int all_segs;           // 1: long segments too (no segment kernel follows)
 };
 
 template <typename T>
@@ -598,7 +599,7 @@ block_pass_kernel(const BlockArgs<T> a) {
         T iw = static_cast<T>(0);
         if (s < a.Gp) {
             const int2 m0 = a.seg_meta[s], m1 = a.seg_meta[s + 1];
-            if (m1.x - m0.x <= kLongSeg) {  // long segments take the long path
+            if (a.all_segs || m1.x - m0.x <= kLongSeg) {  // else the long path
                 rb = m0.y;
                 re = m1.y;
             }
@@ -727,6 +728,93 @@ block_pass_kernel(const BlockArgs<T> a) {
                 run += d;
                 dst[h * CP + c] = run;
             }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Run-level matvec for one large dim and no small dim in the pass (two-way
+// panels, and the coupled matvec, where the small dim enters through its
+// dense coupling rows):  t_s = sum_{m in s} c_m x_f[f_m] / W_s,
+// R_m = c_m (x_f[f_m] - t_s).  A group of CQ lanes owns one primary segment;
+// runs are fetched NB at a time (independent loads in flight) and the first
+// NB are kept in registers for the second pass.
+// ---------------------------------------------------------------------------
+template <typename T, int CQ, int NB>
+__global__ void __launch_bounds__(kBlockThreads)
+run_pass_kernel(const BlockArgs<T> a) {
+    constexpr int CP = 4 * CQ;
+    constexpr int GPW = 32 / CQ;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int gw = lane / CQ;
+    const int q = lane % CQ;
+    const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (kBlockThreads / 32);
+    const int64_t wid = static_cast<int64_t>(blockIdx.x) * (kBlockThreads / 32) + warp;
+    for (int64_t s0 = wid * GPW; s0 < a.Gp; s0 += nwarps * GPW) {
+        const int64_t s = s0 + gw;
+        if (s >= a.Gp) continue;
+        const int2 m0 = a.seg_meta[s], m1 = a.seg_meta[s + 1];
+        if (!a.all_segs && m1.x - m0.x > kLongSeg) continue;  // the long path takes it
+        const int rb = m0.y, re = m1.y;
+        const T iw = static_cast<T>(a.inv_wp[s]);
+        V4<T> xc[NB];
+        T cc[NB];
+        int dc[NB];
+        V4<T> tsum;
+        v4_zero(tsum);
+        for (int m = rb; m < re; m += NB) {
+            int4 rm[NB];
+            T cm[NB];
+#pragma unroll
+            for (int u = 0; u < NB; ++u) {
+                if (m + u < re) {
+                    rm[u] = a.run_meta[m + u];
+                    cm[u] = a.run_w[m + u];
+                } else {
+                    rm[u] = make_int4(0, 0, 0, 0);
+                    cm[u] = static_cast<T>(0);
+                }
+            }
+            V4<T> xv[NB];
+#pragma unroll
+            for (int u = 0; u < NB; ++u) {
+                if (m + u < re) v4_load(a.x + (a.lbase + rm[u].x) * CP + 4 * q, xv[u]);
+                else v4_zero(xv[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < NB; ++u)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) tsum.v[i] = fma(cm[u], xv[u].v[i], tsum.v[i]);
+            if (m == rb) {
+#pragma unroll
+                for (int u = 0; u < NB; ++u) {
+                    xc[u] = xv[u];
+                    cc[u] = cm[u];
+                    dc[u] = rm[u].y;
+                }
+            }
+        }
+        V4<T> t;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) t.v[i] = tsum.v[i] * iw;
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            if (rb + u < re) {
+                V4<T> r;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) r.v[i] = cc[u] * (xc[u].v[i] - t.v[i]);
+                v4_store_stream(a.R + static_cast<int64_t>(dc[u]) * CP + 4 * q, r);
+            }
+        }
+        for (int m = rb + NB; m < re; ++m) {  // runs beyond the first NB
+            const int4 rm = a.run_meta[m];
+            const T cm = a.run_w[m];
+            V4<T> xf, r;
+            v4_load(a.x + (a.lbase + rm.x) * CP + 4 * q, xf);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) r.v[i] = cm * (xf.v[i] - t.v[i]);
+            v4_store_stream(a.R + static_cast<int64_t>(rm.y) * CP + 4 * q, r);
         }
     }
 }
@@ -1178,13 +1266,37 @@ struct GatherArgs {
     double* partial;            // [nchunks][CP] for multi-chunk groups
     const T* dotv;              // alpha rows of this dim (offset) or null
     double* dot_partial;        // [gridDim][CP] or null
+    const T* cfy;               // [G][SGP] dense coupling to the small dim, or null
+    const T* xs;                // small-dim rows of the matvec input [SG][CP]
+    int SG, SGP;                // levels of the small dim; row stride of cfy (SG rounded up to 4)
 };
+
+template <typename T>
+__device__ __forceinline__ void load4(const T* p, T (&v)[4]);
+template <>
+__device__ __forceinline__ void load4<float>(const float* p, float (&v)[4]) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+template <>
+__device__ __forceinline__ void load4<double>(const double* p, double (&v)[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
 
 template <typename T, int CQ>
 __global__ void __launch_bounds__(kRowThreads)
 run_gather_kernel(const GatherArgs<T> a) {
     __shared__ double red[kRowThreads][4];
+    extern __shared__ __align__(16) unsigned char gsmem_raw[];
+    T* xs_s = reinterpret_cast<T*>(gsmem_raw);  // [SGP][CP] small rows of x (coupled matvec)
     const int q = threadIdx.x % CQ;
+    if (a.cfy) {
+        for (int i = threadIdx.x; i < a.SGP * a.CP; i += kRowThreads)
+            xs_s[i] = i < a.SG * a.CP ? a.xs[i] : T(0);
+        __syncthreads();
+    }
     const int64_t grp0 = (static_cast<int64_t>(blockIdx.x) * kRowThreads + threadIdx.x) / CQ;
     const int64_t ngroups = static_cast<int64_t>(gridDim.x) * kRowThreads / CQ;
     double dot[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1197,6 +1309,20 @@ run_gather_kernel(const GatherArgs<T> a) {
         for (int32_t j = b; j < e; ++j)
             add_quad_stream(a.R + static_cast<int64_t>(j) * a.CP + 4 * q, acc);
         if (a.chunk_whole[c]) {
+            if (a.cfy) {  // + C_fy[g] x_small, four levels per load
+                const T* crow = a.cfy + static_cast<int64_t>(g) * a.SGP;
+                for (int h0 = 0; h0 < a.SGP; h0 += 4) {
+                    T c4[4];
+                    load4<T>(crow + h0, c4);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const T* xr = xs_s + (h0 + u) * a.CP + 4 * q;
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            acc.v[j] = fma(static_cast<double>(c4[u]), static_cast<double>(xr[j]), acc.v[j]);
+                    }
+                }
+            }
             T* dst = a.out + static_cast<int64_t>(g) * a.CP + 4 * q;
             store_quad(dst, acc);
             if (a.dotv) {
@@ -1240,13 +1366,19 @@ struct FinalizeArgs {
     const int32_t* multi_c0[kMaxLarge];
     const int32_t* multi_c1[kMaxLarge];
     const double* partial[kMaxLarge];
+    const int32_t* multi_s0[kMaxLarge];     // super-chunk range of each multi row (or null)
+    const int32_t* multi_s1[kMaxLarge];
+    const double* super_partial[kMaxLarge]; // [nsup][CP]
     int64_t lbase[kMaxLarge];
     int SG;                      // small-dim levels (bin rows)
     int64_t sgbase;              // alpha row of bin row 0 (small dims are contiguous)
     const double* bins_partial;  // [nbins_ctas][SG][CP]
     int nbins_ctas;
     const double* small_diag;    // [SG] level weights W_h to add W_h x[h] (block pass), or null
-    const T* x;                  // the matvec input (for small_diag)
+    const double* small_dense;   // [SG][SG] C_yy to add C_yy x_small (coupled matvec), or null
+    const T* cfy;                // [G_0][SGP] C_fy to add C_fy x_small to large dim 0's rows, or null
+    int SGP;                     // row stride of cfy
+    const T* x;                  // the matvec input (for small_diag / small_dense / cfy)
     int64_t nrows;               // sum nmulti + SG
     T* out;                      // alpha rows [GR][CP]
     const T* dotv;               // or null
@@ -1257,47 +1389,132 @@ struct FinalizeArgs {
     unsigned int* ticket;
 };
 
+constexpr int kFinFewParts = 16;  // rows with at most this many partials take one lane group
+constexpr int kSuperParts = 64;   // chunk partials per super-chunk
+
+// Super-chunks: one lane group (CP lanes) sums kSuperParts chunk partials of
+// a large group with four interleaved accumulators combined in a fixed order.
+__global__ void __launch_bounds__(kRowThreads)
+multi_super_kernel(int64_t nsup, const int32_t* __restrict__ sup_c0, const int32_t* __restrict__ sup_c1,
+                   const double* __restrict__ partial, int CP, double* __restrict__ out) {
+    const int NG = kRowThreads / CP;
+    const int gid = threadIdx.x / CP, c = threadIdx.x % CP;
+    for (int64_t sI = static_cast<int64_t>(blockIdx.x) * NG + gid; sI < nsup;
+         sI += static_cast<int64_t>(gridDim.x) * NG) {
+        const int32_t b = sup_c0[sI], e = sup_c1[sI];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int32_t j = b;
+        for (; j + 4 <= e; j += 4) {
+            a0 += __ldcg(partial + static_cast<int64_t>(j) * CP + c);
+            a1 += __ldcg(partial + static_cast<int64_t>(j + 1) * CP + c);
+            a2 += __ldcg(partial + static_cast<int64_t>(j + 2) * CP + c);
+            a3 += __ldcg(partial + static_cast<int64_t>(j + 3) * CP + c);
+        }
+        for (; j < e; ++j) a0 += __ldcg(partial + static_cast<int64_t>(j) * CP + c);
+        out[sI * CP + c] = (a0 + a1) + (a2 + a3);
+    }
+}
+
+// A finalize row: its partial slots, output row and extra terms.
+struct FinRow {
+    const double* part;
+    int64_t np, stride, orow, cgrp, small;  // small: small-dim level, or -1
+};
+
+template <typename T>
+__device__ __forceinline__ FinRow fin_row(const FinalizeArgs<T>& a, int64_t r) {
+    FinRow f{nullptr, 0, a.CP, -1, -1, -1};
+    int64_t ri = r;
+    for (int l = 0; l < a.nL && f.orow < 0; ++l) {
+        if (ri < a.nmulti[l]) {
+            const int32_t c0 = a.multi_c0[l][ri], c1 = a.multi_c1[l][ri];
+            const int32_t s0 = a.multi_s0[l] ? a.multi_s0[l][ri] : 0;
+            const int32_t s1 = a.multi_s0[l] ? a.multi_s1[l][ri] : 0;
+            if (s1 > s0) {  // summed in super-chunk slices
+                f.part = a.super_partial[l] + static_cast<int64_t>(s0) * a.CP;
+                f.np = s1 - s0;
+            } else {
+                f.part = a.partial[l] + static_cast<int64_t>(c0) * a.CP;
+                f.np = c1 - c0;
+            }
+            f.orow = a.lbase[l] + a.multi_grp[l][ri];
+            if (l == 0) f.cgrp = a.multi_grp[l][ri];
+        } else {
+            ri -= a.nmulti[l];
+        }
+    }
+    if (f.orow < 0) {  // small-dim level ri
+        f.part = a.bins_partial + ri * a.CP;
+        f.np = a.nbins_ctas;
+        f.stride = static_cast<int64_t>(a.SG) * a.CP;
+        f.orow = a.sgbase + ri;
+        f.small = ri;
+    }
+    return f;
+}
+
+// The terms a row adds to its partial sum (column c), then the store and the
+// dot with dotv.
+template <typename T>
+__device__ __forceinline__ void fin_store(const FinalizeArgs<T>& a, const FinRow& f, int c, double sum,
+                                          double& dotc) {
+    const int CP = a.CP;
+    if (a.small_dense && f.small >= 0) {
+        const double* crow = a.small_dense + f.small * a.SG;
+#pragma unroll 4
+        for (int h = 0; h < a.SG; ++h)
+            sum = fma(crow[h], static_cast<double>(a.x[(a.sgbase + h) * CP + c]), sum);
+    } else if (a.small_diag && f.small >= 0) {
+        sum = fma(a.small_diag[f.small], static_cast<double>(a.x[f.orow * CP + c]), sum);
+    }
+    if (a.cfy && f.cgrp >= 0) {
+        const T* crow = a.cfy + f.cgrp * a.SGP;
+#pragma unroll 4
+        for (int h = 0; h < a.SG; ++h)
+            sum = fma(static_cast<double>(crow[h]), static_cast<double>(a.x[(a.sgbase + h) * CP + c]), sum);
+    }
+    const T stored = static_cast<T>(sum);
+    a.out[f.orow * CP + c] = stored;
+    if (a.dotv) dotc = fma(static_cast<double>(a.dotv[f.orow * CP + c]), static_cast<double>(stored), dotc);
+}
+
+
 template <typename T>
 __global__ void __launch_bounds__(kRowThreads)
 finalize_kernel(const FinalizeArgs<T> a) {
     __shared__ double red[kRowThreads];
     __shared__ bool last;
     const int CP = a.CP;
-    double dotc = 0.0;  // thread c < CP: this CTA's dot contribution of column c
+    const int NG = kRowThreads / CP;  // lane groups per CTA
+    const int gid = threadIdx.x / CP, c = threadIdx.x % CP;
+    double dotc = 0.0;  // this thread's dot contribution of column c
+    // rows with few partials (most multi-chunk groups): one lane group each,
+    // lane c sums column c serially in slot order
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * NG + gid; r < a.nrows;
+         r += static_cast<int64_t>(gridDim.x) * NG) {
+        const FinRow f = fin_row(a, r);
+        if (f.np > kFinFewParts) continue;
+        double sum = 0.0;
+        for (int64_t p = 0; p < f.np; ++p) sum += __ldcg(f.part + p * f.stride + c);
+        fin_store(a, f, c, sum, dotc);
+    }
+    // rows with many partials (small-dim bins, very large groups): the whole CTA
     for (int64_t r = blockIdx.x; r < a.nrows; r += gridDim.x) {
-        int64_t ri = r;
-        int64_t orow = -1;
-        const double* part = nullptr;
-        int64_t np = 0, stride = CP;
-        for (int l = 0; l < a.nL && orow < 0; ++l) {
-            if (ri < a.nmulti[l]) {
-                const int32_t c0 = a.multi_c0[l][ri], c1 = a.multi_c1[l][ri];
-                part = a.partial[l] + static_cast<int64_t>(c0) * CP;
-                np = c1 - c0;
-                orow = a.lbase[l] + a.multi_grp[l][ri];
-            } else {
-                ri -= a.nmulti[l];
-            }
-        }
-        if (orow < 0) {  // small-dim level ri
-            part = a.bins_partial + ri * CP;
-            np = a.nbins_ctas;
-            stride = static_cast<int64_t>(a.SG) * CP;
-            orow = a.sgbase + ri;
-        }
-        double sum = block_column_sum(part, np, stride, CP, red);
-        if (threadIdx.x < CP) {
-            if (a.small_diag && r >= a.nrows - a.SG)
-                sum = fma(a.small_diag[r - (a.nrows - a.SG)],
-                          static_cast<double>(a.x[orow * CP + threadIdx.x]), sum);
-            const T stored = static_cast<T>(sum);
-            a.out[orow * CP + threadIdx.x] = stored;
-            if (a.dotv)
-                dotc = fma(static_cast<double>(a.dotv[orow * CP + threadIdx.x]),
-                           static_cast<double>(stored), dotc);
-        }
+        const FinRow f = fin_row(a, r);
+        if (f.np <= kFinFewParts) continue;
+        const double sum = block_column_sum(f.part, f.np, f.stride, CP, red);
+        if (threadIdx.x < CP) fin_store(a, f, threadIdx.x, sum, dotc);
         __syncthreads();
     }
+    // this CTA's dot per column: threads of column c summed in group order
+    red[threadIdx.x] = dotc;
+    __syncthreads();
+    if (threadIdx.x < CP) {
+        double d = 0.0;
+        for (int g = 0; g < NG; ++g) d += red[g * CP + threadIdx.x];
+        dotc = d;
+    }
+    __syncthreads();
     if (!a.dot_out) return;
     if (threadIdx.x < CP) a.dot_partial[static_cast<int64_t>(blockIdx.x) * CP + threadIdx.x] = dotc;
     __threadfence();
@@ -1425,6 +1642,49 @@ cg_direction_kernel(int64_t GR, int CP, T* __restrict__ p, const T* __restrict__
     }
     for (int64_t i = start; i < total; i += stride)
         p[i] = static_cast<T>(static_cast<double>(z[i]) + be * static_cast<double>(p[i]));
+}
+
+// ---------------------------------------------------------------------------
+// C_fy' x_f for the coupled matvec: per CTA a contiguous range of groups of
+// the large dim; thread (h, q) accumulates C_fy[g][h] x_f[g][4q..4q+3] in the
+// solve precision and writes the CTA's [SG][CP] partial (summed in CTA order
+// by finalize_kernel, with C_yy x_small, into the small-dim rows).
+// ---------------------------------------------------------------------------
+template <typename T, int CQ>
+__global__ void __launch_bounds__(256)
+coupling_xf_kernel(int64_t G, int SG, int SGP, const T* __restrict__ cfy, const T* __restrict__ xf,
+                   double* __restrict__ partial) {
+    constexpr int CP = 4 * CQ;
+    const int h = threadIdx.x / CQ, q = threadIdx.x % CQ;
+    const int64_t per = (G + gridDim.x - 1) / gridDim.x;
+    const int64_t g0 = static_cast<int64_t>(blockIdx.x) * per;
+    const int64_t g1 = min(G, g0 + per);
+    if (h >= SG) return;
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+    int64_t g = g0;
+    for (; g + 4 <= g1; g += 4) {  // four groups' loads in flight
+        T cv[4];
+        Acc4 xv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            cv[u] = __ldg(cfy + (g + u) * SGP + h);
+            load_quad(xf + (g + u) * CP + 4 * q, xv[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] = fma(cv[u], static_cast<T>(xv[u].v[j]), acc[j]);
+    }
+    for (; g < g1; ++g) {
+        const T c = __ldg(cfy + g * SGP + h);
+        Acc4 xv;
+        load_quad(xf + g * CP + 4 * q, xv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[j] = fma(c, static_cast<T>(xv.v[j]), acc[j]);
+    }
+    double* dst = partial + (static_cast<int64_t>(blockIdx.x) * SG + h) * CP + 4 * q;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dst[j] = static_cast<double>(acc[j]);
 }
 
 }  // namespace b200fe

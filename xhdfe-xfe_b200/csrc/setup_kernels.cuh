@@ -58,6 +58,19 @@ __global__ void histogram_kernel(const int32_t* __restrict__ ids, int64_t n,
         atomicAdd(counts + ids[i], 1);
 }
 
+// off[g] = first position i with sorted[i] >= g, g = 0..G (ids sorted, in
+// [0, G)): each position fills the offsets of the ids it starts, so empty
+// groups get the next group's offset.  No atomics; one pass over the ids.
+__global__ void segment_offsets_kernel(const int32_t* __restrict__ sorted, int64_t n, int32_t G,
+                                       int32_t* __restrict__ off) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t cur = i < n ? sorted[i] : G;
+        const int32_t prev = i > 0 ? sorted[i - 1] : -1;
+        for (int32_t g = prev + 1; g <= cur; ++g) off[g] = static_cast<int32_t>(i);
+    }
+}
+
 // Gather a dense id array (or weights) into primary order.
 template <typename V>
 __global__ void gather_kernel(const V* __restrict__ src, const int32_t* __restrict__ ord,
@@ -502,6 +515,264 @@ __global__ void subtract_mean_kernel(double* __restrict__ v, const int32_t* __re
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
         v[i] -= mean[gid[i]];
+}
+
+// ---------------------------------------------------------------------------
+// Dense small-dim coupling of the block-level structure (one large dim f, one
+// small dim h with SG <= kCoupleMaxSG levels).  With y_m[h] the weight of run
+// m's observations at level h and Y_s[h] that of primary segment s (both read
+// off the blocks: consecutive levels h0 .. h0+len-1 of one weight w_b),
+//     C_fy[f][h]  = sum_{runs m of f} ( y_m[h] - c_m Y_s(m)[h] / W_s(m) ),
+//     C_yy[h][h'] = W_h [h = h'] - sum_s Y_s[h] Y_s[h'] / W_s,
+// i.e. the blocks D_f' W (I - P_p) D_y and D_y' W (I - P_p) D_y of S.  Lane l
+// of a warp owns the levels h = l and h = l + 32.  Sums have a fixed order.
+// ---------------------------------------------------------------------------
+constexpr int kCoupleMaxSG = 64;
+
+__device__ __forceinline__ int lo_clear(int hmin, int SG) { return hmin < SG ? hmin : SG; }
+
+// Adds w to row[h] for the levels of block bm (a lane's private row).
+__device__ __forceinline__ void couple_row_add(double* row, const int2 bm, double w) {
+    for (int h = bm.x; h < bm.x + bm.y; ++h) row[h] += w;
+}
+
+// One warp per chunk of a firm's runs (in firm order).  Lane i takes run
+// j0 + i of the chunk: its metadata and blocks are read by the 32 lanes in
+// parallel, and lane i writes y_m - c_m Y_s / W_s into its own shared-memory
+// row; lane l then sums level l (and l + 32) over the rows in lane order.
+// Rows have stride SGP (SG rounded up to 4) and padding levels are zero.
+constexpr int kCoupleWarps = 8;
+
+__global__ void __launch_bounds__(kCoupleWarps * 32)
+coupling_fy_kernel(int64_t nchunks, const int32_t* __restrict__ chunk_grp,
+                   const int32_t* __restrict__ chunk_beg, const int32_t* __restrict__ chunk_end,
+                   const uint8_t* __restrict__ chunk_whole, const int32_t* __restrict__ sorted_runs,
+                   const int32_t* __restrict__ run_seg, const int4* __restrict__ run_meta,
+                   const int2* __restrict__ seg_meta, const int2* __restrict__ block_meta,
+                   const double* __restrict__ block_w, const double* __restrict__ cw_run,
+                   const double* __restrict__ inv_wp, int SG, int SGP, double* __restrict__ out_fy,
+                   double* __restrict__ partial) {
+    extern __shared__ double cf_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* rows = cf_smem + static_cast<int64_t>(warp) * 32 * SG;
+    double* myrow = rows + lane * SG;
+    const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kCoupleWarps;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * kCoupleWarps + warp; c < nchunks; c += nwarps) {
+        const int32_t b = chunk_beg[c], e = chunk_end[c];
+        double acc[2] = {0.0, 0.0};
+        for (int32_t j0 = b; j0 < e; j0 += 32) {
+            for (int h = 0; h < SG; ++h) myrow[h] = 0.0;
+            if (j0 + lane < e) {
+                const int32_t m = sorted_runs[j0 + lane];
+                const int32_t sg = run_seg[m];
+                const int4 rm = run_meta[m];
+                const int32_t r0 = seg_meta[sg].y, r1 = seg_meta[sg + 1].y;
+                const int sb0 = run_meta[r0].z, sb1 = run_meta[r1 - 1].w;
+                const double cf = cw_run[m] * inv_wp[sg];
+                for (int bb = rm.z; bb < rm.w; ++bb)
+                    couple_row_add(myrow, block_meta[bb], block_w ? block_w[bb] : 1.0);
+                for (int bb = sb0; bb < sb1; ++bb)
+                    couple_row_add(myrow, block_meta[bb], -cf * (block_w ? block_w[bb] : 1.0));
+            }
+            __syncwarp();
+            const int nj = min(32, e - j0);
+            for (int i = 0; i < nj; ++i) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+                    if (lane + 32 * k < SG) acc[k] += rows[i * SG + lane + 32 * k];
+            }
+            __syncwarp();
+        }
+        double* dst = chunk_whole[c] ? out_fy + static_cast<int64_t>(chunk_grp[c]) * SGP
+                                     : partial + c * SGP;
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+            if (lane + 32 * k < SGP) dst[lane + 32 * k] = (lane + 32 * k < SG) ? acc[k] : 0.0;
+    }
+}
+
+// Rows of multi-chunk firms: one CTA per row; warp w sums chunks c0 + w,
+// c0 + w + 8, ... (lanes over levels), then the eight warp sums are added in
+// warp order.
+__global__ void __launch_bounds__(256)
+coupling_fy_combine_kernel(int64_t nmulti, const int32_t* __restrict__ multi_grp,
+                           const int32_t* __restrict__ multi_c0, const int32_t* __restrict__ multi_c1,
+                           const double* __restrict__ partial, int SGP, double* __restrict__ out_fy) {
+    __shared__ double ws[8][kCoupleMaxSG];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t r = blockIdx.x; r < nmulti; r += gridDim.x) {
+        const int32_t c0 = multi_c0[r], c1 = multi_c1[r];
+        double acc[2] = {0.0, 0.0};
+        for (int32_t c = c0 + warp; c < c1; c += 8) {
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+                if (lane + 32 * k < SGP) acc[k] += __ldcg(partial + static_cast<int64_t>(c) * SGP + lane + 32 * k);
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+            if (lane + 32 * k < SGP) ws[warp][lane + 32 * k] = acc[k];
+        __syncthreads();
+        if (threadIdx.x < SGP) {
+            double v = 0.0;
+            for (int w = 0; w < 8; ++w) v += ws[w][threadIdx.x];
+            out_fy[static_cast<int64_t>(multi_grp[r]) * SGP + threadIdx.x] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// sum_s Y_s Y_s' / W_s and the level weights W_h = sum_s Y_s[h].  Lane i of a
+// warp builds Y_s of segment s0 + i in its own shared row (the 32 lanes read
+// their blocks in parallel); then, segment by segment in lane order, lane l
+// adds Y_s[h] Y_s[h'] / W_s to rows h = l and l + 32 of the warp's SG x SG
+// accumulator, for h' in the segment's level range, and Y_s[h] to W_h.
+// Per-CTA partials [SG*SG + SG], summed in CTA order by
+// coupling_yy_reduce_kernel.
+constexpr int kCoupleYyWarps = 2;
+
+__global__ void __launch_bounds__(kCoupleYyWarps * 32)
+coupling_yy_kernel(int32_t Gp, const int2* __restrict__ seg_meta, const int4* __restrict__ run_meta,
+                   const int2* __restrict__ block_meta, const double* __restrict__ block_w,
+                   const double* __restrict__ inv_wp, int SG, double* __restrict__ partial) {
+    extern __shared__ double cy_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int SS = SG * SG;
+    const int WS = SS + SG + 32 * SG;  // per warp: acc, W, 32 rows Y
+    double* acc = cy_smem + static_cast<int64_t>(warp) * WS;
+    double* Wh = acc + SS;
+    double* Y = Wh + SG;
+    double* myY = Y + lane * SG;
+    for (int i = threadIdx.x; i < kCoupleYyWarps * WS; i += blockDim.x) cy_smem[i] = 0.0;
+    __syncthreads();
+    const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kCoupleYyWarps;
+    const int64_t wid = static_cast<int64_t>(blockIdx.x) * kCoupleYyWarps + warp;
+    for (int64_t s0 = wid * 32; s0 < Gp; s0 += nwarps * 32) {
+        int hmin = SG, hmax = 0;
+        double iw = 0.0;
+        if (s0 + lane < Gp) {
+            const int64_t sg = s0 + lane;
+            const int32_t r0 = seg_meta[sg].y, r1 = seg_meta[sg + 1].y;
+            if (r1 > r0) {
+                const int sb0 = run_meta[r0].z, sb1 = run_meta[r1 - 1].w;
+                for (int bb = sb0; bb < sb1; ++bb) {
+                    const int2 bm = block_meta[bb];
+                    couple_row_add(myY, bm, block_w ? block_w[bb] : 1.0);
+                    hmin = min(hmin, bm.x);
+                    hmax = max(hmax, bm.x + bm.y);
+                }
+            }
+            iw = inv_wp[sg];
+        }
+        __syncwarp();
+        const int ns = static_cast<int>(min(static_cast<int64_t>(32), Gp - s0));
+        for (int i = 0; i < ns; ++i) {
+            const int lo = __shfl_sync(0xffffffffu, hmin, i), hi = __shfl_sync(0xffffffffu, hmax, i);
+            const double w_inv = __shfl_sync(0xffffffffu, iw, i);
+            const double* Yi = Y + i * SG;
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int h = lane + 32 * k;
+                if (h >= lo && h < hi) {
+                    const double yh = Yi[h];
+                    Wh[h] += yh;
+                    const double a = yh * w_inv;
+                    if (a != 0.0)
+                        for (int h2 = lo; h2 < hi; ++h2) acc[h * SG + h2] = fma(a, Yi[h2], acc[h * SG + h2]);
+                }
+            }
+        }
+        __syncwarp();
+        for (int h = lo_clear(hmin, SG); h < max(hmax, 0); ++h) myY[h] = 0.0;
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < SS + SG; i += blockDim.x) {
+        double v = 0.0;
+        for (int w = 0; w < kCoupleYyWarps; ++w) v += cy_smem[static_cast<int64_t>(w) * WS + i];
+        partial[static_cast<int64_t>(blockIdx.x) * (SS + SG) + i] = v;
+    }
+}
+
+// C_yy = diag(W) - sum_s Y_s Y_s' / W_s, CTA partials summed in CTA order; the
+// level weights W_h and E_h = sum_s Y_s[h]^2 / W_s also go to the diagonal
+// arrays of the Jacobi preconditioner (diag C_yy = W_h - E_h, exact).
+__global__ void coupling_yy_reduce_kernel(const double* __restrict__ partial, int nparts, int SG,
+                                          double* __restrict__ out_yy, double* __restrict__ W_out,
+                                          double* __restrict__ E_out) {
+    const int SS = SG * SG;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < SS; i += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int b = 0; b < nparts; ++b) acc += partial[static_cast<int64_t>(b) * (SS + SG) + i];
+        const int h = i / SG, h2 = i - h * SG;
+        if (h == h2) {
+            double W = 0.0;
+            for (int b = 0; b < nparts; ++b) W += partial[static_cast<int64_t>(b) * (SS + SG) + SS + h];
+            W_out[h] = W;
+            E_out[h] = acc;
+            out_yy[i] = W - acc;
+        } else {
+            out_yy[i] = -acc;
+        }
+    }
+}
+
+// Diagonal terms of a large dim per group, W_g = sum c_m and
+// E_g = sum c_m^2 / W_s(m) over its runs (in group order), over the chunk list:
+// a chunk that is its group's only one writes the group's sums; the others
+// write partials that multi_wsum_kernel adds in chunk order.
+__global__ void chunk_wsum_kernel(int64_t nchunks, const int32_t* __restrict__ chunk_grp,
+                                  const int32_t* __restrict__ chunk_beg,
+                                  const int32_t* __restrict__ chunk_end,
+                                  const uint8_t* __restrict__ chunk_whole,
+                                  const double* __restrict__ cw_sorted,
+                                  const double* __restrict__ ce_sorted, double* __restrict__ W,
+                                  double* __restrict__ E, double* __restrict__ part2) {
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < nchunks;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double sw = 0.0, se = 0.0;
+        for (int32_t j = chunk_beg[c]; j < chunk_end[c]; ++j) {
+            sw += cw_sorted[j];
+            se += ce_sorted[j];
+        }
+        if (chunk_whole[c]) {
+            W[chunk_grp[c]] = sw;
+            E[chunk_grp[c]] = se;
+        } else {
+            part2[2 * c] = sw;
+            part2[2 * c + 1] = se;
+        }
+    }
+}
+
+// One CTA per multi-chunk group: thread t adds chunks c0 + t, c0 + t + 256,
+// ..., then a fixed-order tree in shared memory.
+__global__ void __launch_bounds__(256)
+multi_wsum_kernel(int64_t nmulti, const int32_t* __restrict__ multi_grp,
+                  const int32_t* __restrict__ multi_c0, const int32_t* __restrict__ multi_c1,
+                  const double* __restrict__ part2, double* __restrict__ W, double* __restrict__ E) {
+    __shared__ double rw[256], re[256];
+    for (int64_t r = blockIdx.x; r < nmulti; r += gridDim.x) {
+        double sw = 0.0, se = 0.0;
+        for (int32_t c = multi_c0[r] + threadIdx.x; c < multi_c1[r]; c += 256) {
+            sw += part2[2 * static_cast<int64_t>(c)];
+            se += part2[2 * static_cast<int64_t>(c) + 1];
+        }
+        rw[threadIdx.x] = sw;
+        re[threadIdx.x] = se;
+        __syncthreads();
+        for (int h = 128; h > 0; h >>= 1) {
+            if (threadIdx.x < h) {
+                rw[threadIdx.x] += rw[threadIdx.x + h];
+                re[threadIdx.x] += re[threadIdx.x + h];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            W[multi_grp[r]] = rw[0];
+            E[multi_grp[r]] = re[0];
+        }
+        __syncthreads();
+    }
 }
 
 }  // namespace b200fe
