@@ -130,6 +130,26 @@ int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X,
                   const double* weights, const b200fe_options* opts,
                   double* y_out, double* X_out, b200fe_result* res);
 
+/* b200fe_absorb that also returns the fixed-effect coefficients (saved FEs):
+ * fe_out[d] is a host array of num_groups[d] x (k + 1) doubles, column-major,
+ * column 0 for y and column j for X column j.  On return, for every row i,
+ * v_i - v~_i = sum_d fe_out[d][gid_d(i), :] (to rounding): the primary
+ * dimension's coefficients are its weighted group means of v - (other FEs),
+ * the others the refined solution of the reduced system.  As in any
+ * multi-way FE model the split between dimensions is identified only up to
+ * the usual normalisations (a constant moved between dimensions); the sum is
+ * unique.  Groups without observations get 0.
+ * Replaces the retain_fixed_effects outputs (fe_alpha_y / fe_alpha_X) of
+ * hdfe::detail::absorb_fixed_effects_cuda (src/fe_absorption_cuda.cu:4663-4690),
+ * which the reference's recover_fixed_effects consumes
+ * (src/fe_absorption.cpp:15484-15520). */
+int b200fe_absorb_fe(b200fe_context* ctx, const double* y, const double* X,
+                     int64_t n, int k, int num_dims,
+                     const int32_t* const* group_ids, const int32_t* num_groups,
+                     const double* weights, const b200fe_options* opts,
+                     double* y_out, double* X_out, double* const* fe_out,
+                     b200fe_result* res);
+
 /* Absorb device arrays (no host copies).  d_v: column-major n x cols with the
  * outcome in column 0; d_out: same shape (may alias nothing of the inputs).
  * stream: a cudaStream_t as void*, or NULL for the context's stream.

@@ -140,6 +140,10 @@ def rlib(path: Path = REF_SO) -> ctypes.CDLL:
         lib.xref_fit.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, _vp, P(XrefOptions), _vp,
                                  _vp, P(_int), P(_dbl), ctypes.c_char_p, _int]
         lib.xref_fit.restype = _int
+        if hasattr(lib, "xref_recover_fe"):
+            lib.xref_recover_fe.argtypes = [_vp, _i64, _vp, _int, _vp, P(XrefOptions), _dbl, _vp,
+                                            P(_int), P(_dbl), ctypes.c_char_p, _int]
+            lib.xref_recover_fe.restype = _int
         if hasattr(lib, "xref_akm_kss"):
             lib.xref_akm_kss.argtypes = [_vp, _vp, _vp, _i64, _vp, ctypes.c_uint64, _dbl, _vp, P(_int),
                                          P(ctypes.c_longlong), ctypes.c_char_p, _int]
@@ -276,3 +280,26 @@ def ref_akm_kss(y, worker, firm, *, leverages="auto", jla_draws=0, seed=20260705
             "gpu_used": bool(info[3]), "gpu_status_code": info[4], "solver_direct": bool(info[5]),
             "converged": bool(info[6]), "jla_draws_used": info[7],
             "solver_iterations": int(iters.value)}
+
+
+def ref_recover_fe(partial, fes, weights=None, *, tol=1e-8, fe_tolerance=0.0, threads=1,
+                   gpu_backend="default", lib_path=REF_SO):
+    """The reference's recover_fixed_effects (include/fe_absorption.hpp:127-130):
+    per-dim FE contributions of ``partial`` (n x dims), iterations, converged,
+    max_delta."""
+    pv = np.ascontiguousarray(partial, dtype=np.float64)
+    n = pv.shape[0]
+    g = np.ascontiguousarray(np.stack([np.asarray(f, dtype=np.int32) for f in fes]))
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    contrib = np.zeros((len(fes), n))
+    info = (_int * 2)()
+    dinfo = (_dbl * 1)()
+    err = ctypes.create_string_buffer(512)
+    o = _xopts(tol, "reghdfe-comparable", "auto", threads, gpu_backend=gpu_backend)
+    rc = rlib(lib_path).xref_recover_fe(pv.ctypes.data, n, g.ctypes.data, len(fes),
+                                        None if w is None else w.ctypes.data, ctypes.byref(o),
+                                        fe_tolerance, contrib.ctypes.data, info, dinfo, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return {"contributions": contrib, "iterations": info[0], "converged": bool(info[1]),
+            "max_delta": dinfo[0]}

@@ -11,6 +11,7 @@
 //   xref_partial_out  -> hdfe::v11::HdfeRegressorV11::partial_out (src/hdfe_regressor_v11.cpp:10275)
 //   xref_fit          -> hdfe::v11::HdfeRegressorV11::fit         (src/hdfe_regressor_v11.cpp:7522)
 //   xref_akm_kss      -> hdfe::akm::akm_kss_decompose              (include/hdfe/akm_kss.hpp:227-233)
+//   xref_recover_fe   -> hdfe::detail::recover_fixed_effects        (include/fe_absorption.hpp:127-130)
 // Every entry point catches all exceptions and returns a nonzero status with
 // the message copied into err (the reference's own fail-closed contract).
 
@@ -282,6 +283,44 @@ int xref_akm_kss(const double* y, const int32_t* worker, const int32_t* firm, in
         info[6] = r.converged ? 1 : 0;
         info[7] = r.jla_draws_used;
         *iters_out = r.solver_iterations;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+// Saved-FE recovery of a partial residual: contrib (n x dims, column-major)
+// receives the per-dim FE contributions; info: [0] iterations, [1] converged;
+// dinfo: [0] max_delta.
+int xref_recover_fe(const double* partial, int64_t n, const int32_t* fe_flat, int dims,
+                    const double* w, const XrefOptions* o, double fe_tolerance, double* contrib,
+                    int* info, double* dinfo, char* err, int err_len) {
+    try {
+        const VectorXd pv = Map<const VectorXd>(partial, n);
+        std::vector<VectorXi> fes = to_fes(fe_flat, n, dims);
+        VectorXd wv;
+        if (w) wv = Map<const VectorXd>(w, n);
+        hdfe::HdfeOptions opts = to_options(o);
+        opts.fe_tolerance = fe_tolerance;
+        auto guard = backend_guard(o);
+        const hdfe::detail::FeRecoveryResult r =
+            hdfe::detail::recover_fixed_effects(pv, fes, w ? &wv : nullptr, opts);
+        for (int d = 0; d < dims; ++d) {
+            if (static_cast<int64_t>(r.contributions.size()) <= d ||
+                r.contributions[d].size() != n) {
+                set_err(err, err_len, "recover_fixed_effects returned no contribution");
+                return 1;
+            }
+            std::memcpy(contrib + static_cast<int64_t>(d) * n, r.contributions[d].data(),
+                        sizeof(double) * n);
+        }
+        info[0] = r.iterations;
+        info[1] = r.converged ? 1 : 0;
+        dinfo[0] = r.max_delta;
         return 0;
     } catch (const std::exception& e) {
         set_err(err, err_len, e.what());

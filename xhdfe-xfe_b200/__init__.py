@@ -8,6 +8,7 @@ from .absorber import (  # noqa: F401
     Absorber,
     AbsorberError,
     AbsorptionResult,
+    FeRecoveryResult,
     absorb_fixed_effects,
     cuda_backend_available,
     demean_raw,
@@ -15,6 +16,7 @@ from .absorber import (  # noqa: F401
     drop_singletons_mask,
     make_options,
     partial_out,
+    recover_fixed_effects,
 )
 from .kss import KssSolver, kss_system, max_lanes, stable_sort_u64  # noqa: F401
 

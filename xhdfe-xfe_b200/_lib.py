@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "b200fe_context_stream",
     "b200fe_absorb",
     "b200fe_absorb_device",
+    "b200fe_absorb_fe",
     "b200fe_demean_raw",
     "b200fe_fe_recovery_max_delta",
     "b200fe_demean_sorted_noalloc",
@@ -134,6 +135,9 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.b200fe_fe_recovery_max_delta.restype = c_int
     lib.b200fe_demean_sorted_noalloc.argtypes = [vp, i64, c_int, vp, ctypes.c_int32, vp, vp, vp]
     lib.b200fe_demean_sorted_noalloc.restype = c_int
+    lib.b200fe_absorb_fe.argtypes = [vp, vp, vp, i64, c_int, c_int, pp, vp, vp,
+                                     ctypes.POINTER(Options), vp, vp, pp, ctypes.POINTER(Result)]
+    lib.b200fe_absorb_fe.restype = c_int
     lib.b200fe_kss_create.argtypes = [c_int, c_int, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp,
                                       ctypes.POINTER(vp)]
     lib.b200fe_kss_create.restype = c_int

@@ -67,6 +67,17 @@ class AbsorptionResult:
     d2h_ms: float = 0.0
     kernel_launches: int = 0
     sample_index: np.ndarray | None = None
+    # saved FEs (save_fe=True): per dim, [G_d, 1 + k] coefficients, column 0 for
+    # y -- the fe_alpha_y / fe_alpha_X of the reference's retain_fixed_effects
+    fe: list | None = None
+
+    @property
+    def fe_alpha_y(self):
+        return None if self.fe is None else [a[:, 0] for a in self.fe]
+
+    @property
+    def fe_alpha_X(self):
+        return None if self.fe is None else [a[:, 1:] for a in self.fe]
 
 
 def cuda_backend_available() -> bool:
@@ -149,8 +160,9 @@ class Absorber:
         return int(self.lib.b200fe_context_stream(self.handle) or 0)
 
     def absorb(self, y, X, group_ids, num_groups, weights=None, options=None,
-               y_out=None, X_out=None) -> AbsorptionResult:
-        """Absorb host arrays with dense ids (absorb_fixed_effects_cuda)."""
+               y_out=None, X_out=None, save_fe=False) -> AbsorptionResult:
+        """Absorb host arrays with dense ids (absorb_fixed_effects_cuda).  With
+        save_fe the result carries the FE coefficients (``fe``)."""
         y = np.ascontiguousarray(y, dtype=np.float64)
         n = y.shape[0]
         X = np.zeros((n, 0)) if X is None else np.asarray(X, dtype=np.float64)
@@ -172,14 +184,18 @@ class Absorber:
             X_out = np.empty((n, k), dtype=np.float64, order="F")
         o = options or make_options()
         r = _lib.Result()
-        rc = self.lib.b200fe_absorb(
+        fe = [np.zeros((int(g), k + 1), order="F") for g in G] if save_fe else None
+        rc = self.lib.b200fe_absorb_fe(
             self.handle, y.ctypes.data, X.ctypes.data if k else None, n, k, len(gids),
             _ptr_array([g.ctypes.data for g in gids]), G.ctypes.data,
             None if w is None else w.ctypes.data, ctypes.byref(o), y_out.ctypes.data,
-            X_out.ctypes.data if k else None, ctypes.byref(r))
+            X_out.ctypes.data if k else None,
+            _ptr_array([a.ctypes.data for a in fe]) if fe else None, ctypes.byref(r))
         if rc not in (_lib.OK, _lib.NOT_CONVERGED):
             raise self._err(rc)
-        return _to_result(r, y_out, X_out, G)
+        res = _to_result(r, y_out, X_out, G)
+        res.fe = fe
+        return res
 
     def absorb_device(self, v, group_ids, num_groups, weights=None, options=None, out=None,
                       stream=None):
@@ -256,9 +272,12 @@ def _check_finite(a, name):
         raise ValueError(f"{name} contains non-finite values")
 
 
-def absorb_fixed_effects(y, X, fes, weights=None, *, device=0, **options) -> AbsorptionResult:
+def absorb_fixed_effects(y, X, fes, weights=None, *, device=0, save_fe=False,
+                         **options) -> AbsorptionResult:
     """Demean y and X on the FE dims ``fes`` (raw nonnegative ids), no singleton
-    drop (absorb_fixed_effects_v6 with the GPU backend)."""
+    drop (absorb_fixed_effects_v6 with the GPU backend).  save_fe: also return
+    the FE coefficients per dim, indexed by the dense ids (``fe``), as the
+    reference's retain_fixed_effects."""
     y = np.asarray(y, dtype=np.float64)
     _check_finite(y, "y")
     if X is not None:
@@ -266,7 +285,45 @@ def absorb_fixed_effects(y, X, fes, weights=None, *, device=0, **options) -> Abs
     dense = [dense_ids(f) for f in fes]
     o = make_options(**options)
     return _thread_absorber(device).absorb(
-        y, X, [d for d, _ in dense], [g for _, g in dense], weights, o)
+        y, X, [d for d, _ in dense], [g for _, g in dense], weights, o, save_fe=save_fe)
+
+
+@dataclass
+class FeRecoveryResult:
+    """hdfe::detail::FeRecoveryResult (include/fe_absorption.hpp:55-60)."""
+    contributions: list
+    iterations: int = 0
+    max_delta: float = 0.0
+    converged: bool = True
+
+
+def recover_fixed_effects(partial, fes, weights=None, *, tol=1e-8, fe_tolerance=0.0, device=0,
+                          **options) -> FeRecoveryResult:
+    """The reference's recover_fixed_effects on its GPU path
+    (src/fe_absorption.cpp:15453-15540): absorb ``partial`` (y - X b) with
+    saved FEs, the per-dim contributions alpha_d[gid_d], then the orthogonality
+    check max_delta of partial - sum_d contributions; converged when
+    max_delta <= fe_tolerance (or tol).  ``fes`` are dense ids."""
+    partial = np.asarray(partial, dtype=np.float64)
+    _check_finite(partial, "partial")
+    gids = [np.ascontiguousarray(f, dtype=np.int32) for f in fes]
+    G = [int(g.max()) + 1 if g.size else 1 for g in gids]
+    ab = _thread_absorber(device)
+    fe_tol = fe_tolerance if fe_tolerance > 0.0 else tol
+    # the check below is absolute (max over groups of the residual's mean), so
+    # the solve runs two orders tighter than the tolerance it must meet
+    solve_tol = max(min(tol, fe_tol) * 1e-2, 1e-14)
+    res = ab.absorb(partial, None, gids, G, weights, make_options(tol=solve_tol, **options),
+                    save_fe=True)
+    contrib = [res.fe[d][gids[d], 0] for d in range(len(gids))]
+    out = FeRecoveryResult(contributions=contrib, iterations=res.iterations)
+    if res.converged and fe_tol > 0.0:
+        resid = partial - np.sum(contrib, axis=0)
+        out.max_delta = ab.fe_recovery_max_delta(resid, gids, G, weights)
+        out.converged = out.max_delta <= fe_tol
+    else:
+        out.converged = bool(res.converged)
+    return out
 
 
 def drop_singletons_mask(fes) -> np.ndarray:

@@ -131,6 +131,11 @@ struct b200fe_context {
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<ProfRec> prof;
+    // saved FEs: device outputs per dim ([G_d][cols] column-major) while a
+    // b200fe_absorb_fe call runs, and the first column of the current block
+    double* fe_dev[B200FE_MAX_DIMS] = {nullptr};
+    int fe_cols = 0;
+    int fe_c0 = 0;
 };
 
 namespace {
@@ -1416,8 +1421,15 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             if (thr64[c] > 0.0) rel_res = std::max(rel_res, tol * std::sqrt(rr[c] / thr64[c]));
     }
 
-    // final pass: out = (I - P_p)(v - D_r a); certificate scatter
+    // final pass: out = (I - P_p)(v - D_r a); certificate scatter; with saved
+    // FEs also the primary segment means (the primary dim's coefficients)
     const bool cert = o.certify != 0;
+    const bool save_fe = ctx->fe_dev[0] != nullptr;
+    double* means = nullptr;
+    if (save_fe) {
+        B_CHECK(get_buf(ctx, "fe_means", static_cast<size_t>(st.G[st.p]) * CP, &means));
+        B_TRY(cudaMemsetAsync(means, 0, sizeof(double) * st.G[st.p] * CP, s));
+    }
     {
         PassArgs<double> a = make_pass_args<double>(st, cols, CP, w64);
         a.wp = st.wp64;
@@ -1425,6 +1437,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         a.out = d_out;
         a.x = a64;
         a.scatter = cert ? 1 : 0;
+        a.mean_out = means;
         ProfScope ps(ctx, B200FE_PROF_FINAL,
                      static_cast<double>(st.n) * cols * 16.0 + struct_obs_bytes(st, 8) +
                          static_cast<double>(GR) * CP * 8.0 +
@@ -1458,6 +1471,25 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             abs_res = std::max(abs_res, ab);
             abs_rel = std::max(abs_rel, rel);
         }
+    }
+    if (save_fe) {
+        FeLayoutArgs f{};
+        f.nd = st.D;
+        for (int d = 0; d < st.D; ++d) {
+            f.G[d] = st.G[d];
+            f.out[d] = ctx->fe_dev[d];
+            f.row0[d] = d == st.p ? -1 : -2;
+        }
+        for (int l = 0; l < st.nL; ++l) f.row0[st.L[l].dim] = st.lbase[l];
+        for (int j = 0; j < st.nS; ++j) f.row0[st.sdim[j]] = st.sbase[j];
+        f.cols_total = ctx->fe_cols;
+        f.c0 = ctx->fe_c0;
+        f.cb = cols;
+        f.CP = CP;
+        f.a = a64;
+        f.means = means;
+        fe_layout_kernel<<<grid_for(ctx, static_cast<int64_t>(st.n) + GR, 256), 256, 0, s>>>(f);
+        B_LAUNCHED();
     }
     B_TRY(cudaStreamSynchronize(s));
     res->iterations += total_iters;
@@ -1514,6 +1546,7 @@ int solve_all(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         const double* v = d_v + static_cast<int64_t>(c0) * n;
         double* out = d_out + static_cast<int64_t>(c0) * n;
         const int cq = (cb + 3) / 4;
+        ctx->fe_c0 = c0;
         int rc;
         if (cq <= 1) rc = solve_dispatch_cq<1>(ctx, v, cb, out, o, res);
         else if (cq <= 2) rc = solve_dispatch_cq<2>(ctx, v, cb, out, o, res);
@@ -1718,10 +1751,10 @@ int b200fe_absorb_device(b200fe_context* ctx, const double* d_v, int64_t n, int 
     return r->status = rc;
 }
 
-int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X, int64_t n, int k,
-                  int num_dims, const int32_t* const* group_ids, const int32_t* num_groups,
-                  const double* weights, const b200fe_options* opts, double* y_out,
-                  double* X_out, b200fe_result* res) {
+int b200fe_absorb_fe(b200fe_context* ctx, const double* y, const double* X, int64_t n, int k,
+                     int num_dims, const int32_t* const* group_ids, const int32_t* num_groups,
+                     const double* weights, const b200fe_options* opts, double* y_out,
+                     double* X_out, double* const* fe_out, b200fe_result* res) {
     b200fe_result local;
     b200fe_result* r = res ? res : &local;
     clear_result(r);
@@ -1732,8 +1765,8 @@ int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X, int64_t
         return r->status = B200FE_INVALID_ARG;
     }
     for (int d = 0; d < num_dims; ++d)
-        if (!group_ids[d]) {
-            ctx->err = "null group id array";
+        if (!group_ids[d] || (fe_out && !fe_out[d])) {
+            ctx->err = "null group id or FE output array";
             return r->status = B200FE_INVALID_ARG;
         }
     b200fe_options o;
@@ -1768,12 +1801,27 @@ int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X, int64_t
         if (k > 0)
             B_TRY(cudaMemcpyAsync(dv + n, X, sizeof(double) * n * k, cudaMemcpyHostToDevice, s));
         B_TRY(cudaEventRecord(h1, s));
+        if (fe_out) {
+            for (int d = 0; d < num_dims; ++d)
+                B_CHECK(get_buf(ctx, "fe_out" + std::to_string(d), static_cast<size_t>(num_groups[d]) * cols,
+                                &ctx->fe_dev[d]));
+            ctx->fe_cols = cols;
+        }
         int rc2 = absorb_device_impl(ctx, dv, n, cols, num_dims, dg, num_groups, dw, o, dout, r);
-        if (rc2 != B200FE_OK && rc2 != B200FE_NOT_CONVERGED) return rc2;
+        if (rc2 != B200FE_OK && rc2 != B200FE_NOT_CONVERGED) {
+            for (double*& q : ctx->fe_dev) q = nullptr;
+            return rc2;
+        }
         B_TRY(cudaEventRecord(d0, s));
         B_TRY(cudaMemcpyAsync(y_out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
         if (k > 0)
             B_TRY(cudaMemcpyAsync(X_out, dout + n, sizeof(double) * n * k, cudaMemcpyDeviceToHost, s));
+        if (fe_out) {
+            for (int d = 0; d < num_dims; ++d)
+                B_TRY(cudaMemcpyAsync(fe_out[d], ctx->fe_dev[d], sizeof(double) * num_groups[d] * cols,
+                                      cudaMemcpyDeviceToHost, s));
+            for (double*& q : ctx->fe_dev) q = nullptr;
+        }
         B_TRY(cudaEventRecord(d1, s));
         B_TRY(cudaEventSynchronize(d1));
         r->h2d_ms = elapsed_ms(h0, h1);
@@ -1790,6 +1838,14 @@ int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X, int64_t
     return r->status = rc;
 }
 
+}
+
+int b200fe_absorb(b200fe_context* ctx, const double* y, const double* X, int64_t n, int k,
+                  int num_dims, const int32_t* const* group_ids, const int32_t* num_groups,
+                  const double* weights, const b200fe_options* opts, double* y_out,
+                  double* X_out, b200fe_result* res) {
+    return b200fe_absorb_fe(ctx, y, X, n, k, num_dims, group_ids, num_groups, weights, opts, y_out,
+                            X_out, nullptr, res);
 }  // extern "C"
 
 namespace {

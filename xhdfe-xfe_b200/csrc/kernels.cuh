@@ -158,6 +158,7 @@ struct PassArgs {
     double* colsq_partial;     // [ctas][CP]: kRhs sum v^2; kFinal sum_s (sum_k z_k)^2
     int bins_cta0;             // first CTA slot of this launch in the partial arrays
     int scatter;               // kFinal: 1 to scatter z for the certificate
+    double* mean_out;          // kFinal: [Gp][CP] primary segment means of v - D_r a, or null
     int bins_no_diag;          // kMatvec: bins get z_k - w_k x_s[h_k] (finalize adds W_h x_s[h])
     // tiles
     const int32_t* tile_seg;   // [ntiles+1] first segment of each tile
@@ -936,6 +937,7 @@ data_pass_kernel(const PassArgs<double> a) {
                 if (MODE == kRhs) colsq = fma(val, val, colsq);
             }
             const double mean = acc * a.inv_wp[s];
+            if (MODE == kFinal && a.mean_out) a.mean_out[static_cast<int64_t>(s) * CP + c] = mean;
             double zs = 0.0;
             for (int kl = b; kl < e; ++kl) {
                 const double d = ubuf[c * LD + kl] - mean;
@@ -1092,6 +1094,10 @@ segment_pass_kernel(const PassArgs<T> a) {
         Acc4 mean;
 #pragma unroll
         for (int j = 0; j < 4; ++j) mean.v[j] = acc.v[j] * inv_w;
+        if (MODE == kFinal && a.mean_out && valid) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) a.mean_out[static_cast<int64_t>(s) * a.CP + 4 * q + j] = mean.v[j];
+        }
         int64_t steps = len;
         if (a.nS > 0 && scatter) {
             int64_t m = len;
@@ -1685,6 +1691,35 @@ coupling_xf_kernel(int64_t G, int SG, int SGP, const T* __restrict__ cfy, const 
     double* dst = partial + (static_cast<int64_t>(blockIdx.x) * SG + h) * CP + 4 * q;
 #pragma unroll
     for (int j = 0; j < 4; ++j) dst[j] = static_cast<double>(acc[j]);
+}
+
+
+// ---------------------------------------------------------------------------
+// Fixed-effect coefficients per dimension (saved FEs): column c of dimension
+// d's [G_d][cols] column-major output from the alpha rows (non-primary dims)
+// or the primary segment means, for the column block starting at c0.
+// ---------------------------------------------------------------------------
+struct FeLayoutArgs {
+    int nd;
+    int32_t G[kMaxDims];
+    int64_t row0[kMaxDims];  // alpha row of level 0, or -1 for the primary dim
+    double* out[kMaxDims];   // [G_d][cols_total] column-major
+    int cols_total, c0, cb, CP;
+    const double* a;         // alpha rows [GR][CP]
+    const double* means;     // primary means [Gp][CP]
+};
+
+__global__ void fe_layout_kernel(const FeLayoutArgs f) {
+    for (int d = 0; d < f.nd; ++d) {
+        const int64_t total = static_cast<int64_t>(f.G[d]) * f.cb;
+        for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+             i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+            const int c = static_cast<int>(i / f.G[d]);
+            const int64_t g = i - static_cast<int64_t>(c) * f.G[d];
+            const double v = f.row0[d] < 0 ? f.means[g * f.CP + c] : f.a[(f.row0[d] + g) * f.CP + c];
+            f.out[d][static_cast<int64_t>(f.c0 + c) * f.G[d] + g] = v;
+        }
+    }
 }
 
 }  // namespace b200fe

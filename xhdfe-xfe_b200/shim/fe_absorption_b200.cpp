@@ -21,12 +21,16 @@
 // when the GPU backend was requested, src/fe_absorption.cpp:9227-9237);
 // return true with converged=false on non-convergence; never throw.  Features
 // this library does not provide yet return false, so the reference fails
-// closed rather than silently using another path: heterogeneous slopes, saved
-// fixed effects (retain_fixed_effects) and group/individual FEs.  The AKM/KSS
-// solver (akm_cuda_*) runs on the library's batched PCG (b200fe_kss_*).
+// closed rather than silently using another path: heterogeneous slopes,
+// group/individual FEs, and saved fixed effects in the reference's per-sweep
+// means mode.  Saved FEs in the coefficient mode (fe_alpha_y / fe_alpha_X,
+// what recover_fixed_effects consumes) come from b200fe_absorb_fe.  The
+// AKM/KSS solver (akm_cuda_*) runs on the library's batched PCG
+// (b200fe_kss_*).
 
 #include <Eigen/Dense>
 
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 #include <vector>
@@ -74,7 +78,14 @@ bool absorb_fixed_effects_cuda(const Eigen::Ref<const Eigen::VectorXd>& y,
             result.converged = true;
             return true;
         }
-        if (fe_inputs.size() > B200FE_MAX_DIMS || options.retain_fixed_effects) return false;
+        if (fe_inputs.size() > B200FE_MAX_DIMS) return false;
+        // saved FEs: the coefficient path of the reference (store_alphas,
+        // src/fe_absorption_cuda.cu:2345-2349); its other retain mode returns
+        // per-sweep means this solver does not form, so it fails closed
+        const bool save_fe = options.retain_fixed_effects;
+        if (save_fe && (options.fe_recovery_method != FeRecoveryMethod::Hybrid ||
+                        k > options.savefe_fastpath_max_cols))
+            return false;
         std::vector<const int32_t*> gids;
         std::vector<int32_t> levels;
         for (const GpuFeInput& fe : fe_inputs) {
@@ -89,17 +100,54 @@ bool absorb_fixed_effects_cuda(const Eigen::Ref<const Eigen::VectorXd>& y,
         o.tol = options.tol > 0.0 ? options.tol : 1e-8;
         o.tolerance_mode = static_cast<int>(options.tolerance_mode);
         if (options.max_iter > 0) o.max_iter = options.max_iter;
+        if (save_fe) {
+            // recover_fixed_effects accepts the coefficients only if the
+            // residual's group means stay below fe_tolerance (an absolute
+            // check): solve two orders tighter than that
+            const double fe_tol = options.fe_tolerance > 0.0 ? options.fe_tolerance : o.tol;
+            o.tol = std::max(std::min(o.tol, fe_tol) * 1e-2, 1e-14);
+        }
         // contiguous copies: Eigen::Ref may have an inner stride
         const Eigen::VectorXd yc = y;
         const Eigen::MatrixXd Xc = X;
         result.y_tilde.resize(n);
         result.X_tilde.resize(n, k);
+        const std::size_t D = fe_inputs.size();
+        std::vector<Eigen::MatrixXd> fe(save_fe ? D : 0);
+        std::vector<double*> fe_ptr(D, nullptr);
+        for (std::size_t d = 0; d < fe.size(); ++d) {
+            fe[d].resize(levels[d], k + 1);  // column-major, column 0 for y
+            fe_ptr[d] = fe[d].data();
+        }
         b200fe_result r;
-        const int rc = b200fe_absorb(ctx, yc.data(), k ? Xc.data() : nullptr, n, k,
-                                     static_cast<int>(gids.size()), gids.data(), levels.data(),
-                                     weights ? weights->data() : nullptr, &o,
-                                     result.y_tilde.data(), k ? result.X_tilde.data() : nullptr, &r);
+        const int rc = b200fe_absorb_fe(ctx, yc.data(), k ? Xc.data() : nullptr, n, k,
+                                        static_cast<int>(gids.size()), gids.data(), levels.data(),
+                                        weights ? weights->data() : nullptr, &o,
+                                        result.y_tilde.data(), k ? result.X_tilde.data() : nullptr,
+                                        save_fe ? fe_ptr.data() : nullptr, &r);
         if (rc != B200FE_OK && rc != B200FE_NOT_CONVERGED) return false;
+        if (save_fe) {  // the fields the reference fills (src/fe_absorption_cuda.cu:4663-4690)
+            result.fe_group_ids.assign(D, {});
+            result.fe_weight_sums.assign(D, Eigen::VectorXd());
+            result.fe_alpha_y.assign(D, Eigen::VectorXd());
+            result.fe_alpha_X.assign(D, Eigen::MatrixXd());
+            result.fe_means.clear();
+            for (std::size_t d = 0; d < D; ++d) {
+                const int G = levels[d];
+                result.fe_group_ids[d].assign(fe_inputs[d].group_ids, fe_inputs[d].group_ids + n);
+                result.fe_weight_sums[d].resize(G);
+                if (fe_inputs[d].weight_sums) {
+                    for (int g = 0; g < G; ++g) result.fe_weight_sums[d][g] = fe_inputs[d].weight_sums[g];
+                } else {
+                    result.fe_weight_sums[d].setZero();
+                    for (int64_t i = 0; i < n; ++i)
+                        result.fe_weight_sums[d][fe_inputs[d].group_ids[i]] +=
+                            weights ? (*weights)[i] : 1.0;
+                }
+                result.fe_alpha_y[d] = fe[d].col(0);
+                result.fe_alpha_X[d] = fe[d].rightCols(k);
+            }
+        }
         result.iterations = r.iterations;
         result.converged = rc == B200FE_OK;
         result.fe_levels.clear();
