@@ -208,6 +208,49 @@ int b200fe_demean_sorted_noalloc(const double* d_v, int64_t n, int cols,
                                  void* stream);
 
 /* ---------------------------------------------------------------------------
+ * OLS on within-transformed data: the reference's hdfe::detail::run_ols
+ * (include/ols.hpp:40-51, src/ols.cpp:1237-1520) with its covariance
+ * conventions (compute_covariance, src/ols.cpp:495-700): coefficients from
+ * X'WX b = X'Wy, residuals e = y - X b, RSS = sum w e^2, df_resid =
+ * max(0, n_eff - p), and
+ *   se_type 0 (homoskedastic): cov = RSS/df_resid (X'WX)^-1;
+ *   se_type 1 (robust):        cov = (X'WX)^-1 [sum (w e)^2 x x'] (X'WX)^-1
+ *                              (frequency weights: sum w e^2 x x');
+ *   se_type 2 (cluster):       cov = scale (X'WX)^-1 [sum_g s_g s_g'] (X'WX)^-1,
+ *                              s_g = sum_{i in g} w e x, scale =
+ *                              G/(G-1) (n_eff-1)/df_resid, G = non-empty clusters.
+ * The data-sized moments (Gram, residual pass, cluster scores in cluster
+ * order) run on the device with fixed-order sums; the p x p algebra on the
+ * host.  X is n x p column-major (ld = n), p <= B200FE_OLS_MAX_P; cluster ids
+ * dense in [0, num_clusters).  n_effective <= 0 means n.
+ * ------------------------------------------------------------------------- */
+#define B200FE_OLS_MAX_P 32
+
+typedef struct b200fe_ols_result {
+    int p;
+    int num_clusters;
+    double rss, sigma2, df_resid, cov_scale, cluster_u2;
+    double coef[B200FE_OLS_MAX_P];
+    double se[B200FE_OLS_MAX_P];
+    double cov[B200FE_OLS_MAX_P * B200FE_OLS_MAX_P];      /* p x p column-major */
+    double xtx_inv[B200FE_OLS_MAX_P * B200FE_OLS_MAX_P];  /* p x p column-major */
+} b200fe_ols_result;
+
+/* Device arrays (e.g. the output of b200fe_absorb_device: y = column 0, X =
+ * the next p columns).  Returns B200FE_INVALID_ARG when X'WX is not
+ * positive definite (the reference throws "Failed to factorize X'X"). */
+int b200fe_ols_device(b200fe_context* ctx, const double* d_y, const double* d_X,
+                      int64_t n, int p, const double* d_weights,
+                      const int32_t* d_clusters, int32_t num_clusters, int se_type,
+                      double n_effective, int weights_are_frequencies,
+                      b200fe_ols_result* out);
+/* Host arrays (copied in on the context's stream). */
+int b200fe_ols(b200fe_context* ctx, const double* y, const double* X, int64_t n, int p,
+               const double* weights, const int32_t* clusters, int32_t num_clusters,
+               int se_type, double n_effective, int weights_are_frequencies,
+               b200fe_ols_result* out);
+
+/* ---------------------------------------------------------------------------
  * AKM/KSS two-way solver: Jacobi-PCG on the grounded worker-partialled firm
  * Laplacian S = Df - B' Dw^{-1} B over the match (worker-firm pair) structure,
  * the firm-side system of the leave-out (KSS) variance decomposition.  The

@@ -144,6 +144,10 @@ def rlib(path: Path = REF_SO) -> ctypes.CDLL:
             lib.xref_recover_fe.argtypes = [_vp, _i64, _vp, _int, _vp, P(XrefOptions), _dbl, _vp,
                                             P(_int), P(_dbl), ctypes.c_char_p, _int]
             lib.xref_recover_fe.restype = _int
+        if hasattr(lib, "xref_run_ols"):
+            lib.xref_run_ols.argtypes = [_vp, _vp, _i64, _int, _vp, _vp, _int, _dbl, _dbl, _dbl, _int,
+                                         _vp, _vp, _vp, _vp, ctypes.c_char_p, _int]
+            lib.xref_run_ols.restype = _int
         if hasattr(lib, "xref_akm_kss"):
             lib.xref_akm_kss.argtypes = [_vp, _vp, _vp, _i64, _vp, ctypes.c_uint64, _dbl, _vp, P(_int),
                                          P(ctypes.c_longlong), ctypes.c_char_p, _int]
@@ -303,3 +307,31 @@ def ref_recover_fe(partial, fes, weights=None, *, tol=1e-8, fe_tolerance=0.0, th
         raise RuntimeError(err.value.decode())
     return {"contributions": contrib, "iterations": info[0], "converged": bool(info[1]),
             "max_delta": dinfo[0]}
+
+
+SE_CODES = {"unadjusted": 0, "robust": 1, "cluster": 2}
+
+
+def ref_run_ols(y, X, weights=None, clusters=None, *, se_type="unadjusted", tss=0.0,
+                within_tss=0.0, n_effective=-1.0, weights_are_frequencies=False, lib_path=REF_SO):
+    """The reference's hdfe::detail::run_ols (include/ols.hpp:40-51)."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    X = np.asfortranarray(X, dtype=np.float64)
+    n, p = X.shape
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    c = None if clusters is None else np.ascontiguousarray(clusters, dtype=np.int32)
+    coef, se = np.zeros(p), np.zeros(p)
+    cov = np.zeros((p, p), order="F")
+    sc = np.zeros(8)
+    err = ctypes.create_string_buffer(512)
+    rc = rlib(lib_path).xref_run_ols(y.ctypes.data, X.ctypes.data, n, p,
+                                    None if w is None else w.ctypes.data,
+                                    None if c is None else c.ctypes.data, SE_CODES[se_type], tss,
+                                    within_tss, n_effective, int(weights_are_frequencies),
+                                    coef.ctypes.data, se.ctypes.data, cov.ctypes.data,
+                                    sc.ctypes.data, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return {"coef": coef, "se": se, "cov": cov, "rss": sc[0], "sigma2": sc[1], "df_resid": sc[2],
+            "cov_scale": sc[3], "cluster_u2": sc[4], "r2": sc[5], "r2_within": sc[6],
+            "num_clusters": int(sc[7])}

@@ -12,6 +12,7 @@
 //   xref_fit          -> hdfe::v11::HdfeRegressorV11::fit         (src/hdfe_regressor_v11.cpp:7522)
 //   xref_akm_kss      -> hdfe::akm::akm_kss_decompose              (include/hdfe/akm_kss.hpp:227-233)
 //   xref_recover_fe   -> hdfe::detail::recover_fixed_effects        (include/fe_absorption.hpp:127-130)
+//   xref_run_ols      -> hdfe::detail::run_ols                      (include/ols.hpp:40-51)
 // Every entry point catches all exceptions and returns a nonzero status with
 // the message copied into err (the reference's own fail-closed contract).
 
@@ -28,6 +29,7 @@
 #include "fe_absorption_cuda.hpp"
 #include "hdfe/hdfe_regressor.hpp"
 #include "hdfe/akm_kss.hpp"
+#include "ols.hpp"
 #include "hdfe/hdfe_regressor_v11.hpp"
 
 namespace {
@@ -321,6 +323,51 @@ int xref_recover_fe(const double* partial, int64_t n, const int32_t* fe_flat, in
         info[0] = r.iterations;
         info[1] = r.converged ? 1 : 0;
         dinfo[0] = r.max_delta;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+// OLS on within-transformed data.  X: n x p column-major; clusters: n dense
+// ids or null.  out_vec (4p): coef, se, then covariance (p x p column-major)
+// follows in out_cov; scalars (8): rss, sigma2, df_resid, cov_scale,
+// cluster_u2, r2, r2_within, num_clusters.
+int xref_run_ols(const double* y, const double* X, int64_t n, int p, const double* w,
+                 const int32_t* clusters, int se_type, double tss, double within_tss,
+                 double n_effective, int weights_are_frequencies, double* coef, double* se,
+                 double* cov, double* scalars, char* err, int err_len) {
+    try {
+        const VectorXd yv = Map<const VectorXd>(y, n);
+        const MatrixXd Xm = Map<const MatrixXd>(X, n, p);
+        VectorXd wv;
+        if (w) wv = Map<const VectorXd>(w, n);
+        VectorXi cv;
+        if (clusters) {
+            cv.resize(n);
+            for (int64_t i = 0; i < n; ++i) cv[i] = clusters[i];
+        }
+        const hdfe::detail::OlsResult r = hdfe::detail::run_ols(
+            yv, Xm, w ? &wv : nullptr, clusters ? &cv : nullptr,
+            static_cast<hdfe::StandardErrorType>(se_type), tss, within_tss, n_effective,
+            weights_are_frequencies != 0);
+        for (int j = 0; j < p; ++j) {
+            coef[j] = r.coefficients[j];
+            se[j] = r.std_errors[j];
+        }
+        std::memcpy(cov, r.covariance.data(), sizeof(double) * p * p);
+        scalars[0] = r.rss;
+        scalars[1] = r.sigma2;
+        scalars[2] = r.df_resid;
+        scalars[3] = r.cov_scale;
+        scalars[4] = r.cluster_u2;
+        scalars[5] = r.r2;
+        scalars[6] = r.r2_within;
+        scalars[7] = r.num_clusters;
         return 0;
     } catch (const std::exception& e) {
         set_err(err, err_len, e.what());

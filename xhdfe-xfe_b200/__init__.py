@@ -9,6 +9,7 @@ from .absorber import (  # noqa: F401
     AbsorberError,
     AbsorptionResult,
     FeRecoveryResult,
+    OlsResult,
     absorb_fixed_effects,
     cuda_backend_available,
     demean_raw,
@@ -17,6 +18,7 @@ from .absorber import (  # noqa: F401
     make_options,
     partial_out,
     recover_fixed_effects,
+    run_ols,
 )
 from .kss import KssSolver, kss_system, max_lanes, stable_sort_u64  # noqa: F401
 

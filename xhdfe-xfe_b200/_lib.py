@@ -42,6 +42,8 @@ EXPORTED_SYMBOLS = (
     "b200fe_demean_raw",
     "b200fe_fe_recovery_max_delta",
     "b200fe_demean_sorted_noalloc",
+    "b200fe_ols_device",
+    "b200fe_ols",
     "b200fe_kss_create",
     "b200fe_kss_destroy",
     "b200fe_kss_last_error",
@@ -66,6 +68,21 @@ class Options(ctypes.Structure):
         ("max_outer", ctypes.c_int),
         ("profile", ctypes.c_int),
         ("pass_kernel", ctypes.c_int),
+    ]
+
+
+OLS_MAX_P = 32
+
+
+class OlsResult(ctypes.Structure):
+    """b200fe_ols_result (include/b200fe.h)."""
+    _fields_ = [
+        ("p", ctypes.c_int), ("num_clusters", ctypes.c_int),
+        ("rss", ctypes.c_double), ("sigma2", ctypes.c_double), ("df_resid", ctypes.c_double),
+        ("cov_scale", ctypes.c_double), ("cluster_u2", ctypes.c_double),
+        ("coef", ctypes.c_double * OLS_MAX_P), ("se", ctypes.c_double * OLS_MAX_P),
+        ("cov", ctypes.c_double * (OLS_MAX_P * OLS_MAX_P)),
+        ("xtx_inv", ctypes.c_double * (OLS_MAX_P * OLS_MAX_P)),
     ]
 
 
@@ -138,6 +155,12 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.b200fe_absorb_fe.argtypes = [vp, vp, vp, i64, c_int, c_int, pp, vp, vp,
                                      ctypes.POINTER(Options), vp, vp, pp, ctypes.POINTER(Result)]
     lib.b200fe_absorb_fe.restype = c_int
+    lib.b200fe_ols_device.argtypes = [vp, vp, vp, i64, c_int, vp, vp, ctypes.c_int32, c_int,
+                                      ctypes.c_double, c_int, ctypes.POINTER(OlsResult)]
+    lib.b200fe_ols_device.restype = c_int
+    lib.b200fe_ols.argtypes = [vp, vp, vp, i64, c_int, vp, vp, ctypes.c_int32, c_int,
+                               ctypes.c_double, c_int, ctypes.POINTER(OlsResult)]
+    lib.b200fe_ols.restype = c_int
     lib.b200fe_kss_create.argtypes = [c_int, c_int, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp,
                                       ctypes.POINTER(vp)]
     lib.b200fe_kss_create.restype = c_int

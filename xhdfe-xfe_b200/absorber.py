@@ -373,6 +373,70 @@ def partial_out(y, X, fes, weights=None, *, drop_singletons=True, device=0,
     return res
 
 
+SE_TYPES = {"unadjusted": 0, "homoskedastic": 0, "robust": 1, "cluster": 2}
+
+
+@dataclass
+class OlsResult:
+    """Fields of hdfe::detail::OlsResult (include/ols.hpp:13-34) this library
+    computes (residuals stay on the device)."""
+    coefficients: np.ndarray
+    std_errors: np.ndarray
+    covariance: np.ndarray
+    xtx_inv: np.ndarray
+    rss: float
+    sigma2: float
+    df_resid: float
+    cov_scale: float
+    cluster_u2: float
+    num_clusters: int
+    nobs: int
+
+
+def run_ols(y, X, weights=None, clusters=None, *, se_type="unadjusted", n_effective=-1.0,
+            weights_are_frequencies=False, device=0) -> OlsResult:
+    """hdfe::detail::run_ols (include/ols.hpp:40-51) on within-transformed host
+    arrays: moments on the device, the p x p algebra on the host.  ``clusters``:
+    ids (made dense here); torch CUDA tensors are taken as device arrays."""
+    se = SE_TYPES[se_type]
+    ab = _thread_absorber(device)
+    r = _lib.OlsResult()
+    try:
+        import torch
+        on_device = isinstance(y, torch.Tensor)
+    except ImportError:
+        on_device = False
+    if on_device:
+        n, p = int(X.shape[1]), int(X.shape[0])  # X: (p, n) contiguous = column-major n x p
+        cl = None if clusters is None else clusters
+        G = 0 if clusters is None else int(clusters.max().item()) + 1
+        rc = ab.lib.b200fe_ols_device(
+            ab.handle, y.data_ptr(), X.data_ptr(), n, p,
+            None if weights is None else weights.data_ptr(),
+            None if cl is None else cl.data_ptr(), G, se, float(n_effective),
+            int(weights_are_frequencies), ctypes.byref(r))
+    else:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        X = np.asfortranarray(X, dtype=np.float64)
+        if X.ndim == 1:
+            X = X[:, None]
+        n, p = X.shape
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        cl, G = (None, 0) if clusters is None else dense_ids(clusters)
+        rc = ab.lib.b200fe_ols(
+            ab.handle, y.ctypes.data, X.ctypes.data, n, p, None if w is None else w.ctypes.data,
+            None if cl is None else cl.ctypes.data, G, se, float(n_effective),
+            int(weights_are_frequencies), ctypes.byref(r))
+    if rc != _lib.OK:
+        raise ab._err(rc)
+    cov = np.ctypeslib.as_array(r.cov)[: p * p].reshape(p, p, order="F").copy()
+    inv = np.ctypeslib.as_array(r.xtx_inv)[: p * p].reshape(p, p, order="F").copy()
+    return OlsResult(coefficients=np.array(r.coef[:p]), std_errors=np.array(r.se[:p]),
+                     covariance=cov, xtx_inv=inv, rss=r.rss, sigma2=r.sigma2,
+                     df_resid=r.df_resid, cov_scale=r.cov_scale, cluster_u2=r.cluster_u2,
+                     num_clusters=int(r.num_clusters), nobs=n)
+
+
 def demean_raw(Y, X, fes, nlev, tol=1e-8, max_iter=0) -> int:
     """In-place demean (schwarz_demean_raw's interface).  Returns iterations."""
     lib = _lib.load()

@@ -10,6 +10,7 @@
 #include <cub/device/device_segmented_reduce.cuh>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -23,6 +24,7 @@
 #include "b200fe.h"
 #include "kernels.cuh"
 #include "setup_kernels.cuh"
+#include "ols_kernels.cuh"
 
 using namespace b200fe;
 
@@ -1963,6 +1965,362 @@ int b200fe_fe_recovery_max_delta(b200fe_context* ctx, const double* residual, in
     }
     return fe_recovery_impl(ctx, residual, n, num_dims, group_ids, num_groups, weights,
                             sweep_order, out_max_delta);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// OLS (run_ols): moments on the device, p x p algebra on the host
+// ---------------------------------------------------------------------------
+namespace {
+
+// Symmetric-pivoted LDL' of the p x p symmetric matrix A (column-major), in
+// long double: at step k the largest remaining diagonal entry is the pivot
+// (the rule of the robust Cholesky in Eigen's LDLT, which the reference's
+// run_ols uses).  Solves apply the pseudo-inverse of D: a pivot of magnitude
+// at most DBL_MIN is treated as zero and its component set to zero, so a
+// rank-deficient X'X yields zero coefficients in its null directions, as the
+// reference's solve does, instead of failing.
+struct Ldlt {
+    int p = 0;
+    std::vector<long double> L;  // unit lower, column-major
+    std::vector<long double> D;
+    std::vector<int> perm;       // row k of the factor is row perm[k] of A
+};
+
+Ldlt ldlt_factor(const std::vector<double>& A, int p) {
+    Ldlt f;
+    f.p = p;
+    std::vector<long double> M(A.begin(), A.end());
+    f.perm.resize(p);
+    for (int i = 0; i < p; ++i) f.perm[i] = i;
+    auto at = [&](int i, int j) -> long double& { return M[static_cast<size_t>(j) * p + i]; };
+    f.D.assign(p, 0.0L);
+    for (int k = 0; k < p; ++k) {
+        int piv = k;
+        for (int i = k + 1; i < p; ++i)
+            if (fabsl(at(i, i)) > fabsl(at(piv, piv))) piv = i;
+        if (piv != k) {
+            for (int j = 0; j < p; ++j) std::swap(at(k, j), at(piv, j));
+            for (int i = 0; i < p; ++i) std::swap(at(i, k), at(i, piv));
+            std::swap(f.perm[k], f.perm[piv]);
+        }
+        const long double d = at(k, k);
+        f.D[k] = d;
+        const bool zero = fabsl(d) <= static_cast<long double>(DBL_MIN);
+        for (int i = k + 1; i < p; ++i) at(i, k) = zero ? 0.0L : at(i, k) / d;
+        for (int j = k + 1; j < p; ++j)
+            for (int i = j; i < p; ++i) {
+                at(i, j) -= at(i, k) * at(j, k) * d;
+                at(j, i) = at(i, j);
+            }
+    }
+    f.L = M;
+    return f;
+}
+
+// x = A^+ b through the factor (b of length p, overwritten)
+void ldlt_solve(const Ldlt& f, std::vector<long double>& b) {
+    const int p = f.p;
+    std::vector<long double> y(p);
+    for (int k = 0; k < p; ++k) y[k] = b[f.perm[k]];
+    for (int i = 0; i < p; ++i)
+        for (int k = 0; k < i; ++k) y[i] -= f.L[static_cast<size_t>(k) * p + i] * y[k];
+    for (int i = 0; i < p; ++i)
+        y[i] = fabsl(f.D[i]) > static_cast<long double>(DBL_MIN) ? y[i] / f.D[i] : 0.0L;
+    for (int i = p - 1; i >= 0; --i)
+        for (int k = i + 1; k < p; ++k) y[i] -= f.L[static_cast<size_t>(i) * p + k] * y[k];
+    for (int k = 0; k < p; ++k) b[f.perm[k]] = y[k];
+}
+
+// sum_i f_i a_i b_i over the column pairs, summed over CTAs; out [npairs]
+int run_moments(b200fe_context* ctx, MomentArgs m, std::vector<double>& out, double* rss) {
+    const cudaStream_t s = ctx->stream;
+    const int npairs = m.P * (m.P + 1) / 2;
+    const int grid = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>((m.n + kOlsTile - 1) / kOlsTile, static_cast<int64_t>(ctx->num_sms) * 4)));
+    double *part, *sum, *rpart = nullptr, *rsum = nullptr;
+    B_CHECK(get_buf(ctx, "ols_part", static_cast<size_t>(grid) * npairs, &part));
+    B_CHECK(get_buf(ctx, "ols_sum", static_cast<size_t>(npairs) + 1, &sum));
+    if (rss) {
+        B_CHECK(get_buf(ctx, "ols_rpart", grid, &rpart));
+        B_CHECK(get_buf(ctx, "ols_rsum", 1, &rsum));
+    }
+    m.partial = part;
+    m.rss_partial = rpart;
+    moments_kernel<<<grid, kOlsThreads, 0, s>>>(m);
+    B_LAUNCHED();
+    partial_sum_kernel<<<grid_for(ctx, npairs, 256, 1), 256, 0, s>>>(part, grid, npairs, sum);
+    B_LAUNCHED();
+    if (rss) {
+        partial_sum_kernel<<<1, 32, 0, s>>>(rpart, grid, 1, rsum);
+        B_LAUNCHED();
+    }
+    out.assign(npairs, 0.0);
+    B_TRY(cudaMemcpyAsync(out.data(), sum, sizeof(double) * npairs, cudaMemcpyDeviceToHost, s));
+    if (rss) B_TRY(cudaMemcpyAsync(rss, rsum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    B_TRY(cudaStreamSynchronize(s));
+    return B200FE_OK;
+}
+
+// upper-triangle pair list -> symmetric P x P (column-major)
+std::vector<double> unpack_pairs(const std::vector<double>& v, int P) {
+    std::vector<double> M(static_cast<size_t>(P) * P);
+    int t = 0;
+    for (int a = 0; a < P; ++a)
+        for (int b = a; b < P; ++b, ++t) {
+            M[static_cast<size_t>(b) * P + a] = v[t];
+            M[static_cast<size_t>(a) * P + b] = v[t];
+        }
+    return M;
+}
+
+int ols_impl(b200fe_context* ctx, const double* d_y, const double* d_X, int64_t n, int p,
+             const double* d_w, const int32_t* d_cl, int32_t G, int se_type, double n_effective,
+             int wfreq, b200fe_ols_result* out) {
+    const cudaStream_t s = ctx->stream;
+    std::memset(out, 0, sizeof(*out));
+    out->p = p;
+    // 1. Gram [X y]' W [X y]
+    MomentArgs m{};
+    m.n = n;
+    m.P = p + 1;
+    m.p = p;
+    m.X = d_X;
+    m.cs = n;
+    m.rs = 1;
+    m.y = d_y;
+    m.w = d_w;
+    m.mode = kMomGram;
+    std::vector<double> g;
+    B_CHECK(run_moments(ctx, m, g, nullptr));
+    const std::vector<double> GM = unpack_pairs(g, p + 1);
+    std::vector<double> xtx(static_cast<size_t>(p) * p);
+    std::vector<long double> xty(p);
+    for (int j = 0; j < p; ++j) {
+        for (int i = 0; i < p; ++i) xtx[static_cast<size_t>(j) * p + i] = GM[static_cast<size_t>(j) * (p + 1) + i];
+        xty[j] = GM[static_cast<size_t>(p) * (p + 1) + j];
+    }
+    for (int i = 0; i < p * p; ++i)
+        if (!std::isfinite(xtx[i])) {
+            ctx->err = "Failed to factorize X'X; matrix may be singular";
+            return B200FE_INVALID_ARG;
+        }
+    const Ldlt fac = ldlt_factor(xtx, p);
+    ldlt_solve(fac, xty);
+    for (int j = 0; j < p; ++j) out->coef[j] = static_cast<double>(xty[j]);
+    std::vector<double> inv(static_cast<size_t>(p) * p);
+    for (int j = 0; j < p; ++j) {
+        std::vector<long double> e(p, 0.0L);
+        e[j] = 1.0L;
+        ldlt_solve(fac, e);
+        for (int i = 0; i < p; ++i) inv[static_cast<size_t>(j) * p + i] = static_cast<double>(e[i]);
+    }
+    for (int i = 0; i < p * p; ++i) out->xtx_inv[i] = inv[i];
+    // 2. residual pass: RSS and the robust meat
+    m.P = p;
+    m.mode = kMomRobust;
+    m.wfreq = wfreq;
+    for (int j = 0; j < p; ++j) m.beta[j] = out->coef[j];
+    std::vector<double> rm;
+    double rss = 0.0;
+    B_CHECK(run_moments(ctx, m, rm, &rss));
+    const double n_eff = n_effective > 0.0 ? n_effective : static_cast<double>(n);
+    const double df_resid = std::max(0.0, n_eff - p);
+    out->rss = rss;
+    out->df_resid = df_resid;
+    out->sigma2 = df_resid > 0.0 ? rss / df_resid : 0.0;
+    out->cov_scale = 1.0;
+    std::vector<double> meat;
+    if (se_type == 1) {
+        meat = unpack_pairs(rm, p);
+    } else if (se_type == 2) {
+        // 3. cluster scores in cluster order (stable sort by cluster id)
+        int32_t *keys, *perm, *skeys, *iota, *off;
+        B_CHECK(get_buf(ctx, "ols_keys", n, &keys));
+        B_CHECK(get_buf(ctx, "ols_perm", n, &perm));
+        B_CHECK(get_buf(ctx, "ols_skeys", n, &skeys));
+        B_CHECK(get_buf(ctx, "ols_iota", n, &iota));
+        B_CHECK(get_buf(ctx, "ols_off", static_cast<size_t>(G) + 1, &off));
+        iota_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(iota, n);
+        B_LAUNCHED();
+        B_CHECK(cub_sort_pairs(ctx, d_cl, skeys, iota, perm, n, G));
+        segment_offsets_kernel<<<grid_for(ctx, n + 1, 256), 256, 0, s>>>(skeys, n, G, off);
+        B_LAUNCHED();
+        (void)keys;
+        int32_t *nch, *ch_off, *mflag, *midx;
+        B_CHECK(get_buf(ctx, "ols_nch", static_cast<size_t>(G) + 1, &nch));
+        B_CHECK(get_buf(ctx, "ols_choff", static_cast<size_t>(G) + 1, &ch_off));
+        B_CHECK(get_buf(ctx, "ols_mflag", static_cast<size_t>(G) + 1, &mflag));
+        B_CHECK(get_buf(ctx, "ols_midx", static_cast<size_t>(G) + 1, &midx));
+        B_TRY(cudaMemsetAsync(nch, 0, sizeof(int32_t) * (static_cast<size_t>(G) + 1), s));
+        B_TRY(cudaMemsetAsync(mflag, 0, sizeof(int32_t) * (static_cast<size_t>(G) + 1), s));
+        chunk_count_kernel<<<grid_for(ctx, G, 256), 256, 0, s>>>(off, G, kOlsChunk, nch);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, nch, ch_off, static_cast<int64_t>(G) + 1));
+        multi_flag_kernel<<<grid_for(ctx, G, 256), 256, 0, s>>>(nch, G, mflag);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, mflag, midx, static_cast<int64_t>(G) + 1));
+        int hc[2];
+        B_CHECK(sync_read_int(ctx, ch_off + G, 1, &hc[0]));
+        B_CHECK(sync_read_int(ctx, midx + G, 1, &hc[1]));
+        const int64_t nchunks = hc[0], nmulti = hc[1];
+        int32_t *cgrp, *cbeg, *cend, *mgrp, *mc0, *mc1;
+        uint8_t* cwhole;
+        B_CHECK(get_buf(ctx, "ols_cgrp", nchunks, &cgrp));
+        B_CHECK(get_buf(ctx, "ols_cbeg", nchunks, &cbeg));
+        B_CHECK(get_buf(ctx, "ols_cend", nchunks, &cend));
+        B_CHECK(get_buf(ctx, "ols_cwhole", nchunks, &cwhole));
+        B_CHECK(get_buf(ctx, "ols_mgrp", std::max<int64_t>(nmulti, 1), &mgrp));
+        B_CHECK(get_buf(ctx, "ols_mc0", std::max<int64_t>(nmulti, 1), &mc0));
+        B_CHECK(get_buf(ctx, "ols_mc1", std::max<int64_t>(nmulti, 1), &mc1));
+        chunk_fill_kernel<<<grid_for(ctx, G, 256), 256, 0, s>>>(off, G, kOlsChunk, ch_off, cgrp, cbeg,
+                                                                cend, cwhole, midx, mgrp, mc0, mc1);
+        B_LAUNCHED();
+        double *scores, *cpart;
+        const int width = p + 1;
+        B_CHECK(get_buf(ctx, "ols_scores", static_cast<size_t>(G) * width, &scores));
+        B_CHECK(get_buf(ctx, "ols_cpart", static_cast<size_t>(nchunks) * width, &cpart));
+        ClusterArgs c{};
+        c.nchunks = nchunks;
+        c.chunk_grp = cgrp;
+        c.chunk_beg = cbeg;
+        c.chunk_end = cend;
+        c.chunk_whole = cwhole;
+        c.perm = perm;
+        c.p = p;
+        c.X = d_X;
+        c.ld = n;
+        c.y = d_y;
+        c.w = d_w;
+        for (int j = 0; j < p; ++j) c.beta[j] = out->coef[j];
+        c.scores = scores;
+        c.chunk_part = cpart;
+        cluster_chunk_kernel<<<grid_for(ctx, nchunks * 32, kOlsThreads, 8), kOlsThreads, 0, s>>>(c);
+        B_LAUNCHED();
+        if (nmulti > 0) {
+            cluster_combine_kernel<<<grid_for(ctx, nmulti * width, 256), 256, 0, s>>>(
+                nmulti, mgrp, mc0, mc1, cpart, width, scores);
+            B_LAUNCHED();
+        }
+        int* cnt;
+        B_CHECK(get_buf(ctx, "ols_cnt", 1, &cnt));
+        B_TRY(cudaMemsetAsync(cnt, 0, sizeof(int), s));
+        count_nonempty_kernel<<<grid_for(ctx, G, 256), 256, 0, s>>>(off, G, cnt);
+        B_LAUNCHED();
+        int ncl = 0;
+        B_CHECK(sync_read_int(ctx, cnt, 1, &ncl));
+        // meat = sum_g s_g s_g', cluster_u2 = sum_g u_g^2: moments of the scores
+        MomentArgs q{};
+        q.n = G;
+        q.P = p + 1;
+        q.p = p;
+        q.X = scores;
+        q.cs = 1;
+        q.rs = width;
+        q.y = scores + p;
+        q.mode = kMomPlain;
+        std::vector<double> sm;
+        B_CHECK(run_moments(ctx, q, sm, nullptr));
+        const std::vector<double> SM = unpack_pairs(sm, p + 1);
+        meat.assign(static_cast<size_t>(p) * p, 0.0);
+        for (int j = 0; j < p; ++j)
+            for (int i = 0; i < p; ++i) meat[static_cast<size_t>(j) * p + i] = SM[static_cast<size_t>(j) * (p + 1) + i];
+        out->cluster_u2 = SM[static_cast<size_t>(p) * (p + 1) + p];
+        out->num_clusters = ncl;
+        if (ncl > 1 && df_resid > 0.0)
+            out->cov_scale = (static_cast<double>(ncl) / (ncl - 1.0)) * ((n_eff - 1.0) / df_resid);
+    }
+    // 4. covariance
+    if (se_type == 0) {
+        for (int i = 0; i < p * p; ++i) out->cov[i] = out->sigma2 * inv[i];
+    } else {
+        std::vector<long double> t(static_cast<size_t>(p) * p, 0.0L);  // inv * meat
+        for (int j = 0; j < p; ++j)
+            for (int k = 0; k < p; ++k) {
+                const long double mk = meat[static_cast<size_t>(j) * p + k];
+                for (int i = 0; i < p; ++i) t[static_cast<size_t>(j) * p + i] += inv[static_cast<size_t>(k) * p + i] * mk;
+            }
+        for (int j = 0; j < p; ++j)
+            for (int i = 0; i < p; ++i) {
+                long double v = 0.0L;
+                for (int k = 0; k < p; ++k) v += t[static_cast<size_t>(k) * p + i] * inv[static_cast<size_t>(j) * p + k];
+                out->cov[static_cast<size_t>(j) * p + i] = static_cast<double>(v) * out->cov_scale;
+            }
+    }
+    for (int j = 0; j < p; ++j) out->se[j] = std::sqrt(std::max(0.0, out->cov[static_cast<size_t>(j) * p + j]));
+    return B200FE_OK;
+}
+
+int ols_check(b200fe_context* ctx, int64_t n, int p, const void* y, const void* X, int se_type,
+              const void* cl, int32_t G, b200fe_ols_result* out) {
+    if (!ctx || !out || !y || !X || n <= 0 || n >= (int64_t(1) << 31) - 1 || p <= 0 ||
+        p > B200FE_OLS_MAX_P || se_type < 0 || se_type > 2 || (se_type == 2 && (!cl || G <= 0))) {
+        if (ctx) ctx->err = "invalid OLS arguments";
+        return B200FE_INVALID_ARG;
+    }
+    return B200FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200fe_ols_device(b200fe_context* ctx, const double* d_y, const double* d_X, int64_t n, int p,
+                      const double* d_weights, const int32_t* d_clusters, int32_t num_clusters,
+                      int se_type, double n_effective, int weights_are_frequencies,
+                      b200fe_ols_result* out) {
+    int rc = ols_check(ctx, n, p, d_y, d_X, se_type, d_clusters, num_clusters, out);
+    if (rc != B200FE_OK) return rc;
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return B200FE_UNAVAILABLE;
+    }
+    if (se_type == 2) {  // cluster ids must be dense in [0, G)
+        int* bad;
+        B_CHECK(get_buf(ctx, "ols_bad", 3, &bad));
+        B_TRY(cudaMemsetAsync(bad, 0, 3 * sizeof(int), ctx->stream));
+        validate_ids_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(d_clusters, n, num_clusters, 0, bad);
+        B_LAUNCHED();
+        int hb = 0;
+        B_CHECK(sync_read_int(ctx, bad, 1, &hb));
+        if (hb) {
+            ctx->err = "cluster ids out of range";
+            return B200FE_INVALID_ARG;
+        }
+    }
+    return ols_impl(ctx, d_y, d_X, n, p, d_weights, se_type == 2 ? d_clusters : nullptr,
+                    num_clusters, se_type, n_effective, weights_are_frequencies, out);
+}
+
+int b200fe_ols(b200fe_context* ctx, const double* y, const double* X, int64_t n, int p,
+               const double* weights, const int32_t* clusters, int32_t num_clusters, int se_type,
+               double n_effective, int weights_are_frequencies, b200fe_ols_result* out) {
+    int rc = ols_check(ctx, n, p, y, X, se_type, clusters, num_clusters, out);
+    if (rc != B200FE_OK) return rc;
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return B200FE_UNAVAILABLE;
+    }
+    const cudaStream_t s = ctx->stream;
+    double *dy, *dX, *dw = nullptr;
+    int32_t* dc = nullptr;
+    B_CHECK(get_buf(ctx, "ols_y", n, &dy));
+    B_CHECK(get_buf(ctx, "ols_X", static_cast<size_t>(n) * p, &dX));
+    B_TRY(cudaMemcpyAsync(dy, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    B_TRY(cudaMemcpyAsync(dX, X, sizeof(double) * n * p, cudaMemcpyHostToDevice, s));
+    if (weights) {
+        B_CHECK(get_buf(ctx, "ols_w", n, &dw));
+        B_TRY(cudaMemcpyAsync(dw, weights, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    }
+    if (se_type == 2) {
+        B_CHECK(get_buf(ctx, "ols_c", n, &dc));
+        B_TRY(cudaMemcpyAsync(dc, clusters, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    }
+    return b200fe_ols_device(ctx, dy, dX, n, p, dw, dc, num_clusters, se_type, n_effective,
+                             weights_are_frequencies, out);
 }
 
 }  // extern "C"
