@@ -208,6 +208,29 @@ int b200fe_demean_sorted_noalloc(const double* d_v, int64_t n, int cols,
                                  void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Preprocessing on the device (the reference does these on the host).
+ * ------------------------------------------------------------------------- */
+/* Dense group ids from raw int32 ids (device arrays), the rule of the
+ * reference's build_indexer (src/fe_absorption.cpp:845-940): if the raw range
+ * R = max - min + 1 is at most 50,000,000 and at most 2n, id = raw - min with
+ * num_groups = R, compacted in raw order (num_groups = distinct values) when
+ * fewer than 90% of the range is present; otherwise id = rank of the raw value
+ * among the distinct values.  num_levels_present = distinct values. */
+int b200fe_dense_ids_device(b200fe_context* ctx, const int32_t* d_raw, int64_t n,
+                            int32_t* d_out, int32_t* num_groups,
+                            int32_t* num_levels_present);
+/* Iterative singleton drop (device arrays): d_keep[i] = 0 for the rows removed
+ * by rounds that drop every kept row alone in its group of some dimension,
+ * until a round drops nothing or max_iter rounds (<= 0: 100, the reference's
+ * cap) ran; the reference's compute_keep_mask_drop_singletons
+ * (src/hdfe_regressor_v11.cpp:4056-4290).  ids dense in [0, num_groups[d]). */
+int b200fe_drop_singletons_device(b200fe_context* ctx, int num_dims,
+                                  const int32_t* const* d_ids,
+                                  const int32_t* num_groups, int64_t n,
+                                  uint8_t* d_keep, int max_iter, int64_t* dropped,
+                                  int* rounds);
+
+/* ---------------------------------------------------------------------------
  * OLS on within-transformed data: the reference's hdfe::detail::run_ols
  * (include/ols.hpp:40-51, src/ols.cpp:1237-1520) with its covariance
  * conventions (compute_covariance, src/ols.cpp:495-700): coefficients from

@@ -1,0 +1,33 @@
+"""CPU checks of the preprocessing oracle (oracle/preprocess_oracle.py): the
+restatement of the reference's build_indexer on hand-computed cases of its
+three branches, and its singleton cascade against the package's host mask
+(both reach the unique fixed point of the rule)."""
+
+import numpy as np
+
+
+def test_build_indexer_branches():
+    from oracle.preprocess_oracle import build_indexer
+    # dense range, >= 90% present: ids = raw - min, num_groups = range (a gap kept)
+    raw = np.array([5, 7, 6, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24, 5])
+    ids, G, present = build_indexer(raw)
+    assert G == 20 and present == 20 and ids.tolist() == (raw - 5).tolist()
+    raw = np.concatenate([np.arange(100, 110), np.arange(111, 200)])  # one gap in 100
+    ids, G, present = build_indexer(raw)
+    assert G == 100 and present == 99 and ids[10] == 11
+    # dense range, < 90% present: compacted in raw order
+    raw = np.array([-3, 10, 4, 10, -3, 7])
+    ids, G, present = build_indexer(raw)
+    assert (G, present) == (4, 4) and ids.tolist() == [0, 3, 1, 3, 0, 2]
+    # sparse range: ranks of the distinct values
+    raw = np.array([2_000_000_000, -7, 15, -7, 2_000_000_000])
+    ids, G, present = build_indexer(raw)
+    assert (G, present) == (3, 3) and ids.tolist() == [2, 0, 1, 0, 2]
+
+
+def test_singleton_oracle_matches_host_mask(pkg, panels):
+    from oracle.preprocess_oracle import singleton_keep
+    p = panels.akm_two_way(30_000, n_firms=2_000, seed=91, three_way=True)
+    keep, rounds = singleton_keep(p.fes)
+    assert rounds >= 1 and not keep.all()
+    assert np.array_equal(keep, pkg.drop_singletons_mask(p.fes))

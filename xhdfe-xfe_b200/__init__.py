@@ -14,6 +14,8 @@ from .absorber import (  # noqa: F401
     cuda_backend_available,
     demean_raw,
     dense_ids,
+    dense_ids_device,
+    drop_singletons_device,
     drop_singletons_mask,
     make_options,
     partial_out,

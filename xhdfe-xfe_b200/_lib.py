@@ -42,6 +42,8 @@ EXPORTED_SYMBOLS = (
     "b200fe_demean_raw",
     "b200fe_fe_recovery_max_delta",
     "b200fe_demean_sorted_noalloc",
+    "b200fe_dense_ids_device",
+    "b200fe_drop_singletons_device",
     "b200fe_ols_device",
     "b200fe_ols",
     "b200fe_kss_create",
@@ -155,6 +157,13 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.b200fe_absorb_fe.argtypes = [vp, vp, vp, i64, c_int, c_int, pp, vp, vp,
                                      ctypes.POINTER(Options), vp, vp, pp, ctypes.POINTER(Result)]
     lib.b200fe_absorb_fe.restype = c_int
+    lib.b200fe_dense_ids_device.argtypes = [vp, vp, i64, vp, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_int32)]
+    lib.b200fe_dense_ids_device.restype = c_int
+    lib.b200fe_drop_singletons_device.argtypes = [vp, c_int, pp, vp, i64, vp, c_int,
+                                                  ctypes.POINTER(ctypes.c_int64),
+                                                  ctypes.POINTER(c_int)]
+    lib.b200fe_drop_singletons_device.restype = c_int
     lib.b200fe_ols_device.argtypes = [vp, vp, vp, i64, c_int, vp, vp, ctypes.c_int32, c_int,
                                       ctypes.c_double, c_int, ctypes.POINTER(OlsResult)]
     lib.b200fe_ols_device.restype = c_int

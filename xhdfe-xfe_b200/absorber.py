@@ -346,6 +346,41 @@ def drop_singletons_mask(fes) -> np.ndarray:
             return keep
 
 
+def dense_ids_device(raw, device=0):
+    """build_indexer on the device (src/fe_absorption.cpp:845-940): raw int32
+    ids (numpy or torch) -> (int32 CUDA tensor of dense ids, num_groups,
+    num_levels_present)."""
+    import torch
+    ab = _thread_absorber(device)
+    r = torch.as_tensor(np.asarray(raw, dtype=np.int32) if not isinstance(raw, torch.Tensor) else raw,
+                        dtype=torch.int32).to(f"cuda:{device}").contiguous()
+    out = torch.empty_like(r)
+    G, present = ctypes.c_int32(), ctypes.c_int32()
+    rc = ab.lib.b200fe_dense_ids_device(ab.handle, r.data_ptr(), r.numel(), out.data_ptr(),
+                                        ctypes.byref(G), ctypes.byref(present))
+    if rc != _lib.OK:
+        raise ab._err(rc)
+    return out, int(G.value), int(present.value)
+
+
+def drop_singletons_device(ids, num_groups, device=0, max_iter=100):
+    """Singleton cascade on the device (compute_keep_mask_drop_singletons,
+    src/hdfe_regressor_v11.cpp:4056-4290): dense int32 CUDA tensors ->
+    (bool CUDA tensor keep, dropped, rounds)."""
+    import torch
+    ab = _thread_absorber(device)
+    n = ids[0].numel()
+    keep = torch.empty(n, dtype=torch.uint8, device=ids[0].device)
+    G = np.ascontiguousarray(num_groups, dtype=np.int32)
+    dropped, rounds = ctypes.c_int64(), ctypes.c_int()
+    rc = ab.lib.b200fe_drop_singletons_device(
+        ab.handle, len(ids), _ptr_array([g.data_ptr() for g in ids]), G.ctypes.data, n,
+        keep.data_ptr(), max_iter, ctypes.byref(dropped), ctypes.byref(rounds))
+    if rc != _lib.OK:
+        raise ab._err(rc)
+    return keep.bool(), int(dropped.value), int(rounds.value)
+
+
 def partial_out(y, X, fes, weights=None, *, drop_singletons=True, device=0,
                 **options) -> AbsorptionResult:
     """HdfeRegressorV11::partial_out: singleton drop, then absorption.  The
@@ -364,11 +399,20 @@ def partial_out(y, X, fes, weights=None, *, drop_singletons=True, device=0,
         w = np.asarray(weights, dtype=np.float64)
         if w.shape[0] != y.size or not np.all(np.isfinite(w)) or np.any(w < 0):
             raise ValueError("weights must be finite and non-negative")
-    keep = drop_singletons_mask(fes) if (drop_singletons and fes) else np.ones(y.size, bool)
+    # preprocessing on the device: dense ids (build_indexer), singleton cascade
+    dense = [dense_ids_device(f, device) for f in fes]
+    if drop_singletons and fes:
+        keep = drop_singletons_device([d for d, _, _ in dense], [g for _, g, _ in dense],
+                                      device)[0].cpu().numpy()
+    else:
+        keep = np.ones(y.size, bool)
     idx = np.flatnonzero(keep).astype(np.int32)
-    res = absorb_fixed_effects(
-        y[keep], np.asfortranarray(X[keep]), [np.asarray(f)[keep] for f in fes],
-        None if weights is None else np.asarray(weights)[keep], device=device, **options)
+    ids = [d.cpu().numpy()[keep] for d, _, _ in dense]
+    G = [g for _, g, _ in dense]
+    o = make_options(**options)
+    res = _thread_absorber(device).absorb(
+        y[keep], np.asfortranarray(X[keep]), ids, G,
+        None if weights is None else np.asarray(weights)[keep], o)
     res.sample_index = idx
     return res
 

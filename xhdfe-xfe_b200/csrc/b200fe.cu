@@ -25,6 +25,7 @@
 #include "kernels.cuh"
 #include "setup_kernels.cuh"
 #include "ols_kernels.cuh"
+#include "prep_kernels.cuh"
 
 using namespace b200fe;
 
@@ -2321,6 +2322,165 @@ int b200fe_ols(b200fe_context* ctx, const double* y, const double* X, int64_t n,
     }
     return b200fe_ols_device(ctx, dy, dX, n, p, dw, dc, num_clusters, se_type, n_effective,
                              weights_are_frequencies, out);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Preprocessing on the device: dense ids (build_indexer) and singleton drop
+// ---------------------------------------------------------------------------
+namespace {
+
+int dense_ids_impl(b200fe_context* ctx, const int32_t* d_raw, int64_t n, int32_t* d_out,
+                   int32_t* G_out, int32_t* present_out) {
+    const cudaStream_t s = ctx->stream;
+    int* mm;
+    B_CHECK(get_buf(ctx, "prep_mm", 4, &mm));
+    const int init[2] = {INT_MAX, INT_MIN};
+    B_TRY(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    minmax_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(d_raw, n, mm);
+    B_LAUNCHED();
+    int hm[2];
+    B_CHECK(sync_read_int(ctx, mm, 2, hm));
+    const int lo = hm[0], hi = hm[1];
+    const long long range = static_cast<long long>(hi) - lo + 1;
+    if (range > 0 && range <= kDenseRangeCap && range <= 2LL * n) {
+        int32_t *seen, *remap;
+        int* cnt;
+        B_CHECK(get_buf(ctx, "prep_seen", range, &seen));
+        B_CHECK(get_buf(ctx, "prep_remap", range + 1, &remap));
+        B_CHECK(get_buf(ctx, "prep_cnt", 1, &cnt));
+        B_TRY(cudaMemsetAsync(seen, 0, sizeof(int32_t) * range, s));
+        B_TRY(cudaMemsetAsync(cnt, 0, sizeof(int), s));
+        mark_seen_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(d_raw, n, lo, seen);
+        B_LAUNCHED();
+        count_ones_kernel<<<grid_for(ctx, range, 256), 256, 0, s>>>(seen, range, cnt);
+        B_LAUNCHED();
+        int unique = 0;
+        B_CHECK(sync_read_int(ctx, cnt, 1, &unique));
+        *present_out = unique;
+        if (static_cast<long long>(unique) * 10 < range * 9) {  // compact in raw order
+            B_CHECK(cub_exclusive_sum(ctx, seen, remap, range));
+            map_ids_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(d_raw, n, lo, remap, d_out);
+            *G_out = unique;
+        } else {
+            map_ids_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(d_raw, n, lo, nullptr, d_out);
+            *G_out = static_cast<int32_t>(range);
+        }
+        B_LAUNCHED();
+        B_TRY(cudaStreamSynchronize(s));
+        return B200FE_OK;
+    }
+    // sparse range: rank of the raw value among the distinct values
+    uint32_t *key, *skey;
+    int32_t *iota, *perm, *flag, *rank;
+    B_CHECK(get_buf(ctx, "prep_key", n, &key));
+    B_CHECK(get_buf(ctx, "prep_skey", n, &skey));
+    B_CHECK(get_buf(ctx, "prep_iota", n, &iota));
+    B_CHECK(get_buf(ctx, "prep_perm", n, &perm));
+    B_CHECK(get_buf(ctx, "prep_flag", n, &flag));
+    B_CHECK(get_buf(ctx, "prep_rank", n, &rank));
+    flip_sign_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(d_raw, n, key);
+    B_LAUNCHED();
+    iota_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(iota, n);
+    B_LAUNCHED();
+    size_t tmp = 0;
+    B_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, iota, perm, n, 0, 32, s));
+    void* t;
+    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+    B_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, key, skey, iota, perm, n, 0, 32, s));
+    ++ctx->lib_calls;
+    new_key_flags_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(skey, n, flag);
+    B_LAUNCHED();
+    B_CHECK(cub_inclusive_sum(ctx, flag, rank, n));
+    scatter_rank_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(rank, perm, n, d_out);
+    B_LAUNCHED();
+    int last = 0;
+    B_CHECK(sync_read_int(ctx, rank + (n - 1), 1, &last));
+    *G_out = last;
+    *present_out = last;
+    return B200FE_OK;
+}
+
+int drop_singletons_impl(b200fe_context* ctx, int nd, const int32_t* const* d_ids, const int32_t* G,
+                         int64_t n, uint8_t* d_keep, int max_iter, int64_t* dropped, int* rounds) {
+    const cudaStream_t s = ctx->stream;
+    SingletonArgs a{};
+    a.nd = nd;
+    for (int d = 0; d < nd; ++d) {
+        a.ids[d] = d_ids[d];
+        B_CHECK(get_buf(ctx, "prep_cnt" + std::to_string(d), G[d], &a.counts[d]));
+    }
+    unsigned long long* dcount;
+    B_CHECK(get_buf(ctx, "prep_dropped", 1, &dcount));
+    B_TRY(cudaMemsetAsync(d_keep, 1, n, s));
+    int64_t total = 0;
+    int r = 0;
+    for (; r < std::max(1, max_iter); ++r) {
+        for (int d = 0; d < nd; ++d)
+            B_TRY(cudaMemsetAsync(a.counts[d], 0, sizeof(int32_t) * G[d], s));
+        B_TRY(cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), s));
+        singleton_count_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(a, n, d_keep);
+        B_LAUNCHED();
+        singleton_drop_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(a, n, d_keep, dcount);
+        B_LAUNCHED();
+        unsigned long long h = 0;
+        B_TRY(cudaMemcpyAsync(&h, dcount, sizeof(h), cudaMemcpyDeviceToHost, s));
+        B_TRY(cudaStreamSynchronize(s));
+        if (h == 0) break;
+        total += static_cast<int64_t>(h);
+    }
+    if (dropped) *dropped = total;
+    if (rounds) *rounds = r;
+    return B200FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200fe_dense_ids_device(b200fe_context* ctx, const int32_t* d_raw, int64_t n, int32_t* d_out,
+                            int32_t* num_groups, int32_t* num_levels_present) {
+    if (!ctx || !d_raw || !d_out || !num_groups || !num_levels_present || n <= 0 ||
+        n >= (int64_t(1) << 31) - 1)
+        return B200FE_INVALID_ARG;
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return B200FE_UNAVAILABLE;
+    }
+    return dense_ids_impl(ctx, d_raw, n, d_out, num_groups, num_levels_present);
+}
+
+int b200fe_drop_singletons_device(b200fe_context* ctx, int num_dims, const int32_t* const* d_ids,
+                                  const int32_t* num_groups, int64_t n, uint8_t* d_keep,
+                                  int max_iter, int64_t* dropped, int* rounds) {
+    if (!ctx || !d_keep || n <= 0 || num_dims < 1 || num_dims > B200FE_MAX_DIMS || !d_ids ||
+        !num_groups)
+        return B200FE_INVALID_ARG;
+    for (int d = 0; d < num_dims; ++d)
+        if (!d_ids[d] || num_groups[d] <= 0) return B200FE_INVALID_ARG;
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return B200FE_UNAVAILABLE;
+    }
+    // ids must be dense in [0, G_d)
+    int* bad;
+    B_CHECK(get_buf(ctx, "prep_bad", 3, &bad));
+    B_TRY(cudaMemsetAsync(bad, 0, 3 * sizeof(int), ctx->stream));
+    for (int d = 0; d < num_dims; ++d) {
+        validate_ids_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(d_ids[d], n, num_groups[d], 0, bad);
+        B_LAUNCHED();
+    }
+    int hb = 0;
+    B_CHECK(sync_read_int(ctx, bad, 1, &hb));
+    if (hb) {
+        ctx->err = "group ids out of range";
+        return B200FE_INVALID_ARG;
+    }
+    return drop_singletons_impl(ctx, num_dims, d_ids, num_groups, n, d_keep,
+                                max_iter > 0 ? max_iter : 100, dropped, rounds);
 }
 
 }  // extern "C"
