@@ -869,7 +869,7 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     if (st.coupled && wk.run_grid > 0 && st.nL == 1)
         wk.couple_grid = static_cast<int>(std::max<int64_t>(
             1, std::min<int64_t>({static_cast<int64_t>(wk.nbins_ctas),
-                                  static_cast<int64_t>(ctx->num_sms) * 4, st.L[0].G})));
+                                  static_cast<int64_t>(ctx->num_sms) * 8, st.L[0].G})));
     B_CHECK(get_buf(ctx, tag + "bins", static_cast<size_t>(wk.nbins_ctas) * std::max(st.SG, 1) * CP,
                     &wk.bins_partial));
     B_CHECK(get_buf(ctx, tag + "colsq", static_cast<size_t>(wk.nbins_ctas) * CP, &wk.colsq_partial));

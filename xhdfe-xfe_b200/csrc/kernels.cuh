@@ -1656,6 +1656,8 @@ cg_direction_kernel(int64_t GR, int CP, T* __restrict__ p, const T* __restrict__
 // solve precision and writes the CTA's [SG][CP] partial (summed in CTA order
 // by finalize_kernel, with C_yy x_small, into the small-dim rows).
 // ---------------------------------------------------------------------------
+constexpr int kCoupleXfUnroll = 8;  // groups whose loads are in flight per step
+
 template <typename T, int CQ>
 __global__ void __launch_bounds__(256)
 coupling_xf_kernel(int64_t G, int SG, int SGP, const T* __restrict__ cfy, const T* __restrict__ xf,
@@ -1668,16 +1670,17 @@ coupling_xf_kernel(int64_t G, int SG, int SGP, const T* __restrict__ cfy, const 
     if (h >= SG) return;
     T acc[4] = {T(0), T(0), T(0), T(0)};
     int64_t g = g0;
-    for (; g + 4 <= g1; g += 4) {  // four groups' loads in flight
-        T cv[4];
-        Acc4 xv[4];
+    constexpr int U = kCoupleXfUnroll;
+    for (; g + U <= g1; g += U) {  // U groups' loads in flight
+        T cv[U];
+        Acc4 xv[U];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < U; ++u) {
             cv[u] = __ldg(cfy + (g + u) * SGP + h);
             load_quad(xf + (g + u) * CP + 4 * q, xv[u]);
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[j] = fma(cv[u], static_cast<T>(xv[u].v[j]), acc[j]);
     }
