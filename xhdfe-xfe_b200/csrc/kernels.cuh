@@ -846,7 +846,7 @@ __host__ __device__ constexpr size_t data_smem_bytes(int CP, int SG, int nL) {
 }
 
 template <int CP, int MODE>
-__global__ void __launch_bounds__(kDataThreads)
+__global__ void __launch_bounds__(kDataThreads, 2)
 data_pass_kernel(const PassArgs<double> a) {
     constexpr int LD = kTileObs + 1;
     constexpr int GPB = kDataThreads / CP;  // lane groups per block
@@ -871,42 +871,138 @@ data_pass_kernel(const PassArgs<double> a) {
     for (int i = tid; i < (kDataThreads / 32) * a.SG * CP; i += kDataThreads) bins[i] = 0.0;
     double colsq = 0.0;
 
-    for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        if (a.tile_long[t]) continue;
-        const int32_t s0 = a.tile_seg[t], s1 = a.tile_seg[t + 1];
-        const int64_t k0 = a.seg_off[s0];
-        const int nk = static_cast<int>(a.seg_off[s1] - k0);
+    // Tile pipeline: the next regular tile's bounds are read at the top of an
+    // iteration, and (RHS pass) its columns, weights, ids and run tables are
+    // loaded into registers right after the current tile is committed to
+    // shared memory, so those loads are in flight while the current tile is
+    // worked on.  Thread tid holds observations tid and tid + kDataThreads of
+    // a tile and run table entries tid + u * kDataThreads, u < 3.
+    static_assert(kTileObs == 2 * kDataThreads, "two observations per thread");
+    struct Meta {
+        int32_t s0, s1;
+        int64_t k0;
+        int nk;
         int32_t rb[kMaxLarge], nr[kMaxLarge];
+    };
+    auto next_tile = [&](int64_t t) {
+        while (t < a.ntiles && a.tile_long[t]) t += gridDim.x;
+        return t;
+    };
+    auto load_meta = [&](int64_t t, Meta& m) {
+        m.s0 = a.tile_seg[t];
+        m.s1 = a.tile_seg[t + 1];
+        m.k0 = a.seg_off[m.s0];
+        m.nk = static_cast<int>(a.seg_off[m.s1] - m.k0);
 #pragma unroll
         for (int l = 0; l < kMaxLarge; ++l) {
-            rb[l] = (l < a.nL && scatter) ? a.run_base[l][s0] : 0;
-            nr[l] = (l < a.nL && scatter) ? a.run_base[l][s1] - rb[l] : 0;
+            m.rb[l] = (l < a.nL && scatter) ? a.run_base[l][m.s0] : 0;
+            m.nr[l] = (l < a.nL && scatter) ? a.run_base[l][m.s1] - m.rb[l] : 0;
         }
-        __syncthreads();
-        // ---- stage columns, weights, ids and run tables (coalesced) -----------
-        for (int kl = tid; kl < nk; kl += kDataThreads) {
-            const int64_t k = k0 + kl;
+    };
+    double pv[2][CP];
+    double pw[2];
+    uint32_t ps[2];
+    int32_t po[3][kMaxLarge], pd[3][kMaxLarge];
+    auto prefetch = [&](const Meta& m) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int kl = tid + u * kDataThreads;
+            if (kl < m.nk) {
+                const int64_t k = m.k0 + kl;
+                const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
+#pragma unroll
+                for (int cc = 0; cc < CP; ++cc)
+                    pv[u][cc] = cc < a.cols ? __ldcs(a.v + static_cast<int64_t>(cc) * a.n + o) : 0.0;
+                pw[u] = a.wp ? a.wp[k] : 1.0;
+                ps[u] = a.nS > 0 ? __ldg(a.sid + k) : 0u;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            const int j = tid + u * kDataThreads;
+#pragma unroll
+            for (int l = 0; l < kMaxLarge; ++l) {
+                if (l < a.nL && scatter && j <= m.nr[l]) {
+                    po[u][l] = __ldg(a.run_start[l] + m.rb[l] + j) - static_cast<int32_t>(m.k0);
+                    pd[u][l] = j < m.nr[l] ? __ldg(a.run_dest[l] + m.rb[l] + j) : 0;
+                }
+            }
+        }
+    };
+    auto commit = [&](const Meta& m) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int kl = tid + u * kDataThreads;
+            if (kl < m.nk) {
+#pragma unroll
+                for (int cc = 0; cc < CP; ++cc) ubuf[cc * LD + kl] = pv[u][cc];
+                wbuf[kl] = pw[u];
+                sidbuf[kl] = ps[u];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            const int j = tid + u * kDataThreads;
+#pragma unroll
+            for (int l = 0; l < kMaxLarge; ++l) {
+                if (l < a.nL && scatter && j <= m.nr[l]) {
+                    offbuf[l * (kTileObs + 2) + j] = static_cast<uint16_t>(po[u][l]);
+                    if (j < m.nr[l]) dstbuf[l * kTileObs + j] = pd[u][l];
+                }
+            }
+        }
+    };
+    // direct staging (final pass): each value goes to shared memory as loaded
+    auto stage_direct = [&](const Meta& m) {
+        for (int kl = tid; kl < m.nk; kl += kDataThreads) {
+            const int64_t k = m.k0 + kl;
             const int64_t o = a.pord ? static_cast<int64_t>(a.pord[k]) : k;
 #pragma unroll
             for (int cc = 0; cc < CP; ++cc)
                 ubuf[cc * LD + kl] = cc < a.cols ? __ldcs(a.v + static_cast<int64_t>(cc) * a.n + o) : 0.0;
             wbuf[kl] = a.wp ? a.wp[k] : 1.0;
-            if (a.nS > 0 && (scatter || MODE == kFinal)) sidbuf[kl] = __ldg(a.sid + k);
-            if (MODE == kFinal) {
+            if (a.nS > 0) sidbuf[kl] = __ldg(a.sid + k);
 #pragma unroll
-                for (int l = 0; l < kMaxLarge; ++l)
-                    if (l < a.nL) ridbuf[l * kTileObs + kl] = __ldg(a.rid[l] + k);
-            }
+            for (int l = 0; l < kMaxLarge; ++l)
+                if (l < a.nL) ridbuf[l * kTileObs + kl] = __ldg(a.rid[l] + k);
         }
 #pragma unroll
         for (int l = 0; l < kMaxLarge; ++l) {
             if (l >= a.nL || !scatter) continue;
-            for (int j = tid; j <= nr[l]; j += kDataThreads) {
+            for (int j = tid; j <= m.nr[l]; j += kDataThreads) {
                 offbuf[l * (kTileObs + 2) + j] =
-                    static_cast<uint16_t>(__ldg(a.run_start[l] + rb[l] + j) - k0);
-                if (j < nr[l]) dstbuf[l * kTileObs + j] = __ldg(a.run_dest[l] + rb[l] + j);
+                    static_cast<uint16_t>(__ldg(a.run_start[l] + m.rb[l] + j) - m.k0);
+                if (j < m.nr[l]) dstbuf[l * kTileObs + j] = __ldg(a.run_dest[l] + m.rb[l] + j);
             }
         }
+    };
+
+    // The register pipeline pays in the RHS pass; the final pass (more
+    // registers for the gather) stages its tile after the barrier instead and
+    // keeps only the one-tile-ahead bounds.
+    constexpr bool kPipe = MODE == kRhs;
+    Meta cur{}, nxt{};
+    int64_t t = next_tile(blockIdx.x);
+    if (t < a.ntiles) {
+        load_meta(t, cur);
+        if (kPipe) prefetch(cur);
+    }
+    while (t < a.ntiles) {
+        const int64_t tn = next_tile(t + gridDim.x);
+        if (tn < a.ntiles) load_meta(tn, nxt);
+        __syncthreads();  // the previous tile is done with shared memory
+        if constexpr (kPipe) {
+            commit(cur);
+            if (tn < a.ntiles) prefetch(nxt);
+        } else {
+            stage_direct(cur);
+        }
+        const int32_t s0 = cur.s0, s1 = cur.s1;
+        const int64_t k0 = cur.k0;
+        const int nk = cur.nk;
+        int32_t nr[kMaxLarge];
+#pragma unroll
+        for (int l = 0; l < kMaxLarge; ++l) nr[l] = cur.nr[l];
         if (MODE == kFinal) {
             __syncthreads();
             // v - D_r a: one alpha row per lane group; the ids come from shared
@@ -1002,6 +1098,8 @@ data_pass_kernel(const PassArgs<double> a) {
                     if (cc < a.cols) __stcs(a.out + static_cast<int64_t>(cc) * a.n + o, ubuf[cc * LD + kl]);
             }
         }
+        cur = nxt;
+        t = tn;
     }
     __syncthreads();
     const int cta = a.bins_cta0 + blockIdx.x;
