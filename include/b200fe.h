@@ -73,6 +73,7 @@ typedef struct b200fe_options {
 #define B200FE_PROF_RHS 4       /* data pass forming the projected right-hand side          */
 #define B200FE_PROF_FINAL 5     /* data pass writing the within transform (+ certificate)   */
 #define B200FE_PROF_SETUP 6     /* FE structure build                                        */
+#define B200FE_PROF_COUPLE 7    /* dense small-dim coupling product C_fy' x_f (CG matvec)    */
 #define B200FE_PROF_CATEGORIES 8
 
 typedef struct b200fe_result {

@@ -17,7 +17,7 @@ OK, NOT_CONVERGED, UNAVAILABLE, CUDA_ERROR, INVALID_ARG = 0, 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
 MAX_DIMS = 8
 PROF_CATEGORIES = 8
-PROF_NAMES = ("pass", "gather", "finalize", "vector", "rhs", "final", "setup", "spare")
+PROF_NAMES = ("pass", "gather", "finalize", "vector", "rhs", "final", "setup", "couple")
 
 STATUS_NAMES = {
     OK: "ok",

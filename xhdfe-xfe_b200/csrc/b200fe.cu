@@ -974,7 +974,7 @@ int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, co
     constexpr int CP = 4 * CQ;
     const int slots = std::max(std::max(wk.tile_grid, wk.run_grid), wk.data_grid);
     if (wk.run_grid > 0 && st.coupled) {
-        // large dim only over every segment, then C_fy' x_f into the bin partials
+        // large dim only over every segment (C_fy' x_f follows in matvec)
         if (st.nL == 1) {
             BlockArgs<T> r{};
             r.Gp = st.G[st.p];
@@ -996,10 +996,6 @@ int launch_matvec_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a, co
             r.bins_cta0 = 0;
             r.all_segs = 1;
             run_pass_kernel<T, CQ, kRunBatch><<<wk.run_grid, kBlockThreads, 0, ctx->stream>>>(r);
-            B_LAUNCHED();
-            coupling_xf_kernel<T, CQ><<<wk.couple_grid, 256, 0, ctx->stream>>>(
-                st.L[0].G, st.SG, st.SGP, pick_prec<T>(st.cfy32, st.cfy64), a.x + st.lbase[0] * CP,
-                wk.bins_partial);
             B_LAUNCHED();
         }
         return B200FE_OK;
@@ -1158,11 +1154,11 @@ int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w,
     a.x = x;
     {
         double pb;
-        if (wk.run_grid > 0 && st.coupled) {  // large-dim runs + dense coupling rows
+        if (wk.run_grid > 0 && st.coupled) {  // large-dim runs (segment meta, run meta + weight, R, x_f)
             pb = static_cast<double>(st.G[st.p]) * 16.0;
             if (st.nL == 1)
                 pb += static_cast<double>(st.L[0].nruns) * (16.0 + sizeof(T) + CP * double(sizeof(T))) +
-                      static_cast<double>(st.L[0].G) * (CP + st.SG) * double(sizeof(T));
+                      static_cast<double>(st.L[0].G) * CP * double(sizeof(T));
         } else if (wk.run_grid > 0) {  // block-level pass: per segment, run and block
             pb = static_cast<double>(st.G[st.p]) * 16.0 + static_cast<double>(st.GR) * CP * sizeof(T) +
                  static_cast<double>(st.nblocks) * (8.0 + (st.weighted ? sizeof(T) : 0.0));
@@ -1175,6 +1171,16 @@ int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w,
         }
         ProfScope ps(ctx, B200FE_PROF_PASS, pb);
         B_CHECK((launch_matvec_pass<T, CQ>(ctx, wk, a, run_w, block_w)));
+    }
+    if (wk.run_grid > 0 && st.coupled && st.nL == 1) {
+        // C_fy' x_f into the bin partials (rows of C_fy and x_f once, partials written)
+        ProfScope ps(ctx, B200FE_PROF_COUPLE,
+                     static_cast<double>(st.L[0].G) * (st.SGP + CP) * double(sizeof(T)) +
+                         static_cast<double>(wk.couple_grid) * st.SG * CP * 8.0);
+        coupling_xf_kernel<T, CQ><<<wk.couple_grid, 256, 0, ctx->stream>>>(
+            st.L[0].G, st.SG, st.SGP, pick_prec<T>(st.cfy32, st.cfy64), x + st.lbase[0] * CP,
+            wk.bins_partial);
+        B_LAUNCHED();
     }
     return reduce_runs<T, CQ>(ctx, wk, q, x, B200FE_PROF_GATHER, B200FE_PROF_FINALIZE,
                               wk.run_grid > 0, wk.run_grid > 0 && st.coupled);
