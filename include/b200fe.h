@@ -231,6 +231,21 @@ int b200fe_drop_singletons_device(b200fe_context* ctx, int num_dims,
                                   uint8_t* d_keep, int max_iter, int64_t* dropped,
                                   int* rounds);
 
+/* Mobility groups of the first FE pair (device arrays of raw int32 ids, each
+ * ranked as build_indexer does): the connected components of the bipartite
+ * graph whose nodes are the groups of both dims and whose edges are the
+ * observations.  Returns the number of components with observations, the
+ * largest one's observation count and share, and its weight share (the largest
+ * component weight over the total; weights must be finite and positive, NULL
+ * for the observation share).  Replaces hdfe::v11::compute_first_pair_component_stats
+ * (include/hdfe/hdfe_regressor_v11.hpp:68-79, src/hdfe_regressor_v11.cpp:7192-7270). */
+int b200fe_first_pair_components_device(b200fe_context* ctx, const int32_t* d_fe1,
+                                        const int32_t* d_fe2, int64_t n,
+                                        const double* d_weights, int* num_components,
+                                        int64_t* largest_component_n_obs,
+                                        double* largest_component_obs_share,
+                                        double* largest_component_weight_share);
+
 /* ---------------------------------------------------------------------------
  * OLS on within-transformed data: the reference's hdfe::detail::run_ols
  * (include/ols.hpp:40-51, src/ols.cpp:1237-1520) with its covariance

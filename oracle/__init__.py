@@ -148,6 +148,10 @@ def rlib(path: Path = REF_SO) -> ctypes.CDLL:
             lib.xref_run_ols.argtypes = [_vp, _vp, _i64, _int, _vp, _vp, _int, _dbl, _dbl, _dbl, _int,
                                          _vp, _vp, _vp, _vp, ctypes.c_char_p, _int]
             lib.xref_run_ols.restype = _int
+        if hasattr(lib, "xref_components"):
+            lib.xref_components.argtypes = [_vp, _vp, _i64, _vp, P(_int), P(ctypes.c_longlong),
+                                            P(_dbl), ctypes.c_char_p, _int]
+            lib.xref_components.restype = _int
         if hasattr(lib, "xref_akm_kss"):
             lib.xref_akm_kss.argtypes = [_vp, _vp, _vp, _i64, _vp, ctypes.c_uint64, _dbl, _vp, P(_int),
                                          P(ctypes.c_longlong), ctypes.c_char_p, _int]
@@ -335,3 +339,20 @@ def ref_run_ols(y, X, weights=None, clusters=None, *, se_type="unadjusted", tss=
     return {"coef": coef, "se": se, "cov": cov, "rss": sc[0], "sigma2": sc[1], "df_resid": sc[2],
             "cov_scale": sc[3], "cluster_u2": sc[4], "r2": sc[5], "r2_within": sc[6],
             "num_clusters": int(sc[7])}
+
+
+def ref_components(fe1, fe2, weights=None, lib_path=REF_SO):
+    """The reference's compute_first_pair_component_stats."""
+    a = np.ascontiguousarray(fe1, dtype=np.int32)
+    b = np.ascontiguousarray(fe2, dtype=np.int32)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    oi = (_int * 1)()
+    ol = (ctypes.c_longlong * 1)()
+    od = (_dbl * 2)()
+    err = ctypes.create_string_buffer(512)
+    rc = rlib(lib_path).xref_components(a.ctypes.data, b.ctypes.data, a.size,
+                                       None if w is None else w.ctypes.data, oi, ol, od, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return {"num_components": oi[0], "largest_component_n_obs": int(ol[0]),
+            "largest_component_obs_share": od[0], "largest_component_weight_share": od[1]}

@@ -11,6 +11,11 @@ singleton_keep restates compute_keep_mask_drop_singletons
 alone in its group of some dimension, until a round drops nothing (at most
 max_iter rounds, 100 in the reference).
 
+component_stats restates compute_first_pair_component_stats
+(src/hdfe_regressor_v11.cpp:7192-7270): connected components of the bipartite
+graph of the two dims' groups, components with observations, the largest one's
+observation count and share, and its weight share.
+
 Only tests/ import this module, and only as the checker.
 """
 
@@ -51,3 +56,24 @@ def singleton_keep(ids, max_iter=100):
             return keep, rounds - 1
         keep &= ~single
     return keep, rounds
+
+
+def component_stats(fe1, fe2, weights=None):
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    g1, G1, _ = build_indexer(fe1)
+    g2, G2, _ = build_indexer(fe2)
+    n = g1.size
+    adj = coo_matrix((np.ones(n), (g1, G1 + g2)), shape=(G1 + G2, G1 + G2))
+    _, lab = connected_components(adj, directed=False)
+    comp = lab[g1]
+    counts = np.bincount(comp)
+    big = int(counts.max())
+    out = {"num_components": int((counts > 0).sum()), "largest_component_n_obs": big,
+           "largest_component_obs_share": big / n}
+    if weights is None:
+        out["largest_component_weight_share"] = big / n
+    else:
+        ws = np.bincount(comp, weights=np.asarray(weights, dtype=np.float64))
+        out["largest_component_weight_share"] = float(ws.max() / ws.sum())
+    return out

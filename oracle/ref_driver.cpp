@@ -13,6 +13,7 @@
 //   xref_akm_kss      -> hdfe::akm::akm_kss_decompose              (include/hdfe/akm_kss.hpp:227-233)
 //   xref_recover_fe   -> hdfe::detail::recover_fixed_effects        (include/fe_absorption.hpp:127-130)
 //   xref_run_ols      -> hdfe::detail::run_ols                      (include/ols.hpp:40-51)
+//   xref_components   -> hdfe::v11::compute_first_pair_component_stats (include/hdfe/hdfe_regressor_v11.hpp:75-78)
 // Every entry point catches all exceptions and returns a nonzero status with
 // the message copied into err (the reference's own fail-closed contract).
 
@@ -368,6 +369,34 @@ int xref_run_ols(const double* y, const double* X, int64_t n, int p, const doubl
         scalars[5] = r.r2;
         scalars[6] = r.r2_within;
         scalars[7] = r.num_clusters;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+// Mobility groups of the first FE pair: out_i[0] num_components; out_l[0]
+// largest_component_n_obs; out_d[0..1] obs and weight shares.
+int xref_components(const int32_t* fe1, const int32_t* fe2, int64_t n, const double* w, int* out_i,
+                    long long* out_l, double* out_d, char* err, int err_len) {
+    try {
+        VectorXi a(n), b(n);
+        for (int64_t i = 0; i < n; ++i) {
+            a[i] = fe1[i];
+            b[i] = fe2[i];
+        }
+        VectorXd wv;
+        if (w) wv = Map<const VectorXd>(w, n);
+        const hdfe::v11::FeComponentStats st =
+            hdfe::v11::compute_first_pair_component_stats(a, b, w ? &wv : nullptr);
+        out_i[0] = st.num_components;
+        out_l[0] = st.largest_component_n_obs;
+        out_d[0] = st.largest_component_obs_share;
+        out_d[1] = st.largest_component_weight_share;
         return 0;
     } catch (const std::exception& e) {
         set_err(err, err_len, e.what());

@@ -56,3 +56,23 @@ def test_partial_out_uses_device_preprocessing(pkg, panels, oracle_mod):
     out = np.column_stack([res.y_tilde, res.X_tilde])
     err = np.linalg.norm(out - ref, axis=0) / np.linalg.norm(V, axis=0)
     assert err.max() <= 1e-8
+
+
+@pytest.mark.parametrize("case", ["akm_low_mobility", "akm_50k_weighted", "raw_sparse_ids"])
+def test_first_pair_components_match_reference(pkg, panels, oracle_mod, case):
+    from oracle.preprocess_oracle import component_stats
+    rng = np.random.default_rng(23)
+    p = panels.akm_two_way(50_000, n_firms=4_000, seed=97, move_prob=0.02)
+    f1, f2 = np.asarray(p.fes[0]), np.asarray(p.fes[1])
+    w = rng.lognormal(0.0, 0.5, size=p.n) if case == "akm_50k_weighted" else None
+    if case == "raw_sparse_ids":
+        f1 = (f1.astype(np.int64) * 40_503 - 1_000_000_000).astype(np.int32)
+        f2 = (f2.astype(np.int64) * 7 + 3).astype(np.int32)
+    ours = pkg.first_pair_component_stats(f1, f2, w)
+    want = (oracle_mod.ref_components(f1, f2, w) if oracle_mod.ref_available()
+            else component_stats(f1, f2, w))
+    assert ours.num_components == want["num_components"] > 1
+    assert ours.largest_component_n_obs == want["largest_component_n_obs"]
+    assert ours.largest_component_obs_share == pytest.approx(want["largest_component_obs_share"], abs=1e-15)
+    assert ours.largest_component_weight_share == pytest.approx(
+        want["largest_component_weight_share"], abs=1e-12)

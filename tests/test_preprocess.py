@@ -31,3 +31,18 @@ def test_singleton_oracle_matches_host_mask(pkg, panels):
     keep, rounds = singleton_keep(p.fes)
     assert rounds >= 1 and not keep.all()
     assert np.array_equal(keep, pkg.drop_singletons_mask(p.fes))
+
+
+def test_component_oracle_matches_reference(oracle_mod, panels):
+    from oracle.preprocess_oracle import component_stats
+    if not oracle_mod.ref_available():
+        import pytest
+        pytest.skip("oracle/_ref/libxhdfe_ref.so not built")
+    p = panels.akm_two_way(20_000, n_firms=2_000, seed=7, move_prob=0.02)
+    w = np.random.default_rng(2).lognormal(0.0, 0.5, size=p.n)
+    for ww in (None, w):
+        ref = oracle_mod.ref_components(p.fes[0], p.fes[1], ww)
+        ours = component_stats(p.fes[0], p.fes[1], ww)
+        assert ref["num_components"] == ours["num_components"] > 1
+        assert ref["largest_component_n_obs"] == ours["largest_component_n_obs"]
+        assert abs(ref["largest_component_weight_share"] - ours["largest_component_weight_share"]) <= 1e-12

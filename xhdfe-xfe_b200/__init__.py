@@ -8,6 +8,7 @@ from .absorber import (  # noqa: F401
     Absorber,
     AbsorberError,
     AbsorptionResult,
+    FeComponentStats,
     FeRecoveryResult,
     OlsResult,
     absorb_fixed_effects,
@@ -17,6 +18,7 @@ from .absorber import (  # noqa: F401
     dense_ids_device,
     drop_singletons_device,
     drop_singletons_mask,
+    first_pair_component_stats,
     make_options,
     partial_out,
     recover_fixed_effects,

@@ -44,6 +44,7 @@ EXPORTED_SYMBOLS = (
     "b200fe_demean_sorted_noalloc",
     "b200fe_dense_ids_device",
     "b200fe_drop_singletons_device",
+    "b200fe_first_pair_components_device",
     "b200fe_ols_device",
     "b200fe_ols",
     "b200fe_kss_create",
@@ -164,6 +165,10 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
                                                   ctypes.POINTER(ctypes.c_int64),
                                                   ctypes.POINTER(c_int)]
     lib.b200fe_drop_singletons_device.restype = c_int
+    lib.b200fe_first_pair_components_device.argtypes = [
+        vp, vp, vp, i64, vp, ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_int64),
+        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.b200fe_first_pair_components_device.restype = c_int
     lib.b200fe_ols_device.argtypes = [vp, vp, vp, i64, c_int, vp, vp, ctypes.c_int32, c_int,
                                       ctypes.c_double, c_int, ctypes.POINTER(OlsResult)]
     lib.b200fe_ols_device.restype = c_int

@@ -381,6 +381,37 @@ def drop_singletons_device(ids, num_groups, device=0, max_iter=100):
     return keep.bool(), int(dropped.value), int(rounds.value)
 
 
+@dataclass
+class FeComponentStats:
+    """hdfe::v11::FeComponentStats (include/hdfe/hdfe_regressor_v11.hpp:68-73)."""
+    num_components: int
+    largest_component_n_obs: int
+    largest_component_obs_share: float
+    largest_component_weight_share: float
+
+
+def first_pair_component_stats(first_fe, second_fe, weights=None, device=0) -> FeComponentStats:
+    """compute_first_pair_component_stats on the device: the mobility groups
+    (connected components) of the first two FE dims, raw int32 ids."""
+    import torch
+    ab = _thread_absorber(device)
+    dev = f"cuda:{device}"
+    f1 = torch.as_tensor(np.asarray(first_fe, dtype=np.int32)).to(dev).contiguous()
+    f2 = torch.as_tensor(np.asarray(second_fe, dtype=np.int32)).to(dev).contiguous()
+    if f1.numel() != f2.numel():
+        raise ValueError("First-pair FE vectors must have the same length")
+    w = None if weights is None else torch.as_tensor(
+        np.asarray(weights, dtype=np.float64)).to(dev).contiguous()
+    nc, big = ctypes.c_int(), ctypes.c_int64()
+    share, wshare = ctypes.c_double(), ctypes.c_double()
+    rc = ab.lib.b200fe_first_pair_components_device(
+        ab.handle, f1.data_ptr(), f2.data_ptr(), f1.numel(), None if w is None else w.data_ptr(),
+        ctypes.byref(nc), ctypes.byref(big), ctypes.byref(share), ctypes.byref(wshare))
+    if rc != _lib.OK:
+        raise ab._err(rc)
+    return FeComponentStats(int(nc.value), int(big.value), float(share.value), float(wshare.value))
+
+
 def partial_out(y, X, fes, weights=None, *, drop_singletons=True, device=0,
                 **options) -> AbsorptionResult:
     """HdfeRegressorV11::partial_out: singleton drop, then absorption.  The

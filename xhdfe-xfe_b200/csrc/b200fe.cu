@@ -6,8 +6,9 @@
 // blocks of CG iterations.
 
 #include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
+#include <cub/device/device_reduce.cuh>
 #include <cub/device/device_segmented_reduce.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cfloat>
@@ -2441,9 +2442,146 @@ int drop_singletons_impl(b200fe_context* ctx, int nd, const int32_t* const* d_id
     return B200FE_OK;
 }
 
+int component_stats_impl(b200fe_context* ctx, const int32_t* d_fe1, const int32_t* d_fe2, int64_t n,
+                         const double* d_w, int* num_components, int64_t* largest_n_obs,
+                         double* obs_share, double* weight_share) {
+    const cudaStream_t s = ctx->stream;
+    int32_t *g1, *g2;
+    B_CHECK(get_buf(ctx, "cc_g1", n, &g1));
+    B_CHECK(get_buf(ctx, "cc_g2", n, &g2));
+    int32_t G1 = 0, G2 = 0, p1 = 0, p2 = 0;
+    B_CHECK(dense_ids_impl(ctx, d_fe1, n, g1, &G1, &p1));
+    B_CHECK(dense_ids_impl(ctx, d_fe2, n, g2, &G2, &p2));
+    const int64_t N = static_cast<int64_t>(G1) + G2;
+    if (N >= INT32_MAX) {
+        ctx->err = "too many groups";
+        return B200FE_INVALID_ARG;
+    }
+    int32_t *parent, *label, *slabel, *off;
+    int* flags;
+    B_CHECK(get_buf(ctx, "cc_parent", N, &parent));
+    B_CHECK(get_buf(ctx, "cc_label", n, &label));
+    B_CHECK(get_buf(ctx, "cc_slabel", n, &slabel));
+    B_CHECK(get_buf(ctx, "cc_off", N + 1, &off));
+    B_CHECK(get_buf(ctx, "cc_flags", 4, &flags));
+    iota_kernel<<<grid_for(ctx, N, 256), 256, 0, s>>>(parent, N);
+    B_LAUNCHED();
+    int rounds = 0;
+    for (;; ++rounds) {
+        if (rounds >= 1000) {  // min-label hooking converges in a few rounds
+            ctx->err = "connected components did not converge";
+            return B200FE_CUDA_ERROR;
+        }
+        B_TRY(cudaMemsetAsync(flags, 0, sizeof(int), s));
+        cc_hook_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(g1, g2, n, G1, parent, flags);
+        B_LAUNCHED();
+        cc_compress_kernel<<<grid_for(ctx, N, 256), 256, 0, s>>>(parent, static_cast<int32_t>(N));
+        B_LAUNCHED();
+        int changed = 0;
+        B_CHECK(sync_read_int(ctx, flags, 1, &changed));
+        if (!changed) break;
+    }
+    cc_label_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(g1, n, parent, label);
+    B_LAUNCHED();
+    // observations sorted by component (stable), offsets per node: exact counts
+    // and, with weights, per-component sums in a fixed order
+    double *w_sorted = nullptr, *wsum = nullptr, *tot = nullptr;
+    int32_t *iota = nullptr, *perm = nullptr;
+    if (d_w) {
+        B_TRY(cudaMemsetAsync(flags + 1, 0, sizeof(int), s));
+        positive_weights_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(d_w, n, flags + 1);
+        B_LAUNCHED();
+        int bad = 0;
+        B_CHECK(sync_read_int(ctx, flags + 1, 1, &bad));
+        if (bad) {
+            ctx->err = "First-pair component weights must be finite and positive";
+            return B200FE_INVALID_ARG;
+        }
+        B_CHECK(get_buf(ctx, "cc_iota", n, &iota));
+        B_CHECK(get_buf(ctx, "cc_perm", n, &perm));
+        iota_kernel<<<grid_for(ctx, n, 256), 256, 0, s>>>(iota, n);
+        B_LAUNCHED();
+    }
+    {
+        size_t tmp = 0;
+        const uint32_t* ki = reinterpret_cast<const uint32_t*>(label);
+        uint32_t* ko = reinterpret_cast<uint32_t*>(slabel);
+        const int eb = bits_for(static_cast<int32_t>(N));
+        if (d_w) {
+            B_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ki, ko, iota, perm, n, 0, eb, s));
+        } else {
+            B_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tmp, ki, ko, n, 0, eb, s));
+        }
+        void* t;
+        B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+        if (d_w) {
+            B_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, ki, ko, iota, perm, n, 0, eb, s));
+        } else {
+            B_TRY(cub::DeviceRadixSort::SortKeys(t, tmp, ki, ko, n, 0, eb, s));
+        }
+        ++ctx->lib_calls;
+    }
+    segment_offsets_kernel<<<grid_for(ctx, n + 1, 256), 256, 0, s>>>(slabel, n, static_cast<int32_t>(N), off);
+    B_LAUNCHED();
+    B_TRY(cudaMemsetAsync(flags + 2, 0, 2 * sizeof(int), s));
+    cc_count_kernel<<<grid_for(ctx, N, 256), 256, 0, s>>>(off, static_cast<int32_t>(N), flags + 2, flags + 3);
+    B_LAUNCHED();
+    int hc[2];
+    B_CHECK(sync_read_int(ctx, flags + 2, 2, hc));
+    *num_components = hc[0];
+    *largest_n_obs = hc[1];
+    *obs_share = static_cast<double>(hc[1]) / static_cast<double>(n);
+    *weight_share = *obs_share;
+    if (d_w) {
+        B_CHECK(get_buf(ctx, "cc_wsorted", n, &w_sorted));
+        B_CHECK(get_buf(ctx, "cc_wsum", N, &wsum));
+        B_CHECK(get_buf(ctx, "cc_tot", 1, &tot));
+        gather_kernel<double><<<grid_for(ctx, n, 256), 256, 0, s>>>(d_w, perm, n, w_sorted);
+        B_LAUNCHED();
+        size_t tmp = 0;
+        B_TRY(cub::DeviceSegmentedReduce::Sum(nullptr, tmp, w_sorted, wsum, static_cast<int>(N), off, off + 1, s));
+        void* t;
+        B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+        B_TRY(cub::DeviceSegmentedReduce::Sum(t, tmp, w_sorted, wsum, static_cast<int>(N), off, off + 1, s));
+        B_TRY(cub::DeviceReduce::Max(nullptr, tmp, wsum, tot, static_cast<int>(N), s));
+        B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+        B_TRY(cub::DeviceReduce::Max(t, tmp, wsum, tot, static_cast<int>(N), s));
+        ctx->lib_calls += 2;
+        double largest_w = 0.0;
+        B_CHECK(sync_read_double(ctx, tot, 1, &largest_w));
+        // total weight: the component sums in node order
+        B_TRY(cub::DeviceReduce::Sum(nullptr, tmp, wsum, tot, static_cast<int>(N), s));
+        B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+        B_TRY(cub::DeviceReduce::Sum(t, tmp, wsum, tot, static_cast<int>(N), s));
+        ++ctx->lib_calls;
+        double total_w = 0.0;
+        B_CHECK(sync_read_double(ctx, tot, 1, &total_w));
+        *weight_share = total_w > 0.0 ? largest_w / total_w : 0.0;
+    }
+    return B200FE_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int b200fe_first_pair_components_device(b200fe_context* ctx, const int32_t* d_fe1,
+                                        const int32_t* d_fe2, int64_t n, const double* d_weights,
+                                        int* num_components, int64_t* largest_component_n_obs,
+                                        double* largest_component_obs_share,
+                                        double* largest_component_weight_share) {
+    if (!ctx || !d_fe1 || !d_fe2 || n <= 0 || n >= (int64_t(1) << 31) - 1 || !num_components ||
+        !largest_component_n_obs || !largest_component_obs_share || !largest_component_weight_share)
+        return B200FE_INVALID_ARG;
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return B200FE_UNAVAILABLE;
+    }
+    return component_stats_impl(ctx, d_fe1, d_fe2, n, d_weights, num_components,
+                                largest_component_n_obs, largest_component_obs_share,
+                                largest_component_weight_share);
+}
 
 int b200fe_dense_ids_device(b200fe_context* ctx, const int32_t* d_raw, int64_t n, int32_t* d_out,
                             int32_t* num_groups, int32_t* num_levels_present) {

@@ -123,4 +123,80 @@ __global__ void singleton_drop_kernel(const SingletonArgs a, int64_t n, uint8_t*
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(dropped, static_cast<unsigned long long>(local));
 }
 
+// ---------------------------------------------------------------------------
+// Connected components of the bipartite graph of two FE dimensions (nodes:
+// the groups of both dims; edges: observations), the mobility groups of the
+// reference's compute_first_pair_component_stats
+// (src/hdfe_regressor_v11.cpp:7192-7270).  Min-label hooking: every edge
+// points the larger of its two roots at the smaller (atomicMin), then pointer
+// jumping flattens the trees; repeated until no edge joins two roots.  The
+// final label of a node is the smallest node id of its component, whatever
+// the order of the atomics.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int32_t cc_root(const int32_t* parent, int32_t x) {
+    int32_t p = parent[x];
+    while (p != x) {
+        x = p;
+        p = parent[x];
+    }
+    return x;
+}
+
+__global__ void cc_hook_kernel(const int32_t* __restrict__ g1, const int32_t* __restrict__ g2,
+                               int64_t n, int32_t G1, int32_t* parent, int* changed) {
+    int local = 0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t ru = cc_root(parent, g1[i]);
+        const int32_t rv = cc_root(parent, G1 + g2[i]);
+        if (ru != rv) {
+            atomicMin(parent + max(ru, rv), min(ru, rv));
+            local = 1;
+        }
+    }
+    if (__syncthreads_or(local) && threadIdx.x == 0) atomicOr(changed, 1);
+}
+
+__global__ void cc_compress_kernel(int32_t* parent, int32_t N) {
+    for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < N;
+         v += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        parent[v] = cc_root(parent, static_cast<int32_t>(v));
+}
+
+// component label of every observation (trees already flat)
+__global__ void cc_label_kernel(const int32_t* __restrict__ g1, int64_t n,
+                                const int32_t* __restrict__ parent, int32_t* __restrict__ label) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        label[i] = parent[g1[i]];
+}
+
+// per-node observation counts from the offsets; the largest, and the number of
+// non-empty components (integer atomics: order-free)
+__global__ void cc_count_kernel(const int32_t* __restrict__ off, int32_t N, int* __restrict__ ncomp,
+                                int* __restrict__ largest) {
+    int c = 0, m = 0;
+    for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < N;
+         v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int k = off[v + 1] - off[v];
+        c += k > 0;
+        m = max(m, k);
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    m = static_cast<int>(__reduce_max_sync(0xffffffffu, static_cast<unsigned>(m)));
+    if ((threadIdx.x & 31) == 0) {
+        if (c) atomicAdd(ncomp, c);
+        atomicMax(largest, m);
+    }
+}
+
+// flags[0] |= 1 when a weight is not finite and positive
+__global__ void positive_weights_kernel(const double* __restrict__ w, int64_t n, int* flags) {
+    int bad = 0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        bad |= !(w[i] > 0.0) || !(w[i] < 1e300);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags, 1);
+}
+
 }  // namespace b200fe
