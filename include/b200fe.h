@@ -162,6 +162,38 @@ int b200fe_absorb_device(b200fe_context* ctx, const double* d_v, int64_t n,
                          const b200fe_options* opts, double* d_out,
                          b200fe_result* res, void* stream);
 
+/* Absorption with heterogeneous slopes.  Dimension d spans, per group g, the
+ * intercept 1_g when slope_values[d] is NULL (a plain FE); otherwise the slope
+ * z_d 1_g (z_d = slope_values[d], n doubles) and, when
+ * slope_has_intercept[d] is nonzero, also 1_g.  slope_values may be NULL
+ * (all plain).  A group's 2x2 block is inverted with the reference's rule:
+ * determinant above 1e-12 max(1, W ZZ), else the intercept alone.  FP64
+ * block-Jacobi CGLS over all FE blocks; at most 256 columns.  primary_dim in
+ * res is the dimension whose order the observations are processed in.
+ * Replaces the is_slope path of hdfe::detail::absorb_fixed_effects_cuda
+ * (GpuFeInput.is_slope / slope_has_intercept / slope_values,
+ * include/fe_absorption_cuda.hpp:12-22; src/fe_absorption_cuda.cu:2316-2420,
+ * 586-650) and the slopes argument of absorb_fixed_effects_v6
+ * (include/fe_absorption.hpp:95-101). */
+int b200fe_absorb_slopes(b200fe_context* ctx, const double* y, const double* X,
+                         int64_t n, int k, int num_dims,
+                         const int32_t* const* group_ids, const int32_t* num_groups,
+                         const double* const* slope_values,
+                         const unsigned char* slope_has_intercept,
+                         const double* weights, const b200fe_options* opts,
+                         double* y_out, double* X_out, b200fe_result* res);
+
+/* b200fe_absorb_slopes on device arrays (d_v / d_out as b200fe_absorb_device;
+ * d_slope_values[d] device pointers or NULL). */
+int b200fe_absorb_slopes_device(b200fe_context* ctx, const double* d_v, int64_t n,
+                                int cols, int num_dims,
+                                const int32_t* const* d_group_ids,
+                                const int32_t* num_groups,
+                                const double* const* d_slope_values,
+                                const unsigned char* slope_has_intercept,
+                                const double* d_weights, const b200fe_options* opts,
+                                double* d_out, b200fe_result* res, void* stream);
+
 /* In-place demean of host arrays, the raw interface of the reference's
  * block-PCG absorber: Y (n) and X (n x k column-major) are overwritten with
  * their within transforms; iters_out receives the PCG iteration count.

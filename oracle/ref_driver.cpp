@@ -8,6 +8,7 @@
 //
 // Entry points mirror the reference's public calls:
 //   xref_absorb       -> hdfe::detail::absorb_fixed_effects_v6  (src/fe_absorption.cpp:8750)
+//   xref_absorb_slopes-> the same, with HeterogeneousSlopeTerm slopes (include/fe_absorption.hpp:49-53)
 //   xref_partial_out  -> hdfe::v11::HdfeRegressorV11::partial_out (src/hdfe_regressor_v11.cpp:10275)
 //   xref_fit          -> hdfe::v11::HdfeRegressorV11::fit         (src/hdfe_regressor_v11.cpp:7522)
 //   xref_akm_kss      -> hdfe::akm::akm_kss_decompose              (include/hdfe/akm_kss.hpp:227-233)
@@ -120,6 +121,57 @@ int xref_absorb(const double* y, const double* X, int64_t n, int k,
         auto guard = backend_guard(o);
         hdfe::detail::AbsorptionResult r = hdfe::detail::absorb_fixed_effects_v6(
             ym, Xm, fes, w ? &wv : nullptr, opts, opts.absorption_method);
+        std::memcpy(y_out, r.y_tilde.data(), sizeof(double) * static_cast<std::size_t>(n));
+        if (k > 0) {
+            std::memcpy(X_out, r.X_tilde.data(),
+                        sizeof(double) * static_cast<std::size_t>(n) * k);
+        }
+        info[0] = r.iterations;
+        info[1] = r.converged ? 1 : 0;
+        info[2] = r.precision_certified ? 1 : 0;
+        info[3] = r.gpu_status_code;
+        dinfo[0] = r.abs_residual;
+        dinfo[1] = r.abs_residual_rel;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+// absorb_fixed_effects_v6 with heterogeneous slopes: slope_kind[d] is 0 for a
+// plain FE, 1 for a slope without intercept, 2 for intercept and slope; the
+// slope values of dim d are slope_flat[d * n .. d * n + n).  Same outputs as
+// xref_absorb.
+int xref_absorb_slopes(const double* y, const double* X, int64_t n, int k,
+                       const int32_t* fe_flat, int dims, const double* w,
+                       const double* slope_flat, const int* slope_kind,
+                       const XrefOptions* o, double* y_out, double* X_out,
+                       int* info, double* dinfo, char* err, int err_len) {
+    try {
+        Map<const VectorXd> ym(y, n);
+        Map<const MatrixXd> Xm(X, n, k);
+        std::vector<VectorXi> fes = to_fes(fe_flat, n, dims);
+        VectorXd wv;
+        if (w) {
+            wv = Map<const VectorXd>(w, n);
+        }
+        std::vector<hdfe::detail::HeterogeneousSlopeTerm> slopes;
+        for (int d = 0; d < dims; ++d) {
+            if (slope_kind[d] == 0) continue;
+            hdfe::detail::HeterogeneousSlopeTerm t;
+            t.fe_index = d;
+            t.values = Map<const VectorXd>(slope_flat + static_cast<std::size_t>(d) * n, n);
+            t.include_intercept = slope_kind[d] == 2;
+            slopes.push_back(std::move(t));
+        }
+        hdfe::HdfeOptions opts = to_options(o);
+        auto guard = backend_guard(o);
+        hdfe::detail::AbsorptionResult r = hdfe::detail::absorb_fixed_effects_v6(
+            ym, Xm, fes, w ? &wv : nullptr, opts, opts.absorption_method, slopes);
         std::memcpy(y_out, r.y_tilde.data(), sizeof(double) * static_cast<std::size_t>(n));
         if (k > 0) {
             std::memcpy(X_out, r.X_tilde.data(),

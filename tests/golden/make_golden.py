@@ -15,6 +15,11 @@ For each case it stores, in <case>.npz:
     converged, abs_residual_rel;
   * the reference's HdfeRegressorV11::fit coefficients and standard errors.
 
+Slope cases (``python tests/golden/make_golden.py slopes``, slopes_<case>.npz)
+hold the reference's absorb_fixed_effects_v6 with heterogeneous slopes at
+tol 1e-13 (reghdfe-comparable; strict-residual is refused for slopes): the within transform on all rows (on a row subset
+beyond 5000 rows) and its column norms, with the input digests.
+
 KSS cases (kss_<case>.npz) hold the inputs of an AKM leave-out decomposition
 and the reference's hdfe::akm::akm_kss_decompose results on them:
   * kss_felsdvsimul: the reference's own example data (data/felsdvsimul.dta,
@@ -187,7 +192,99 @@ def make_kss(name: str) -> dict:
 KSS_CASES = ("felsdvsimul", "akm20k")
 
 
+# ---------------------------------------------------------------------------
+# Heterogeneous slopes (slopes_<case>.npz): absorb_fixed_effects_v6 with
+# HeterogeneousSlopeTerm slopes, (fe_index, values, include_intercept).
+# ---------------------------------------------------------------------------
+def slope_stata600():
+    """The design of the reference's tests/stata/part1/heterogeneous-slopes.do:
+    600 rows, firm##c.z and year."""
+    i = np.arange(1, 601, dtype=np.float64)
+    firm = ((i - 1) % 60).astype(np.int32)
+    year = (((i - 1) // 60) % 10).astype(np.int32)
+    z = np.mod(i * 17, 23) / 10
+    x1, x2 = np.sin(i / 7), np.cos(i / 11)
+    y = (1 + .7 * x1 - .3 * x2 + (firm + 1) / 20 + (year + 1) / 9 + .02 * (firm + 1) * z
+         + np.sin(i / 13) / 10)
+    return dict(y=y, X=np.c_[x1, x2], fes=[firm, year], slopes=[(0, z, True)], weights=None)
+
+
+def slope_mixed3k(weighted: bool):
+    """Seeded 3k rows: a slope without intercept on a dim that also enters as a
+    plain FE, and a second slope with intercept on another dim."""
+    rng = np.random.default_rng(20260711)
+    n = 3000
+    g1 = rng.integers(0, 300, n).astype(np.int32)
+    g2 = rng.integers(0, 40, n).astype(np.int32)
+    z1 = rng.uniform(0, 5, n)
+    z2 = rng.standard_normal(n)
+    X = rng.standard_normal((n, 3))
+    y = X @ np.array([1.0, -2.0, 0.5]) + 0.3 * z1 + rng.standard_normal(n)
+    w = rng.uniform(0.5, 2.0, n) if weighted else None
+    return dict(y=y, X=X, fes=[g1, g2, g2], slopes=[(0, z1, True), (2, z2, False)], weights=w)
+
+
+def slope_degenerate2k():
+    """Groups whose slope block is singular: z constant within every fifth firm
+    (det 0: the intercept alone), z = 0 on a slope-only dim's group."""
+    rng = np.random.default_rng(20260712)
+    n = 2000
+    firm = rng.integers(0, 100, n).astype(np.int32)
+    year = rng.integers(0, 12, n).astype(np.int32)
+    z = rng.uniform(-1, 1, n)
+    z[firm % 5 == 0] = 2.5
+    z2 = rng.standard_normal(n)
+    z2[year == 3] = 0.0
+    X = rng.standard_normal((n, 2))
+    y = X @ np.array([0.4, 0.2]) + z + rng.standard_normal(n)
+    return dict(y=y, X=X, fes=[firm, year, year], slopes=[(0, z, True), (2, z2, False)],
+                weights=None)
+
+
+def slope_akm20k():
+    p, sl = ge.load_module("panels").akm_firm_tenure_slopes(20_000, n_firms=600, seed=20260713)
+    return dict(y=p.y, X=p.X, fes=p.fes, slopes=sl, weights=None)
+
+
+SLOPE_CASES = {
+    "stata600": slope_stata600,
+    "mixed3k": lambda: slope_mixed3k(False),
+    "mixed3kw": lambda: slope_mixed3k(True),
+    "degenerate2k": slope_degenerate2k,
+    "akm20k": slope_akm20k,
+}
+
+
+def slope_digest(c) -> str:
+    arrs = [c["y"], np.asarray(c["X"], dtype=np.float64),
+            *[np.asarray(f, dtype=np.int32) for f in c["fes"]],
+            *[np.asarray(z, dtype=np.float64) for _, z, _ in c["slopes"]]]
+    if c["weights"] is not None:
+        arrs.append(c["weights"])
+    return digest(*arrs)
+
+
+def make_slopes(name: str) -> dict:
+    c = SLOPE_CASES[name]()
+    ref = oracle.ref_absorb_slopes(c["y"], c["X"], c["fes"], c["slopes"], c["weights"],
+                                   tol=1e-13, tolerance_mode="reghdfe-comparable", threads=1,
+                                   max_iter=1_000_000)
+    n = c["y"].shape[0]
+    rows = subset_rows(n) if n > 5000 else np.arange(n, dtype=np.int64)
+    meta = {"case": name, "n": n, "iterations": ref["iterations"],
+            "converged": ref["converged"], "abs_residual_rel": ref["abs_residual_rel"],
+            "slopes": [[d, bool(i)] for d, _, i in c["slopes"]],
+            "input_digest": slope_digest(c)}
+    np.savez_compressed(OUT / f"slopes_{name}.npz", rows=rows, ref_rows=ref["V"][rows],
+                        ref_colnorm=np.linalg.norm(ref["V"], axis=0), meta=np.array(json.dumps(meta)))
+    return meta
+
+
 if __name__ == "__main__":
+    if sys.argv[1:2] == ["slopes"]:
+        for nm in sys.argv[2:] or list(SLOPE_CASES):
+            print(nm, json.dumps(make_slopes(nm)))
+        sys.exit(0)
     if sys.argv[1:2] == ["kss"]:
         for nm in sys.argv[2:] or KSS_CASES:
             print(nm, json.dumps(make_kss(nm)))

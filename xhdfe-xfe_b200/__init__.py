@@ -10,6 +10,7 @@ from .absorber import (  # noqa: F401
     AbsorptionResult,
     FeComponentStats,
     FeRecoveryResult,
+    HeterogeneousSlopeTerm,
     OlsResult,
     absorb_fixed_effects,
     cuda_backend_available,

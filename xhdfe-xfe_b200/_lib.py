@@ -39,6 +39,8 @@ EXPORTED_SYMBOLS = (
     "b200fe_absorb",
     "b200fe_absorb_device",
     "b200fe_absorb_fe",
+    "b200fe_absorb_slopes",
+    "b200fe_absorb_slopes_device",
     "b200fe_demean_raw",
     "b200fe_fe_recovery_max_delta",
     "b200fe_demean_sorted_noalloc",
@@ -158,6 +160,13 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.b200fe_absorb_fe.argtypes = [vp, vp, vp, i64, c_int, c_int, pp, vp, vp,
                                      ctypes.POINTER(Options), vp, vp, pp, ctypes.POINTER(Result)]
     lib.b200fe_absorb_fe.restype = c_int
+    lib.b200fe_absorb_slopes.argtypes = [vp, vp, vp, i64, c_int, c_int, pp, vp, pp, vp, vp,
+                                         ctypes.POINTER(Options), vp, vp, ctypes.POINTER(Result)]
+    lib.b200fe_absorb_slopes.restype = c_int
+    lib.b200fe_absorb_slopes_device.argtypes = [vp, vp, i64, c_int, c_int, pp, vp, pp, vp, vp,
+                                                ctypes.POINTER(Options), vp,
+                                                ctypes.POINTER(Result), vp]
+    lib.b200fe_absorb_slopes_device.restype = c_int
     lib.b200fe_dense_ids_device.argtypes = [vp, vp, i64, vp, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.POINTER(ctypes.c_int32)]
     lib.b200fe_dense_ids_device.restype = c_int

@@ -4,6 +4,9 @@ Reference counterparts (reisportela/xhdfe-xfe):
 
 * ``Absorber.absorb``         -> hdfe::detail::absorb_fixed_effects_cuda
                                  (include/fe_absorption_cuda.hpp:127-134)
+* ``HeterogeneousSlopeTerm``  -> the struct of the same name (include/fe_absorption.hpp:49-53);
+                                 ``Absorber.absorb(slopes=...)`` is the is_slope path of
+                                 absorb_fixed_effects_cuda (src/fe_absorption_cuda.cu:2316)
 * ``absorb_fixed_effects``    -> hdfe::detail::absorb_fixed_effects_v6 with the
                                  CUDA backend (src/fe_absorption.cpp:8750, GPU
                                  dispatch :9203-9237): raw ids are ranked densely
@@ -33,6 +36,38 @@ from . import _lib
 
 TOLERANCE_MODES = {"xhdfe-fast": 0, "reghdfe-comparable": 1, "strict-residual": 2}
 PRECISIONS = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+
+
+@dataclass
+class HeterogeneousSlopeTerm:
+    """A slope on FE dimension ``fe_index`` with per-observation ``values``;
+    ``include_intercept`` keeps the group intercept in the same block
+    (the reference's struct of the same name, include/fe_absorption.hpp:49-53).
+    Tuples (fe_index, values, include_intercept) are accepted wherever a list
+    of terms is."""
+    fe_index: int
+    values: np.ndarray
+    include_intercept: bool = False
+
+
+def _slope_table(slopes, num_dims: int, n: int):
+    """Per-dim slope values (or None) and intercept flags from a term list."""
+    vals = [None] * num_dims
+    icpt = np.ones(num_dims, dtype=np.uint8)
+    for t in slopes:
+        d, z, inc = (t.fe_index, t.values, t.include_intercept) if isinstance(
+            t, HeterogeneousSlopeTerm) else t
+        d = int(d)
+        if d < 0 or d >= num_dims:
+            raise ValueError("Heterogeneous slope FE index out of range")
+        if vals[d] is not None:
+            raise ValueError("at most one slope term per FE dimension")
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        if z.shape != (n,):
+            raise ValueError("slope values must have the same length as y")
+        vals[d] = z
+        icpt[d] = 1 if inc else 0
+    return vals, icpt
 
 
 class AbsorberError(RuntimeError):
@@ -160,9 +195,11 @@ class Absorber:
         return int(self.lib.b200fe_context_stream(self.handle) or 0)
 
     def absorb(self, y, X, group_ids, num_groups, weights=None, options=None,
-               y_out=None, X_out=None, save_fe=False) -> AbsorptionResult:
+               y_out=None, X_out=None, save_fe=False, slopes=None) -> AbsorptionResult:
         """Absorb host arrays with dense ids (absorb_fixed_effects_cuda).  With
-        save_fe the result carries the FE coefficients (``fe``)."""
+        save_fe the result carries the FE coefficients (``fe``).  ``slopes``:
+        heterogeneous slope terms (GpuFeInput.is_slope); saved FEs are not
+        available with slopes."""
         y = np.ascontiguousarray(y, dtype=np.float64)
         n = y.shape[0]
         X = np.zeros((n, 0)) if X is None else np.asarray(X, dtype=np.float64)
@@ -184,6 +221,22 @@ class Absorber:
             X_out = np.empty((n, k), dtype=np.float64, order="F")
         o = options or make_options()
         r = _lib.Result()
+        if slopes:
+            if save_fe:
+                raise ValueError("saved fixed effects are not available with heterogeneous slopes")
+            zv, icpt = _slope_table(slopes, len(gids), n)
+            for z in zv:
+                if z is not None:
+                    _check_finite(z, "slope values")
+            rc = self.lib.b200fe_absorb_slopes(
+                self.handle, y.ctypes.data, X.ctypes.data if k else None, n, k, len(gids),
+                _ptr_array([g.ctypes.data for g in gids]), G.ctypes.data,
+                _ptr_array([z.ctypes.data if z is not None else None for z in zv]),
+                icpt.ctypes.data, None if w is None else w.ctypes.data, ctypes.byref(o),
+                y_out.ctypes.data, X_out.ctypes.data if k else None, ctypes.byref(r))
+            if rc not in (_lib.OK, _lib.NOT_CONVERGED):
+                raise self._err(rc)
+            return _to_result(r, y_out, X_out, G)
         fe = [np.zeros((int(g), k + 1), order="F") for g in G] if save_fe else None
         rc = self.lib.b200fe_absorb_fe(
             self.handle, y.ctypes.data, X.ctypes.data if k else None, n, k, len(gids),
@@ -218,6 +271,43 @@ class Absorber:
             _ptr_array([g.data_ptr() for g in group_ids]), G.ctypes.data,
             None if weights is None else weights.data_ptr(), ctypes.byref(o), out.data_ptr(),
             ctypes.byref(r), stream)
+        if rc not in (_lib.OK, _lib.NOT_CONVERGED):
+            raise self._err(rc)
+        return out, r
+
+    def absorb_slopes_device(self, v, group_ids, num_groups, slopes, weights=None,
+                             options=None, out=None, stream=None):
+        """absorb_device with heterogeneous slopes; the terms' values are
+        float64 CUDA tensors of length n.  Returns (out, _lib.Result)."""
+        import torch
+        if v.dtype != torch.float64 or not v.is_cuda or v.dim() != 2 or not v.is_contiguous():
+            raise ValueError("v must be a contiguous float64 CUDA tensor of shape (cols, n)")
+        cols, n = v.shape
+        if out is None:
+            out = torch.empty_like(v)
+        for g in group_ids:
+            if g.dtype != torch.int32 or not g.is_cuda or g.numel() != n:
+                raise ValueError("group ids must be int32 CUDA tensors of length n")
+        zp = [None] * len(group_ids)
+        icpt = np.ones(len(group_ids), dtype=np.uint8)
+        for t in slopes:
+            d, z, inc = (t.fe_index, t.values, t.include_intercept) if isinstance(
+                t, HeterogeneousSlopeTerm) else t
+            if not 0 <= int(d) < len(group_ids):
+                raise ValueError("Heterogeneous slope FE index out of range")
+            if (z.dtype != torch.float64 or not z.is_cuda or z.numel() != n
+                    or not z.is_contiguous()):
+                raise ValueError("slope values must be contiguous float64 CUDA tensors of length n")
+            zp[int(d)] = z.data_ptr()
+            icpt[int(d)] = 1 if inc else 0
+        G = np.ascontiguousarray(num_groups, dtype=np.int32)
+        o = options or make_options()
+        r = _lib.Result()
+        rc = self.lib.b200fe_absorb_slopes_device(
+            self.handle, v.data_ptr(), n, cols, len(group_ids),
+            _ptr_array([g.data_ptr() for g in group_ids]), G.ctypes.data, _ptr_array(zp),
+            icpt.ctypes.data, None if weights is None else weights.data_ptr(), ctypes.byref(o),
+            out.data_ptr(), ctypes.byref(r), stream)
         if rc not in (_lib.OK, _lib.NOT_CONVERGED):
             raise self._err(rc)
         return out, r
@@ -272,12 +362,13 @@ def _check_finite(a, name):
         raise ValueError(f"{name} contains non-finite values")
 
 
-def absorb_fixed_effects(y, X, fes, weights=None, *, device=0, save_fe=False,
+def absorb_fixed_effects(y, X, fes, weights=None, *, device=0, save_fe=False, slopes=None,
                          **options) -> AbsorptionResult:
     """Demean y and X on the FE dims ``fes`` (raw nonnegative ids), no singleton
     drop (absorb_fixed_effects_v6 with the GPU backend).  save_fe: also return
     the FE coefficients per dim, indexed by the dense ids (``fe``), as the
-    reference's retain_fixed_effects."""
+    reference's retain_fixed_effects.  slopes: heterogeneous slope terms
+    (fe_index, values, include_intercept), the v6 call's ``slopes``."""
     y = np.asarray(y, dtype=np.float64)
     _check_finite(y, "y")
     if X is not None:
@@ -285,7 +376,8 @@ def absorb_fixed_effects(y, X, fes, weights=None, *, device=0, save_fe=False,
     dense = [dense_ids(f) for f in fes]
     o = make_options(**options)
     return _thread_absorber(device).absorb(
-        y, X, [d for d, _ in dense], [g for _, g in dense], weights, o, save_fe=save_fe)
+        y, X, [d for d, _ in dense], [g for _, g in dense], weights, o, save_fe=save_fe,
+        slopes=slopes)
 
 
 @dataclass

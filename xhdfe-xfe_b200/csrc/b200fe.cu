@@ -27,6 +27,7 @@
 #include "setup_kernels.cuh"
 #include "ols_kernels.cuh"
 #include "prep_kernels.cuh"
+#include "slope_kernels.cuh"
 
 using namespace b200fe;
 
@@ -2625,6 +2626,481 @@ int b200fe_drop_singletons_device(b200fe_context* ctx, int num_dims, const int32
     }
     return drop_singletons_impl(ctx, num_dims, d_ids, num_groups, n, d_keep,
                                 max_iter > 0 ? max_iter : 100, dropped, rounds);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Heterogeneous slopes (slope_kernels.cuh): block-Jacobi CGLS over all FE
+// blocks, the path the reference's absorb_fixed_effects_cuda takes when a
+// GpuFeInput has is_slope set (src/fe_absorption_cuda.cu:2316-2420).
+// ---------------------------------------------------------------------------
+namespace {
+
+// The stop test bounds the preconditioned gradient sqrt(s' M^-1 s) =
+// sqrt(sum_d ||P_d r||_W^2); the distance to the exact projection is at most
+// that over sqrt(lambda_min) of the preconditioned operator, so the gradient
+// is driven two orders below the requested tolerance.
+constexpr double kSlopeTolFactor = 1e-2;
+
+int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C, int nd,
+                       const int32_t* const* d_gids, const int32_t* G,
+                       const double* const* d_z, const unsigned char* icpt, const double* d_w,
+                       const b200fe_options& o, double* d_out, b200fe_result* res) {
+    const cudaStream_t s = ctx->stream;
+    const int T = kSlopeThreads;
+    cudaEvent_t e0, e1, e2;
+    B_TRY(cudaEventCreate(&e0));
+    B_TRY(cudaEventCreate(&e1));
+    B_TRY(cudaEventCreate(&e2));
+    B_TRY(cudaEventRecord(e0, s));
+    // ---- validation
+    int* flags;
+    B_CHECK(get_buf(ctx, "sl_flags", 8, &flags));
+    B_TRY(cudaMemsetAsync(flags, 0, 8 * sizeof(int), s));
+    int p = 0;
+    for (int d = 0; d < nd; ++d)
+        if (G[d] > G[p]) p = d;
+    for (int d = 0; d < nd; ++d) {
+        validate_ids_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(d_gids[d], n, G[d], d == p, flags);
+        B_LAUNCHED();
+        if (d_z[d]) {
+            finite_values_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(d_z[d], n, flags);
+            B_LAUNCHED();
+        }
+    }
+    if (d_w) {
+        validate_weights_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(d_w, n, flags);
+        B_LAUNCHED();
+    }
+    int hf[4];
+    B_CHECK(sync_read_int(ctx, flags, 4, hf));
+    if (hf[0]) {
+        ctx->err = "group ids out of range";
+        return B200FE_INVALID_ARG;
+    }
+    if (hf[2]) {
+        ctx->err = "weights must be non-negative and finite";
+        return B200FE_INVALID_ARG;
+    }
+    if (hf[3]) {
+        ctx->err = "slope values must be finite";
+        return B200FE_INVALID_ARG;
+    }
+    // ---- observations in primary order
+    int32_t *pord = nullptr, *iota = nullptr, *gp = nullptr;
+    B_CHECK(get_buf(ctx, "sl_iota", n, &iota));
+    iota_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(iota, n);
+    B_LAUNCHED();
+    if (hf[1]) {
+        B_CHECK(get_buf(ctx, "sl_pord", n, &pord));
+        B_CHECK(get_buf(ctx, "sl_gp", n, &gp));
+        B_CHECK(cub_sort_pairs(ctx, d_gids[p], gp, iota, pord, n, G[p]));
+    } else {
+        gp = const_cast<int32_t*>(d_gids[p]);
+    }
+    const double* w = d_w;
+    if (d_w && pord) {
+        double* wp;
+        B_CHECK(get_buf(ctx, "sl_w", n, &wp));
+        gather_kernel<double><<<grid_for(ctx, n, T), T, 0, s>>>(d_w, pord, n, wp);
+        B_LAUNCHED();
+        w = wp;
+    }
+    double *R, *Q;
+    B_CHECK(get_buf(ctx, "sl_R", static_cast<size_t>(n) * C, &R));
+    B_CHECK(get_buf(ctx, "sl_Q", static_cast<size_t>(n) * C, &Q));
+    slope_load_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(d_v, pord, n, C, R);
+    B_LAUNCHED();
+    // ---- per-dim structure
+    SlopeDim dims[B200FE_MAX_DIMS];
+    int order[B200FE_MAX_DIMS];  // segment passes: the primary (writer) last
+    int no = 0;
+    for (int d = 0; d < nd; ++d)
+        if (d != p) order[no++] = d;
+    order[no++] = p;
+    double op_norm2 = 0.0;
+    int present[B200FE_MAX_DIMS] = {0};
+    int fin_grid[B200FE_MAX_DIMS] = {0};
+    const int RB = T / C;
+    for (int d = 0; d < nd; ++d) {
+        const std::string sx = std::to_string(d);
+        SlopeDim& D = dims[d];
+        D = SlopeDim{};
+        D.G = G[d];
+        D.has_b = d_z[d] ? 1 : 0;
+        D.has_a = d_z[d] ? (icpt && icpt[d] ? 1 : 0) : 1;
+        D.nb = D.has_a + D.has_b;
+        int32_t *sorted = gp, *off, *nch, *grp_ch;
+        if (d == p) {
+            D.ids = gp;
+        } else {
+            int32_t* ids = const_cast<int32_t*>(d_gids[d]);
+            if (pord) {
+                B_CHECK(get_buf(ctx, "sl_ids" + sx, n, &ids));
+                gather_kernel<int32_t><<<grid_for(ctx, n, T), T, 0, s>>>(d_gids[d], pord, n, ids);
+                B_LAUNCHED();
+            }
+            D.ids = ids;
+            int32_t* perm;
+            B_CHECK(get_buf(ctx, "sl_perm" + sx, n, &perm));
+            B_CHECK(get_buf(ctx, "sl_sorted", n, &sorted));
+            B_CHECK(cub_sort_pairs(ctx, ids, sorted, iota, perm, n, G[d]));
+            D.perm = perm;
+        }
+        if (d_z[d]) {
+            double* z = const_cast<double*>(d_z[d]);
+            if (pord) {
+                B_CHECK(get_buf(ctx, "sl_z" + sx, n, &z));
+                gather_kernel<double><<<grid_for(ctx, n, T), T, 0, s>>>(d_z[d], pord, n, z);
+                B_LAUNCHED();
+            }
+            D.z = z;
+        }
+        B_CHECK(get_buf(ctx, "sl_off" + sx, static_cast<size_t>(G[d]) + 1, &off));
+        segment_offsets_kernel<<<grid_for(ctx, n + 1, T), T, 0, s>>>(sorted, n, G[d], off);
+        B_LAUNCHED();
+        B_CHECK(get_buf(ctx, "sl_nch", static_cast<size_t>(G[d]) + 1, &nch));
+        B_CHECK(get_buf(ctx, "sl_grpch" + sx, static_cast<size_t>(G[d]) + 1, &grp_ch));
+        slope_chunk_count_kernel<<<grid_for(ctx, G[d] + 1, T), T, 0, s>>>(off, G[d], nch);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, nch, grp_ch, static_cast<int64_t>(G[d]) + 1));
+        int* cnt;
+        B_CHECK(get_buf(ctx, "sl_cnt", 1, &cnt));
+        B_TRY(cudaMemsetAsync(cnt, 0, sizeof(int), s));
+        count_nonempty_kernel<<<grid_for(ctx, G[d], T), T, 0, s>>>(off, G[d], cnt);
+        B_LAUNCHED();
+        int hc[2];
+        B_CHECK(sync_read_int(ctx, grp_ch + G[d], 1, &hc[0]));
+        B_CHECK(sync_read_int(ctx, cnt, 1, &hc[1]));
+        D.nch = hc[0];
+        present[d] = hc[1];
+        int32_t *cb, *ce;
+        B_CHECK(get_buf(ctx, "sl_chb" + sx, D.nch, &cb));
+        B_CHECK(get_buf(ctx, "sl_che" + sx, D.nch, &ce));
+        slope_chunk_fill_kernel<<<grid_for(ctx, G[d], T), T, 0, s>>>(off, G[d], grp_ch, cb, ce);
+        B_LAUNCHED();
+        D.ch_beg = cb;
+        D.ch_end = ce;
+        D.grp_ch = grp_ch;
+        // moments and block inverses
+        double *cm, *minv, *pop;
+        B_CHECK(get_buf(ctx, "sl_cm", static_cast<size_t>(D.nch) * 5, &cm));
+        B_CHECK(get_buf(ctx, "sl_minv" + sx, static_cast<size_t>(G[d]) * 3, &minv));
+        slope_moments_kernel<<<grid_for(ctx, static_cast<int64_t>(D.nch) * 32, T), T, 0, s>>>(D, w, cm);
+        B_LAUNCHED();
+        const int gb = grid_for(ctx, G[d], T, 4);
+        B_CHECK(get_buf(ctx, "sl_pop", gb, &pop));
+        slope_block_inverse_kernel<<<gb, T, 0, s>>>(D, cm, minv, pop);
+        B_LAUNCHED();
+        D.minv = minv;
+        std::vector<double> hp(gb);
+        B_TRY(cudaMemcpyAsync(hp.data(), pop, sizeof(double) * gb, cudaMemcpyDeviceToHost, s));
+        B_TRY(cudaStreamSynchronize(s));
+        for (double v : hp) op_norm2 += v;
+        const size_t cw = static_cast<size_t>(G[d]) * D.nb * C;
+        B_CHECK(get_buf(ctx, "sl_part" + sx, static_cast<size_t>(D.nch) * D.nb * C, &D.part));
+        B_CHECK(get_buf(ctx, "sl_zv" + sx, cw, &D.zv));
+        B_CHECK(get_buf(ctx, "sl_p" + sx, cw, &D.p));
+        fin_grid[d] = grid_for(ctx, (G[d] + RB - 1) / RB, 1, 4);
+    }
+    // ---- input norms and stop thresholds
+    const int gN = grid_for(ctx, (n + RB - 1) / RB, 1, 8);
+    double *pw, *pu;
+    B_CHECK(get_buf(ctx, "sl_pw", static_cast<size_t>(gN) * C, &pw));
+    B_CHECK(get_buf(ctx, "sl_pu", static_cast<size_t>(gN) * C, &pu));
+    slope_norms_kernel<<<gN, C * RB, 0, s>>>(R, w, n, C, RB, pw, pu);
+    B_LAUNCHED();
+    std::vector<double> hpw(static_cast<size_t>(gN) * C), hpu(static_cast<size_t>(gN) * C);
+    B_TRY(cudaMemcpyAsync(hpw.data(), pw, sizeof(double) * hpw.size(), cudaMemcpyDeviceToHost, s));
+    B_TRY(cudaMemcpyAsync(hpu.data(), pu, sizeof(double) * hpu.size(), cudaMemcpyDeviceToHost, s));
+    B_TRY(cudaStreamSynchronize(s));
+    std::vector<double> vw(C, 0.0), vu(C, 0.0), thr(C);
+    for (int b = 0; b < gN; ++b)
+        for (int c = 0; c < C; ++c) {
+            vw[c] += hpw[static_cast<size_t>(b) * C + c];
+            vu[c] += hpu[static_cast<size_t>(b) * C + c];
+        }
+    const double ti = std::max(tol_eff(o), 0.0) * kSlopeTolFactor;
+    for (int c = 0; c < C; ++c) thr[c] = ti * ti * vw[c];
+    // scalars: thr, gamma, beta, nu, alpha [C] each; active [C]; done
+    double* sc;
+    int *active, *done;
+    B_CHECK(get_buf(ctx, "sl_scal", static_cast<size_t>(5) * C, &sc));
+    B_CHECK(get_buf(ctx, "sl_active", C, &active));
+    B_CHECK(get_buf(ctx, "sl_done", 1, &done));
+    double *d_thr = sc, *gamma = sc + C, *beta = sc + 2 * C, *nu = sc + 3 * C, *alpha = sc + 4 * C;
+    B_TRY(cudaMemcpyAsync(d_thr, thr.data(), sizeof(double) * C, cudaMemcpyHostToDevice, s));
+    int stride = 1;
+    for (int d = 0; d < nd; ++d) stride = std::max(stride, fin_grid[d]);
+    double *pg, *pn, *pq;
+    B_CHECK(get_buf(ctx, "sl_pg", static_cast<size_t>(nd) * stride * C, &pg));
+    B_CHECK(get_buf(ctx, "sl_pn", static_cast<size_t>(nd) * stride * C, &pn));
+    const int gG = gN;
+    B_CHECK(get_buf(ctx, "sl_pq", static_cast<size_t>(gG) * C, &pq));
+    B_TRY(cudaEventRecord(e1, s));
+
+    // ---- iteration pieces
+    const int CW = C <= 32 ? 1 : C <= 64 ? 2 : C <= 128 ? 4 : 8;
+    auto segment = [&](int d, bool update) -> int {
+        SlopeSegArgs a{};
+        a.d = dims[d];
+        a.C = C;
+        a.slots = CW == 1 ? 32 / C : 1;
+        a.R = R;
+        a.Q = update ? Q : nullptr;
+        a.alpha = alpha;
+        a.w = w;
+        a.write = update && d == p;
+        const int g = grid_for(ctx, static_cast<int64_t>(dims[d].nch) * 32, T, 16);
+        if (CW == 1) slope_segment_kernel<1><<<g, T, 0, s>>>(a);
+        else if (CW == 2) slope_segment_kernel<2><<<g, T, 0, s>>>(a);
+        else if (CW == 4) slope_segment_kernel<4><<<g, T, 0, s>>>(a);
+        else slope_segment_kernel<8><<<g, T, 0, s>>>(a);
+        B_LAUNCHED();
+        return B200FE_OK;
+    };
+    auto gradient = [&](bool update, bool init) -> int {
+        for (int i = 0; i < nd; ++i) B_CHECK(segment(order[i], update));
+        for (int d = 0; d < nd; ++d) {
+            slope_finalize_kernel<<<fin_grid[d], C * RB, 0, s>>>(
+                dims[d], C, RB, pg + static_cast<size_t>(d) * stride * C,
+                pn + static_cast<size_t>(d) * stride * C);
+            B_LAUNCHED();
+        }
+        SlopeBetaArgs b{};
+        b.nd = nd;
+        b.C = C;
+        for (int d = 0; d < nd; ++d) b.grid[d] = fin_grid[d];
+        b.stride = stride;
+        b.part_g = pg;
+        b.part_n = pn;
+        b.thr = d_thr;
+        b.gamma = gamma;
+        b.beta = beta;
+        b.nu = nu;
+        b.active = active;
+        b.done = done;
+        b.init = init ? 1 : 0;
+        slope_beta_kernel<<<1, T, 0, s>>>(b);
+        B_LAUNCHED();
+        for (int d = 0; d < nd; ++d) {
+            const int64_t tot = static_cast<int64_t>(dims[d].G) * dims[d].nb * C;
+            slope_direction_kernel<<<grid_for(ctx, tot, T), T, 0, s>>>(dims[d], C, beta);
+            B_LAUNCHED();
+        }
+        return B200FE_OK;
+    };
+    SlopeGatherArgs ga{};
+    ga.nd = nd;
+    for (int d = 0; d < nd; ++d) ga.dim[d] = dims[d];
+    ga.n = n;
+    ga.C = C;
+    ga.RB = RB;
+    ga.w = w;
+    ga.Q = Q;
+    ga.part = pq;
+
+    B_CHECK(gradient(false, true));
+    const int ci = std::max(1, o.check_interval);
+    const int max_it = o.max_iter > 0 ? o.max_iter : 10000;
+    int it = 0, hd = 0;
+    B_CHECK(sync_read_int(ctx, done, 1, &hd));
+    while (!hd && it < max_it) {
+        const int steps = std::min(ci, max_it - it);
+        for (int k = 0; k < steps; ++k) {
+            slope_gather_kernel<<<gG, C * RB, 0, s>>>(ga);
+            B_LAUNCHED();
+            slope_alpha_kernel<<<1, T, 0, s>>>(pq, gG, C, gamma, active, alpha);
+            B_LAUNCHED();
+            B_CHECK(gradient(true, false));
+        }
+        it += steps;
+        B_CHECK(sync_read_int(ctx, done, 1, &hd));
+    }
+    slope_store_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(R, pord, n, C, d_out);
+    B_LAUNCHED();
+    std::vector<double> hs(C);
+    B_TRY(cudaMemcpyAsync(hs.data(), gamma, sizeof(double) * C, cudaMemcpyDeviceToHost, s));
+    std::vector<double> hnu(C);
+    B_TRY(cudaMemcpyAsync(hnu.data(), nu, sizeof(double) * C, cudaMemcpyDeviceToHost, s));
+    B_TRY(cudaEventRecord(e2, s));
+    B_TRY(cudaEventSynchronize(e2));
+    res->setup_ms = elapsed_ms(e0, e1);
+    res->solve_ms = elapsed_ms(e1, e2);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    // ---- result fields
+    const double opn = std::sqrt(std::max(0.0, op_norm2));
+    double abs_res = 0.0, abs_rel = 0.0, rel = 0.0;
+    for (int c = 0; c < C; ++c) {
+        const double ab = std::sqrt(std::max(0.0, hnu[c]));
+        const double scl = opn * std::sqrt(std::max(0.0, vu[c]));
+        double r = 0.0;
+        if (scl > 0.0) r = ab / scl;
+        else if (ab > 0.0) r = std::numeric_limits<double>::max();
+        abs_res = std::max(abs_res, ab);
+        abs_rel = std::max(abs_rel, r);
+        if (vw[c] > 0.0) rel = std::max(rel, std::sqrt(std::max(0.0, hs[c]) / vw[c]));
+    }
+    res->iterations = it;
+    res->outer_iterations = 1;
+    res->converged = hd ? 1 : 0;
+    res->abs_residual = abs_res;
+    res->abs_residual_rel = abs_rel;
+    res->rel_residual = rel;
+    res->primary_dim = p;
+    for (int d = 0; d < nd; ++d) res->num_levels_present[d] = present[d];
+    const double limit = std::max(8.0 * std::max(0.0, tol_eff(o)),
+                                  64.0 * std::numeric_limits<double>::epsilon());
+    res->precision_certified = res->converged && (o.certify ? abs_rel <= limit : 1);
+    return res->converged ? B200FE_OK : B200FE_NOT_CONVERGED;
+}
+
+int check_slopes(b200fe_context* ctx, int cols, int num_dims) {
+    if (cols > kSlopeMaxCols) {
+        ctx->err = "the slope absorber takes at most 256 columns";
+        return B200FE_INVALID_ARG;
+    }
+    if (num_dims < 1) {
+        ctx->err = "need at least one FE dimension";
+        return B200FE_INVALID_ARG;
+    }
+    return B200FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200fe_absorb_slopes_device(b200fe_context* ctx, const double* d_v, int64_t n, int cols,
+                                int num_dims, const int32_t* const* d_group_ids,
+                                const int32_t* num_groups, const double* const* d_slope_values,
+                                const unsigned char* slope_has_intercept, const double* d_weights,
+                                const b200fe_options* opts, double* d_out, b200fe_result* res,
+                                void* stream) {
+    b200fe_result local;
+    b200fe_result* r = res ? res : &local;
+    clear_result(r);
+    int rc = check_common(ctx, n, cols, num_dims, num_groups);
+    if (rc != B200FE_OK) return r->status = rc;
+    if (!d_v || !d_out || !d_group_ids) {
+        ctx->err = "null pointer argument";
+        return r->status = B200FE_INVALID_ARG;
+    }
+    rc = check_slopes(ctx, cols, num_dims);
+    if (rc != B200FE_OK) return r->status = rc;
+    const double* z[B200FE_MAX_DIMS] = {nullptr};
+    for (int d = 0; d < num_dims; ++d) {
+        if (!d_group_ids[d]) {
+            ctx->err = "null group id array";
+            return r->status = B200FE_INVALID_ARG;
+        }
+        z[d] = d_slope_values ? d_slope_values[d] : nullptr;
+    }
+    b200fe_options o;
+    if (opts) o = *opts;
+    else b200fe_default_options(&o);
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return r->status = B200FE_UNAVAILABLE;
+    }
+    const cudaStream_t own = ctx->stream;
+    if (stream) ctx->stream = static_cast<cudaStream_t>(stream);
+    const long long l0 = ctx->launches, c0 = ctx->lib_calls;
+    rc = slopes_device_impl(ctx, d_v, n, cols, num_dims, d_group_ids, num_groups, z,
+                            slope_has_intercept, d_weights, o, d_out, r);
+    ctx->stream = own;
+    r->kernel_launches = ctx->launches - l0;
+    r->library_calls = ctx->lib_calls - c0;
+    return r->status = rc;
+}
+
+int b200fe_absorb_slopes(b200fe_context* ctx, const double* y, const double* X, int64_t n, int k,
+                         int num_dims, const int32_t* const* group_ids, const int32_t* num_groups,
+                         const double* const* slope_values, const unsigned char* slope_has_intercept,
+                         const double* weights, const b200fe_options* opts, double* y_out,
+                         double* X_out, b200fe_result* res) {
+    b200fe_result local;
+    b200fe_result* r = res ? res : &local;
+    clear_result(r);
+    int rc = check_common(ctx, n, k + 1, num_dims, num_groups);
+    if (rc != B200FE_OK) return r->status = rc;
+    if (!y || !y_out || (k > 0 && (!X || !X_out)) || !group_ids) {
+        ctx->err = "null pointer argument";
+        return r->status = B200FE_INVALID_ARG;
+    }
+    rc = check_slopes(ctx, k + 1, num_dims);
+    if (rc != B200FE_OK) return r->status = rc;
+    for (int d = 0; d < num_dims; ++d)
+        if (!group_ids[d]) {
+            ctx->err = "null group id array";
+            return r->status = B200FE_INVALID_ARG;
+        }
+    b200fe_options o;
+    if (opts) o = *opts;
+    else b200fe_default_options(&o);
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return r->status = B200FE_UNAVAILABLE;
+    }
+    const cudaStream_t s = ctx->stream;
+    const long long l0 = ctx->launches, c0 = ctx->lib_calls;
+    const int cols = k + 1;
+    auto run = [&]() -> int {
+        double *dv, *dout, *dw = nullptr;
+        B_CHECK(get_buf(ctx, "io_v", static_cast<size_t>(n) * cols, &dv));
+        B_CHECK(get_buf(ctx, "io_out", static_cast<size_t>(n) * cols, &dout));
+        int32_t* dg[B200FE_MAX_DIMS] = {nullptr};
+        double* dz[B200FE_MAX_DIMS] = {nullptr};
+        for (int d = 0; d < num_dims; ++d) {
+            B_CHECK(get_buf(ctx, "io_g" + std::to_string(d), n, &dg[d]));
+            if (slope_values && slope_values[d])
+                B_CHECK(get_buf(ctx, "io_z" + std::to_string(d), n, &dz[d]));
+        }
+        if (weights) B_CHECK(get_buf(ctx, "io_w", n, &dw));
+        cudaEvent_t h0, h1, d0, d1;
+        B_TRY(cudaEventCreate(&h0));
+        B_TRY(cudaEventCreate(&h1));
+        B_TRY(cudaEventCreate(&d0));
+        B_TRY(cudaEventCreate(&d1));
+        B_TRY(cudaEventRecord(h0, s));
+        for (int d = 0; d < num_dims; ++d) {
+            B_TRY(cudaMemcpyAsync(dg[d], group_ids[d], sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+            if (dz[d])
+                B_TRY(cudaMemcpyAsync(dz[d], slope_values[d], sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        }
+        if (weights) B_TRY(cudaMemcpyAsync(dw, weights, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaMemcpyAsync(dv, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        if (k > 0)
+            B_TRY(cudaMemcpyAsync(dv + n, X, sizeof(double) * n * k, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaEventRecord(h1, s));
+        const double* zc[B200FE_MAX_DIMS];
+        for (int d = 0; d < B200FE_MAX_DIMS; ++d) zc[d] = dz[d];
+        int rc2 = slopes_device_impl(ctx, dv, n, cols, num_dims, dg, num_groups, zc,
+                                     slope_has_intercept, dw, o, dout, r);
+        if (rc2 != B200FE_OK && rc2 != B200FE_NOT_CONVERGED) return rc2;
+        B_TRY(cudaEventRecord(d0, s));
+        B_TRY(cudaMemcpyAsync(y_out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        if (k > 0)
+            B_TRY(cudaMemcpyAsync(X_out, dout + n, sizeof(double) * n * k, cudaMemcpyDeviceToHost, s));
+        B_TRY(cudaEventRecord(d1, s));
+        B_TRY(cudaEventSynchronize(d1));
+        r->h2d_ms = elapsed_ms(h0, h1);
+        r->d2h_ms = elapsed_ms(d0, d1);
+        cudaEventDestroy(h0);
+        cudaEventDestroy(h1);
+        cudaEventDestroy(d0);
+        cudaEventDestroy(d1);
+        return rc2;
+    };
+    rc = run();
+    r->kernel_launches = ctx->launches - l0;
+    r->library_calls = ctx->lib_calls - c0;
+    return r->status = rc;
 }
 
 }  // extern "C"

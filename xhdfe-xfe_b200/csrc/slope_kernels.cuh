@@ -1,0 +1,473 @@
+// Absorption with heterogeneous slopes: the FE space of a dimension d is
+// spanned per group g by the intercept 1_g, the slope z_d 1_g, or both
+// (the reference's HeterogeneousSlopeTerm, include/fe_absorption.hpp:49-53;
+// GpuFeInput.is_slope / slope_has_intercept / slope_values,
+// include/fe_absorption_cuda.hpp:12-22).  The within transform is the
+// W-orthogonal residual of every column on the sum of those spaces.
+//
+// Solver: CG on the normal equations in residual form (CGLS), all columns in
+// lock step, preconditioned by the exact per-group block inverse of every
+// dimension (block Jacobi = additive Schwarz over the FE blocks).  A group's
+// 2x2 block [W Z; Z ZZ] (W = sum w, Z = sum w z, ZZ = sum w z^2) is inverted
+// with the reference's determinant rule (compute_slope_coefficients_kernel,
+// src/fe_absorption_cuda.cu:586-650): det > 1e-12 max(1, W ZZ), otherwise the
+// group keeps its intercept only; a slope without intercept needs
+// ZZ > 1e-12 max(1, ZZ).  FP64 throughout.
+//
+// Layout (observations in the order of the primary dimension, the one with
+// the most groups):
+//   R, Q      [n][C] row-major FP64: residual and the search image D p
+//   ids_d     [n]   group of every observation in dimension d
+//   z_d       [n]   slope values (slope dims)
+//   perm_d    [n]   positions sorted by ids_d (stable); null for the primary
+//   chunks    per dim: ranges of <= ceil(len / nch) positions of one group,
+//             nch <= 1024 per group, so the per-group combine stays short
+//   coefficients per dim [G][nb][C]: block 0 the intercept (if any), then the
+//             slope (if any)
+// Every sum is taken in a fixed order (chunk, then lane slots, then chunks in
+// group order, then CTAs in order), so results are bitwise reproducible.
+
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b200fe {
+
+constexpr int kSlopeThreads = 256;
+constexpr int kSlopeChunkRows = 64;   // minimum rows per chunk
+constexpr int kSlopeMaxChunks = 1024; // chunks per group at most
+constexpr int kSlopeMaxCols = 256;
+constexpr double kSlopeDetTol = 1e-12;
+
+struct SlopeDim {
+    const int32_t* ids;     // [n] group per observation (primary order)
+    const double* z;        // [n] slope values or null
+    const int32_t* perm;    // [n] sorted positions or null (identity)
+    const int32_t* ch_beg;  // [nch] chunk ranges in sorted positions
+    const int32_t* ch_end;
+    const int32_t* grp_ch;  // [G + 1] first chunk of every group
+    const double* minv;     // [G][3] block inverse (m00, m01, m11)
+    double* part;           // [nch][nb][C] chunk sums
+    double* zv;             // [G][nb][C] preconditioned gradient
+    double* p;              // [G][nb][C] search direction
+    int32_t G;
+    int32_t nch;
+    int has_a, has_b, nb;
+};
+
+// ---------------------------------------------------------------------------
+// Setup: chunk ranges and per-group moments
+// ---------------------------------------------------------------------------
+
+// number of chunks of every group (0 for an empty group)
+__global__ void slope_chunk_count_kernel(const int32_t* __restrict__ off, int32_t G,
+                                         int32_t* __restrict__ nch) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g <= G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (g == G) {
+            nch[g] = 0;
+            continue;
+        }
+        const int32_t len = off[g + 1] - off[g];
+        int32_t c = (len + kSlopeChunkRows - 1) / kSlopeChunkRows;
+        nch[g] = min(c, kSlopeMaxChunks);
+    }
+}
+
+__global__ void slope_chunk_fill_kernel(const int32_t* __restrict__ off, int32_t G,
+                                        const int32_t* __restrict__ grp_ch,
+                                        int32_t* __restrict__ ch_beg, int32_t* __restrict__ ch_end) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t b = off[g], e = off[g + 1];
+        const int32_t c0 = grp_ch[g], nc = grp_ch[g + 1] - c0;
+        if (nc == 0) continue;
+        const int32_t L = (e - b + nc - 1) / nc;
+        for (int32_t i = 0; i < nc; ++i) {
+            ch_beg[c0 + i] = min(e, b + i * L);
+            ch_end[c0 + i] = min(e, b + (i + 1) * L);
+        }
+    }
+}
+
+// Per chunk: sum w, sum w z, sum w z^2, sum w^2, sum w^2 z^2 over its rows,
+// one warp per chunk (lanes stride the rows, fixed shuffle tree).
+__global__ void __launch_bounds__(kSlopeThreads)
+slope_moments_kernel(const SlopeDim d, const double* __restrict__ w, double* __restrict__ cm) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = static_cast<int64_t>(gridDim.x) * (kSlopeThreads / 32);
+    for (int64_t j = static_cast<int64_t>(blockIdx.x) * (kSlopeThreads / 32) + (threadIdx.x >> 5);
+         j < d.nch; j += nw) {
+        double m[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int32_t pos = d.ch_beg[j] + lane; pos < d.ch_end[j]; pos += 32) {
+            const int32_t k = d.perm ? d.perm[pos] : pos;
+            const double wk = w ? w[k] : 1.0;
+            const double zk = d.z ? d.z[k] : 0.0;
+            m[0] += wk;
+            m[1] = fma(wk, zk, m[1]);
+            m[2] = fma(wk * zk, zk, m[2]);
+            m[3] = fma(wk, wk, m[3]);
+            m[4] = fma(wk * zk, wk * zk, m[4]);
+        }
+#pragma unroll
+        for (int u = 0; u < 5; ++u) {
+            double v = m[u];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            m[u] = v;
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int u = 0; u < 5; ++u) cm[j * 5 + u] = m[u];
+        }
+    }
+}
+
+// Per group: combine the chunk moments in chunk order, form the block inverse
+// and the group's share of ||D'W||_F^2 (sum of the squared multipliers w and
+// w z of its basis columns); CTA partials of the latter in part_op[block].
+__global__ void __launch_bounds__(kSlopeThreads)
+slope_block_inverse_kernel(const SlopeDim d, const double* __restrict__ cm,
+                           double* __restrict__ minv, double* __restrict__ part_op) {
+    __shared__ double red[kSlopeThreads];
+    double op = 0.0;
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < d.G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double m[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int32_t j = d.grp_ch[g]; j < d.grp_ch[g + 1]; ++j)
+#pragma unroll
+            for (int u = 0; u < 5; ++u) m[u] += cm[static_cast<int64_t>(j) * 5 + u];
+        const double W = m[0], Z = m[1], ZZ = m[2];
+        double m00 = 0.0, m01 = 0.0, m11 = 0.0;
+        if (d.has_a && d.has_b) {
+            if (W > 0.0) {
+                const double det = W * ZZ - Z * Z;
+                const double scale = fmax(1.0, W * ZZ);
+                if (det > kSlopeDetTol * scale) {
+                    m00 = ZZ / det;
+                    m01 = -Z / det;
+                    m11 = W / det;
+                } else {
+                    m00 = 1.0 / W;
+                }
+            }
+        } else if (d.has_a) {
+            if (W > 0.0) m00 = 1.0 / W;
+        } else {
+            const double scale = fmax(1.0, ZZ);
+            if (ZZ > kSlopeDetTol * scale) m11 = 1.0 / ZZ;
+        }
+        minv[g * 3 + 0] = m00;
+        minv[g * 3 + 1] = m01;
+        minv[g * 3 + 2] = m11;
+        op += (d.has_a ? m[3] : 0.0) + (d.has_b ? m[4] : 0.0);
+    }
+    red[threadIdx.x] = op;
+    __syncthreads();
+    for (int s = kSlopeThreads / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part_op[blockIdx.x] = red[0];
+}
+
+// R[k][c] = v[c * n + pord[k]] (row-major in primary order)
+__global__ void slope_load_kernel(const double* __restrict__ v, const int32_t* __restrict__ pord,
+                                  int64_t n, int C, double* __restrict__ R) {
+    const int64_t total = n * C;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t k = e / C;
+        const int c = static_cast<int>(e - k * C);
+        const int64_t src = pord ? pord[k] : k;
+        R[e] = v[static_cast<int64_t>(c) * n + src];
+    }
+}
+
+// out[c * n + pord[k]] = R[k][c]
+__global__ void slope_store_kernel(const double* __restrict__ R, const int32_t* __restrict__ pord,
+                                   int64_t n, int C, double* __restrict__ out) {
+    const int64_t total = n * C;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t k = e / C;
+        const int c = static_cast<int>(e - k * C);
+        const int64_t dst = pord ? pord[k] : k;
+        out[static_cast<int64_t>(c) * n + dst] = R[e];
+    }
+}
+
+// flags[3] |= 1 when a slope value is not finite
+__global__ void finite_values_kernel(const double* __restrict__ z, int64_t n, int* flags) {
+    int bad = 0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        bad |= !(fabs(z[i]) <= 1.7976931348623157e308);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags + 3, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Column-wise CTA reduction for element kernels whose block holds RB rows of
+// C columns (thread t owns column t % C for the whole grid-stride loop).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void column_reduce(double* red, double v, int C, int RB, double* out) {
+    red[threadIdx.x] = v;
+    __syncthreads();
+    if (static_cast<int>(threadIdx.x) < C) {
+        double s = 0.0;
+        for (int r = 0; r < RB; ++r) s += red[r * C + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// per column, CTA partials of sum w r^2 and sum r^2 (the norms of the input)
+__global__ void __launch_bounds__(kSlopeThreads)
+slope_norms_kernel(const double* __restrict__ R, const double* __restrict__ w, int64_t n, int C,
+                   int RB, double* __restrict__ part_w, double* __restrict__ part_u) {
+    __shared__ double red[kSlopeThreads];
+    const int col = threadIdx.x % C, rr = threadIdx.x / C;
+    double aw = 0.0, au = 0.0;
+    if (rr < RB) {
+        for (int64_t k = static_cast<int64_t>(blockIdx.x) * RB + rr; k < n;
+             k += static_cast<int64_t>(gridDim.x) * RB) {
+            const double r = R[k * C + col];
+            const double wk = w ? w[k] : 1.0;
+            aw = fma(wk * r, r, aw);
+            au = fma(r, r, au);
+        }
+    }
+    column_reduce(red, aw, C, RB, part_w + static_cast<int64_t>(blockIdx.x) * C);
+    column_reduce(red, au, C, RB, part_u + static_cast<int64_t>(blockIdx.x) * C);
+}
+
+struct SlopeGatherArgs {
+    int nd;
+    SlopeDim dim[8];
+    int64_t n;
+    int C, RB;
+    const double* w;
+    double* Q;
+    double* part;  // [grid][C] sums of w q^2
+};
+
+// Q = D p, with CTA partials of q' W q per column.
+__global__ void __launch_bounds__(kSlopeThreads)
+slope_gather_kernel(const SlopeGatherArgs a) {
+    __shared__ double red[kSlopeThreads];
+    const int C = a.C;
+    const int col = threadIdx.x % C, rr = threadIdx.x / C;
+    double acc = 0.0;
+    if (rr < a.RB) {
+        for (int64_t k = static_cast<int64_t>(blockIdx.x) * a.RB + rr; k < a.n;
+             k += static_cast<int64_t>(gridDim.x) * a.RB) {
+            double q = 0.0;
+            for (int d = 0; d < a.nd; ++d) {
+                const SlopeDim& D = a.dim[d];
+                const int64_t base = (static_cast<int64_t>(D.ids[k]) * D.nb) * C + col;
+                if (D.has_a) q += D.p[base];
+                if (D.has_b) q = fma(D.z[k], D.p[base + (D.has_a ? C : 0)], q);
+            }
+            a.Q[k * C + col] = q;
+            const double wk = a.w ? a.w[k] : 1.0;
+            acc = fma(wk * q, q, acc);
+        }
+    }
+    column_reduce(red, acc, C, a.RB, a.part + static_cast<int64_t>(blockIdx.x) * C);
+}
+
+// alpha_c = gamma_c / (q' W q)_c for the columns still iterating
+__global__ void slope_alpha_kernel(const double* __restrict__ part, int nparts, int C,
+                                   const double* __restrict__ gamma, const int* __restrict__ active,
+                                   double* __restrict__ alpha) {
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        double dl = 0.0;
+        for (int b = 0; b < nparts; ++b) dl += part[static_cast<int64_t>(b) * C + c];
+        alpha[c] = (active[c] && dl > 0.0) ? gamma[c] / dl : 0.0;
+    }
+}
+
+struct SlopeSegArgs {
+    SlopeDim d;
+    int C;
+    int slots;           // rows a warp takes per step (32 / C for C <= 32, else 1)
+    double* R;
+    const double* Q;     // null: no update (the first gradient)
+    const double* alpha; // [C]
+    const double* w;
+    int write;           // store the updated residual (the primary dim only)
+};
+
+// Chunk sums of w r and w z r per column, r = R - alpha Q (stored back by the
+// writer).  One warp per chunk.  For C <= 32 the lanes form `slots` row slots
+// of C columns; for C > 32 lane l owns columns l, l + 32, ... (CW of them).
+template <int CW>
+__global__ void __launch_bounds__(kSlopeThreads)
+slope_segment_kernel(const SlopeSegArgs a) {
+    __shared__ double sred[kSlopeThreads / 32][2][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int C = a.C;
+    const SlopeDim& D = a.d;
+    const int S = a.slots;
+    const int slot = CW == 1 ? lane / C : 0;
+    const int col0 = CW == 1 ? lane - slot * C : lane;
+    const bool live = CW == 1 ? slot < S : true;
+    double al[CW];
+#pragma unroll
+    for (int u = 0; u < CW; ++u) {
+        const int c = col0 + 32 * u;
+        al[u] = (a.Q && live && c < C) ? a.alpha[c] : 0.0;
+    }
+    const int64_t nw = static_cast<int64_t>(gridDim.x) * (kSlopeThreads / 32);
+    for (int64_t j = static_cast<int64_t>(blockIdx.x) * (kSlopeThreads / 32) + wid; j < D.nch;
+         j += nw) {
+        double sa[CW], sb[CW];
+#pragma unroll
+        for (int u = 0; u < CW; ++u) sa[u] = sb[u] = 0.0;
+        if (live) {
+            const int32_t e = D.ch_end[j];
+            for (int32_t pos = D.ch_beg[j] + slot; pos < e; pos += S) {
+                const int64_t k = D.perm ? D.perm[pos] : pos;
+                const double wk = a.w ? a.w[k] : 1.0;
+                const double zk = D.has_b ? D.z[k] : 0.0;
+#pragma unroll
+                for (int u = 0; u < CW; ++u) {
+                    const int c = col0 + 32 * u;
+                    if (c < C) {
+                        double r = a.R[k * C + c];
+                        if (a.Q) r = fma(-al[u], a.Q[k * C + c], r);
+                        if (a.write) a.R[k * C + c] = r;
+                        const double wr = wk * r;
+                        sa[u] += wr;
+                        sb[u] = fma(wr, zk, sb[u]);
+                    }
+                }
+            }
+        }
+        double* out = D.part + (j * D.nb) * C;
+        if (CW == 1) {
+            // combine the row slots in slot order
+            sred[wid][0][lane] = sa[0];
+            sred[wid][1][lane] = sb[0];
+            __syncwarp();
+            if (lane < C) {
+                double ta = 0.0, tb = 0.0;
+                for (int s = 0; s < S; ++s) {
+                    ta += sred[wid][0][s * C + lane];
+                    tb += sred[wid][1][s * C + lane];
+                }
+                if (D.has_a) out[lane] = ta;
+                if (D.has_b) out[(D.has_a ? C : 0) + lane] = tb;
+            }
+            __syncwarp();
+        } else {
+#pragma unroll
+            for (int u = 0; u < CW; ++u) {
+                const int c = col0 + 32 * u;
+                if (c < C) {
+                    if (D.has_a) out[c] = sa[u];
+                    if (D.has_b) out[(D.has_a ? C : 0) + c] = sb[u];
+                }
+            }
+        }
+    }
+}
+
+// Per group and column: the gradient s (chunk sums in chunk order), the
+// preconditioned gradient zv = M^-1 s, and CTA partials of s'zv (gamma) and
+// s's (the certificate's ||D'W r||^2).
+__global__ void __launch_bounds__(kSlopeThreads)
+slope_finalize_kernel(SlopeDim d, int C, int RB, double* __restrict__ part_g,
+                      double* __restrict__ part_n) {
+    __shared__ double red[kSlopeThreads];
+    const int col = threadIdx.x % C, rr = threadIdx.x / C;
+    double ag = 0.0, an = 0.0;
+    if (rr < RB) {
+        for (int64_t g = static_cast<int64_t>(blockIdx.x) * RB + rr; g < d.G;
+             g += static_cast<int64_t>(gridDim.x) * RB) {
+            double sa = 0.0, sb = 0.0;
+            for (int32_t j = d.grp_ch[g]; j < d.grp_ch[g + 1]; ++j) {
+                const double* pj = d.part + (static_cast<int64_t>(j) * d.nb) * C + col;
+                if (d.has_a) sa += pj[0];
+                if (d.has_b) sb += pj[d.has_a ? C : 0];
+            }
+            const double m00 = d.minv[g * 3 + 0], m01 = d.minv[g * 3 + 1], m11 = d.minv[g * 3 + 2];
+            double* zg = d.zv + (g * d.nb) * C + col;
+            if (d.has_a && d.has_b) {
+                const double za = fma(m00, sa, m01 * sb);
+                const double zb = fma(m01, sa, m11 * sb);
+                zg[0] = za;
+                zg[C] = zb;
+                ag = fma(sa, za, fma(sb, zb, ag));
+            } else if (d.has_a) {
+                const double za = m00 * sa;
+                zg[0] = za;
+                ag = fma(sa, za, ag);
+            } else {
+                const double zb = m11 * sb;
+                zg[0] = zb;
+                ag = fma(sb, zb, ag);
+            }
+            an = fma(sa, sa, fma(sb, sb, an));
+        }
+    }
+    column_reduce(red, ag, C, RB, part_g + static_cast<int64_t>(blockIdx.x) * C);
+    column_reduce(red, an, C, RB, part_n + static_cast<int64_t>(blockIdx.x) * C);
+}
+
+struct SlopeBetaArgs {
+    int nd, C;
+    int grid[8];             // finalize CTAs per dim
+    int64_t stride;          // partial slots per dim
+    const double* part_g;    // [nd][stride][C]
+    const double* part_n;
+    const double* thr;       // [C] stop threshold on gamma
+    double* gamma;           // [C]
+    double* beta;            // [C]
+    double* nu;              // [C] ||D'W r||^2 at the last gradient
+    int* active;             // [C]
+    int* done;               // all columns stopped
+    int init;
+};
+
+// One CTA: gamma_new = sum over dims and CTAs (fixed order), beta, stop test.
+__global__ void slope_beta_kernel(const SlopeBetaArgs a) {
+    int any = 0;
+    for (int c = threadIdx.x; c < a.C; c += blockDim.x) {
+        double g = 0.0, nu = 0.0;
+        for (int d = 0; d < a.nd; ++d)
+            for (int b = 0; b < a.grid[d]; ++b) {
+                const int64_t o = (d * a.stride + b) * a.C + c;
+                g += a.part_g[o];
+                nu += a.part_n[o];
+            }
+        a.nu[c] = nu;
+        if (a.init) {
+            a.gamma[c] = g;
+            a.beta[c] = 0.0;
+            a.active[c] = g > a.thr[c] ? 1 : 0;
+        } else if (a.active[c]) {
+            a.beta[c] = a.gamma[c] > 0.0 ? g / a.gamma[c] : 0.0;
+            a.gamma[c] = g;
+            if (!(g > a.thr[c])) a.active[c] = 0;
+        } else {
+            a.beta[c] = 0.0;
+        }
+        any |= a.active[c];
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) *a.done = any ? 0 : 1;
+}
+
+// p = zv + beta p (p = zv where beta is 0, so p needs no initial value)
+__global__ void slope_direction_kernel(SlopeDim d, int C, const double* __restrict__ beta) {
+    const int64_t total = static_cast<int64_t>(d.G) * d.nb * C;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double b = beta[e % C];
+        d.p[e] = b == 0.0 ? d.zv[e] : fma(b, d.p[e], d.zv[e]);
+    }
+}
+
+}  // namespace b200fe

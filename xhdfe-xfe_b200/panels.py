@@ -129,6 +129,42 @@ def akm_two_way(n_obs: int = 1_000_000, *, n_firms: int = 10_000, n_years: int =
                  meta={"n_workers": W, "seed": seed, "design": "akm_two_way"})
 
 
+def akm_firm_tenure_slopes(n_obs: int = 1_000_000, *, n_firms: int = 10_000,
+                           n_years: int = 10, seed: int = 0, move_prob: float = 0.1,
+                           zipf: float = 1.1) -> tuple[Panel, list]:
+    """AKM panel with firm-specific tenure slopes (``firm##c.tenure``).
+
+    The heterogeneous firm-seniority design of the reference's hardest
+    benchmark spec, on synthetic spells: worker, firm and year FEs, plus a
+    slope on tenure (years in the current spell) per firm with the firm
+    intercept.  x1, x2 as in ``akm_two_way``;
+    y = 0.5 x1 - 0.3 x2 + worker FE + firm FE + firm slope * tenure + year FE + N(0, 1),
+    firm slopes ~ N(0.05, 0.02^2).  Returns the panel (fes: worker, firm, year)
+    and the slope list [(1, tenure, True)] in the reference's
+    HeterogeneousSlopeTerm form (fe_index, values, include_intercept).
+    """
+    rng, worker, firm, year, ten, _pos, W = akm_spells(
+        n_obs, n_firms, n_years, seed=seed, move_prob=move_prob, zipf=zipf)
+    a = rng.standard_normal(W)
+    psi = 0.5 * rng.standard_normal(n_firms)
+    slope = 0.05 + 0.02 * rng.standard_normal(n_firms)
+    gam = 0.1 * rng.standard_normal(n_years)
+    aw = a[worker]
+    tenure = ten.astype(np.float64)
+    X = np.empty((n_obs, 2), dtype=np.float64, order="F")
+    X[:, 0] = 0.3 * aw + np.sqrt(0.91) * rng.standard_normal(n_obs)
+    X[:, 1] = 0.3 * aw + np.sqrt(0.91) * rng.standard_normal(n_obs)
+    y = (0.5 * X[:, 0] - 0.3 * X[:, 1] + aw + psi[firm] + slope[firm] * tenure + gam[year]
+         + rng.standard_normal(n_obs))
+    w_id, gw = _dense(worker, W)
+    f_id, gf = _dense(firm, n_firms)
+    t_id, gt = _dense(year, n_years)
+    panel = Panel(y=y, X=X, fes=[w_id, f_id, t_id], fe_names=["worker", "firm", "year"],
+                  levels=[gw, gf, gt], cluster=w_id.copy(),
+                  meta={"n_workers": W, "seed": seed, "design": "akm_firm_tenure_slopes"})
+    return panel, [(1, tenure, True)]
+
+
 def akm_batched(n_obs: int = 50_000_000, *, n_firms: int = 800_000, n_years: int = 36,
                 seed: int = 0, move_prob: float = 0.1, zipf: float = 1.1,
                 n_noise: int = 7) -> Panel:

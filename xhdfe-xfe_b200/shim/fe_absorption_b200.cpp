@@ -21,10 +21,12 @@
 // when the GPU backend was requested, src/fe_absorption.cpp:9227-9237);
 // return true with converged=false on non-convergence; never throw.  Features
 // this library does not provide yet return false, so the reference fails
-// closed rather than silently using another path: heterogeneous slopes,
-// group/individual FEs, and saved fixed effects in the reference's per-sweep
-// means mode.  Saved FEs in the coefficient mode (fe_alpha_y / fe_alpha_X,
-// what recover_fixed_effects consumes) come from b200fe_absorb_fe.  The
+// closed rather than silently using another path: group/individual FEs, saved
+// fixed effects together with heterogeneous slopes, and saved fixed effects in
+// the reference's per-sweep means mode.  Heterogeneous slopes (GpuFeInput with
+// is_slope) run on b200fe_absorb_slopes.  Saved FEs in the coefficient mode
+// (fe_alpha_y / fe_alpha_X, what recover_fixed_effects consumes) come from
+// b200fe_absorb_fe.  The
 // AKM/KSS solver (akm_cuda_*) runs on the library's batched PCG
 // (b200fe_kss_*).
 
@@ -88,11 +90,20 @@ bool absorb_fixed_effects_cuda(const Eigen::Ref<const Eigen::VectorXd>& y,
             return false;
         std::vector<const int32_t*> gids;
         std::vector<int32_t> levels;
+        std::vector<const double*> zvals;
+        std::vector<unsigned char> icpt;
+        bool any_slope = false;
         for (const GpuFeInput& fe : fe_inputs) {
-            if (fe.is_slope || !fe.group_ids) return false;
+            if (!fe.group_ids) return false;
+            if (fe.is_slope && !fe.slope_values) return false;
+            any_slope = any_slope || fe.is_slope;
             gids.push_back(fe.group_ids);
             levels.push_back(fe.num_groups);
+            zvals.push_back(fe.is_slope ? fe.slope_values : nullptr);
+            icpt.push_back(fe.is_slope ? (fe.slope_has_intercept ? 1 : 0) : 1);
         }
+        // saved FEs with slopes: not provided, fail closed
+        if (any_slope && save_fe) return false;
         b200fe_context* ctx = thread_ctx();
         if (!ctx) return false;
         b200fe_options o;
@@ -120,11 +131,19 @@ bool absorb_fixed_effects_cuda(const Eigen::Ref<const Eigen::VectorXd>& y,
             fe_ptr[d] = fe[d].data();
         }
         b200fe_result r;
-        const int rc = b200fe_absorb_fe(ctx, yc.data(), k ? Xc.data() : nullptr, n, k,
-                                        static_cast<int>(gids.size()), gids.data(), levels.data(),
-                                        weights ? weights->data() : nullptr, &o,
-                                        result.y_tilde.data(), k ? result.X_tilde.data() : nullptr,
-                                        save_fe ? fe_ptr.data() : nullptr, &r);
+        const int rc =
+            any_slope
+                ? b200fe_absorb_slopes(ctx, yc.data(), k ? Xc.data() : nullptr, n, k,
+                                       static_cast<int>(gids.size()), gids.data(), levels.data(),
+                                       zvals.data(), icpt.data(),
+                                       weights ? weights->data() : nullptr, &o,
+                                       result.y_tilde.data(), k ? result.X_tilde.data() : nullptr,
+                                       &r)
+                : b200fe_absorb_fe(ctx, yc.data(), k ? Xc.data() : nullptr, n, k,
+                                   static_cast<int>(gids.size()), gids.data(), levels.data(),
+                                   weights ? weights->data() : nullptr, &o,
+                                   result.y_tilde.data(), k ? result.X_tilde.data() : nullptr,
+                                   save_fe ? fe_ptr.data() : nullptr, &r);
         if (rc != B200FE_OK && rc != B200FE_NOT_CONVERGED) return false;
         if (save_fe) {  // the fields the reference fills (src/fe_absorption_cuda.cu:4663-4690)
             result.fe_group_ids.assign(D, {});
