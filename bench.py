@@ -17,6 +17,8 @@ Lines printed by rank 0 (one JSON line):
            sample of the same workload, scaled linearly in N to 50M rows
 
 --impl reference runs the reference's own CPU core instead (rank 0 only).
+--workload slopes times the same panel with firm-specific tenure slopes
+(firm##c.tenure) on b200fe_absorb_slopes (one GPU; its own JSON line).
 With --gpus N > 1 every rank absorbs its own replica panel (no collective in
 the data path; replicas only), launched by torch.distributed.run.
 """
@@ -61,6 +63,9 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--workload", default="akm3", choices=["akm3", "slopes"],
+                    help="akm3: the headline workload; slopes: the same panel with "
+                         "firm-specific tenure slopes (firm##c.tenure)")
     return ap.parse_args()
 
 
@@ -389,8 +394,171 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# heterogeneous slopes: the same panel with firm##c.tenure (1 GPU)
+# ---------------------------------------------------------------------------
+SLOPE_METRIC = ("demeaning time to 1e-8 tol, AKM 3-way 50M obs with firm-specific tenure "
+                "slopes (firm##c.tenure, 13 columns, one absorption call)")
+
+
+def slope_terms(panel):
+    """firm##c.tenure: slope on tenure (the panel's first regressor) per firm."""
+    return [(1, np.ascontiguousarray(panel.X[:, 0]), True)]
+
+
+def run_slopes(args):
+    import torch
+    import oracle
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    if args.impl == "reference":
+        vals, info = [], None
+        for i in range(args.warmup + args.steps):
+            p = make_panel(args.cpu_sample, seed=12345)
+            t0 = time.perf_counter()
+            r = oracle.ref_absorb_slopes(p.y, p.X, p.fes, slope_terms(p), None, tol=1e-8,
+                                         threads=threads)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                vals.append(dt * N_OBS / p.n)
+            info = (p.n, r["iterations"], dt)
+        v = statistics.median(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": SLOPE_METRIC, "value": v, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000.0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded AKM generator)",
+            "config": {"workload": "akm_3way_50M_13col_firm_tenure_slopes", "n_obs": N_OBS},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{info[0]} rows, {info[1]} iterations, {info[2]:.2f} s, "
+                                       "scaled linearly to 50M rows"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    torch.cuda.set_device(0)
+    pkg = ge.load_package()
+    panel = make_panel(args.n, seed=0)
+    sl = slope_terms(panel)
+    n, k = panel.n, panel.k
+    cols = k + 1
+    dev = torch.device("cuda", 0)
+    v = torch.empty((cols, n), dtype=torch.float64, device=dev)
+    v[0].copy_(torch.from_numpy(panel.y))
+    v[1:].copy_(torch.from_numpy(np.ascontiguousarray(panel.X.T)))
+    gids = [torch.from_numpy(f).to(dev) for f in panel.fes]
+    zt = [(d, torch.from_numpy(z).to(dev), i) for d, z, i in sl]
+    out = torch.empty_like(v)
+    absorber = pkg.Absorber(0)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    opts = pkg.make_options(tol=1e-8, profile=True)
+
+    def step():
+        return absorber.absorb_slopes_device(v, gids, panel.levels, zt, None, opts, out=out,
+                                             stream=sh)[1]
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    results = [step() for _ in range(args.steps)]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    r_last = results[-1]
+    libm = ge.load_module("_lib")
+    prof = {}
+    for ci, name in enumerate(libm.PROF_NAMES):
+        tms = sum(r.prof_ms[ci] for r in results)
+        tb = sum(r.prof_bytes[ci] for r in results)
+        nl = sum(r.prof_launches[ci] for r in results)
+        if nl:
+            prof[name] = {"ms_total": tms, "launches": int(nl), "bytes_total": tb,
+                          "gbs": (tb / (tms * 1e-3) / 1e9) if tms > 0 else None,
+                          "share": tms / (ms * args.steps)}
+    hot = max((k2 for k2 in prof if k2 != "setup"), key=lambda k2: prof[k2]["ms_total"])
+    peaks, peak_kind = measured_peaks()
+    hp = prof[hot]
+    achieved = hp["bytes_total"] / (hp["ms_total"] * 1e-3) / 1e9
+    roofline = {"kernel": hot, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_kind": peak_kind,
+                "bytes_per_launch": hp["bytes_total"] / hp["launches"],
+                "ms_per_launch": hp["ms_total"] / hp["launches"], "traffic": None}
+    e2e = None
+    if args.e2e_steps > 0:
+        y_h = torch.from_numpy(panel.y).pin_memory().numpy()
+        X_h = torch.from_numpy(np.ascontiguousarray(panel.X.T)).pin_memory().numpy().T
+        g_h = [torch.from_numpy(f).pin_memory().numpy() for f in panel.fes]
+        s_h = [(d, torch.from_numpy(z).pin_memory().numpy(), i) for d, z, i in sl]
+        yo = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        Xo = torch.empty((k, n), dtype=torch.float64).pin_memory().numpy().T
+        o_e = pkg.make_options(tol=1e-8)
+        absorber.absorb(y_h, X_h, g_h, panel.levels, None, o_e, y_out=yo, X_out=Xo, slopes=s_h)
+        times = []
+        for _ in range(args.e2e_steps):
+            t1 = time.perf_counter()
+            re = absorber.absorb(y_h, X_h, g_h, panel.levels, None, o_e, y_out=yo, X_out=Xo,
+                                 slopes=s_h)
+            times.append(time.perf_counter() - t1)
+        e2e = {"value": statistics.median(times), "unit": UNIT,
+               "h2d_bytes_per_step": int(n * cols * 8 + n * 4 * len(panel.fes) + n * 8),
+               "d2h_bytes_per_step": int(n * cols * 8), "h2d_ms": re.h2d_ms, "d2h_ms": re.d2h_ms,
+               "converged": re.converged}
+    cpu = None
+    if not args.no_cpu_baseline and oracle.ref_available():
+        p = make_panel(args.cpu_sample, seed=12345)
+        t0 = time.perf_counter()
+        rr = oracle.ref_absorb_slopes(p.y, p.X, p.fes, slope_terms(p), None, tol=1e-8,
+                                      threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": dt * N_OBS / p.n, "unit": UNIT, "cores": threads, "kind": "reference",
+               "sample": (f"reference CPU core (absorb_fixed_effects_v6 with the slope term, "
+                          f"tol 1e-8, {threads} threads) on a {p.n}-row panel of the same "
+                          f"generator: {dt:.3f} s, {rr['iterations']} iterations, scaled "
+                          f"linearly to 50M rows")}
+    ref_gpu = None
+    if not args.no_reference_gpu and oracle.REF_CUDA_SO.exists():
+        t0 = time.perf_counter()
+        rg = oracle.ref_absorb_slopes(panel.y, panel.X, panel.fes, sl, None, tol=1e-8,
+                                      threads=threads, gpu_backend="cuda",
+                                      lib_path=oracle.REF_CUDA_SO)
+        ref_gpu = {"value": time.perf_counter() - t0, "unit": UNIT,
+                   "kind": "reference CUDA backend built for sm_100a, host arrays",
+                   "iterations": rg["iterations"], "converged": rg["converged"],
+                   "gpu_status_code": rg["gpu_status_code"]}
+    print(json.dumps({
+        "metric": SLOPE_METRIC, "value": ms / 1000.0, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded AKM generator)",
+        "config": {"workload": "akm_3way_50M_13col_firm_tenure_slopes", "n_obs_generated": args.n,
+                   "n_obs_after_singleton_drop": n, "columns": cols,
+                   "fe_dims": ["worker", "firm##c.tenure", "year"], "levels": panel.levels,
+                   "tol": 1e-8,
+                   "l2_policy": f"inputs larger than L2 ({n * cols * 8 / 1e9:.1f} GB of columns per step)"},
+        "gpu_launches": int(sum(r.kernel_launches for r in results)),
+        "iterations": r_last.iterations, "converged": bool(r_last.converged),
+        "rel_residual": r_last.rel_residual, "abs_residual_rel": r_last.abs_residual_rel,
+        "precision_certified": bool(r_last.precision_certified),
+        "setup_ms": r_last.setup_ms, "solve_ms": r_last.solve_ms,
+        "roofline": roofline, "profile": prof, "clocks": clocks, "e2e": e2e,
+        "cpu_baseline": cpu, "reference_gpu": ref_gpu}))
+    absorber.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "slopes":
+        return run_slopes(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -75,6 +75,11 @@ typedef struct b200fe_options {
 #define B200FE_PROF_SETUP 6     /* FE structure build                                        */
 #define B200FE_PROF_COUPLE 7    /* dense small-dim coupling product C_fy' x_f (CG matvec)    */
 #define B200FE_PROF_CATEGORIES 8
+/* b200fe_absorb_slopes fills the same slots: PASS the per-dim chunk sums of
+ * w r and w z r (with the residual update), GATHER the image D p, FINALIZE the
+ * per-group gradient and block preconditioner, VECTOR the CG scalars and
+ * directions, RHS / FINAL the load into and store out of the row-major
+ * residual, SETUP the sorts, chunks and block inverses. */
 
 typedef struct b200fe_result {
     int status;

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <cstdlib>
 #include <limits>
+#include <memory>
 #include <type_traits>
 #include <string>
 #include <unordered_map>
@@ -2654,6 +2655,10 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     B_TRY(cudaEventCreate(&e1));
     B_TRY(cudaEventCreate(&e2));
     B_TRY(cudaEventRecord(e0, s));
+    ctx->profiling = o.profile != 0;
+    ctx->prof.clear();
+    ctx->ev_used = 0;
+    std::unique_ptr<ProfScope> setup_scope(new ProfScope(ctx, B200FE_PROF_SETUP, 0.0));
     // ---- validation
     int* flags;
     B_CHECK(get_buf(ctx, "sl_flags", 8, &flags));
@@ -2710,8 +2715,11 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     double *R, *Q;
     B_CHECK(get_buf(ctx, "sl_R", static_cast<size_t>(n) * C, &R));
     B_CHECK(get_buf(ctx, "sl_Q", static_cast<size_t>(n) * C, &Q));
-    slope_load_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(d_v, pord, n, C, R);
-    B_LAUNCHED();
+    {
+        ProfScope ps(ctx, B200FE_PROF_RHS, 16.0 * n * C + (pord ? 4.0 * n : 0.0));
+        slope_load_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(d_v, pord, n, C, R);
+        B_LAUNCHED();
+    }
     // ---- per-dim structure
     SlopeDim dims[B200FE_MAX_DIMS];
     int order[B200FE_MAX_DIMS];  // segment passes: the primary (writer) last
@@ -2838,7 +2846,24 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     B_CHECK(get_buf(ctx, "sl_pn", static_cast<size_t>(nd) * stride * C, &pn));
     const int gG = gN;
     B_CHECK(get_buf(ctx, "sl_pq", static_cast<size_t>(gG) * C, &pq));
+    setup_scope.reset();
     B_TRY(cudaEventRecord(e1, s));
+    // algorithmic bytes per launch (profile categories)
+    const double wb = w ? 8.0 : 0.0;
+    double gather_bytes = 8.0 * n * C + wb * n;
+    for (int d = 0; d < nd; ++d)
+        gather_bytes += 4.0 * n + (dims[d].has_b ? 8.0 * n : 0.0) +
+                        8.0 * dims[d].G * dims[d].nb * C;
+    auto seg_bytes = [&](int d, bool update) {
+        const SlopeDim& D = dims[d];
+        return n * (8.0 * C * (update ? 2 : 1) + (update && d == p ? 8.0 * C : 0.0) + wb +
+                    (D.has_b ? 8.0 : 0.0) + (D.perm ? 4.0 : 0.0)) +
+               D.nch * (8.0 + 8.0 * D.nb * C);
+    };
+    auto fin_bytes = [&](int d) {
+        const SlopeDim& D = dims[d];
+        return D.nch * 8.0 * D.nb * C + D.G * (4.0 + 24.0 + 8.0 * D.nb * C);
+    };
 
     // ---- iteration pieces
     const int CW = C <= 32 ? 1 : C <= 64 ? 2 : C <= 128 ? 4 : 8;
@@ -2853,6 +2878,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         a.w = w;
         a.write = update && d == p;
         const int g = grid_for(ctx, static_cast<int64_t>(dims[d].nch) * 32, T, 16);
+        ProfScope ps(ctx, B200FE_PROF_PASS, seg_bytes(d, update));
         if (CW == 1) slope_segment_kernel<1><<<g, T, 0, s>>>(a);
         else if (CW == 2) slope_segment_kernel<2><<<g, T, 0, s>>>(a);
         else if (CW == 4) slope_segment_kernel<4><<<g, T, 0, s>>>(a);
@@ -2863,6 +2889,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     auto gradient = [&](bool update, bool init) -> int {
         for (int i = 0; i < nd; ++i) B_CHECK(segment(order[i], update));
         for (int d = 0; d < nd; ++d) {
+            ProfScope ps(ctx, B200FE_PROF_FINALIZE, fin_bytes(d));
             slope_finalize_kernel<<<fin_grid[d], C * RB, 0, s>>>(
                 dims[d], C, RB, pg + static_cast<size_t>(d) * stride * C,
                 pn + static_cast<size_t>(d) * stride * C);
@@ -2882,6 +2909,9 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         b.active = active;
         b.done = done;
         b.init = init ? 1 : 0;
+        double vb = 0.0;
+        for (int d = 0; d < nd; ++d) vb += 24.0 * dims[d].G * dims[d].nb * C;
+        ProfScope ps(ctx, B200FE_PROF_VECTOR, vb);
         slope_beta_kernel<<<1, T, 0, s>>>(b);
         B_LAUNCHED();
         for (int d = 0; d < nd; ++d) {
@@ -2909,17 +2939,26 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     while (!hd && it < max_it) {
         const int steps = std::min(ci, max_it - it);
         for (int k = 0; k < steps; ++k) {
-            slope_gather_kernel<<<gG, C * RB, 0, s>>>(ga);
-            B_LAUNCHED();
-            slope_alpha_kernel<<<1, T, 0, s>>>(pq, gG, C, gamma, active, alpha);
-            B_LAUNCHED();
+            {
+                ProfScope ps(ctx, B200FE_PROF_GATHER, gather_bytes);
+                slope_gather_kernel<<<gG, C * RB, 0, s>>>(ga);
+                B_LAUNCHED();
+            }
+            {
+                ProfScope ps(ctx, B200FE_PROF_VECTOR, 0.0);
+                slope_alpha_kernel<<<1, T, 0, s>>>(pq, gG, C, gamma, active, alpha);
+                B_LAUNCHED();
+            }
             B_CHECK(gradient(true, false));
         }
         it += steps;
         B_CHECK(sync_read_int(ctx, done, 1, &hd));
     }
-    slope_store_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(R, pord, n, C, d_out);
-    B_LAUNCHED();
+    {
+        ProfScope ps(ctx, B200FE_PROF_FINAL, 16.0 * n * C + (pord ? 4.0 * n : 0.0));
+        slope_store_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(R, pord, n, C, d_out);
+        B_LAUNCHED();
+    }
     std::vector<double> hs(C);
     B_TRY(cudaMemcpyAsync(hs.data(), gamma, sizeof(double) * C, cudaMemcpyDeviceToHost, s));
     std::vector<double> hnu(C);
@@ -2931,6 +2970,16 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
+    if (ctx->profiling) {
+        for (const auto& pr : ctx->prof) {
+            if (pr.cat < 0 || pr.cat >= B200FE_PROF_CATEGORIES) continue;
+            res->prof_ms[pr.cat] += elapsed_ms(pr.a, pr.b);
+            res->prof_bytes[pr.cat] += pr.bytes;
+            res->prof_launches[pr.cat] += 1;
+        }
+        ctx->prof.clear();
+        ctx->profiling = false;
+    }
     // ---- result fields
     const double opn = std::sqrt(std::max(0.0, op_norm2));
     double abs_res = 0.0, abs_rel = 0.0, rel = 0.0;
