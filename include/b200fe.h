@@ -199,6 +199,40 @@ int b200fe_absorb_slopes_device(b200fe_context* ctx, const double* d_v, int64_t 
                                 const double* d_weights, const b200fe_options* opts,
                                 double* d_out, b200fe_result* res, void* stream);
 
+/* Group/individual structure (host arrays), the reference's
+ * GroupIndividualStructure (include/fe_absorption.hpp:13-21): every row of the
+ * data is a group; group g holds the individuals
+ * group_individual[group_ptr[g] .. group_ptr[g+1]), individual i appears in the
+ * groups individual_group[individual_ptr[i] .. individual_ptr[i+1]) (both CSR
+ * arrays list the same num_edges edges), and the basis column of individual i
+ * is group_scale[g] at every group g that holds i (1 for sum aggregation,
+ * 1 / group size for mean aggregation). */
+typedef struct b200fe_group_individual {
+    int32_t num_individuals;
+    int64_t num_edges;
+    const int32_t* group_ptr;         /* n + 1            */
+    const int32_t* group_individual;  /* num_edges        */
+    const int32_t* individual_ptr;    /* num_individuals + 1 */
+    const int32_t* individual_group;  /* num_edges        */
+    const double* group_scale;        /* n                */
+} b200fe_group_individual;
+
+/* Absorption of the standard FE dims (group_ids, num_dims >= 0) together with
+ * the individual FEs of a group/individual design, on host arrays.  The CSR
+ * arrays are range-checked on the host before any device work
+ * (B200FE_INVALID_ARG when inconsistent).  Same solver as b200fe_absorb_slopes
+ * with the individual dimension as one more block (diagonal preconditioner
+ * sum over its groups of w scale^2); primary_dim is -1 when num_dims == 0.
+ * Replaces hdfe::detail::absorb_fixed_effects_group_individual_cuda
+ * (include/fe_absorption_cuda.hpp:136-145, src/fe_absorption_cuda.cu:4740). */
+int b200fe_absorb_group_individual(b200fe_context* ctx, const double* y, const double* X,
+                                   int64_t n, int k, int num_dims,
+                                   const int32_t* const* group_ids,
+                                   const int32_t* num_groups,
+                                   const b200fe_group_individual* gi,
+                                   const double* weights, const b200fe_options* opts,
+                                   double* y_out, double* X_out, b200fe_result* res);
+
 /* In-place demean of host arrays, the raw interface of the reference's
  * block-PCG absorber: Y (n) and X (n x k column-major) are overwritten with
  * their within transforms; iters_out receives the PCG iteration count.

@@ -145,6 +145,11 @@ def rlib(path: Path = REF_SO) -> ctypes.CDLL:
                                                P(XrefOptions), _vp, _vp, P(_int), P(_dbl),
                                                ctypes.c_char_p, _int]
             lib.xref_absorb_slopes.restype = _int
+        if hasattr(lib, "xref_absorb_gi"):
+            lib.xref_absorb_gi.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, _vp, _vp, _vp,
+                                           _vp, _vp, _int, _i64, P(XrefOptions), _vp, _vp,
+                                           P(_int), P(_dbl), ctypes.c_char_p, _int]
+            lib.xref_absorb_gi.restype = _int
         if hasattr(lib, "xref_recover_fe"):
             lib.xref_recover_fe.argtypes = [_vp, _i64, _vp, _int, _vp, P(XrefOptions), _dbl, _vp,
                                             P(_int), P(_dbl), ctypes.c_char_p, _int]
@@ -229,6 +234,33 @@ def ref_absorb_slopes(y, X, fes, slopes, weights=None, *, tol=1e-8,
         len(fes), None if w is None else w.ctypes.data, zf.ctypes.data, kind.ctypes.data,
         ctypes.byref(o), Vo[:, 0].ctypes.data, Vo[:, 1:].ctypes.data if C > 1 else None, info,
         dinfo, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return {"V": Vo, "iterations": info[0], "converged": bool(info[1]),
+            "precision_certified": bool(info[2]), "gpu_status_code": info[3],
+            "abs_residual": dinfo[0], "abs_residual_rel": dinfo[1]}
+
+
+def ref_absorb_gi(y, X, fes, gi, weights=None, *, tol=1e-8, tolerance_mode="reghdfe-comparable",
+                  method="auto", threads=1, max_iter=0, gpu_backend="default", lib_path=REF_SO):
+    """Reference absorb_fixed_effects_group_individual.  ``gi`` has the fields of
+    the reference's GroupIndividualStructure (group_ptr, group_individual,
+    individual_ptr, individual_group, group_scale, num_individuals)."""
+    V, g, _, w = _pack(y, X, fes, [1] * len(fes), weights)
+    n, C = V.shape
+    a = [np.ascontiguousarray(x, dtype=np.int32) for x in
+         (gi.group_ptr, gi.group_individual, gi.individual_ptr, gi.individual_group)]
+    sc = np.ascontiguousarray(gi.group_scale, dtype=np.float64)
+    Vo = np.empty_like(V, order="F")
+    info = (_int * 8)()
+    dinfo = (_dbl * 2)()
+    err = ctypes.create_string_buffer(512)
+    o = _xopts(tol, tolerance_mode, method, threads, max_iter, gpu_backend=gpu_backend)
+    rc = rlib(lib_path).xref_absorb_gi(
+        V[:, 0].ctypes.data, V[:, 1:].ctypes.data if C > 1 else None, n, C - 1, g.ctypes.data,
+        len(fes), None if w is None else w.ctypes.data, *[x.ctypes.data for x in a],
+        sc.ctypes.data, int(gi.num_individuals), int(a[1].shape[0]), ctypes.byref(o),
+        Vo[:, 0].ctypes.data, Vo[:, 1:].ctypes.data if C > 1 else None, info, dinfo, err, 512)
     if rc != 0:
         raise RuntimeError(err.value.decode())
     return {"V": Vo, "iterations": info[0], "converged": bool(info[1]),

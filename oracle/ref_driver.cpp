@@ -9,6 +9,7 @@
 // Entry points mirror the reference's public calls:
 //   xref_absorb       -> hdfe::detail::absorb_fixed_effects_v6  (src/fe_absorption.cpp:8750)
 //   xref_absorb_slopes-> the same, with HeterogeneousSlopeTerm slopes (include/fe_absorption.hpp:49-53)
+//   xref_absorb_gi    -> hdfe::detail::absorb_fixed_effects_group_individual (include/fe_absorption.hpp:103-109)
 //   xref_partial_out  -> hdfe::v11::HdfeRegressorV11::partial_out (src/hdfe_regressor_v11.cpp:10275)
 //   xref_fit          -> hdfe::v11::HdfeRegressorV11::fit         (src/hdfe_regressor_v11.cpp:7522)
 //   xref_akm_kss      -> hdfe::akm::akm_kss_decompose              (include/hdfe/akm_kss.hpp:227-233)
@@ -172,6 +173,56 @@ int xref_absorb_slopes(const double* y, const double* X, int64_t n, int k,
         auto guard = backend_guard(o);
         hdfe::detail::AbsorptionResult r = hdfe::detail::absorb_fixed_effects_v6(
             ym, Xm, fes, w ? &wv : nullptr, opts, opts.absorption_method, slopes);
+        std::memcpy(y_out, r.y_tilde.data(), sizeof(double) * static_cast<std::size_t>(n));
+        if (k > 0) {
+            std::memcpy(X_out, r.X_tilde.data(),
+                        sizeof(double) * static_cast<std::size_t>(n) * k);
+        }
+        info[0] = r.iterations;
+        info[1] = r.converged ? 1 : 0;
+        info[2] = r.precision_certified ? 1 : 0;
+        info[3] = r.gpu_status_code;
+        dinfo[0] = r.abs_residual;
+        dinfo[1] = r.abs_residual_rel;
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
+// absorb_fixed_effects_group_individual: rows are groups; the structure's
+// CSR arrays as in GroupIndividualStructure (include/fe_absorption.hpp:13-21).
+// Same outputs as xref_absorb.
+int xref_absorb_gi(const double* y, const double* X, int64_t n, int k, const int32_t* fe_flat,
+                   int dims, const double* w, const int32_t* group_ptr,
+                   const int32_t* group_individual, const int32_t* individual_ptr,
+                   const int32_t* individual_group, const double* group_scale,
+                   int num_individuals, int64_t num_edges, const XrefOptions* o, double* y_out,
+                   double* X_out, int* info, double* dinfo, char* err, int err_len) {
+    try {
+        const VectorXd yv = Map<const VectorXd>(y, n);
+        const MatrixXd Xm = Map<const MatrixXd>(X, n, k);
+        std::vector<VectorXi> fes = to_fes(fe_flat, n, dims);
+        VectorXd wv;
+        if (w) {
+            wv = Map<const VectorXd>(w, n);
+        }
+        hdfe::detail::GroupIndividualStructure gi;
+        gi.num_groups = static_cast<int>(n);
+        gi.num_individuals = num_individuals;
+        gi.group_ptr.assign(group_ptr, group_ptr + n + 1);
+        gi.group_individual.assign(group_individual, group_individual + num_edges);
+        gi.individual_ptr.assign(individual_ptr, individual_ptr + num_individuals + 1);
+        gi.individual_group.assign(individual_group, individual_group + num_edges);
+        gi.group_scale.assign(group_scale, group_scale + n);
+        hdfe::HdfeOptions opts = to_options(o);
+        auto guard = backend_guard(o);
+        hdfe::detail::AbsorptionResult r = hdfe::detail::absorb_fixed_effects_group_individual(
+            yv, Xm, fes, gi, w ? &wv : nullptr, opts, opts.absorption_method);
         std::memcpy(y_out, r.y_tilde.data(), sizeof(double) * static_cast<std::size_t>(n));
         if (k > 0) {
             std::memcpy(X_out, r.X_tilde.data(),

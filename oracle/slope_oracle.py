@@ -11,6 +11,10 @@ compute_slope_coefficients_kernel, src/fe_absorption_cuda.cu:586-650):
 * a group keeps its intercept alone when its 2x2 block [W Z; Z ZZ] has
   det <= 1e-12 max(1, W ZZ), and drops its slope column when
   ZZ <= 1e-12 max(1, ZZ) without intercept (the reference's rule);
+* group/individual designs (absorb_fixed_effects_group_individual,
+  src/fe_absorption.cpp:9741; GroupIndividualStructure,
+  include/fe_absorption.hpp:13-21): rows are groups and the basis column of
+  individual i is group_scale[g] at every group g that holds i;
 * the within transform is v - D a with a the minimum-norm weighted
   least-squares solution (dense, so for small cases only).
 
@@ -66,4 +70,21 @@ def slope_projection(V, fes, slopes, weights=None):
     A = D * sw[:, None]
     B = V * sw[:, None]
     a, *_ = np.linalg.lstsq(A, B, rcond=None)
+    return V - D @ a
+
+
+def gi_projection(V, fes, gi, weights=None):
+    """Within transform on the standard FEs plus the individual FEs of a
+    group/individual structure (exact, min-norm LS)."""
+    V = np.asarray(V, dtype=np.float64)
+    n = V.shape[0]
+    Ds = slope_basis(fes, [], weights, n)
+    Di = np.zeros((n, int(gi.num_individuals)))
+    gp = np.asarray(gi.group_ptr)
+    for g in range(n):
+        for e in range(gp[g], gp[g + 1]):
+            Di[g, gi.group_individual[e]] = gi.group_scale[g]
+    D = np.hstack([Ds, Di[:, np.any(Di != 0, axis=0)]])
+    sw = np.ones(n) if weights is None else np.sqrt(np.asarray(weights, dtype=np.float64))
+    a, *_ = np.linalg.lstsq(D * sw[:, None], V * sw[:, None], rcond=None)
     return V - D @ a

@@ -20,6 +20,10 @@ hold the reference's absorb_fixed_effects_v6 with heterogeneous slopes at
 tol 1e-13 (reghdfe-comparable; strict-residual is refused for slopes): the within transform on all rows (on a row subset
 beyond 5000 rows) and its column norms, with the input digests.
 
+Group/individual cases (``python tests/golden/make_golden.py gi``, gi_<case>.npz)
+hold the reference's absorb_fixed_effects_group_individual at tol 1e-13 on
+structures built from seeded group x individual edge lists.
+
 KSS cases (kss_<case>.npz) hold the inputs of an AKM leave-out decomposition
 and the reference's hdfe::akm::akm_kss_decompose results on them:
   * kss_felsdvsimul: the reference's own example data (data/felsdvsimul.dta,
@@ -280,7 +284,77 @@ def make_slopes(name: str) -> dict:
     return meta
 
 
+# ---------------------------------------------------------------------------
+# Group/individual FEs (gi_<case>.npz): absorb_fixed_effects_group_individual
+# on structures built from seeded edge lists (patent x inventor style: groups
+# of 1-4 individuals), standard FEs on the group rows.
+# ---------------------------------------------------------------------------
+def gi_edges(n_groups, n_individuals, seed, max_size=4):
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(1, max_size + 1, n_groups)
+    eg = np.repeat(np.arange(n_groups), sizes)
+    # popular individuals: Zipf-like draws, no repeat inside a group
+    p = 1.0 / np.arange(1, n_individuals + 1) ** 0.8
+    p /= p.sum()
+    ei = np.concatenate([rng.choice(n_individuals, s, replace=False, p=p) for s in sizes])
+    return rng, eg, ei
+
+
+def gi_case(n_groups, n_individuals, seed, aggregation, n_fes, weighted):
+    rng, eg, ei = gi_edges(n_groups, n_individuals, seed)
+    gi, _, _ = ge.load_package().build_group_individual(eg * 7 + 3, ei + 1000, aggregation)
+    n = gi.num_groups
+    fes = []
+    if n_fes >= 1:
+        fes.append(rng.integers(0, 15, n).astype(np.int32))
+    if n_fes >= 2:
+        fes.append(rng.integers(0, max(2, n // 20), n).astype(np.int32))
+    X = rng.standard_normal((n, 3))
+    y = X @ np.array([0.7, -0.2, 0.1]) + rng.standard_normal(n)
+    w = rng.uniform(0.5, 2.0, n) if weighted else None
+    return dict(y=y, X=X, fes=fes, gi=gi, weights=w, edges=(eg, ei), aggregation=aggregation)
+
+
+GI_CASES = {
+    "mean1500": lambda: gi_case(1500, 400, 20260721, "mean", 1, False),
+    "sum1500w": lambda: gi_case(1500, 400, 20260722, "sum", 1, True),
+    "nofe1200": lambda: gi_case(1200, 300, 20260723, "mean", 0, False),
+    "mean20k": lambda: gi_case(20_000, 5_000, 20260724, "mean", 2, False),
+}
+
+
+def gi_digest(c) -> str:
+    gi = c["gi"]
+    arrs = [c["y"], np.asarray(c["X"], dtype=np.float64),
+            *[np.asarray(f, dtype=np.int32) for f in c["fes"]],
+            np.asarray(gi.group_ptr, dtype=np.int32), np.asarray(gi.group_individual, dtype=np.int32),
+            np.asarray(gi.individual_ptr, dtype=np.int32),
+            np.asarray(gi.individual_group, dtype=np.int32), np.asarray(gi.group_scale)]
+    if c["weights"] is not None:
+        arrs.append(c["weights"])
+    return digest(*arrs)
+
+
+def make_gi(name: str) -> dict:
+    c = GI_CASES[name]()
+    ref = oracle.ref_absorb_gi(c["y"], c["X"], c["fes"], c["gi"], c["weights"], tol=1e-13,
+                               threads=1, max_iter=1_000_000)
+    n = c["y"].shape[0]
+    rows = subset_rows(n) if n > 5000 else np.arange(n, dtype=np.int64)
+    meta = {"case": name, "n": n, "num_individuals": int(c["gi"].num_individuals),
+            "num_edges": int(len(c["gi"].group_individual)), "iterations": ref["iterations"],
+            "converged": ref["converged"], "abs_residual_rel": ref["abs_residual_rel"],
+            "input_digest": gi_digest(c)}
+    np.savez_compressed(OUT / f"gi_{name}.npz", rows=rows, ref_rows=ref["V"][rows],
+                        ref_colnorm=np.linalg.norm(ref["V"], axis=0), meta=np.array(json.dumps(meta)))
+    return meta
+
+
 if __name__ == "__main__":
+    if sys.argv[1:2] == ["gi"]:
+        for nm in sys.argv[2:] or list(GI_CASES):
+            print(nm, json.dumps(make_gi(nm)))
+        sys.exit(0)
     if sys.argv[1:2] == ["slopes"]:
         for nm in sys.argv[2:] or list(SLOPE_CASES):
             print(nm, json.dumps(make_slopes(nm)))

@@ -10,9 +10,11 @@ from .absorber import (  # noqa: F401
     AbsorptionResult,
     FeComponentStats,
     FeRecoveryResult,
+    GroupIndividualStructure,
     HeterogeneousSlopeTerm,
     OlsResult,
     absorb_fixed_effects,
+    build_group_individual,
     cuda_backend_available,
     demean_raw,
     dense_ids,

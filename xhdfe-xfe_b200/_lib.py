@@ -41,6 +41,7 @@ EXPORTED_SYMBOLS = (
     "b200fe_absorb_fe",
     "b200fe_absorb_slopes",
     "b200fe_absorb_slopes_device",
+    "b200fe_absorb_group_individual",
     "b200fe_demean_raw",
     "b200fe_fe_recovery_max_delta",
     "b200fe_demean_sorted_noalloc",
@@ -58,6 +59,18 @@ EXPORTED_SYMBOLS = (
     "b200fe_kss_solve",
     "b200fe_stable_sort_u64",
 )
+
+
+class GroupIndividual(ctypes.Structure):
+    _fields_ = [
+        ("num_individuals", ctypes.c_int32),
+        ("num_edges", ctypes.c_int64),
+        ("group_ptr", ctypes.c_void_p),
+        ("group_individual", ctypes.c_void_p),
+        ("individual_ptr", ctypes.c_void_p),
+        ("individual_group", ctypes.c_void_p),
+        ("group_scale", ctypes.c_void_p),
+    ]
 
 
 class Options(ctypes.Structure):
@@ -167,6 +180,10 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
                                                 ctypes.POINTER(Options), vp,
                                                 ctypes.POINTER(Result), vp]
     lib.b200fe_absorb_slopes_device.restype = c_int
+    lib.b200fe_absorb_group_individual.argtypes = [
+        vp, vp, vp, i64, c_int, c_int, pp, vp, ctypes.POINTER(GroupIndividual), vp,
+        ctypes.POINTER(Options), vp, vp, ctypes.POINTER(Result)]
+    lib.b200fe_absorb_group_individual.restype = c_int
     lib.b200fe_dense_ids_device.argtypes = [vp, vp, i64, vp, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.POINTER(ctypes.c_int32)]
     lib.b200fe_dense_ids_device.restype = c_int

@@ -7,6 +7,11 @@ Reference counterparts (reisportela/xhdfe-xfe):
 * ``HeterogeneousSlopeTerm``  -> the struct of the same name (include/fe_absorption.hpp:49-53);
                                  ``Absorber.absorb(slopes=...)`` is the is_slope path of
                                  absorb_fixed_effects_cuda (src/fe_absorption_cuda.cu:2316)
+* ``Absorber.absorb_group_individual`` -> absorb_fixed_effects_group_individual_cuda
+                                 (include/fe_absorption_cuda.hpp:136-145);
+                                 ``GroupIndividualStructure`` / ``build_group_individual``
+                                 -> the reference's structure and its builder
+                                 (src/hdfe_regressor_v11.cpp:5780-5920)
 * ``absorb_fixed_effects``    -> hdfe::detail::absorb_fixed_effects_v6 with the
                                  CUDA backend (src/fe_absorption.cpp:8750, GPU
                                  dispatch :9203-9237): raw ids are ranked densely
@@ -48,6 +53,58 @@ class HeterogeneousSlopeTerm:
     fe_index: int
     values: np.ndarray
     include_intercept: bool = False
+
+
+@dataclass
+class GroupIndividualStructure:
+    """The reference's GroupIndividualStructure (include/fe_absorption.hpp:13-21):
+    rows of the data are groups; CSR lists of the individuals of every group
+    and of the groups of every individual; group_scale per group (1 for sum
+    aggregation, 1 / group size for mean)."""
+    num_groups: int
+    num_individuals: int
+    group_ptr: np.ndarray
+    group_individual: np.ndarray
+    individual_ptr: np.ndarray
+    individual_group: np.ndarray
+    group_scale: np.ndarray
+
+
+def build_group_individual(group_ids, individual_ids, aggregation: str = "mean"
+                           ) -> tuple[GroupIndividualStructure, np.ndarray, np.ndarray]:
+    """Build the structure from edge-level data, one (group, individual) pair
+    per edge, as the reference's builder does (src/hdfe_regressor_v11.cpp:
+    5780-5920): groups and individuals ranked densely by value, edges sorted by
+    (group, individual), a repeated pair is an error, mean aggregation scales
+    a group by 1 / its number of individuals.  Returns the structure and the
+    group and individual values in dense order."""
+    g_raw = np.asarray(group_ids)
+    i_raw = np.asarray(individual_ids)
+    if g_raw.shape != i_raw.shape or g_raw.ndim != 1 or g_raw.size == 0:
+        raise ValueError("group_ids and individual_ids must be non-empty vectors of one length")
+    g_vals, g = np.unique(g_raw, return_inverse=True)
+    i_vals, ind = np.unique(i_raw, return_inverse=True)
+    G, I = g_vals.size, i_vals.size
+    key = g.astype(np.int64) * I + ind
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    if np.any(ks[1:] == ks[:-1]):
+        raise ValueError("group_ids and individual_ids do not uniquely identify the observations")
+    ge, ie = (ks // I).astype(np.int32), (ks % I).astype(np.int32)
+    group_ptr = np.zeros(G + 1, dtype=np.int32)
+    np.cumsum(np.bincount(ge, minlength=G), out=group_ptr[1:])
+    individual_ptr = np.zeros(I + 1, dtype=np.int32)
+    np.cumsum(np.bincount(ie, minlength=I), out=individual_ptr[1:])
+    by_ind = np.argsort(ie, kind="stable")  # groups ascending within an individual
+    if aggregation == "mean":
+        scale = 1.0 / np.diff(group_ptr).astype(np.float64)
+    elif aggregation == "sum":
+        scale = np.ones(G)
+    else:
+        raise ValueError("aggregation must be 'mean' or 'sum'")
+    gi = GroupIndividualStructure(G, I, group_ptr, ie.copy(), individual_ptr,
+                                  ge[by_ind].copy(), scale)
+    return gi, g_vals, i_vals
 
 
 def _slope_table(slopes, num_dims: int, n: int):
@@ -274,6 +331,44 @@ class Absorber:
         if rc not in (_lib.OK, _lib.NOT_CONVERGED):
             raise self._err(rc)
         return out, r
+
+    def absorb_group_individual(self, y, X, group_ids, num_groups, gi, weights=None,
+                                options=None) -> AbsorptionResult:
+        """Absorb the standard FE dims (dense ids; may be empty) and the
+        individual FEs of ``gi`` (a GroupIndividualStructure; rows = groups),
+        absorb_fixed_effects_group_individual_cuda."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        n = y.shape[0]
+        X = np.zeros((n, 0)) if X is None else np.asarray(X, dtype=np.float64)
+        if X.ndim == 1:
+            X = X[:, None]
+        X = np.asfortranarray(X)
+        k = X.shape[1]
+        if X.shape[0] != n or int(gi.num_groups) != n:
+            raise ValueError("y, X and the group/individual structure must have one row per group")
+        gids = [np.ascontiguousarray(g, dtype=np.int32) for g in group_ids]
+        G = np.ascontiguousarray(num_groups, dtype=np.int32)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in
+                (gi.group_ptr, gi.group_individual, gi.individual_ptr, gi.individual_group)]
+        sc = np.ascontiguousarray(gi.group_scale, dtype=np.float64)
+        _check_finite(sc, "group_scale")
+        st = _lib.GroupIndividual(int(gi.num_individuals), int(arrs[1].shape[0]),
+                                  *[a.ctypes.data for a in arrs], sc.ctypes.data)
+        y_out = np.empty_like(y)
+        X_out = np.empty((n, k), dtype=np.float64, order="F")
+        o = options or make_options()
+        r = _lib.Result()
+        rc = self.lib.b200fe_absorb_group_individual(
+            self.handle, y.ctypes.data, X.ctypes.data if k else None, n, k, len(gids),
+            _ptr_array([g.ctypes.data for g in gids]), G.ctypes.data, ctypes.byref(st),
+            None if w is None else w.ctypes.data, ctypes.byref(o), y_out.ctypes.data,
+            X_out.ctypes.data if k else None, ctypes.byref(r))
+        if rc not in (_lib.OK, _lib.NOT_CONVERGED):
+            raise self._err(rc)
+        res = _to_result(r, y_out, X_out, G)
+        res.fe_levels = [int(x) for x in G] + [int(gi.num_individuals)]
+        return res
 
     def absorb_slopes_device(self, v, group_ids, num_groups, slopes, weights=None,
                              options=None, out=None, stream=None):

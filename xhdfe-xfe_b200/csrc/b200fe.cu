@@ -2644,10 +2644,22 @@ namespace {
 // is driven two orders below the requested tolerance.
 constexpr double kSlopeTolFactor = 1e-2;
 
+// Device copy of a group/individual structure (rows = groups, original order).
+struct GiDev {
+    int32_t I;
+    int64_t E;
+    const int32_t* gptr;   // [n + 1]
+    const int32_t* gind;   // [E]
+    const int32_t* iptr;   // [I + 1]
+    const int32_t* igrp;   // [E]
+    const double* scale;   // [n]
+};
+
 int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C, int nd,
                        const int32_t* const* d_gids, const int32_t* G,
                        const double* const* d_z, const unsigned char* icpt, const double* d_w,
-                       const b200fe_options& o, double* d_out, b200fe_result* res) {
+                       const GiDev* gi, const b200fe_options& o, double* d_out,
+                       b200fe_result* res) {
     const cudaStream_t s = ctx->stream;
     const int T = kSlopeThreads;
     cudaEvent_t e0, e1, e2;
@@ -2663,9 +2675,13 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     int* flags;
     B_CHECK(get_buf(ctx, "sl_flags", 8, &flags));
     B_TRY(cudaMemsetAsync(flags, 0, 8 * sizeof(int), s));
-    int p = 0;
+    int p = -1;  // primary: the FE dimension with the most groups (none: -1)
     for (int d = 0; d < nd; ++d)
-        if (G[d] > G[p]) p = d;
+        if (p < 0 || G[d] > G[p]) p = d;
+    if (gi) {
+        finite_values_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(gi->scale, n, flags);
+        B_LAUNCHED();
+    }
     for (int d = 0; d < nd; ++d) {
         validate_ids_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(d_gids[d], n, G[d], d == p, flags);
         B_LAUNCHED();
@@ -2689,7 +2705,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         return B200FE_INVALID_ARG;
     }
     if (hf[3]) {
-        ctx->err = "slope values must be finite";
+        ctx->err = gi ? "slope values and group scales must be finite" : "slope values must be finite";
         return B200FE_INVALID_ARG;
     }
     // ---- observations in primary order
@@ -2697,11 +2713,11 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     B_CHECK(get_buf(ctx, "sl_iota", n, &iota));
     iota_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(iota, n);
     B_LAUNCHED();
-    if (hf[1]) {
+    if (p >= 0 && hf[1]) {
         B_CHECK(get_buf(ctx, "sl_pord", n, &pord));
         B_CHECK(get_buf(ctx, "sl_gp", n, &gp));
         B_CHECK(cub_sort_pairs(ctx, d_gids[p], gp, iota, pord, n, G[p]));
-    } else {
+    } else if (p >= 0) {
         gp = const_cast<int32_t*>(d_gids[p]);
     }
     const double* w = d_w;
@@ -2721,72 +2737,101 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         B_LAUNCHED();
     }
     // ---- per-dim structure
-    SlopeDim dims[B200FE_MAX_DIMS];
-    int order[B200FE_MAX_DIMS];  // segment passes: the primary (writer) last
+    const int ndt = nd + (gi ? 1 : 0);  // the individual dimension is dims[nd]
+    SlopeDim dims[kSlopeMaxDims];
+    int order[kSlopeMaxDims];  // segment passes: the primary (the writer) last
     int no = 0;
-    for (int d = 0; d < nd; ++d)
+    for (int d = 0; d < ndt; ++d)
         if (d != p) order[no++] = d;
-    order[no++] = p;
+    if (p >= 0) order[no++] = p;
     double op_norm2 = 0.0;
-    int present[B200FE_MAX_DIMS] = {0};
-    int fin_grid[B200FE_MAX_DIMS] = {0};
+    int present[kSlopeMaxDims] = {0};
+    int fin_grid[kSlopeMaxDims] = {0};
     const int RB = T / C;
-    for (int d = 0; d < nd; ++d) {
+    int32_t* inv_pord = nullptr;
+    if (gi && pord) {
+        B_CHECK(get_buf(ctx, "sl_invp", n, &inv_pord));
+        inverse_perm_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(pord, n, inv_pord);
+        B_LAUNCHED();
+    }
+    for (int d = 0; d < ndt; ++d) {
         const std::string sx = std::to_string(d);
+        const int32_t Gd = d < nd ? G[d] : gi->I;
         SlopeDim& D = dims[d];
         D = SlopeDim{};
-        D.G = G[d];
-        D.has_b = d_z[d] ? 1 : 0;
-        D.has_a = d_z[d] ? (icpt && icpt[d] ? 1 : 0) : 1;
-        D.nb = D.has_a + D.has_b;
+        D.G = Gd;
         int32_t *sorted = gp, *off, *nch, *grp_ch;
-        if (d == p) {
-            D.ids = gp;
-        } else {
-            int32_t* ids = const_cast<int32_t*>(d_gids[d]);
-            if (pord) {
-                B_CHECK(get_buf(ctx, "sl_ids" + sx, n, &ids));
-                gather_kernel<int32_t><<<grid_for(ctx, n, T), T, 0, s>>>(d_gids[d], pord, n, ids);
-                B_LAUNCHED();
-            }
-            D.ids = ids;
+        if (d == nd) {
+            // individuals: positions are the edges in individual order, each
+            // mapped to its row in primary order; multiplier the group scale
+            D.has_a = 0;
+            D.has_b = 1;
+            D.nb = 1;
             int32_t* perm;
-            B_CHECK(get_buf(ctx, "sl_perm" + sx, n, &perm));
-            B_CHECK(get_buf(ctx, "sl_sorted", n, &sorted));
-            B_CHECK(cub_sort_pairs(ctx, ids, sorted, iota, perm, n, G[d]));
+            B_CHECK(get_buf(ctx, "sl_perm" + sx, gi->E, &perm));
+            map_rows_kernel<<<grid_for(ctx, gi->E, T), T, 0, s>>>(gi->igrp, gi->E, inv_pord, perm);
+            B_LAUNCHED();
             D.perm = perm;
-        }
-        if (d_z[d]) {
-            double* z = const_cast<double*>(d_z[d]);
+            double* z = const_cast<double*>(gi->scale);
             if (pord) {
                 B_CHECK(get_buf(ctx, "sl_z" + sx, n, &z));
-                gather_kernel<double><<<grid_for(ctx, n, T), T, 0, s>>>(d_z[d], pord, n, z);
+                gather_kernel<double><<<grid_for(ctx, n, T), T, 0, s>>>(gi->scale, pord, n, z);
                 B_LAUNCHED();
             }
             D.z = z;
+            off = const_cast<int32_t*>(gi->iptr);
+        } else {
+            D.has_b = d_z[d] ? 1 : 0;
+            D.has_a = d_z[d] ? (icpt && icpt[d] ? 1 : 0) : 1;
+            D.nb = D.has_a + D.has_b;
+            if (d == p) {
+                D.ids = gp;
+            } else {
+                int32_t* ids = const_cast<int32_t*>(d_gids[d]);
+                if (pord) {
+                    B_CHECK(get_buf(ctx, "sl_ids" + sx, n, &ids));
+                    gather_kernel<int32_t><<<grid_for(ctx, n, T), T, 0, s>>>(d_gids[d], pord, n, ids);
+                    B_LAUNCHED();
+                }
+                D.ids = ids;
+                int32_t* perm;
+                B_CHECK(get_buf(ctx, "sl_perm" + sx, n, &perm));
+                B_CHECK(get_buf(ctx, "sl_sorted", n, &sorted));
+                B_CHECK(cub_sort_pairs(ctx, ids, sorted, iota, perm, n, G[d]));
+                D.perm = perm;
+            }
+            if (d_z[d]) {
+                double* z = const_cast<double*>(d_z[d]);
+                if (pord) {
+                    B_CHECK(get_buf(ctx, "sl_z" + sx, n, &z));
+                    gather_kernel<double><<<grid_for(ctx, n, T), T, 0, s>>>(d_z[d], pord, n, z);
+                    B_LAUNCHED();
+                }
+                D.z = z;
+            }
+            B_CHECK(get_buf(ctx, "sl_off" + sx, static_cast<size_t>(G[d]) + 1, &off));
+            segment_offsets_kernel<<<grid_for(ctx, n + 1, T), T, 0, s>>>(sorted, n, G[d], off);
+            B_LAUNCHED();
         }
-        B_CHECK(get_buf(ctx, "sl_off" + sx, static_cast<size_t>(G[d]) + 1, &off));
-        segment_offsets_kernel<<<grid_for(ctx, n + 1, T), T, 0, s>>>(sorted, n, G[d], off);
+        B_CHECK(get_buf(ctx, "sl_nch", static_cast<size_t>(Gd) + 1, &nch));
+        B_CHECK(get_buf(ctx, "sl_grpch" + sx, static_cast<size_t>(Gd) + 1, &grp_ch));
+        slope_chunk_count_kernel<<<grid_for(ctx, Gd + 1, T), T, 0, s>>>(off, Gd, nch);
         B_LAUNCHED();
-        B_CHECK(get_buf(ctx, "sl_nch", static_cast<size_t>(G[d]) + 1, &nch));
-        B_CHECK(get_buf(ctx, "sl_grpch" + sx, static_cast<size_t>(G[d]) + 1, &grp_ch));
-        slope_chunk_count_kernel<<<grid_for(ctx, G[d] + 1, T), T, 0, s>>>(off, G[d], nch);
-        B_LAUNCHED();
-        B_CHECK(cub_exclusive_sum(ctx, nch, grp_ch, static_cast<int64_t>(G[d]) + 1));
+        B_CHECK(cub_exclusive_sum(ctx, nch, grp_ch, static_cast<int64_t>(Gd) + 1));
         int* cnt;
         B_CHECK(get_buf(ctx, "sl_cnt", 1, &cnt));
         B_TRY(cudaMemsetAsync(cnt, 0, sizeof(int), s));
-        count_nonempty_kernel<<<grid_for(ctx, G[d], T), T, 0, s>>>(off, G[d], cnt);
+        count_nonempty_kernel<<<grid_for(ctx, Gd, T), T, 0, s>>>(off, Gd, cnt);
         B_LAUNCHED();
         int hc[2];
-        B_CHECK(sync_read_int(ctx, grp_ch + G[d], 1, &hc[0]));
+        B_CHECK(sync_read_int(ctx, grp_ch + Gd, 1, &hc[0]));
         B_CHECK(sync_read_int(ctx, cnt, 1, &hc[1]));
         D.nch = hc[0];
         present[d] = hc[1];
         int32_t *cb, *ce;
         B_CHECK(get_buf(ctx, "sl_chb" + sx, D.nch, &cb));
         B_CHECK(get_buf(ctx, "sl_che" + sx, D.nch, &ce));
-        slope_chunk_fill_kernel<<<grid_for(ctx, G[d], T), T, 0, s>>>(off, G[d], grp_ch, cb, ce);
+        slope_chunk_fill_kernel<<<grid_for(ctx, Gd, T), T, 0, s>>>(off, Gd, grp_ch, cb, ce);
         B_LAUNCHED();
         D.ch_beg = cb;
         D.ch_end = ce;
@@ -2794,10 +2839,10 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         // moments and block inverses
         double *cm, *minv, *pop;
         B_CHECK(get_buf(ctx, "sl_cm", static_cast<size_t>(D.nch) * 5, &cm));
-        B_CHECK(get_buf(ctx, "sl_minv" + sx, static_cast<size_t>(G[d]) * 3, &minv));
+        B_CHECK(get_buf(ctx, "sl_minv" + sx, static_cast<size_t>(Gd) * 3, &minv));
         slope_moments_kernel<<<grid_for(ctx, static_cast<int64_t>(D.nch) * 32, T), T, 0, s>>>(D, w, cm);
         B_LAUNCHED();
-        const int gb = grid_for(ctx, G[d], T, 4);
+        const int gb = grid_for(ctx, Gd, T, 4);
         B_CHECK(get_buf(ctx, "sl_pop", gb, &pop));
         slope_block_inverse_kernel<<<gb, T, 0, s>>>(D, cm, minv, pop);
         B_LAUNCHED();
@@ -2806,11 +2851,11 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         B_TRY(cudaMemcpyAsync(hp.data(), pop, sizeof(double) * gb, cudaMemcpyDeviceToHost, s));
         B_TRY(cudaStreamSynchronize(s));
         for (double v : hp) op_norm2 += v;
-        const size_t cw = static_cast<size_t>(G[d]) * D.nb * C;
+        const size_t cw = static_cast<size_t>(Gd) * D.nb * C;
         B_CHECK(get_buf(ctx, "sl_part" + sx, static_cast<size_t>(D.nch) * D.nb * C, &D.part));
         B_CHECK(get_buf(ctx, "sl_zv" + sx, cw, &D.zv));
         B_CHECK(get_buf(ctx, "sl_p" + sx, cw, &D.p));
-        fin_grid[d] = grid_for(ctx, (G[d] + RB - 1) / RB, 1, 4);
+        fin_grid[d] = grid_for(ctx, (Gd + RB - 1) / RB, 1, 4);
     }
     // ---- input norms and stop thresholds
     const int gN = grid_for(ctx, (n + RB - 1) / RB, 1, 8);
@@ -2840,10 +2885,10 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     double *d_thr = sc, *gamma = sc + C, *beta = sc + 2 * C, *nu = sc + 3 * C, *alpha = sc + 4 * C;
     B_TRY(cudaMemcpyAsync(d_thr, thr.data(), sizeof(double) * C, cudaMemcpyHostToDevice, s));
     int stride = 1;
-    for (int d = 0; d < nd; ++d) stride = std::max(stride, fin_grid[d]);
+    for (int d = 0; d < ndt; ++d) stride = std::max(stride, fin_grid[d]);
     double *pg, *pn, *pq;
-    B_CHECK(get_buf(ctx, "sl_pg", static_cast<size_t>(nd) * stride * C, &pg));
-    B_CHECK(get_buf(ctx, "sl_pn", static_cast<size_t>(nd) * stride * C, &pn));
+    B_CHECK(get_buf(ctx, "sl_pg", static_cast<size_t>(ndt) * stride * C, &pg));
+    B_CHECK(get_buf(ctx, "sl_pn", static_cast<size_t>(ndt) * stride * C, &pn));
     const int gG = gN;
     B_CHECK(get_buf(ctx, "sl_pq", static_cast<size_t>(gG) * C, &pq));
     setup_scope.reset();
@@ -2854,9 +2899,11 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     for (int d = 0; d < nd; ++d)
         gather_bytes += 4.0 * n + (dims[d].has_b ? 8.0 * n : 0.0) +
                         8.0 * dims[d].G * dims[d].nb * C;
+    if (gi) gather_bytes += 16.0 * n + 4.0 * gi->E + 8.0 * gi->I * C;
     auto seg_bytes = [&](int d, bool update) {
         const SlopeDim& D = dims[d];
-        return n * (8.0 * C * (update ? 2 : 1) + (update && d == p ? 8.0 * C : 0.0) + wb +
+        const double pos = d == nd ? static_cast<double>(gi->E) : static_cast<double>(n);
+        return pos * (8.0 * C * (update ? 2 : 1) + (update && d == p ? 8.0 * C : 0.0) + wb +
                     (D.has_b ? 8.0 : 0.0) + (D.perm ? 4.0 : 0.0)) +
                D.nch * (8.0 + 8.0 * D.nb * C);
     };
@@ -2873,7 +2920,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         a.C = C;
         a.slots = CW == 1 ? 32 / C : 1;
         a.R = R;
-        a.Q = update ? Q : nullptr;
+        a.Q = update && p >= 0 ? Q : nullptr;  // without a primary, R is updated first
         a.alpha = alpha;
         a.w = w;
         a.write = update && d == p;
@@ -2887,8 +2934,13 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         return B200FE_OK;
     };
     auto gradient = [&](bool update, bool init) -> int {
-        for (int i = 0; i < nd; ++i) B_CHECK(segment(order[i], update));
-        for (int d = 0; d < nd; ++d) {
+        if (update && p < 0) {
+            ProfScope ps(ctx, B200FE_PROF_VECTOR, 24.0 * n * C);
+            slope_update_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(R, Q, alpha, n, C);
+            B_LAUNCHED();
+        }
+        for (int i = 0; i < no; ++i) B_CHECK(segment(order[i], update));
+        for (int d = 0; d < ndt; ++d) {
             ProfScope ps(ctx, B200FE_PROF_FINALIZE, fin_bytes(d));
             slope_finalize_kernel<<<fin_grid[d], C * RB, 0, s>>>(
                 dims[d], C, RB, pg + static_cast<size_t>(d) * stride * C,
@@ -2896,9 +2948,9 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
             B_LAUNCHED();
         }
         SlopeBetaArgs b{};
-        b.nd = nd;
+        b.nd = ndt;
         b.C = C;
-        for (int d = 0; d < nd; ++d) b.grid[d] = fin_grid[d];
+        for (int d = 0; d < ndt; ++d) b.grid[d] = fin_grid[d];
         b.stride = stride;
         b.part_g = pg;
         b.part_n = pn;
@@ -2910,11 +2962,11 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         b.done = done;
         b.init = init ? 1 : 0;
         double vb = 0.0;
-        for (int d = 0; d < nd; ++d) vb += 24.0 * dims[d].G * dims[d].nb * C;
+        for (int d = 0; d < ndt; ++d) vb += 24.0 * dims[d].G * dims[d].nb * C;
         ProfScope ps(ctx, B200FE_PROF_VECTOR, vb);
         slope_beta_kernel<<<1, T, 0, s>>>(b);
         B_LAUNCHED();
-        for (int d = 0; d < nd; ++d) {
+        for (int d = 0; d < ndt; ++d) {
             const int64_t tot = static_cast<int64_t>(dims[d].G) * dims[d].nb * C;
             slope_direction_kernel<<<grid_for(ctx, tot, T), T, 0, s>>>(dims[d], C, beta);
             B_LAUNCHED();
@@ -2930,6 +2982,19 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     ga.w = w;
     ga.Q = Q;
     ga.part = pq;
+    if (gi) {
+        int32_t *rb, *re;
+        B_CHECK(get_buf(ctx, "sl_gi_rb", n, &rb));
+        B_CHECK(get_buf(ctx, "sl_gi_re", n, &re));
+        row_edges_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(gi->gptr, pord, n, rb, re);
+        B_LAUNCHED();
+        ga.has_gi = 1;
+        ga.gi.beg = rb;
+        ga.gi.end = re;
+        ga.gi.ind = gi->gind;
+        ga.gi.scale = dims[nd].z;
+        ga.gi.p = dims[nd].p;
+    }
 
     B_CHECK(gradient(false, true));
     const int ci = std::max(1, o.check_interval);
@@ -3060,7 +3125,7 @@ int b200fe_absorb_slopes_device(b200fe_context* ctx, const double* d_v, int64_t 
     if (stream) ctx->stream = static_cast<cudaStream_t>(stream);
     const long long l0 = ctx->launches, c0 = ctx->lib_calls;
     rc = slopes_device_impl(ctx, d_v, n, cols, num_dims, d_group_ids, num_groups, z,
-                            slope_has_intercept, d_weights, o, d_out, r);
+                            slope_has_intercept, d_weights, nullptr, o, d_out, r);
     ctx->stream = own;
     r->kernel_launches = ctx->launches - l0;
     r->library_calls = ctx->lib_calls - c0;
@@ -3130,7 +3195,124 @@ int b200fe_absorb_slopes(b200fe_context* ctx, const double* y, const double* X, 
         const double* zc[B200FE_MAX_DIMS];
         for (int d = 0; d < B200FE_MAX_DIMS; ++d) zc[d] = dz[d];
         int rc2 = slopes_device_impl(ctx, dv, n, cols, num_dims, dg, num_groups, zc,
-                                     slope_has_intercept, dw, o, dout, r);
+                                     slope_has_intercept, dw, nullptr, o, dout, r);
+        if (rc2 != B200FE_OK && rc2 != B200FE_NOT_CONVERGED) return rc2;
+        B_TRY(cudaEventRecord(d0, s));
+        B_TRY(cudaMemcpyAsync(y_out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        if (k > 0)
+            B_TRY(cudaMemcpyAsync(X_out, dout + n, sizeof(double) * n * k, cudaMemcpyDeviceToHost, s));
+        B_TRY(cudaEventRecord(d1, s));
+        B_TRY(cudaEventSynchronize(d1));
+        r->h2d_ms = elapsed_ms(h0, h1);
+        r->d2h_ms = elapsed_ms(d0, d1);
+        cudaEventDestroy(h0);
+        cudaEventDestroy(h1);
+        cudaEventDestroy(d0);
+        cudaEventDestroy(d1);
+        return rc2;
+    };
+    rc = run();
+    r->kernel_launches = ctx->launches - l0;
+    r->library_calls = ctx->lib_calls - c0;
+    return r->status = rc;
+}
+
+
+int b200fe_absorb_group_individual(b200fe_context* ctx, const double* y, const double* X,
+                                   int64_t n, int k, int num_dims,
+                                   const int32_t* const* group_ids, const int32_t* num_groups,
+                                   const b200fe_group_individual* gi, const double* weights,
+                                   const b200fe_options* opts, double* y_out, double* X_out,
+                                   b200fe_result* res) {
+    b200fe_result local;
+    b200fe_result* r = res ? res : &local;
+    clear_result(r);
+    int rc = check_common(ctx, n, k + 1, num_dims, num_groups);
+    if (rc != B200FE_OK) return r->status = rc;
+    if (!y || !y_out || (k > 0 && (!X || !X_out)) || (num_dims > 0 && !group_ids) || !gi) {
+        ctx->err = "null pointer argument";
+        return r->status = B200FE_INVALID_ARG;
+    }
+    if (k + 1 > kSlopeMaxCols) {
+        ctx->err = "the group/individual absorber takes at most 256 columns";
+        return r->status = B200FE_INVALID_ARG;
+    }
+    for (int d = 0; d < num_dims; ++d)
+        if (!group_ids[d]) {
+            ctx->err = "null group id array";
+            return r->status = B200FE_INVALID_ARG;
+        }
+    // the structure's CSR arrays index each other: check every range on the host
+    const int32_t I = gi->num_individuals;
+    const int64_t E = gi->num_edges;
+    if (I <= 0 || E < 0 || E >= (int64_t(1) << 31) - 1 || !gi->group_ptr || !gi->individual_ptr ||
+        !gi->group_scale || (E > 0 && (!gi->group_individual || !gi->individual_group))) {
+        ctx->err = "invalid group/individual structure";
+        return r->status = B200FE_INVALID_ARG;
+    }
+    auto csr_ok = [](const int32_t* ptr, int64_t rows, int64_t edges) {
+        if (ptr[0] != 0 || ptr[rows] != edges) return false;
+        for (int64_t i = 0; i < rows; ++i)
+            if (ptr[i + 1] < ptr[i]) return false;
+        return true;
+    };
+    bool ok = csr_ok(gi->group_ptr, n, E) && csr_ok(gi->individual_ptr, I, E);
+    for (int64_t e = 0; ok && e < E; ++e)
+        ok = gi->group_individual[e] >= 0 && gi->group_individual[e] < I &&
+             gi->individual_group[e] >= 0 && gi->individual_group[e] < n;
+    if (!ok) {
+        ctx->err = "invalid group/individual structure (pointer arrays or ids out of range)";
+        return r->status = B200FE_INVALID_ARG;
+    }
+    b200fe_options o;
+    if (opts) o = *opts;
+    else b200fe_default_options(&o);
+    cudaGetLastError();
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return r->status = B200FE_UNAVAILABLE;
+    }
+    const cudaStream_t s = ctx->stream;
+    const long long l0 = ctx->launches, c0 = ctx->lib_calls;
+    const int cols = k + 1;
+    auto run = [&]() -> int {
+        double *dv, *dout, *dw = nullptr, *dscale;
+        int32_t *gptr, *gind, *iptr, *igrp;
+        B_CHECK(get_buf(ctx, "io_v", static_cast<size_t>(n) * cols, &dv));
+        B_CHECK(get_buf(ctx, "io_out", static_cast<size_t>(n) * cols, &dout));
+        B_CHECK(get_buf(ctx, "io_gptr", static_cast<size_t>(n) + 1, &gptr));
+        B_CHECK(get_buf(ctx, "io_gind", E, &gind));
+        B_CHECK(get_buf(ctx, "io_iptr", static_cast<size_t>(I) + 1, &iptr));
+        B_CHECK(get_buf(ctx, "io_igrp", E, &igrp));
+        B_CHECK(get_buf(ctx, "io_gscale", n, &dscale));
+        int32_t* dg[B200FE_MAX_DIMS] = {nullptr};
+        for (int d = 0; d < num_dims; ++d) B_CHECK(get_buf(ctx, "io_g" + std::to_string(d), n, &dg[d]));
+        if (weights) B_CHECK(get_buf(ctx, "io_w", n, &dw));
+        cudaEvent_t h0, h1, d0, d1;
+        B_TRY(cudaEventCreate(&h0));
+        B_TRY(cudaEventCreate(&h1));
+        B_TRY(cudaEventCreate(&d0));
+        B_TRY(cudaEventCreate(&d1));
+        B_TRY(cudaEventRecord(h0, s));
+        for (int d = 0; d < num_dims; ++d)
+            B_TRY(cudaMemcpyAsync(dg[d], group_ids[d], sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+        if (weights) B_TRY(cudaMemcpyAsync(dw, weights, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaMemcpyAsync(gptr, gi->group_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, s));
+        B_TRY(cudaMemcpyAsync(iptr, gi->individual_ptr, sizeof(int32_t) * (static_cast<size_t>(I) + 1),
+                              cudaMemcpyHostToDevice, s));
+        if (E > 0) {
+            B_TRY(cudaMemcpyAsync(gind, gi->group_individual, sizeof(int32_t) * E, cudaMemcpyHostToDevice, s));
+            B_TRY(cudaMemcpyAsync(igrp, gi->individual_group, sizeof(int32_t) * E, cudaMemcpyHostToDevice, s));
+        }
+        B_TRY(cudaMemcpyAsync(dscale, gi->group_scale, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaMemcpyAsync(dv, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        if (k > 0)
+            B_TRY(cudaMemcpyAsync(dv + n, X, sizeof(double) * n * k, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaEventRecord(h1, s));
+        const double* zc[B200FE_MAX_DIMS] = {nullptr};
+        GiDev g{I, E, gptr, gind, iptr, igrp, dscale};
+        int rc2 = slopes_device_impl(ctx, dv, n, cols, num_dims, dg, num_groups, zc, nullptr, dw,
+                                     &g, o, dout, r);
         if (rc2 != B200FE_OK && rc2 != B200FE_NOT_CONVERGED) return rc2;
         B_TRY(cudaEventRecord(d0, s));
         B_TRY(cudaMemcpyAsync(y_out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost, s));

@@ -39,6 +39,7 @@ constexpr int kSlopeChunkRows = 64;   // minimum rows per chunk
 constexpr int kSlopeMaxChunks = 1024; // chunks per group at most
 constexpr int kSlopeMaxCols = 256;
 constexpr double kSlopeDetTol = 1e-12;
+constexpr int kSlopeMaxDims = 9;  // 8 FE dimensions + the individual dimension
 
 struct SlopeDim {
     const int32_t* ids;     // [n] group per observation (primary order)
@@ -242,9 +243,23 @@ slope_norms_kernel(const double* __restrict__ R, const double* __restrict__ w, i
     column_reduce(red, au, C, RB, part_u + static_cast<int64_t>(blockIdx.x) * C);
 }
 
+// The individual dimension of a group/individual design (the reference's
+// GroupIndividualStructure, include/fe_absorption.hpp:13-21): observation k
+// (a group) holds the individuals ind[beg[k] .. end[k]), and the basis column
+// of individual i is scale_k at every group k that holds i.
+struct GiRows {
+    const int32_t* beg;   // [n] first edge of every row (primary order)
+    const int32_t* end;   // [n]
+    const int32_t* ind;   // [E] individual of every edge (group-major)
+    const double* scale;  // [n] group scale (primary order)
+    const double* p;      // [I][C] search direction of the individual dim
+};
+
 struct SlopeGatherArgs {
     int nd;
     SlopeDim dim[8];
+    int has_gi;
+    GiRows gi;
     int64_t n;
     int C, RB;
     const double* w;
@@ -268,6 +283,12 @@ slope_gather_kernel(const SlopeGatherArgs a) {
                 const int64_t base = (static_cast<int64_t>(D.ids[k]) * D.nb) * C + col;
                 if (D.has_a) q += D.p[base];
                 if (D.has_b) q = fma(D.z[k], D.p[base + (D.has_a ? C : 0)], q);
+            }
+            if (a.has_gi) {
+                double t = 0.0;
+                for (int32_t e = a.gi.beg[k]; e < a.gi.end[k]; ++e)
+                    t += a.gi.p[static_cast<int64_t>(a.gi.ind[e]) * C + col];
+                q = fma(a.gi.scale[k], t, q);
             }
             a.Q[k * C + col] = q;
             const double wk = a.w ? a.w[k] : 1.0;
@@ -418,7 +439,7 @@ slope_finalize_kernel(SlopeDim d, int C, int RB, double* __restrict__ part_g,
 
 struct SlopeBetaArgs {
     int nd, C;
-    int grid[8];             // finalize CTAs per dim
+    int grid[kSlopeMaxDims]; // finalize CTAs per dim
     int64_t stride;          // partial slots per dim
     const double* part_g;    // [nd][stride][C]
     const double* part_n;
@@ -458,6 +479,42 @@ __global__ void slope_beta_kernel(const SlopeBetaArgs a) {
     }
     any = __syncthreads_or(any);
     if (threadIdx.x == 0) *a.done = any ? 0 : 1;
+}
+
+// R -= alpha Q (designs without an FE dimension that covers every row once)
+__global__ void slope_update_kernel(double* __restrict__ R, const double* __restrict__ Q,
+                                    const double* __restrict__ alpha, int64_t n, int C) {
+    const int64_t total = n * C;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        R[e] = fma(-alpha[e % C], Q[e], R[e]);
+}
+
+// inv[ord[k]] = k
+__global__ void inverse_perm_kernel(const int32_t* __restrict__ ord, int64_t n,
+                                    int32_t* __restrict__ inv) {
+    for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        inv[ord[k]] = static_cast<int32_t>(k);
+}
+
+// edge -> row position in primary order (map null: identity)
+__global__ void map_rows_kernel(const int32_t* __restrict__ rows, int64_t E,
+                                const int32_t* __restrict__ map, int32_t* __restrict__ out) {
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < E;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[e] = map ? map[rows[e]] : rows[e];
+}
+
+// per row in primary order: its edge range in the group-major edge list
+__global__ void row_edges_kernel(const int32_t* __restrict__ gptr, const int32_t* __restrict__ pord,
+                                 int64_t n, int32_t* __restrict__ beg, int32_t* __restrict__ end) {
+    for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t g = pord ? pord[k] : k;
+        beg[k] = gptr[g];
+        end[k] = gptr[g + 1];
+    }
 }
 
 // p = zv + beta p (p = zv where beta is 0, so p needs no initial value)

@@ -21,10 +21,10 @@
 // when the GPU backend was requested, src/fe_absorption.cpp:9227-9237);
 // return true with converged=false on non-convergence; never throw.  Features
 // this library does not provide yet return false, so the reference fails
-// closed rather than silently using another path: group/individual FEs, saved
-// fixed effects together with heterogeneous slopes, and saved fixed effects in
-// the reference's per-sweep means mode.  Heterogeneous slopes (GpuFeInput with
-// is_slope) run on b200fe_absorb_slopes.  Saved FEs in the coefficient mode
+// closed rather than silently using another path: saved fixed effects together
+// with heterogeneous slopes, and saved fixed effects in the reference's
+// per-sweep means mode.  Heterogeneous slopes (GpuFeInput with is_slope) run on
+// b200fe_absorb_slopes, group/individual FEs on b200fe_absorb_group_individual.  Saved FEs in the coefficient mode
 // (fe_alpha_y / fe_alpha_X, what recover_fixed_effects consumes) come from
 // b200fe_absorb_fe.  The
 // AKM/KSS solver (akm_cuda_*) runs on the library's batched PCG
@@ -182,10 +182,61 @@ bool absorb_fixed_effects_cuda(const Eigen::Ref<const Eigen::VectorXd>& y,
 }
 
 bool absorb_fixed_effects_group_individual_cuda(
-    const Eigen::Ref<const Eigen::VectorXd>&, const Eigen::Ref<const Eigen::MatrixXd>&,
-    const std::vector<GpuFeInput>&, const GroupIndividualStructure&, const Eigen::VectorXd*,
-    const std::vector<std::size_t>&, const HdfeOptions&, AbsorptionMethod, AbsorptionResult&) {
-    return false;  // not provided: the caller fails closed
+    const Eigen::Ref<const Eigen::VectorXd>& y, const Eigen::Ref<const Eigen::MatrixXd>& X,
+    const std::vector<GpuFeInput>& standard_fe_inputs, const GroupIndividualStructure& gi,
+    const Eigen::VectorXd* weights, const std::vector<std::size_t>& sweep_order,
+    const HdfeOptions& options, AbsorptionMethod /*method*/, AbsorptionResult& result) {
+    try {
+        const int64_t n = y.size();
+        const int k = static_cast<int>(X.cols());
+        // the reference's own preconditions (src/fe_absorption_cuda.cu:4750-4770)
+        if (X.rows() != n || gi.num_groups != n || gi.num_individuals <= 0 ||
+            static_cast<int64_t>(gi.group_ptr.size()) != n + 1 ||
+            static_cast<int64_t>(gi.group_scale.size()) != n ||
+            static_cast<int64_t>(gi.individual_ptr.size()) != int64_t(gi.num_individuals) + 1 ||
+            gi.group_individual.size() != gi.individual_group.size() ||
+            static_cast<std::size_t>(gi.group_ptr.back()) != gi.group_individual.size())
+            return false;
+        if (standard_fe_inputs.size() > B200FE_MAX_DIMS) return false;
+        std::vector<const int32_t*> gids;
+        std::vector<int32_t> levels;
+        for (const GpuFeInput& fe : standard_fe_inputs) {
+            if (fe.is_slope || !fe.group_ids) return false;
+            gids.push_back(fe.group_ids);
+            levels.push_back(fe.num_groups);
+        }
+        b200fe_context* ctx = thread_ctx();
+        if (!ctx) return false;
+        b200fe_options o;
+        b200fe_default_options(&o);
+        o.tol = options.tol > 0.0 ? options.tol : 1e-8;
+        o.tolerance_mode = static_cast<int>(options.tolerance_mode);
+        if (options.max_iter > 0) o.max_iter = options.max_iter;
+        b200fe_group_individual g;
+        g.num_individuals = gi.num_individuals;
+        g.num_edges = static_cast<int64_t>(gi.group_individual.size());
+        g.group_ptr = gi.group_ptr.data();
+        g.group_individual = gi.group_individual.data();
+        g.individual_ptr = gi.individual_ptr.data();
+        g.individual_group = gi.individual_group.data();
+        g.group_scale = gi.group_scale.data();
+        const Eigen::VectorXd yc = y;
+        const Eigen::MatrixXd Xc = X;
+        result.y_tilde.resize(n);
+        result.X_tilde.resize(n, k);
+        b200fe_result r;
+        const int rc = b200fe_absorb_group_individual(
+            ctx, yc.data(), k ? Xc.data() : nullptr, n, k, static_cast<int>(gids.size()),
+            gids.data(), levels.data(), &g, weights ? weights->data() : nullptr, &o,
+            result.y_tilde.data(), k ? result.X_tilde.data() : nullptr, &r);
+        if (rc != B200FE_OK && rc != B200FE_NOT_CONVERGED) return false;
+        result.iterations = r.iterations;
+        result.converged = rc == B200FE_OK;
+        result.sweep_order_used.assign(sweep_order.begin(), sweep_order.end());
+        return true;
+    } catch (...) {
+        return false;
+    }
 }
 
 static bool recovery_max_delta(const Eigen::Ref<const Eigen::VectorXd>& residual,
