@@ -18,7 +18,9 @@ Lines printed by rank 0 (one JSON line):
 
 --impl reference runs the reference's own CPU core instead (rank 0 only).
 --workload slopes times the same panel with firm-specific tenure slopes
-(firm##c.tenure) on b200fe_absorb_slopes (one GPU; its own JSON line).
+(firm##c.tenure) on b200fe_absorb_slopes; --workload gi a 10M-group
+group/individual design on b200fe_absorb_group_individual (one GPU each; their
+own JSON lines).
 With --gpus N > 1 every rank absorbs its own replica panel (no collective in
 the data path; replicas only), launched by torch.distributed.run.
 """
@@ -63,9 +65,10 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
-    ap.add_argument("--workload", default="akm3", choices=["akm3", "slopes"],
+    ap.add_argument("--workload", default="akm3", choices=["akm3", "slopes", "gi"],
                     help="akm3: the headline workload; slopes: the same panel with "
-                         "firm-specific tenure slopes (firm##c.tenure)")
+                         "firm-specific tenure slopes (firm##c.tenure); gi: 10M groups "
+                         "with individual FEs (group/individual design)")
     return ap.parse_args()
 
 
@@ -555,8 +558,145 @@ def run_slopes(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# group/individual FEs: 10M groups x 2.5M individuals (1 GPU)
+# ---------------------------------------------------------------------------
+GI_GROUPS = 10_000_000
+GI_METRIC = ("demeaning time to 1e-8 tol, group/individual FEs: 10M groups, 2.5M individuals "
+             "(mean aggregation), year + class FEs, 13 columns, one absorption call")
+
+
+def gi_panel(n_groups: int, seed: int):
+    panels = ge.load_module("panels")
+    pkg = ge.load_package()
+    ni = max(1000, n_groups // 4)
+    y, X, fes, eg, ei = panels.group_individual_panel(n_groups, n_individuals=ni, seed=seed)
+    gi, _, _ = pkg.build_group_individual(eg, ei, "mean")
+    return y, X, fes, gi
+
+
+def run_gi(args):
+    import oracle
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n_groups = args.n if args.n != N_OBS else GI_GROUPS
+
+    def cpu_sample():
+        sn = max(10_000, args.cpu_sample // 2)
+        y, X, fes, gi = gi_panel(sn, seed=777)
+        t0 = time.perf_counter()
+        r = oracle.ref_absorb_gi(y, X, fes, gi, None, tol=1e-8, threads=threads,
+                                 method="symmetric-gauss-seidel")
+        dt = time.perf_counter() - t0
+        return {"value": dt * GI_GROUPS / sn, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": (f"reference CPU core (absorb_fixed_effects_group_individual, "
+                           f"symmetric Gauss-Seidel as the regressor selects it, tol 1e-8, "
+                           f"{threads} threads) on {sn} groups of the same generator: {dt:.3f} s, "
+                           f"{r['iterations']} iterations, scaled linearly to 10M groups")}
+
+    if args.impl == "reference":
+        vals = []
+        info = None
+        for i in range(args.warmup + args.steps):
+            info = cpu_sample()
+            if i >= args.warmup:
+                vals.append(info["value"])
+        v = statistics.median(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": GI_METRIC, "value": v, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000.0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded group/individual generator)",
+            "config": {"workload": "gi_10M_groups_13col", "n_groups": GI_GROUPS},
+            "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import torch
+    torch.cuda.set_device(0)
+    pkg = ge.load_package()
+    y, X, fes, gi = gi_panel(n_groups, seed=0)
+    n, k = y.shape[0], X.shape[1]
+    G = [int(f.max()) + 1 for f in fes]
+    absorber = pkg.Absorber(0)
+    opts = pkg.make_options(tol=1e-8, profile=True)
+    y_h = torch.from_numpy(y).pin_memory().numpy()
+    X_h = torch.from_numpy(np.ascontiguousarray(X.T)).pin_memory().numpy().T
+    yo = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    Xo = torch.empty((k, n), dtype=torch.float64).pin_memory().numpy().T
+
+    def call():
+        return absorber.absorb_group_individual(y_h, X_h, fes, G, gi, None, opts, y_out=yo,
+                                                X_out=Xo)
+
+    for _ in range(args.warmup):
+        call()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    results, walls = [], []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        results.append(call())
+        walls.append(time.perf_counter() - t1)
+    clocks = sampler.stop()
+    dev_ms = [r.setup_ms + r.solve_ms for r in results]
+    ms = statistics.median(dev_ms)
+    r_last = results[-1]
+    libm = ge.load_module("_lib")
+    prof = {}
+    tot_ms = sum(dev_ms)
+    for ci, name in enumerate(libm.PROF_NAMES):
+        tms = sum(r.prof_ms[ci] for r in results)
+        tb = sum(r.prof_bytes[ci] for r in results)
+        nl = sum(r.prof_launches[ci] for r in results)
+        if nl:
+            prof[name] = {"ms_total": tms, "launches": int(nl), "bytes_total": tb,
+                          "gbs": (tb / (tms * 1e-3) / 1e9) if tms > 0 else None,
+                          "share": tms / tot_ms}
+    hot = max((k2 for k2 in prof if k2 != "setup"), key=lambda k2: prof[k2]["ms_total"])
+    peaks, peak_kind = measured_peaks()
+    hp = prof[hot]
+    achieved = hp["bytes_total"] / (hp["ms_total"] * 1e-3) / 1e9
+    roofline = {"kernel": hot, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_kind": peak_kind,
+                "bytes_per_launch": hp["bytes_total"] / hp["launches"],
+                "ms_per_launch": hp["ms_total"] / hp["launches"], "traffic": None}
+    cpu = None if args.no_cpu_baseline or not oracle.ref_available() else cpu_sample()
+    E = int(len(gi.group_individual))
+    print(json.dumps({
+        "metric": GI_METRIC, "value": ms / 1000.0, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded group/individual generator)",
+        "config": {"workload": "gi_10M_groups_13col", "n_groups": n, "num_individuals":
+                   int(gi.num_individuals), "num_edges": E, "columns": k + 1,
+                   "fe_dims": ["year", "class", "individual (mean)"], "tol": 1e-8,
+                   "timing": "value: CUDA-event device time of setup + solve inside the call "
+                             "(inputs copied in before it); e2e: wall time of the host call",
+                   "l2_policy": f"inputs larger than L2 ({n * (k + 1) * 8 / 1e9:.1f} GB of columns per step)"},
+        "gpu_launches": int(sum(r.kernel_launches for r in results)),
+        "iterations": r_last.iterations, "converged": bool(r_last.converged),
+        "abs_residual_rel": r_last.abs_residual_rel,
+        "precision_certified": bool(r_last.precision_certified),
+        "setup_ms": r_last.setup_ms, "solve_ms": r_last.solve_ms, "clocks": clocks,
+        "roofline": roofline, "profile": prof,
+        "e2e": {"value": statistics.median(walls), "unit": UNIT,
+                "h2d_bytes_per_step": int(n * (k + 1) * 8 + n * 4 * len(fes) + (n + 1) * 4
+                                          + 8 * E + 4 * (gi.num_individuals + 1) + 8 * n),
+                "d2h_bytes_per_step": int(n * (k + 1) * 8), "h2d_ms": r_last.h2d_ms,
+                "d2h_ms": r_last.d2h_ms},
+        "cpu_baseline": cpu}))
+    absorber.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "gi":
+        return run_gi(args)
     if args.workload == "slopes":
         return run_slopes(args)
     if args.impl == "reference":

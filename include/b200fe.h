@@ -173,8 +173,11 @@ int b200fe_absorb_device(b200fe_context* ctx, const double* d_v, int64_t n,
  * slope_has_intercept[d] is nonzero, also 1_g.  slope_values may be NULL
  * (all plain).  A group's 2x2 block is inverted with the reference's rule:
  * determinant above 1e-12 max(1, W ZZ), else the intercept alone.  FP64
- * block-Jacobi CGLS over all FE blocks; at most 256 columns.  primary_dim in
- * res is the dimension whose order the observations are processed in.
+ * CGLS; when the dimension with the most groups (primary_dim in res) has no
+ * slope, it is eliminated exactly (Schur form) and the other blocks are
+ * preconditioned by the exact block diagonal of the Schur complement;
+ * opts->pass_kernel == 1 forces block Jacobi over every dimension instead.
+ * At most 256 columns.
  * Replaces the is_slope path of hdfe::detail::absorb_fixed_effects_cuda
  * (GpuFeInput.is_slope / slope_has_intercept / slope_values,
  * include/fe_absorption_cuda.hpp:12-22; src/fe_absorption_cuda.cu:2316-2420,

@@ -26,7 +26,7 @@ import make_golden  # noqa: E402
 REL_TOL = 1e-8  # within transform vs reference / exact projection, per column norm
 
 
-def _opts(pkg, tol=1e-10, **kw):
+def _opts(pkg, tol=1e-10, **kw):  # pass_kernel 1: block Jacobi over every dim
     return pkg.make_options(tol=tol, **kw)
 
 
@@ -172,3 +172,31 @@ def test_reference_slopes_dispatch_to_b200(oracle_mod):
     assert g["gpu_status_code"] == 1 and g["converged"]
     d = np.load(GOLDEN / "slopes_mixed3kw.npz")
     assert _rel(g["V"], d["ref_rows"], d["rows"], d["ref_colnorm"]) <= REL_TOL
+
+
+def test_slopes_schur_and_block_jacobi_agree(absorber, pkg):
+    """Worker (plain, the most groups) eliminated exactly vs block Jacobi over
+    every dimension: same projection, fewer iterations."""
+    c = make_golden.SLOPE_CASES["akm20k"]()
+    a = _absorb(absorber, pkg, c, tol=1e-11)
+    b = _absorb(absorber, pkg, c, tol=1e-11, pass_kernel=1)
+    assert a.converged and b.converged
+    Va = np.column_stack([a.y_tilde, a.X_tilde])
+    Vb = np.column_stack([b.y_tilde, b.X_tilde])
+    scale = np.linalg.norm(np.column_stack([c["y"], c["X"]]), axis=0)
+    assert (np.linalg.norm(Va - Vb, axis=0) / scale).max() <= 1e-9
+    assert a.iterations < b.iterations
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_slopes_schur_matches_exact_projection(absorber, pkg, panels, weighted):
+    from oracle.slope_oracle import slope_projection
+    p, sl = panels.akm_firm_tenure_slopes(3000, n_firms=80, seed=12)
+    w = np.random.default_rng(1).uniform(0.3, 3.0, p.n) if weighted else None
+    c = dict(y=p.y, X=p.X, fes=p.fes, slopes=sl, weights=w)
+    r = _absorb(absorber, pkg, c, tol=1e-12)
+    assert r.converged and r.primary_dim == 0
+    V0 = np.column_stack([p.y, p.X])
+    o = slope_projection(V0, p.fes, sl, w)
+    V = np.column_stack([r.y_tilde, r.X_tilde])
+    assert (np.linalg.norm(V - o, axis=0) / np.linalg.norm(V0, axis=0)).max() <= REL_TOL * 1e-1

@@ -158,6 +158,11 @@ class AbsorptionResult:
     h2d_ms: float = 0.0
     d2h_ms: float = 0.0
     kernel_launches: int = 0
+    # options.profile: per kernel category (_lib.PROF_NAMES) CUDA-event ms,
+    # algorithmic bytes and launches
+    prof_ms: list = field(default_factory=list)
+    prof_bytes: list = field(default_factory=list)
+    prof_launches: list = field(default_factory=list)
     sample_index: np.ndarray | None = None
     # saved FEs (save_fe=True): per dim, [G_d, 1 + k] coefficients, column 0 for
     # y -- the fe_alpha_y / fe_alpha_X of the reference's retain_fixed_effects
@@ -333,7 +338,7 @@ class Absorber:
         return out, r
 
     def absorb_group_individual(self, y, X, group_ids, num_groups, gi, weights=None,
-                                options=None) -> AbsorptionResult:
+                                options=None, y_out=None, X_out=None) -> AbsorptionResult:
         """Absorb the standard FE dims (dense ids; may be empty) and the
         individual FEs of ``gi`` (a GroupIndividualStructure; rows = groups),
         absorb_fixed_effects_group_individual_cuda."""
@@ -355,8 +360,10 @@ class Absorber:
         _check_finite(sc, "group_scale")
         st = _lib.GroupIndividual(int(gi.num_individuals), int(arrs[1].shape[0]),
                                   *[a.ctypes.data for a in arrs], sc.ctypes.data)
-        y_out = np.empty_like(y)
-        X_out = np.empty((n, k), dtype=np.float64, order="F")
+        if y_out is None:
+            y_out = np.empty_like(y)
+        if X_out is None:
+            X_out = np.empty((n, k), dtype=np.float64, order="F")
         o = options or make_options()
         r = _lib.Result()
         rc = self.lib.b200fe_absorb_group_individual(
@@ -438,7 +445,8 @@ def _to_result(r: _lib.Result, y_out, X_out, G) -> AbsorptionResult:
         outer_iterations=int(r.outer_iterations), rel_residual=float(r.rel_residual),
         primary_dim=int(r.primary_dim), setup_ms=float(r.setup_ms),
         solve_ms=float(r.solve_ms), h2d_ms=float(r.h2d_ms), d2h_ms=float(r.d2h_ms),
-        kernel_launches=int(r.kernel_launches))
+        kernel_launches=int(r.kernel_launches), prof_ms=list(r.prof_ms),
+        prof_bytes=list(r.prof_bytes), prof_launches=list(r.prof_launches))
 
 
 _tls = threading.local()

@@ -2857,6 +2857,64 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         B_CHECK(get_buf(ctx, "sl_p" + sx, cw, &D.p));
         fin_grid[d] = grid_for(ctx, (Gd + RB - 1) / RB, 1, 4);
     }
+    // ---- Schur form: a plain primary dimension eliminated exactly (auto, or
+    // pass_kernel 1 for block Jacobi over every dimension)
+    const bool schur = !gi && p >= 0 && !dims[p].has_b && nd >= 2 && o.pass_kernel != 1;
+    std::vector<int> cg;  // dimensions the CG runs over, in pass order (writer last)
+    for (int i = 0; i < no; ++i)
+        if (!(schur && order[i] == p)) cg.push_back(order[i]);
+    const int ncg = static_cast<int>(cg.size());
+    const int writer = schur ? (ncg ? cg.back() : -1) : p;
+    if (schur) {
+        for (int d : cg) {
+            SlopeDim& D = dims[d];
+            const std::string sx = std::to_string(d);
+            int32_t *flag, *pid, *start, *off;
+            double* contrib;
+            B_CHECK(get_buf(ctx, "sl_pflag", n, &flag));
+            B_CHECK(get_buf(ctx, "sl_pid", n, &pid));
+            pair_flags_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(D.perm, D.ids, dims[p].ids, n, flag);
+            B_LAUNCHED();
+            B_CHECK(cub_inclusive_sum(ctx, flag, pid, n));
+            int np = 0;
+            B_CHECK(sync_read_int(ctx, pid + (n - 1), 1, &np));
+            B_CHECK(get_buf(ctx, "sl_pstart", static_cast<size_t>(np) + 1, &start));
+            pair_start_kernel<<<grid_for(ctx, n + 1, T), T, 0, s>>>(flag, pid, n, start);
+            B_LAUNCHED();
+            B_CHECK(get_buf(ctx, "sl_contrib", static_cast<size_t>(np) * 3, &contrib));
+            pair_contrib_kernel<<<grid_for(ctx, np, T), T, 0, s>>>(D, dims[p].ids, dims[p].minv, w,
+                                                                   start, np, contrib);
+            B_LAUNCHED();
+            B_CHECK(get_buf(ctx, "sl_off" + sx, static_cast<size_t>(D.G) + 1, &off));
+            // per group sums of the pair planes: one block per group, fixed order
+            int32_t* poff;
+            double* csum;
+            B_CHECK(get_buf(ctx, "sl_poff", static_cast<size_t>(D.G) + 1, &poff));
+            B_CHECK(get_buf(ctx, "sl_csum", static_cast<size_t>(D.G) * 3, &csum));
+            pair_offsets_kernel<<<grid_for(ctx, static_cast<int64_t>(D.G) + 1, T), T, 0, s>>>(
+                off, pid, D.G, n, np, poff);
+            B_LAUNCHED();
+            for (int m = 0; m < 3; ++m) {
+                size_t tmp = 0;
+                const double* in = contrib + static_cast<size_t>(m) * np;
+                double* out = csum + static_cast<size_t>(m) * D.G;
+                B_TRY(cub::DeviceSegmentedReduce::Sum(nullptr, tmp, in, out, D.G, poff, poff + 1, s));
+                uint8_t* t;
+                B_CHECK(get_buf(ctx, "cub_tmp", tmp, &t));
+                B_TRY(cub::DeviceSegmentedReduce::Sum(t, tmp, in, out, D.G, poff, poff + 1, s));
+                ++ctx->lib_calls;
+            }
+            double *cm, *pop;
+            B_CHECK(get_buf(ctx, "sl_cm", static_cast<size_t>(D.nch) * 5, &cm));
+            slope_moments_kernel<<<grid_for(ctx, static_cast<int64_t>(D.nch) * 32, T), T, 0, s>>>(D, w, cm);
+            B_LAUNCHED();
+            const int gb = grid_for(ctx, D.G, T, 4);
+            B_CHECK(get_buf(ctx, "sl_pop", gb, &pop));
+            schur_block_inverse_kernel<<<gb, T, 0, s>>>(D, cm, csum, const_cast<double*>(D.minv),
+                                                        pop);
+            B_LAUNCHED();
+        }
+    }
     // ---- input norms and stop thresholds
     const int gN = grid_for(ctx, (n + RB - 1) / RB, 1, 8);
     double *pw, *pu;
@@ -2884,11 +2942,12 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     B_CHECK(get_buf(ctx, "sl_done", 1, &done));
     double *d_thr = sc, *gamma = sc + C, *beta = sc + 2 * C, *nu = sc + 3 * C, *alpha = sc + 4 * C;
     B_TRY(cudaMemcpyAsync(d_thr, thr.data(), sizeof(double) * C, cudaMemcpyHostToDevice, s));
+    // finalize partials: slot i for cg[i], slot ncg for the primary (Schur form)
     int stride = 1;
     for (int d = 0; d < ndt; ++d) stride = std::max(stride, fin_grid[d]);
     double *pg, *pn, *pq;
-    B_CHECK(get_buf(ctx, "sl_pg", static_cast<size_t>(ndt) * stride * C, &pg));
-    B_CHECK(get_buf(ctx, "sl_pn", static_cast<size_t>(ndt) * stride * C, &pn));
+    B_CHECK(get_buf(ctx, "sl_pg", static_cast<size_t>(ndt + 1) * stride * C, &pg));
+    B_CHECK(get_buf(ctx, "sl_pn", static_cast<size_t>(ndt + 1) * stride * C, &pn));
     const int gG = gN;
     B_CHECK(get_buf(ctx, "sl_pq", static_cast<size_t>(gG) * C, &pq));
     setup_scope.reset();
@@ -2896,15 +2955,16 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     // algorithmic bytes per launch (profile categories)
     const double wb = w ? 8.0 : 0.0;
     double gather_bytes = 8.0 * n * C + wb * n;
-    for (int d = 0; d < nd; ++d)
-        gather_bytes += 4.0 * n + (dims[d].has_b ? 8.0 * n : 0.0) +
-                        8.0 * dims[d].G * dims[d].nb * C;
+    for (int d : cg)
+        if (d < nd)
+            gather_bytes += 4.0 * n + (dims[d].has_b ? 8.0 * n : 0.0) +
+                            8.0 * dims[d].G * dims[d].nb * C;
     if (gi) gather_bytes += 16.0 * n + 4.0 * gi->E + 8.0 * gi->I * C;
-    auto seg_bytes = [&](int d, bool update) {
+    auto seg_bytes = [&](int d, bool update, bool write) {
         const SlopeDim& D = dims[d];
         const double pos = d == nd ? static_cast<double>(gi->E) : static_cast<double>(n);
-        return pos * (8.0 * C * (update ? 2 : 1) + (update && d == p ? 8.0 * C : 0.0) + wb +
-                    (D.has_b ? 8.0 : 0.0) + (D.perm ? 4.0 : 0.0)) +
+        return pos * (8.0 * C * (update ? 2 : 1) + (write ? 8.0 * C : 0.0) + wb +
+                      (D.has_b ? 8.0 : 0.0) + (D.perm ? 4.0 : 0.0)) +
                D.nch * (8.0 + 8.0 * D.nb * C);
     };
     auto fin_bytes = [&](int d) {
@@ -2914,22 +2974,43 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
 
     // ---- iteration pieces
     const int CW = C <= 32 ? 1 : C <= 64 ? 2 : C <= 128 ? 4 : 8;
-    auto segment = [&](int d, bool update) -> int {
+    // chunk sums of w x and w z x over dim d's groups, x = R - alpha Q (update)
+    // or the rows of X (X given); the writer stores the updated residual
+    auto segment = [&](int d, bool update, const double* X) -> int {
         SlopeSegArgs a{};
         a.d = dims[d];
         a.C = C;
         a.slots = CW == 1 ? 32 / C : 1;
-        a.R = R;
-        a.Q = update && p >= 0 ? Q : nullptr;  // without a primary, R is updated first
+        a.R = X ? const_cast<double*>(X) : R;
+        a.Q = !X && update && p >= 0 ? Q : nullptr;  // without a primary, R is updated first
         a.alpha = alpha;
         a.w = w;
-        a.write = update && d == p;
+        a.write = !X && update && d == writer;
         const int g = grid_for(ctx, static_cast<int64_t>(dims[d].nch) * 32, T, 16);
-        ProfScope ps(ctx, B200FE_PROF_PASS, seg_bytes(d, update));
+        ProfScope ps(ctx, B200FE_PROF_PASS, seg_bytes(d, update && !X, a.write != 0));
         if (CW == 1) slope_segment_kernel<1><<<g, T, 0, s>>>(a);
         else if (CW == 2) slope_segment_kernel<2><<<g, T, 0, s>>>(a);
         else if (CW == 4) slope_segment_kernel<4><<<g, T, 0, s>>>(a);
         else slope_segment_kernel<8><<<g, T, 0, s>>>(a);
+        B_LAUNCHED();
+        return B200FE_OK;
+    };
+    auto finalize = [&](int d, int slot) -> int {
+        ProfScope ps(ctx, B200FE_PROF_FINALIZE, fin_bytes(d));
+        slope_finalize_kernel<<<fin_grid[d], C * RB, 0, s>>>(
+            dims[d], C, RB, pg + static_cast<size_t>(slot) * stride * C,
+            pn + static_cast<size_t>(slot) * stride * C);
+        B_LAUNCHED();
+        return B200FE_OK;
+    };
+    // X -= its weighted primary-group means (Schur form), with partials of
+    // x' W x into pq when dots is set
+    auto project = [&](double* X, bool dots) -> int {
+        B_CHECK(segment(p, false, X));
+        B_CHECK(finalize(p, ncg));  // zv of the primary = the group means
+        ProfScope ps(ctx, B200FE_PROF_GATHER, n * (16.0 * C + 4.0 + wb) + 8.0 * dims[p].G * C);
+        slope_project_kernel<<<gG, C * RB, 0, s>>>(X, dims[p].ids, dims[p].zv, w, n, C, RB,
+                                                   dots ? pq : nullptr);
         B_LAUNCHED();
         return B200FE_OK;
     };
@@ -2939,18 +3020,12 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
             slope_update_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(R, Q, alpha, n, C);
             B_LAUNCHED();
         }
-        for (int i = 0; i < no; ++i) B_CHECK(segment(order[i], update));
-        for (int d = 0; d < ndt; ++d) {
-            ProfScope ps(ctx, B200FE_PROF_FINALIZE, fin_bytes(d));
-            slope_finalize_kernel<<<fin_grid[d], C * RB, 0, s>>>(
-                dims[d], C, RB, pg + static_cast<size_t>(d) * stride * C,
-                pn + static_cast<size_t>(d) * stride * C);
-            B_LAUNCHED();
-        }
+        for (int d : cg) B_CHECK(segment(d, update, nullptr));
+        for (int i = 0; i < ncg; ++i) B_CHECK(finalize(cg[i], i));
         SlopeBetaArgs b{};
-        b.nd = ndt;
+        b.nd = ncg;
         b.C = C;
-        for (int d = 0; d < ndt; ++d) b.grid[d] = fin_grid[d];
+        for (int i = 0; i < ncg; ++i) b.grid[i] = fin_grid[cg[i]];
         b.stride = stride;
         b.part_g = pg;
         b.part_n = pn;
@@ -2967,6 +3042,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         slope_beta_kernel<<<1, T, 0, s>>>(b);
         B_LAUNCHED();
         for (int d = 0; d < ndt; ++d) {
+            if (schur && d == p) continue;
             const int64_t tot = static_cast<int64_t>(dims[d].G) * dims[d].nb * C;
             slope_direction_kernel<<<grid_for(ctx, tot, T), T, 0, s>>>(dims[d], C, beta);
             B_LAUNCHED();
@@ -2974,8 +3050,9 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         return B200FE_OK;
     };
     SlopeGatherArgs ga{};
-    ga.nd = nd;
-    for (int d = 0; d < nd; ++d) ga.dim[d] = dims[d];
+    ga.nd = 0;
+    for (int d = 0; d < nd; ++d)
+        if (!(schur && d == p)) ga.dim[ga.nd++] = dims[d];
     ga.n = n;
     ga.C = C;
     ga.RB = RB;
@@ -2996,6 +3073,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         ga.gi.p = dims[nd].p;
     }
 
+    if (schur) B_CHECK(project(R, false));
     B_CHECK(gradient(false, true));
     const int ci = std::max(1, o.check_interval);
     const int max_it = o.max_iter > 0 ? o.max_iter : 10000;
@@ -3009,6 +3087,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
                 slope_gather_kernel<<<gG, C * RB, 0, s>>>(ga);
                 B_LAUNCHED();
             }
+            if (schur) B_CHECK(project(Q, true));
             {
                 ProfScope ps(ctx, B200FE_PROF_VECTOR, 0.0);
                 slope_alpha_kernel<<<1, T, 0, s>>>(pq, gG, C, gamma, active, alpha);
@@ -3018,6 +3097,18 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         }
         it += steps;
         B_CHECK(sync_read_int(ctx, done, 1, &hd));
+    }
+    // Schur form: the primary's share of the certificate, ||D_p' W r||^2
+    std::vector<double> nu_p(C, 0.0);
+    if (schur) {
+        B_CHECK(segment(p, false, R));
+        B_CHECK(finalize(p, ncg));
+        std::vector<double> hq(static_cast<size_t>(fin_grid[p]) * C);
+        B_TRY(cudaMemcpyAsync(hq.data(), pn + static_cast<size_t>(ncg) * stride * C,
+                              sizeof(double) * hq.size(), cudaMemcpyDeviceToHost, s));
+        B_TRY(cudaStreamSynchronize(s));
+        for (int b = 0; b < fin_grid[p]; ++b)
+            for (int c = 0; c < C; ++c) nu_p[c] += hq[static_cast<size_t>(b) * C + c];
     }
     {
         ProfScope ps(ctx, B200FE_PROF_FINAL, 16.0 * n * C + (pord ? 4.0 * n : 0.0));
@@ -3049,7 +3140,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     const double opn = std::sqrt(std::max(0.0, op_norm2));
     double abs_res = 0.0, abs_rel = 0.0, rel = 0.0;
     for (int c = 0; c < C; ++c) {
-        const double ab = std::sqrt(std::max(0.0, hnu[c]));
+        const double ab = std::sqrt(std::max(0.0, hnu[c] + nu_p[c]));
         const double scl = opn * std::sqrt(std::max(0.0, vu[c]));
         double r = 0.0;
         if (scl > 0.0) r = ab / scl;

@@ -517,6 +517,149 @@ __global__ void row_edges_kernel(const int32_t* __restrict__ gptr, const int32_t
     }
 }
 
+// ---------------------------------------------------------------------------
+// Schur form (a plain primary dimension eliminated exactly).  The CGLS runs on
+// min || (I - P_p)(v - D_r a) ||_W over the other dimensions' coefficients a,
+// P_p the W-projection on the primary groups (segment means in primary
+// order).  Its block-Jacobi preconditioner is the exact block diagonal of the
+// Schur complement D_r' W (I - P_p) D_r: for group g of dimension d,
+//   S_g = B_g - sum over primary groups j meeting g of c_jg c_jg' / W_j,
+// c_jg the sums of the basis multipliers (w, w z) over the rows in (j, g).
+// In dimension d's stable sorted order the rows of g are in primary order, so
+// every pair (j, g) is one contiguous run there.
+// ---------------------------------------------------------------------------
+constexpr double kSchurRel = 1e-11;  // null-space test of a Schur block, relative to B
+
+// flag[pos] = 1 where a (primary group, group of d) pair starts in d's order
+__global__ void pair_flags_kernel(const int32_t* __restrict__ perm, const int32_t* __restrict__ ids_d,
+                                  const int32_t* __restrict__ ids_p, int64_t n,
+                                  int32_t* __restrict__ flag) {
+    for (int64_t pos = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; pos < n;
+         pos += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        int32_t f = 1;
+        if (pos > 0) {
+            const int32_t k = perm[pos], kp = perm[pos - 1];
+            f = (ids_d[k] != ids_d[kp] || ids_p[k] != ids_p[kp]) ? 1 : 0;
+        }
+        flag[pos] = f;
+    }
+}
+
+// start[pid[pos] - 1] = pos at every pair start; start[npairs] = n
+__global__ void pair_start_kernel(const int32_t* __restrict__ flag, const int32_t* __restrict__ pid,
+                                  int64_t n, int32_t* __restrict__ start) {
+    for (int64_t pos = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; pos <= n;
+         pos += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (pos == n) start[pid[n - 1]] = static_cast<int32_t>(n);
+        else if (flag[pos]) start[pid[pos] - 1] = static_cast<int32_t>(pos);
+    }
+}
+
+// per pair: (c_a^2, c_a c_b, c_b^2) / W_j, c = sums of w and w z over its rows
+// (three planes of npairs values)
+__global__ void pair_contrib_kernel(const SlopeDim d, const int32_t* __restrict__ ids_p,
+                                    const double* __restrict__ minv_p, const double* __restrict__ w,
+                                    const int32_t* __restrict__ start, int64_t npairs,
+                                    double* __restrict__ contrib) {
+    for (int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < npairs;
+         q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double ca = 0.0, cb = 0.0;
+        const int32_t b = start[q], e = start[q + 1];
+        for (int32_t pos = b; pos < e; ++pos) {
+            const int32_t k = d.perm[pos];
+            const double wk = w ? w[k] : 1.0;
+            ca += wk;
+            if (d.has_b) cb = fma(wk, d.z[k], cb);
+        }
+        const double iw = minv_p[static_cast<int64_t>(ids_p[d.perm[b]]) * 3];  // 1 / W_j
+        contrib[q] = ca * ca * iw;
+        contrib[npairs + q] = ca * cb * iw;
+        contrib[2 * npairs + q] = cb * cb * iw;
+    }
+}
+
+// first pair of every group of d (groups own contiguous pair ranges; an empty
+// group gets the next group's first pair)
+__global__ void pair_offsets_kernel(const int32_t* __restrict__ off, const int32_t* __restrict__ pid,
+                                    int32_t G, int64_t n, int32_t npairs,
+                                    int32_t* __restrict__ pair_off) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g <= G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        pair_off[g] = off[g] < n ? pid[off[g]] - 1 : npairs;
+}
+
+// Block inverse of the Schur block of every group (pseudo-inverse on the
+// null space: a block whose projected intercept or slope vanishes against its
+// unprojected size keeps the other direction; a slope the reference's rule
+// drops from the basis stays dropped), and the group's share of ||D'W||_F^2.
+__global__ void __launch_bounds__(kSlopeThreads)
+schur_block_inverse_kernel(const SlopeDim d, const double* __restrict__ cm,
+                           const double* __restrict__ csum, double* __restrict__ minv,
+                           double* __restrict__ part_op) {
+    __shared__ double red[kSlopeThreads];
+    double op = 0.0;
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < d.G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double m[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int32_t j = d.grp_ch[g]; j < d.grp_ch[g + 1]; ++j)
+#pragma unroll
+            for (int u = 0; u < 5; ++u) m[u] += cm[static_cast<int64_t>(j) * 5 + u];
+        const double W = m[0], Z = m[1], ZZ = m[2];
+        // csum: per group the sums of the three pair planes (segmented reduce)
+        const double s11 = W - csum[g], s12 = Z - csum[d.G + g], s22 = ZZ - csum[2 * static_cast<int64_t>(d.G) + g];
+        bool slope_in = false;  // the reference's basis rule on the unprojected block
+        if (d.has_a && d.has_b)
+            slope_in = W > 0.0 && W * ZZ - Z * Z > kSlopeDetTol * fmax(1.0, W * ZZ);
+        else if (d.has_b)
+            slope_in = ZZ > kSlopeDetTol * fmax(1.0, ZZ);
+        const bool a_ok = d.has_a && W > 0.0 && s11 > kSchurRel * W;
+        const bool b_ok = slope_in && s22 > kSchurRel * ZZ;
+        double m00 = 0.0, m01 = 0.0, m11 = 0.0;
+        const double det = s11 * s22 - s12 * s12;
+        if (a_ok && b_ok && det > kSchurRel * W * ZZ) {
+            m00 = s22 / det;
+            m01 = -s12 / det;
+            m11 = s11 / det;
+        } else if (a_ok) {
+            m00 = 1.0 / s11;
+        } else if (b_ok) {
+            m11 = 1.0 / s22;
+        }
+        minv[g * 3 + 0] = m00;
+        minv[g * 3 + 1] = m01;
+        minv[g * 3 + 2] = m11;
+        op += (d.has_a ? m[3] : 0.0) + (d.has_b ? m[4] : 0.0);
+    }
+    red[threadIdx.x] = op;
+    __syncthreads();
+    for (int st = kSlopeThreads / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part_op[blockIdx.x] = red[0];
+}
+
+// X[k][c] -= mean[ids_p[k]][c] (the primary groups' weighted means), with CTA
+// partials of sum w x^2 per column when part is not null.
+__global__ void __launch_bounds__(kSlopeThreads)
+slope_project_kernel(double* __restrict__ X, const int32_t* __restrict__ ids_p,
+                     const double* __restrict__ mean, const double* __restrict__ w, int64_t n,
+                     int C, int RB, double* __restrict__ part) {
+    __shared__ double red[kSlopeThreads];
+    const int col = threadIdx.x % C, rr = threadIdx.x / C;
+    double acc = 0.0;
+    if (rr < RB) {
+        for (int64_t k = static_cast<int64_t>(blockIdx.x) * RB + rr; k < n;
+             k += static_cast<int64_t>(gridDim.x) * RB) {
+            const double x = X[k * C + col] - mean[static_cast<int64_t>(ids_p[k]) * C + col];
+            X[k * C + col] = x;
+            const double wk = w ? w[k] : 1.0;
+            acc = fma(wk * x, x, acc);
+        }
+    }
+    if (part) column_reduce(red, acc, C, RB, part + static_cast<int64_t>(blockIdx.x) * C);
+}
+
 // p = zv + beta p (p = zv where beta is 0, so p needs no initial value)
 __global__ void slope_direction_kernel(SlopeDim d, int C, const double* __restrict__ beta) {
     const int64_t total = static_cast<int64_t>(d.G) * d.nb * C;

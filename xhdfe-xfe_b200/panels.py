@@ -165,6 +165,37 @@ def akm_firm_tenure_slopes(n_obs: int = 1_000_000, *, n_firms: int = 10_000,
     return panel, [(1, tenure, True)]
 
 
+def group_individual_panel(n_groups: int = 10_000_000, *, n_individuals: int = 2_500_000,
+                           n_years: int = 36, n_classes: int = 600, seed: int = 0,
+                           zipf: float = 0.8, k: int = 12):
+    """Group-level data with individual FEs (patents x inventors style).
+
+    Every group (a row) holds 1-4 distinct individuals drawn with Zipf(s)
+    popularity; the rows carry a year and a class FE and k regressors
+    (N(0, 1)); y = 0.1 sum(X) + mean of the members' FEs + year + class FE +
+    N(0, 1).  Returns (y, X, fes [year, class], edge_group, edge_individual),
+    edges group-major with no repeated (group, individual) pair.
+    """
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(1, 5, n_groups)
+    eg = np.repeat(np.arange(n_groups, dtype=np.int64), sizes)
+    draw = _zipf_sampler(rng, n_individuals, zipf)
+    ei = draw(eg.size)
+    key = np.unique(eg * n_individuals + ei)  # drop repeats inside a group
+    eg, ei = key // n_individuals, key % n_individuals
+    alpha = rng.standard_normal(n_individuals)
+    cnt = np.bincount(eg, minlength=n_groups)
+    if np.any(cnt == 0):
+        raise RuntimeError("a group lost all its individuals")
+    mean_alpha = np.bincount(eg, weights=alpha[ei], minlength=n_groups) / cnt
+    year = rng.integers(0, n_years, n_groups).astype(np.int32)
+    cls = rng.integers(0, n_classes, n_groups).astype(np.int32)
+    X = np.asfortranarray(rng.standard_normal((n_groups, k)))
+    y = (0.1 * X.sum(axis=1) + mean_alpha + 0.1 * rng.standard_normal(n_years)[year]
+         + 0.3 * rng.standard_normal(n_classes)[cls] + rng.standard_normal(n_groups))
+    return y, X, [year, cls], eg, ei
+
+
 def akm_batched(n_obs: int = 50_000_000, *, n_firms: int = 800_000, n_years: int = 36,
                 seed: int = 0, move_prob: float = 0.1, zipf: float = 1.1,
                 n_noise: int = 7) -> Panel:
