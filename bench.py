@@ -229,20 +229,45 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# rank coordination (one process per GPU, launched by torch.distributed.run)
+# ---------------------------------------------------------------------------
+def init_ranks(backend: str = "nccl", timeout_s: int = 600):
+    """(world, rank, local_rank, dist or None) from the torchrun environment;
+    the process group exists only when world > 1."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+    return world, rank, local, dist
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest value over all ranks (every rank gets it); value itself at N=1."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def run_ours(args):
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local, dist = init_ranks("nccl")
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     pkg = ge.load_package()
     t0 = time.perf_counter()
@@ -270,8 +295,7 @@ def run_ours(args):
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    if dist:
-        dist.barrier()
+    barrier(dist)
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -281,14 +305,9 @@ def run_ours(args):
         results.append(step(opts))
     ev1.record(stream)
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    barrier(dist)
     clocks = sampler.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, dev)
     r_last = results[-1]
     launches = int(sum(r.kernel_launches for r in results))
     lib_calls = int(sum(r.library_calls for r in results))
@@ -344,16 +363,11 @@ def run_ours(args):
         absorber.absorb(y_h, X_h, g_h, panel.levels, None, o_e, y_out=yo, X_out=Xo)
         times = []
         for _ in range(args.e2e_steps):
-            if dist:
-                dist.barrier()
+            barrier(dist)
             t1 = time.perf_counter()
             re = absorber.absorb(y_h, X_h, g_h, panel.levels, None, o_e, y_out=yo, X_out=Xo)
             times.append(time.perf_counter() - t1)
-        et = statistics.median(times)
-        if dist:
-            t = torch.tensor([et], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            et = float(t.item())
+        et = max_over_ranks(statistics.median(times), dist, dev)
         e2e = {"value": et, "unit": UNIT,
                "h2d_bytes_per_step": int(n * cols * 8 + n * 4 * len(panel.fes)),
                "d2h_bytes_per_step": int(n * cols * 8),
