@@ -200,3 +200,45 @@ def test_slopes_schur_matches_exact_projection(absorber, pkg, panels, weighted):
     o = slope_projection(V0, p.fes, sl, w)
     V = np.column_stack([r.y_tilde, r.X_tilde])
     assert (np.linalg.norm(V - o, axis=0) / np.linalg.norm(V0, axis=0)).max() <= REL_TOL * 1e-1
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_slopes_schur_long_primary_groups(absorber, pkg, weighted):
+    """Primary groups longer than one chunk (the fused projection's fix-up
+    path): Schur form equals block Jacobi over every dimension."""
+    rng = np.random.default_rng(21)
+    k = 12_000  # primary groups: mostly 2-7 rows, 2% of them 65-600 rows
+    sizes = np.where(rng.random(k) < 0.02, rng.integers(65, 600, k), rng.integers(2, 8, k))
+    g1 = np.repeat(np.arange(k), sizes).astype(np.int32)
+    n = g1.size
+    g2 = rng.integers(0, 300, n).astype(np.int32)
+    g3 = rng.integers(0, 12, n).astype(np.int32)
+    z = rng.uniform(0, 4, n)
+    X = rng.standard_normal((n, 3))
+    y = X @ np.array([0.5, -1.0, 0.2]) + 0.1 * z * (g2 % 7) + rng.standard_normal(n)
+    w = rng.uniform(0.3, 3.0, n) if weighted else None
+    c = dict(y=y, X=X, fes=[g1, g2, g3], slopes=[(1, z, True)], weights=w)
+    assert np.bincount(g1).max() > 64 and int(g1.max()) + 1 > 300
+    a = _absorb(absorber, pkg, c, tol=1e-11)
+    b = _absorb(absorber, pkg, c, tol=1e-11, pass_kernel=1)
+    assert a.converged and b.converged and a.primary_dim == 0
+    Va = np.column_stack([a.y_tilde, a.X_tilde])
+    Vb = np.column_stack([b.y_tilde, b.X_tilde])
+    scale = np.linalg.norm(np.column_stack([y, X]), axis=0)
+    assert (np.linalg.norm(Va - Vb, axis=0) / scale).max() <= 1e-9
+    assert a.precision_certified
+
+
+def test_slopes_many_columns(absorber, pkg, panels):
+    """40 columns (two column words per lane) through both forms."""
+    p, sl = panels.akm_firm_tenure_slopes(20_000, n_firms=300, seed=31)
+    rng = np.random.default_rng(5)
+    X = np.column_stack([p.X, rng.standard_normal((p.n, 37))])
+    c = dict(y=p.y, X=X, fes=p.fes, slopes=sl, weights=None)
+    a = _absorb(absorber, pkg, c, tol=1e-11)
+    b = _absorb(absorber, pkg, c, tol=1e-11, pass_kernel=1)
+    Va = np.column_stack([a.y_tilde, a.X_tilde])
+    Vb = np.column_stack([b.y_tilde, b.X_tilde])
+    scale = np.linalg.norm(np.column_stack([p.y, X]), axis=0)
+    assert Va.shape[1] == 40
+    assert (np.linalg.norm(Va - Vb, axis=0) / scale).max() <= 1e-9

@@ -2748,6 +2748,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     int present[kSlopeMaxDims] = {0};
     int fin_grid[kSlopeMaxDims] = {0};
     const int RB = T / C;
+    int32_t* p_ch_grp = nullptr;
     int32_t* inv_pord = nullptr;
     if (gi && pord) {
         B_CHECK(get_buf(ctx, "sl_invp", n, &inv_pord));
@@ -2831,11 +2832,14 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         int32_t *cb, *ce;
         B_CHECK(get_buf(ctx, "sl_chb" + sx, D.nch, &cb));
         B_CHECK(get_buf(ctx, "sl_che" + sx, D.nch, &ce));
-        slope_chunk_fill_kernel<<<grid_for(ctx, Gd, T), T, 0, s>>>(off, Gd, grp_ch, cb, ce);
+        int32_t* cg_of = nullptr;  // chunk -> group, kept for the primary (Schur gather)
+        if (d == p) B_CHECK(get_buf(ctx, "sl_chgrp", D.nch, &cg_of));
+        slope_chunk_fill_kernel<<<grid_for(ctx, Gd, T), T, 0, s>>>(off, Gd, grp_ch, cb, ce, cg_of);
         B_LAUNCHED();
         D.ch_beg = cb;
         D.ch_end = ce;
         D.grp_ch = grp_ch;
+        if (d == p) p_ch_grp = cg_of;
         // moments and block inverses
         double *cm, *minv, *pop;
         B_CHECK(get_buf(ctx, "sl_cm", static_cast<size_t>(D.nch) * 5, &cm));
@@ -2864,7 +2868,10 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     for (int i = 0; i < no; ++i)
         if (!(schur && order[i] == p)) cg.push_back(order[i]);
     const int ncg = static_cast<int>(cg.size());
-    const int writer = schur ? (ncg ? cg.back() : -1) : p;
+    // Schur form: the residual is updated by one coalesced pass in primary order
+    // (slope_update_kernel) and the CG dims' passes read it through their
+    // permutations; otherwise the primary's in-order segment pass stores it.
+    const int writer = schur ? -1 : p;
     if (schur) {
         for (int d : cg) {
             SlopeDim& D = dims[d];
@@ -2915,6 +2922,38 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
             B_LAUNCHED();
         }
     }
+    // Schur gather: the primary groups spread over several chunks, and their chunks
+    int32_t *multi_groups = nullptr, *multi_chunks = nullptr;
+    int n_multi_groups = 0, n_multi_chunks = 0;
+    if (schur) {
+        const SlopeDim& P = dims[p];
+        int32_t *flag, *idx;
+        const int64_t m = std::max<int64_t>(P.G, P.nch);
+        B_CHECK(get_buf(ctx, "sl_mflag", m, &flag));
+        B_CHECK(get_buf(ctx, "sl_midx", m, &idx));
+        for (int pass = 0; pass < 2; ++pass) {
+            const int64_t cnt = pass == 0 ? P.G : P.nch;
+            multi_chunk_flags_kernel<<<grid_for(ctx, cnt, T), T, 0, s>>>(
+                P.grp_ch, pass == 0 ? nullptr : p_ch_grp, cnt, flag);
+            B_LAUNCHED();
+            B_CHECK(cub_exclusive_sum(ctx, flag, idx, cnt));
+            int hv[2];
+            B_CHECK(sync_read_int(ctx, idx + (cnt - 1), 1, &hv[0]));
+            B_CHECK(sync_read_int(ctx, flag + (cnt - 1), 1, &hv[1]));
+            const int total = hv[0] + hv[1];
+            int32_t* list;
+            B_CHECK(get_buf(ctx, pass == 0 ? "sl_mgroups" : "sl_mchunks", total, &list));
+            compact_kernel<<<grid_for(ctx, cnt, T), T, 0, s>>>(flag, idx, cnt, list);
+            B_LAUNCHED();
+            if (pass == 0) {
+                multi_groups = list;
+                n_multi_groups = total;
+            } else {
+                multi_chunks = list;
+                n_multi_chunks = total;
+            }
+        }
+    }
     // ---- input norms and stop thresholds
     const int gN = grid_for(ctx, (n + RB - 1) / RB, 1, 8);
     double *pw, *pu;
@@ -2949,7 +2988,11 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     B_CHECK(get_buf(ctx, "sl_pg", static_cast<size_t>(ndt + 1) * stride * C, &pg));
     B_CHECK(get_buf(ctx, "sl_pn", static_cast<size_t>(ndt + 1) * stride * C, &pn));
     const int gG = gN;
-    B_CHECK(get_buf(ctx, "sl_pq", static_cast<size_t>(gG) * C, &pq));
+    const int gS = schur ? grid_for(ctx, static_cast<int64_t>(dims[p].nch) * 32, T, 16) : 0;
+    const int gF = n_multi_chunks ? grid_for(ctx, static_cast<int64_t>(n_multi_chunks) * 32, T, 16) : 0;
+    double* pq2;
+    B_CHECK(get_buf(ctx, "sl_pq", static_cast<size_t>(std::max(gG, gS)) * C, &pq));
+    B_CHECK(get_buf(ctx, "sl_pq2", static_cast<size_t>(std::max(gF, 1)) * C, &pq2));
     setup_scope.reset();
     B_TRY(cudaEventRecord(e1, s));
     // algorithmic bytes per launch (profile categories)
@@ -2982,12 +3025,12 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         a.C = C;
         a.slots = CW == 1 ? 32 / C : 1;
         a.R = X ? const_cast<double*>(X) : R;
-        a.Q = !X && update && p >= 0 ? Q : nullptr;  // without a primary, R is updated first
+        a.Q = !X && update && writer >= 0 ? Q : nullptr;  // else R was updated first
         a.alpha = alpha;
         a.w = w;
         a.write = !X && update && d == writer;
         const int g = grid_for(ctx, static_cast<int64_t>(dims[d].nch) * 32, T, 16);
-        ProfScope ps(ctx, B200FE_PROF_PASS, seg_bytes(d, update && !X, a.write != 0));
+        ProfScope ps(ctx, B200FE_PROF_PASS, seg_bytes(d, a.Q != nullptr, a.write != 0));
         if (CW == 1) slope_segment_kernel<1><<<g, T, 0, s>>>(a);
         else if (CW == 2) slope_segment_kernel<2><<<g, T, 0, s>>>(a);
         else if (CW == 4) slope_segment_kernel<4><<<g, T, 0, s>>>(a);
@@ -3015,7 +3058,7 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         return B200FE_OK;
     };
     auto gradient = [&](bool update, bool init) -> int {
-        if (update && p < 0) {
+        if (update && writer < 0) {
             ProfScope ps(ctx, B200FE_PROF_VECTOR, 24.0 * n * C);
             slope_update_kernel<<<grid_for(ctx, n * C, T), T, 0, s>>>(R, Q, alpha, n, C);
             B_LAUNCHED();
@@ -3073,6 +3116,71 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         ga.gi.p = dims[nd].p;
     }
 
+    // Schur form: Q = (I - P_p) D_r p, fused for single-chunk primary groups
+    SchurGatherArgs sga{};
+    if (schur) {
+        sga.nd = 0;
+        for (int d : cg) sga.dim[sga.nd++] = dims[d];
+        const SlopeDim& P = dims[p];
+        sga.ch_beg = P.ch_beg;
+        sga.ch_end = P.ch_end;
+        sga.ch_grp = p_ch_grp;
+        sga.grp_ch = P.grp_ch;
+        sga.minv_p = P.minv;
+        sga.nch = P.nch;
+        sga.part_p = P.part;
+        sga.n = n;
+        sga.C = C;
+        sga.slots = CW == 1 ? 32 / C : 1;
+        sga.w = w;
+        sga.Q = Q;
+        sga.dpart = pq;
+    }
+    auto schur_gather = [&]() -> int {
+        {
+            ProfScope ps(ctx, B200FE_PROF_GATHER, gather_bytes);
+            if (CW == 1) {
+                if (sga.nd == 1) schur_gather_kernel<1, 1><<<gS, T, 0, s>>>(sga);
+                else if (sga.nd == 2) schur_gather_kernel<1, 2><<<gS, T, 0, s>>>(sga);
+                else if (sga.nd == 3) schur_gather_kernel<1, 3><<<gS, T, 0, s>>>(sga);
+                else schur_gather_kernel<1, 0><<<gS, T, 0, s>>>(sga);
+            } else if (CW == 2) {
+                schur_gather_kernel<2, 0><<<gS, T, 0, s>>>(sga);
+            } else if (CW == 4) {
+                schur_gather_kernel<4, 0><<<gS, T, 0, s>>>(sga);
+            } else {
+                schur_gather_kernel<8, 0><<<gS, T, 0, s>>>(sga);
+            }
+            B_LAUNCHED();
+        }
+        if (n_multi_chunks) {
+            ProfScope ps(ctx, B200FE_PROF_FINALIZE, 0.0);
+            schur_fix_mean_kernel<<<grid_for(ctx, static_cast<int64_t>(n_multi_groups) * C, T), T, 0, s>>>(
+                multi_groups, n_multi_groups, dims[p].grp_ch, dims[p].part, dims[p].minv, C,
+                dims[p].zv);
+            B_LAUNCHED();
+            const int S = CW == 1 ? 32 / C : 1;
+            if (CW == 1)
+                schur_fix_apply_kernel<1><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, dims[p].ch_beg,
+                                                            dims[p].ch_end, p_ch_grp, dims[p].zv, w, Q,
+                                                            C, S, pq2);
+            else if (CW == 2)
+                schur_fix_apply_kernel<2><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, dims[p].ch_beg,
+                                                            dims[p].ch_end, p_ch_grp, dims[p].zv, w, Q,
+                                                            C, S, pq2);
+            else if (CW == 4)
+                schur_fix_apply_kernel<4><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, dims[p].ch_beg,
+                                                            dims[p].ch_end, p_ch_grp, dims[p].zv, w, Q,
+                                                            C, S, pq2);
+            else
+                schur_fix_apply_kernel<8><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, dims[p].ch_beg,
+                                                            dims[p].ch_end, p_ch_grp, dims[p].zv, w, Q,
+                                                            C, S, pq2);
+            B_LAUNCHED();
+        }
+        return B200FE_OK;
+    };
+
     if (schur) B_CHECK(project(R, false));
     B_CHECK(gradient(false, true));
     const int ci = std::max(1, o.check_interval);
@@ -3082,15 +3190,17 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     while (!hd && it < max_it) {
         const int steps = std::min(ci, max_it - it);
         for (int k = 0; k < steps; ++k) {
-            {
+            if (schur) {
+                B_CHECK(schur_gather());
+            } else {
                 ProfScope ps(ctx, B200FE_PROF_GATHER, gather_bytes);
                 slope_gather_kernel<<<gG, C * RB, 0, s>>>(ga);
                 B_LAUNCHED();
             }
-            if (schur) B_CHECK(project(Q, true));
             {
                 ProfScope ps(ctx, B200FE_PROF_VECTOR, 0.0);
-                slope_alpha_kernel<<<1, T, 0, s>>>(pq, gG, C, gamma, active, alpha);
+                slope_alpha_kernel<<<1, T, 0, s>>>(pq, schur ? gS : gG, pq2, schur ? gF : 0, C,
+                                                   gamma, active, alpha);
                 B_LAUNCHED();
             }
             B_CHECK(gradient(true, false));

@@ -78,7 +78,8 @@ __global__ void slope_chunk_count_kernel(const int32_t* __restrict__ off, int32_
 
 __global__ void slope_chunk_fill_kernel(const int32_t* __restrict__ off, int32_t G,
                                         const int32_t* __restrict__ grp_ch,
-                                        int32_t* __restrict__ ch_beg, int32_t* __restrict__ ch_end) {
+                                        int32_t* __restrict__ ch_beg, int32_t* __restrict__ ch_end,
+                                        int32_t* __restrict__ ch_grp) {
     for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
          g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int32_t b = off[g], e = off[g + 1];
@@ -88,6 +89,7 @@ __global__ void slope_chunk_fill_kernel(const int32_t* __restrict__ off, int32_t
         for (int32_t i = 0; i < nc; ++i) {
             ch_beg[c0 + i] = min(e, b + i * L);
             ch_end[c0 + i] = min(e, b + (i + 1) * L);
+            if (ch_grp) ch_grp[c0 + i] = static_cast<int32_t>(g);
         }
     }
 }
@@ -298,13 +300,16 @@ slope_gather_kernel(const SlopeGatherArgs a) {
     column_reduce(red, acc, C, a.RB, a.part + static_cast<int64_t>(blockIdx.x) * C);
 }
 
-// alpha_c = gamma_c / (q' W q)_c for the columns still iterating
-__global__ void slope_alpha_kernel(const double* __restrict__ part, int nparts, int C,
+// alpha_c = gamma_c / (q' W q)_c for the columns still iterating; the dots
+// come as CTA partials of one or two kernels, summed in order
+__global__ void slope_alpha_kernel(const double* __restrict__ part, int nparts,
+                                   const double* __restrict__ part2, int nparts2, int C,
                                    const double* __restrict__ gamma, const int* __restrict__ active,
                                    double* __restrict__ alpha) {
     for (int c = threadIdx.x; c < C; c += blockDim.x) {
         double dl = 0.0;
         for (int b = 0; b < nparts; ++b) dl += part[static_cast<int64_t>(b) * C + c];
+        for (int b = 0; b < nparts2; ++b) dl += part2[static_cast<int64_t>(b) * C + c];
         alpha[c] = (active[c] && dl > 0.0) ? gamma[c] / dl : 0.0;
     }
 }
@@ -658,6 +663,269 @@ slope_project_kernel(double* __restrict__ X, const int32_t* __restrict__ ids_p,
         }
     }
     if (part) column_reduce(red, acc, C, RB, part + static_cast<int64_t>(blockIdx.x) * C);
+}
+
+// ---------------------------------------------------------------------------
+// Schur-form image Q = (I - P_p) D_r p in one pass for the primary groups held
+// by a single chunk (every primary group of at most 64 rows): a warp forms the
+// rows of D_r p, sums w q per column over the group, and forms the rows again
+// (the same loads, the same order, so the same values) to store q - mean and
+// accumulate q' W q.  Rows of groups spread over several chunks are stored
+// raw with their chunk sums, and schur_fix_mean_kernel /
+// schur_fix_apply_kernel finish them.
+// ---------------------------------------------------------------------------
+struct SchurGatherArgs {
+    int nd;
+    SlopeDim dim[8];          // the CG dimensions (all but the primary)
+    const int32_t* ch_beg;    // primary chunks
+    const int32_t* ch_end;
+    const int32_t* ch_grp;    // primary chunk -> group
+    const int32_t* grp_ch;    // primary group -> first chunk
+    const double* minv_p;     // [Gp][3], m00 = 1 / W
+    int32_t nch;
+    double* part_p;           // [nch][C] sums of w q of multi-chunk groups' chunks
+    int64_t n;
+    int C, slots;
+    const double* w;
+    double* Q;
+    double* dpart;            // [grid][C] sums of w q'^2 of the single-chunk groups
+};
+
+// (D_r p)_k for column c; ND > 0 unrolls the dimension loop (the
+// descriptors then load once per kernel), ND == 0 loops over a.nd
+template <int ND>
+__device__ __forceinline__ double schur_q(const SchurGatherArgs& a, int64_t k, int c) {
+    double q = 0.0;
+#pragma unroll
+    for (int d = 0; d < (ND > 0 ? ND : 8); ++d) {
+        if (ND == 0 && d >= a.nd) break;
+        const SlopeDim& D = a.dim[d];
+        const int64_t base = (static_cast<int64_t>(D.ids[k]) * D.nb) * a.C + c;
+        if (D.has_a) q += D.p[base];
+        if (D.has_b) q = fma(D.z[k], D.p[base + (D.has_a ? a.C : 0)], q);
+    }
+    return q;
+}
+
+template <int CW, int ND>
+__global__ void __launch_bounds__(kSlopeThreads)
+schur_gather_kernel(const SchurGatherArgs a) {
+    constexpr int kSchurRows = CW == 1 ? 8 : (CW == 2 ? 4 : (CW == 4 ? 2 : 1));
+    __shared__ double sred[kSlopeThreads / 32][32];
+    __shared__ double dred[kSlopeThreads / 32][32 * CW];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int C = a.C;
+    const int S = a.slots;
+    const int slot = CW == 1 ? lane / C : 0;
+    const int col0 = CW == 1 ? lane - slot * C : lane;
+    const bool live = CW == 1 ? slot < S : true;
+    double dacc[CW];
+#pragma unroll
+    for (int u = 0; u < CW; ++u) dacc[u] = 0.0;
+    const int64_t nw = static_cast<int64_t>(gridDim.x) * (kSlopeThreads / 32);
+    for (int64_t j = static_cast<int64_t>(blockIdx.x) * (kSlopeThreads / 32) + wid; j < a.nch;
+         j += nw) {
+        const int32_t b = a.ch_beg[j], e = a.ch_end[j], g = a.ch_grp[j];
+        const bool single = a.grp_ch[g + 1] - a.grp_ch[g] == 1;
+        double sw[CW];
+#pragma unroll
+        for (int u = 0; u < CW; ++u) sw[u] = 0.0;
+        // the lane's first kSchurRows rows: formed together (their loads in
+        // flight at once) and kept in registers for the second phase
+        double qc[kSchurRows][CW];
+        if (live) {
+#pragma unroll
+            for (int t = 0; t < kSchurRows; ++t) {
+                const int32_t pos = b + slot + t * S;
+#pragma unroll
+                for (int u = 0; u < CW; ++u) {
+                    const int c = col0 + 32 * u;
+                    qc[t][u] = (pos < e && c < C) ? schur_q<ND>(a, pos, c) : 0.0;
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < kSchurRows; ++t) {
+                const int32_t pos = b + slot + t * S;
+                if (pos < e) {
+                    const double wk = a.w ? a.w[pos] : 1.0;
+#pragma unroll
+                    for (int u = 0; u < CW; ++u) {
+                        const int c = col0 + 32 * u;
+                        if (c < C) {
+                            sw[u] = fma(wk, qc[t][u], sw[u]);
+                            if (!single) a.Q[static_cast<int64_t>(pos) * C + c] = qc[t][u];
+                        }
+                    }
+                }
+            }
+            for (int32_t pos = b + slot + kSchurRows * S; pos < e; pos += S) {
+                const double wk = a.w ? a.w[pos] : 1.0;
+#pragma unroll
+                for (int u = 0; u < CW; ++u) {
+                    const int c = col0 + 32 * u;
+                    if (c < C) {
+                        const double q = schur_q<ND>(a, pos, c);
+                        sw[u] = fma(wk, q, sw[u]);
+                        if (!single) a.Q[static_cast<int64_t>(pos) * C + c] = q;
+                    }
+                }
+            }
+        }
+        // column totals over the row slots, in slot order, seen by every lane
+        double tot[CW];
+        if (CW == 1) {
+            sred[wid][lane] = sw[0];
+            __syncwarp();
+            double t = 0.0;
+            if (live && col0 < C)
+                for (int sl = 0; sl < S; ++sl) t += sred[wid][sl * C + col0];
+            tot[0] = t;
+            __syncwarp();
+        } else {
+#pragma unroll
+            for (int u = 0; u < CW; ++u) tot[u] = sw[u];
+        }
+        if (single) {
+            const double iw = a.minv_p[static_cast<int64_t>(g) * 3];
+            if (live) {
+                for (int32_t t = 0, pos = b + slot; pos < e; ++t, pos += S) {
+                    const double wk = a.w ? a.w[pos] : 1.0;
+#pragma unroll
+                    for (int u = 0; u < CW; ++u) {
+                        const int c = col0 + 32 * u;
+                        if (c < C) {
+                            double q = 0.0;
+                            if (t < kSchurRows) {
+#pragma unroll
+                                for (int tt = 0; tt < kSchurRows; ++tt)
+                                    if (tt == t) q = qc[tt][u];
+                            } else {
+                                q = schur_q<ND>(a, pos, c);
+                            }
+                            const double x = q - tot[u] * iw;
+                            a.Q[static_cast<int64_t>(pos) * C + c] = x;
+                            dacc[u] = fma(wk * x, x, dacc[u]);
+                        }
+                    }
+                }
+            }
+        } else if (slot == 0) {
+#pragma unroll
+            for (int u = 0; u < CW; ++u) {
+                const int c = col0 + 32 * u;
+                if (c < C) a.part_p[j * C + c] = tot[u];
+            }
+        }
+    }
+    // CTA partials of q' W q per column: warps, then row slots, in order
+#pragma unroll
+    for (int u = 0; u < CW; ++u) dred[wid][lane + 32 * u] = dacc[u];
+    __syncthreads();
+    if (static_cast<int>(threadIdx.x) < C) {
+        const int c = threadIdx.x;
+        double t = 0.0;
+        for (int w8 = 0; w8 < kSlopeThreads / 32; ++w8) {
+            if (CW == 1) {
+                for (int sl = 0; sl < S; ++sl) t += dred[w8][sl * C + c];
+            } else {
+                t += dred[w8][c];
+            }
+        }
+        a.dpart[static_cast<int64_t>(blockIdx.x) * C + c] = t;
+    }
+}
+
+// mean[g] = (sum of g's chunk sums, in chunk order) / W_g for the listed
+// multi-chunk primary groups, into mean_p[g][C]
+__global__ void schur_fix_mean_kernel(const int32_t* __restrict__ groups, int32_t ngroups,
+                                      const int32_t* __restrict__ grp_ch,
+                                      const double* __restrict__ part_p,
+                                      const double* __restrict__ minv_p, int C,
+                                      double* __restrict__ mean_p) {
+    const int64_t total = static_cast<int64_t>(ngroups) * C;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t i = e / C;
+        const int c = static_cast<int>(e - i * C);
+        const int32_t g = groups[i];
+        double s = 0.0;
+        for (int32_t j = grp_ch[g]; j < grp_ch[g + 1]; ++j) s += part_p[static_cast<int64_t>(j) * C + c];
+        mean_p[static_cast<int64_t>(g) * C + c] = s * minv_p[static_cast<int64_t>(g) * 3];
+    }
+}
+
+// Q -= mean over the rows of the listed chunks (multi-chunk groups), with CTA
+// partials of q' W q; one warp per chunk, row slots as in the gather
+template <int CW>
+__global__ void __launch_bounds__(kSlopeThreads)
+schur_fix_apply_kernel(const int32_t* __restrict__ chunks, int32_t nchunks,
+                       const int32_t* __restrict__ ch_beg, const int32_t* __restrict__ ch_end,
+                       const int32_t* __restrict__ ch_grp, const double* __restrict__ mean_p,
+                       const double* __restrict__ w, double* __restrict__ Q, int C, int S,
+                       double* __restrict__ dpart) {
+    __shared__ double dred[kSlopeThreads / 32][32 * CW];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int slot = CW == 1 ? lane / C : 0;
+    const int col0 = CW == 1 ? lane - slot * C : lane;
+    const bool live = CW == 1 ? slot < S : true;
+    double dacc[CW];
+#pragma unroll
+    for (int u = 0; u < CW; ++u) dacc[u] = 0.0;
+    const int64_t nw = static_cast<int64_t>(gridDim.x) * (kSlopeThreads / 32);
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * (kSlopeThreads / 32) + wid; i < nchunks;
+         i += nw) {
+        if (!live) continue;
+        const int32_t j = chunks[i];
+        const int32_t g = ch_grp[j];
+        for (int32_t pos = ch_beg[j] + slot; pos < ch_end[j]; pos += S) {
+            const double wk = w ? w[pos] : 1.0;
+#pragma unroll
+            for (int u = 0; u < CW; ++u) {
+                const int c = col0 + 32 * u;
+                if (c < C) {
+                    const int64_t o = static_cast<int64_t>(pos) * C + c;
+                    const double x = Q[o] - mean_p[static_cast<int64_t>(g) * C + c];
+                    Q[o] = x;
+                    dacc[u] = fma(wk * x, x, dacc[u]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < CW; ++u) dred[wid][lane + 32 * u] = dacc[u];
+    __syncthreads();
+    if (static_cast<int>(threadIdx.x) < C) {
+        const int c = threadIdx.x;
+        double t = 0.0;
+        for (int w8 = 0; w8 < kSlopeThreads / 32; ++w8) {
+            if (CW == 1) {
+                for (int sl = 0; sl < S; ++sl) t += dred[w8][sl * C + c];
+            } else {
+                t += dred[w8][c];
+            }
+        }
+        dpart[static_cast<int64_t>(blockIdx.x) * C + c] = t;
+    }
+}
+
+// flag[i] = 1 where a group holds more than one chunk (groups) or a chunk
+// belongs to such a group (chunks, ch_grp given)
+__global__ void multi_chunk_flags_kernel(const int32_t* __restrict__ grp_ch,
+                                         const int32_t* __restrict__ ch_grp, int64_t m,
+                                         int32_t* __restrict__ flag) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t g = ch_grp ? ch_grp[i] : i;
+        flag[i] = grp_ch[g + 1] - grp_ch[g] > 1 ? 1 : 0;
+    }
+}
+
+// list[idx[i]] = i where flag[i] (idx: exclusive scan of the flags)
+__global__ void compact_kernel(const int32_t* __restrict__ flag, const int32_t* __restrict__ idx,
+                               int64_t m, int32_t* __restrict__ list) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        if (flag[i]) list[idx[i]] = static_cast<int32_t>(i);
 }
 
 // p = zv + beta p (p = zv where beta is 0, so p needs no initial value)
