@@ -3194,7 +3194,10 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
                 B_CHECK(schur_gather());
             } else {
                 ProfScope ps(ctx, B200FE_PROF_GATHER, gather_bytes);
-                slope_gather_kernel<<<gG, C * RB, 0, s>>>(ga);
+                if (ga.nd == 1) slope_gather_kernel<1><<<gG, C * RB, 0, s>>>(ga);
+                else if (ga.nd == 2) slope_gather_kernel<2><<<gG, C * RB, 0, s>>>(ga);
+                else if (ga.nd == 3) slope_gather_kernel<3><<<gG, C * RB, 0, s>>>(ga);
+                else slope_gather_kernel<0><<<gG, C * RB, 0, s>>>(ga);
                 B_LAUNCHED();
             }
             {

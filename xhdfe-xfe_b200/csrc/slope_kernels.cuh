@@ -269,7 +269,9 @@ struct SlopeGatherArgs {
     double* part;  // [grid][C] sums of w q^2
 };
 
-// Q = D p, with CTA partials of q' W q per column.
+// Q = D p, with CTA partials of q' W q per column.  ND > 0 unrolls the
+// dimension loop (descriptors load once), ND == 0 loops over a.nd.
+template <int ND>
 __global__ void __launch_bounds__(kSlopeThreads)
 slope_gather_kernel(const SlopeGatherArgs a) {
     __shared__ double red[kSlopeThreads];
@@ -280,7 +282,9 @@ slope_gather_kernel(const SlopeGatherArgs a) {
         for (int64_t k = static_cast<int64_t>(blockIdx.x) * a.RB + rr; k < a.n;
              k += static_cast<int64_t>(gridDim.x) * a.RB) {
             double q = 0.0;
-            for (int d = 0; d < a.nd; ++d) {
+#pragma unroll
+            for (int d = 0; d < (ND > 0 ? ND : 8); ++d) {
+                if (ND == 0 && d >= a.nd) break;
                 const SlopeDim& D = a.dim[d];
                 const int64_t base = (static_cast<int64_t>(D.ids[k]) * D.nb) * C + col;
                 if (D.has_a) q += D.p[base];
