@@ -10,8 +10,9 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
-SOURCES = ["b200fe.cu", "noalloc.cu", "kss.cu"]
-HEADERS = ["kernels.cuh", "setup_kernels.cuh", "ols_kernels.cuh", "prep_kernels.cuh", "slope_kernels.cuh"]
+SOURCES = ["b200fe.cu", "slopes.cu", "noalloc.cu", "kss.cu"]
+HEADERS = ["limits.cuh", "context.cuh", "common_kernels.cuh", "kernels.cuh", "setup_kernels.cuh",
+           "ols_kernels.cuh", "prep_kernels.cuh", "slope_kernels.cuh"]
 OUT = HERE / "libb200fe.so"
 
 NVCC_FLAGS = [

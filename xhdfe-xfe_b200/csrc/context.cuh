@@ -1,0 +1,354 @@
+// Internal to the library (not installed): the context every entry point
+// works on, its grow-only device workspace, the FE structure of the main
+// solver, and the host helpers the translation units share (error macros,
+// workspace buffers, grid sizing, CUB calls, event profiling).
+
+#pragma once
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
+#include <cub/device/device_segmented_reduce.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <cstdlib>
+#include <limits>
+#include <memory>
+#include <type_traits>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "b200fe.h"
+#include "limits.cuh"
+
+namespace b200fe_host {
+
+using namespace b200fe;
+
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct LargeDim {
+    int dim = -1;
+    int32_t G = 0;
+    int64_t nruns = 0;
+    int64_t nchunks = 0;
+    int64_t nmulti = 0;
+    int32_t *rid = nullptr, *run_base = nullptr, *run_dest = nullptr, *run_start = nullptr;
+    int32_t* run_grp = nullptr;
+    double* cw_run = nullptr;
+    int32_t *chunk_grp = nullptr, *chunk_beg = nullptr, *chunk_end = nullptr;
+    uint8_t* chunk_whole = nullptr;
+    int32_t *multi_grp = nullptr, *multi_c0 = nullptr, *multi_c1 = nullptr;
+    // second reduction level for groups of more than kFinFewParts chunks:
+    // super-chunks of at most kSuperParts chunk partials
+    int64_t nsup = 0;
+    int32_t *multi_s0 = nullptr, *multi_s1 = nullptr;  // [nmulti] super range (empty: none)
+    int32_t *sup_c0 = nullptr, *sup_c1 = nullptr;      // [nsup] chunk range of each super-chunk
+};
+
+struct Structure {
+    bool valid = false;
+    int64_t n = 0;
+    int D = 0;
+    int p = 0;
+    int32_t G[B200FE_MAX_DIMS] = {0};
+    int32_t present[B200FE_MAX_DIMS] = {0};
+    int nL = 0, nS = 0;
+    LargeDim L[kMaxLarge];
+    int sdim[kMaxSmall] = {0};
+    int32_t sG[kMaxSmall] = {0};
+    int64_t lbase[kMaxLarge] = {0};
+    int64_t sbase[kMaxSmall] = {0};
+    int64_t GR = 0;
+    bool weighted = false;
+    double sum_w2 = 0.0;
+    int32_t* pord = nullptr;
+    int32_t* seg_off = nullptr;
+    double* inv_wp = nullptr;
+    double* wp64 = nullptr;
+    float* wp32 = nullptr;
+    uint32_t* sid = nullptr;
+    double* dinv64 = nullptr;
+    float* dinv32 = nullptr;
+    int32_t* gp = nullptr;  // primary ids in primary order (setup only)
+    int SG = 0;             // bin rows over all small dims
+    int sgoff[kMaxSmall] = {0};
+    int32_t* tile_seg = nullptr;
+    uint8_t* tile_long = nullptr;
+    int64_t ntiles = 0;
+    int32_t* long_segs = nullptr;
+    int64_t nlong = 0;
+    // block-level pass metadata (at most one large and one small dim)
+    bool block_ok = false;
+    int2* seg_meta = nullptr;
+    int4* run_meta = nullptr;
+    double* run_w64 = nullptr;
+    float* run_w32 = nullptr;
+    int2* block_meta = nullptr;
+    double* block_w64 = nullptr;
+    float* block_w32 = nullptr;
+    int64_t nblocks = 0;
+    double* small_w = nullptr;  // [SG] level weights of the small dim
+    // dense coupling of the small dim (block level, one small dim): the CG
+    // matvec then runs the block pass over the large dim only and adds
+    // C_fy x_small, C_fy' x_f and C_yy x_small
+    bool coupled = false;
+    int SGP = 0;              // row stride of cfy: SG rounded up to 4 (padding zero)
+    double* cfy64 = nullptr;  // [G_f][SGP]
+    float* cfy32 = nullptr;
+    double* cyy = nullptr;    // [SG][SG]
+};
+
+constexpr int32_t kChunkRuns = 64;
+
+}  // namespace b200fe_host
+
+struct b200fe_context {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::unordered_map<std::string, b200fe_host::Buf> bufs;
+    b200fe_host::Structure st;
+    long long launches = 0;
+    long long lib_calls = 0;
+    int* h_pinned = nullptr;     // small pinned scratch
+    double* h_pinned_d = nullptr;
+    // opt-in event profiler (b200fe_options.profile)
+    struct ProfRec {
+        cudaEvent_t a, b;
+        int cat;
+        double bytes;
+    };
+    bool profiling = false;
+    int pass_kernel = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<ProfRec> prof;
+    // saved FEs: device outputs per dim ([G_d][cols] column-major) while a
+    // b200fe_absorb_fe call runs, and the first column of the current block
+    double* fe_dev[B200FE_MAX_DIMS] = {nullptr};
+    int fe_cols = 0;
+    int fe_c0 = 0;
+};
+
+namespace b200fe_host {
+
+using namespace b200fe;
+
+#define B_TRY(expr)                                                              \
+    do {                                                                         \
+        cudaError_t e_ = (expr);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            ctx->err = std::string(#expr) + ": " + cudaGetErrorString(e_);       \
+            return B200FE_CUDA_ERROR;                                            \
+        }                                                                        \
+    } while (0)
+
+#define B_LAUNCHED()                                                             \
+    do {                                                                         \
+        ++ctx->launches;                                                         \
+        cudaError_t e_ = cudaGetLastError();                                     \
+        if (e_ != cudaSuccess) {                                                 \
+            ctx->err = std::string("kernel launch: ") + cudaGetErrorString(e_);  \
+            return B200FE_CUDA_ERROR;                                            \
+        }                                                                        \
+    } while (0)
+
+#define B_CHECK(...)                                                             \
+    do {                                                                         \
+        int rc_ = (__VA_ARGS__);                                                        \
+        if (rc_ != B200FE_OK) return rc_;                                        \
+    } while (0)
+
+// Debug aid: B200FE_POISON=<substring> fills newly allocated floating-point
+// workspace whose name contains the substring ("*" for all) with NaN bytes,
+// so a read before the first write shows up as a NaN.  Index arrays are never
+// poisoned.
+inline const char* poison_filter() {
+    static const char* f = std::getenv("B200FE_POISON");
+    return f;
+}
+
+template <typename T>
+inline int get_buf(b200fe_context* ctx, const std::string& name, size_t count, T** out) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    bytes = (bytes + 255) & ~size_t(255);
+    Buf& b = ctx->bufs[name];
+    if (b.bytes < bytes) {
+        if (b.p) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(b.p);
+            b.p = nullptr;
+            b.bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&b.p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ctx->err = "cudaMalloc(" + name + ", " + std::to_string(bytes) + " B): " +
+                       cudaGetErrorString(e);
+            return B200FE_CUDA_ERROR;
+        }
+        b.bytes = bytes;
+        const char* pf = poison_filter();
+        if (pf && (std::is_same<T, double>::value || std::is_same<T, float>::value) &&
+            (std::strcmp(pf, "*") == 0 || name.find(pf) != std::string::npos)) {
+            cudaMemsetAsync(b.p, 0xff, bytes, ctx->stream);
+            cudaStreamSynchronize(ctx->stream);
+        }
+    }
+    *out = static_cast<T*>(b.p);
+    return B200FE_OK;
+}
+
+inline int grid_for(b200fe_context* ctx, int64_t work, int threads, int per_sm = 8) {
+    int64_t g = (work + threads - 1) / threads;
+    g = std::max<int64_t>(1, std::min<int64_t>(g, static_cast<int64_t>(ctx->num_sms) * per_sm));
+    return static_cast<int>(g);
+}
+
+// Records a CUDA-event interval on the context stream around a scope when
+// profiling is on; the bytes are the launches' algorithmic traffic.
+struct ProfScope {
+    b200fe_context* ctx;
+    int cat;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    static cudaEvent_t event(b200fe_context* c) {
+        if (c->ev_used < c->ev_pool.size()) return c->ev_pool[c->ev_used++];
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        c->ev_pool.push_back(e);
+        ++c->ev_used;
+        return e;
+    }
+    ProfScope(b200fe_context* c, int category, double b) : ctx(c), cat(category), bytes(b) {
+        if (ctx->profiling) {
+            a = event(ctx);
+            if (a) cudaEventRecord(a, ctx->stream);
+        }
+    }
+    ~ProfScope() {
+        if (ctx->profiling && a) {
+            cudaEvent_t b = event(ctx);
+            if (b) {
+                cudaEventRecord(b, ctx->stream);
+                ctx->prof.push_back({a, b, cat, bytes});
+            }
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// CUB helpers (setup only)
+// ---------------------------------------------------------------------------
+inline int cub_exclusive_sum(b200fe_context* ctx, const int32_t* in, int32_t* out, int64_t n) {
+    size_t tmp = 0;
+    B_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, ctx->stream));
+    void* t;
+    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+    B_TRY(cub::DeviceScan::ExclusiveSum(t, tmp, in, out, n, ctx->stream));
+    ++ctx->lib_calls;
+    return B200FE_OK;
+}
+
+inline int cub_inclusive_sum(b200fe_context* ctx, const int32_t* in, int32_t* out, int64_t n) {
+    size_t tmp = 0;
+    B_TRY(cub::DeviceScan::InclusiveSum(nullptr, tmp, in, out, n, ctx->stream));
+    void* t;
+    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+    B_TRY(cub::DeviceScan::InclusiveSum(t, tmp, in, out, n, ctx->stream));
+    ++ctx->lib_calls;
+    return B200FE_OK;
+}
+
+inline int bits_for(int32_t G) {
+    int b = 1;
+    while (b < 31 && (int64_t(1) << b) < G) ++b;
+    return b;
+}
+
+// Stable sort of (key, value) pairs by key.
+inline int cub_sort_pairs(b200fe_context* ctx, const int32_t* keys_in, int32_t* keys_out,
+                   const int32_t* vals_in, int32_t* vals_out, int64_t n, int32_t G) {
+    size_t tmp = 0;
+    const uint32_t* ki = reinterpret_cast<const uint32_t*>(keys_in);
+    uint32_t* ko = reinterpret_cast<uint32_t*>(keys_out);
+    const int eb = bits_for(G);
+    B_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ki, ko, vals_in, vals_out, n, 0, eb,
+                                          ctx->stream));
+    void* t;
+    B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+    B_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, ki, ko, vals_in, vals_out, n, 0, eb,
+                                          ctx->stream));
+    ++ctx->lib_calls;
+    return B200FE_OK;
+}
+
+inline int sync_read_int(b200fe_context* ctx, const int32_t* dptr, int count, int* host) {
+    B_TRY(cudaMemcpyAsync(ctx->h_pinned, dptr, sizeof(int) * count, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+    B_TRY(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(host, ctx->h_pinned, sizeof(int) * count);
+    return B200FE_OK;
+}
+
+inline int sync_read_double(b200fe_context* ctx, const double* dptr, int count, double* host) {
+    B_TRY(cudaMemcpyAsync(ctx->h_pinned_d, dptr, sizeof(double) * count,
+                          cudaMemcpyDeviceToHost, ctx->stream));
+    B_TRY(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(host, ctx->h_pinned_d, sizeof(double) * count);
+    return B200FE_OK;
+}
+
+inline int check_common(b200fe_context* ctx, int64_t n, int cols, int num_dims, const int32_t* G) {
+    if (!ctx) return B200FE_INVALID_ARG;
+    if (n <= 0 || n >= (int64_t(1) << 31) - 1) {
+        ctx->err = "n must be in [1, 2^31-2]";
+        return B200FE_INVALID_ARG;
+    }
+    if (cols <= 0) {
+        ctx->err = "need at least one column";
+        return B200FE_INVALID_ARG;
+    }
+    if (num_dims < 0 || num_dims > B200FE_MAX_DIMS) {
+        ctx->err = "num_dims must be in [0, 8]";
+        return B200FE_INVALID_ARG;
+    }
+    for (int d = 0; d < num_dims; ++d) {
+        if (!G || G[d] <= 0) {
+            ctx->err = "num_groups must be positive";
+            return B200FE_INVALID_ARG;
+        }
+    }
+    return B200FE_OK;
+}
+inline double tol_eff(const b200fe_options& o) {
+    if (o.tol > 0.0 && o.tolerance_mode == 1) return std::min(o.tol, 1e-9);
+    return o.tol;
+}
+inline float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.0f;
+    }
+    return ms;
+}
+inline void clear_result(b200fe_result* r) {
+    std::memset(r, 0, sizeof(*r));
+    r->primary_dim = -1;
+}
+
+}  // namespace b200fe_host

@@ -35,19 +35,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "limits.cuh"
+
 namespace b200fe {
 
-constexpr int kMaxDims = 8;
-constexpr int kMaxLarge = 2;
-constexpr int kMaxSmall = 4;
-constexpr int kSmallLevels = 64;   // a non-primary dim with <= 64 levels is "small"
-constexpr int kMaxSmallRows = 128; // total levels over all small dims
-constexpr int kPassThreads = 128;  // long-segment pass CTA size (4 warps)
-constexpr int kTileThreads = 256;  // tile pass CTA size (8 warps)
-constexpr int kRowThreads = 256;   // alpha-space row kernels
-constexpr int kTileObs = 512;      // observations staged per tile
-constexpr int kTileStride = 384;   // tiles start within windows of this many obs
-constexpr int kLongSeg = kTileObs - kTileStride;  // longer segments take the long path
 
 // ---------------------------------------------------------------------------
 // 4-wide column quads.  A lane owns columns 4q..4q+3 of an alpha row.

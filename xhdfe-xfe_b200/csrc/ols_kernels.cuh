@@ -21,6 +21,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "common_kernels.cuh"
+
 namespace b200fe {
 
 constexpr int kOlsMaxP = 32;      // regressors
@@ -224,16 +226,6 @@ __global__ void cluster_combine_kernel(int64_t nmulti, const int32_t* __restrict
         for (int32_t k = multi_c0[r]; k < multi_c1[r]; ++k) s += chunk_part[static_cast<int64_t>(k) * width + j];
         scores[static_cast<int64_t>(multi_grp[r]) * width + j] = s;
     }
-}
-
-// number of non-empty clusters
-__global__ void count_nonempty_kernel(const int32_t* __restrict__ off, int32_t G, int* __restrict__ out) {
-    int c = 0;
-    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
-         g += static_cast<int64_t>(gridDim.x) * blockDim.x)
-        c += off[g + 1] > off[g] ? 1 : 0;
-    c = __reduce_add_sync(0xffffffffu, c);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);  // integer count: order-free
 }
 
 }  // namespace b200fe
