@@ -100,3 +100,31 @@ def test_reference_gi_dispatches_to_b200(oracle_mod):
     d = np.load(GOLDEN / "gi_sum1500w.npz")
     err = np.abs(g["V"][d["rows"]] - d["ref_rows"]).max(axis=0) / d["ref_colnorm"]
     assert err.max() <= REL_TOL
+
+
+def test_gi_edge_cases(absorber, pkg):
+    """An individual in no group, single-individual groups, zero weights,
+    sum aggregation without standard FEs."""
+    from oracle.slope_oracle import gi_projection
+    rng = np.random.default_rng(4)
+    ng = 400
+    sizes = rng.integers(1, 4, ng)
+    eg = np.repeat(np.arange(ng), sizes)
+    ei = np.concatenate([rng.choice(60, s, replace=False) for s in sizes])
+    gi, _, _ = pkg.build_group_individual(eg, ei, "sum")
+    # append an individual that no group holds
+    gi = pkg.GroupIndividualStructure(gi.num_groups, gi.num_individuals + 1, gi.group_ptr,
+                                      gi.group_individual,
+                                      np.append(gi.individual_ptr, gi.individual_ptr[-1]),
+                                      gi.individual_group, gi.group_scale)
+    n = gi.num_groups
+    X = rng.standard_normal((n, 2))
+    y = rng.standard_normal(n)
+    w = rng.uniform(0.5, 2.0, n)
+    w[::13] = 0.0
+    r = absorber.absorb_group_individual(y, X, [], [], gi, w, pkg.make_options(tol=1e-12))
+    V0 = np.column_stack([y, X])
+    o = gi_projection(V0, [], gi, w)
+    V = np.column_stack([r.y_tilde, r.X_tilde])
+    assert r.converged
+    assert (np.linalg.norm(V - o, axis=0) / np.linalg.norm(V0, axis=0)).max() <= 1e-9

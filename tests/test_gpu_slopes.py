@@ -242,3 +242,43 @@ def test_slopes_many_columns(absorber, pkg, panels):
     scale = np.linalg.norm(np.column_stack([p.y, X]), axis=0)
     assert Va.shape[1] == 40
     assert (np.linalg.norm(Va - Vb, axis=0) / scale).max() <= 1e-9
+
+
+def _oracle_check(absorber, pkg, y, X, fes, G, slopes, w, tol=REL_TOL * 1e-1, **kw):
+    from oracle.slope_oracle import slope_projection
+    r = absorber.absorb(y, X, [np.asarray(f, dtype=np.int32) for f in fes], G, w,
+                        _opts(pkg, 1e-12, **kw), slopes=slopes)
+    V0 = np.column_stack([y, X])
+    V = np.column_stack([r.y_tilde, r.X_tilde])
+    o = slope_projection(V0, fes, slopes, w)
+    scale = np.maximum(np.linalg.norm(V0, axis=0), 1e-300)
+    assert (np.linalg.norm(V - o, axis=0) / scale).max() <= tol
+    return r
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_slopes_edge_cases(absorber, pkg, form):
+    """Empty groups (num_groups above the ids present), zero weights, a slope
+    that is zero everywhere, a group whose slope values are constant."""
+    rng = np.random.default_rng(8)
+    n = 900
+    f1 = rng.integers(0, 150, n).astype(np.int32)
+    f2 = rng.integers(0, 20, n).astype(np.int32)
+    X = rng.standard_normal((n, 2))
+    y = rng.standard_normal(n)
+    z = rng.uniform(-2, 2, n)
+    z[f2 == 3] = 1.5                   # constant slope values in one group
+    w = rng.uniform(0.5, 2.0, n)
+    w[::17] = 0.0                      # zero weights
+    zero = np.zeros(n)
+    r = _oracle_check(absorber, pkg, y, X, [f1, f2, f2], [160, 25, 25],
+                      [(1, z, True), (2, zero, False)], w, pass_kernel=form)
+    assert r.fe_levels == [160, 25, 25]
+
+
+def test_slopes_tiny(absorber, pkg):
+    y = np.array([1.0, 2.0, 4.0, 3.0, 5.0])
+    X = np.array([[0.5], [1.0], [0.0], [2.0], [1.5]])
+    f = np.array([0, 0, 1, 1, 1], dtype=np.int32)
+    z = np.array([1.0, 2.0, 1.0, 2.0, 4.0])
+    _oracle_check(absorber, pkg, y, X, [f], [2], [(0, z, True)], None)
