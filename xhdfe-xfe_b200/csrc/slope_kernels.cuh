@@ -36,10 +36,11 @@ namespace b200fe {
 
 constexpr int kSlopeThreads = 256;
 constexpr int kSlopeChunkRows = 64;   // minimum rows per chunk
-constexpr int kSlopeMaxChunks = 1024; // chunks per group at most
+constexpr int kSlopeMaxChunks = 4096; // chunks per group at most
 constexpr int kSlopeMaxCols = 256;
 constexpr double kSlopeDetTol = 1e-12;
 constexpr int kSlopeMaxDims = 9;  // 8 FE dimensions + the individual dimension
+constexpr int kFinSerialChunks = 32;  // more chunk partials: a warp sums them first
 
 struct SlopeDim {
     const int32_t* ids;     // [n] group per observation (primary order)
@@ -52,6 +53,7 @@ struct SlopeDim {
     double* part;           // [nch][nb][C] chunk sums
     double* zv;             // [G][nb][C] preconditioned gradient
     double* p;              // [G][nb][C] search direction
+    double* big;            // [G][nb][C] chunk sums of groups with many chunks, or null
     int32_t G;
     int32_t nch;
     int has_a, has_b, nb;
@@ -417,10 +419,17 @@ slope_finalize_kernel(SlopeDim d, int C, int RB, double* __restrict__ part_g,
         for (int64_t g = static_cast<int64_t>(blockIdx.x) * RB + rr; g < d.G;
              g += static_cast<int64_t>(gridDim.x) * RB) {
             double sa = 0.0, sb = 0.0;
-            for (int32_t j = d.grp_ch[g]; j < d.grp_ch[g + 1]; ++j) {
-                const double* pj = d.part + (static_cast<int64_t>(j) * d.nb) * C + col;
-                if (d.has_a) sa += pj[0];
-                if (d.has_b) sb += pj[d.has_a ? C : 0];
+            if (d.big && d.grp_ch[g + 1] - d.grp_ch[g] > kFinSerialChunks) {
+                // summed by slope_big_reduce_kernel
+                const double* bj = d.big + (g * d.nb) * C + col;
+                if (d.has_a) sa = bj[0];
+                if (d.has_b) sb = bj[d.has_a ? C : 0];
+            } else {
+                for (int32_t j = d.grp_ch[g]; j < d.grp_ch[g + 1]; ++j) {
+                    const double* pj = d.part + (static_cast<int64_t>(j) * d.nb) * C + col;
+                    if (d.has_a) sa += pj[0];
+                    if (d.has_b) sb += pj[d.has_a ? C : 0];
+                }
             }
             const double m00 = d.minv[g * 3 + 0], m01 = d.minv[g * 3 + 1], m11 = d.minv[g * 3 + 2];
             double* zg = d.zv + (g * d.nb) * C + col;
@@ -912,15 +921,15 @@ schur_fix_apply_kernel(const int32_t* __restrict__ chunks, int32_t nchunks,
     }
 }
 
-// flag[i] = 1 where a group holds more than one chunk (groups) or a chunk
+// flag[i] = 1 where a group holds more than `above` chunks (groups) or a chunk
 // belongs to such a group (chunks, ch_grp given)
 __global__ void multi_chunk_flags_kernel(const int32_t* __restrict__ grp_ch,
                                          const int32_t* __restrict__ ch_grp, int64_t m,
-                                         int32_t* __restrict__ flag) {
+                                         int32_t* __restrict__ flag, int32_t above = 1) {
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int64_t g = ch_grp ? ch_grp[i] : i;
-        flag[i] = grp_ch[g + 1] - grp_ch[g] > 1 ? 1 : 0;
+        flag[i] = grp_ch[g + 1] - grp_ch[g] > above ? 1 : 0;
     }
 }
 
@@ -930,6 +939,30 @@ __global__ void compact_kernel(const int32_t* __restrict__ flag, const int32_t* 
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
         if (flag[i]) list[idx[i]] = static_cast<int32_t>(i);
+}
+
+// Groups with more than kFinSerialChunks chunks: one warp per (listed group,
+// column, block); lane l sums partials l, l + 32, ... in order, then a fixed
+// shuffle tree combines the lanes.  Result in d.big[g][b][c].
+__global__ void __launch_bounds__(kSlopeThreads)
+slope_big_reduce_kernel(const SlopeDim d, const int32_t* __restrict__ groups, int32_t ngroups,
+                        int C) {
+    const int lane = threadIdx.x & 31;
+    const int64_t total = static_cast<int64_t>(ngroups) * d.nb * C;
+    const int64_t nw = static_cast<int64_t>(gridDim.x) * (kSlopeThreads / 32);
+    for (int64_t t = static_cast<int64_t>(blockIdx.x) * (kSlopeThreads / 32) + (threadIdx.x >> 5);
+         t < total; t += nw) {
+        const int64_t i = t / (static_cast<int64_t>(d.nb) * C);
+        const int rem = static_cast<int>(t - i * d.nb * C);
+        const int b = rem / C, c = rem - b * C;
+        const int32_t g = groups[i];
+        double v = 0.0;
+        for (int32_t j = d.grp_ch[g] + lane; j < d.grp_ch[g + 1]; j += 32)
+            v += d.part[(static_cast<int64_t>(j) * d.nb + b) * C + c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) d.big[(static_cast<int64_t>(g) * d.nb + b) * C + c] = v;
+    }
 }
 
 // p = zv + beta p (p = zv where beta is 0, so p needs no initial value)

@@ -125,6 +125,8 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     double op_norm2 = 0.0;
     int present[kSlopeMaxDims] = {0};
     int fin_grid[kSlopeMaxDims] = {0};
+    int32_t* big_list[kSlopeMaxDims] = {nullptr};  // groups of more than kFinSerialChunks chunks
+    int n_big[kSlopeMaxDims] = {0};
     const int RB = T / C;
     int32_t* p_ch_grp = nullptr;
     int32_t* inv_pord = nullptr;
@@ -238,6 +240,25 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         B_CHECK(get_buf(ctx, "sl_zv" + sx, cw, &D.zv));
         B_CHECK(get_buf(ctx, "sl_p" + sx, cw, &D.p));
         fin_grid[d] = grid_for(ctx, (Gd + RB - 1) / RB, 1, 4);
+        {
+            int32_t *flag, *idx;
+            B_CHECK(get_buf(ctx, "sl_bflag", Gd, &flag));
+            B_CHECK(get_buf(ctx, "sl_bidx", Gd, &idx));
+            multi_chunk_flags_kernel<<<grid_for(ctx, Gd, T), T, 0, s>>>(grp_ch, nullptr, Gd, flag,
+                                                                        kFinSerialChunks);
+            B_LAUNCHED();
+            B_CHECK(cub_exclusive_sum(ctx, flag, idx, Gd));
+            int hv[2];
+            B_CHECK(sync_read_int(ctx, idx + (Gd - 1), 1, &hv[0]));
+            B_CHECK(sync_read_int(ctx, flag + (Gd - 1), 1, &hv[1]));
+            n_big[d] = hv[0] + hv[1];
+            if (n_big[d] > 0) {
+                B_CHECK(get_buf(ctx, "sl_blist" + sx, n_big[d], &big_list[d]));
+                compact_kernel<<<grid_for(ctx, Gd, T), T, 0, s>>>(flag, idx, Gd, big_list[d]);
+                B_LAUNCHED();
+                B_CHECK(get_buf(ctx, "sl_big" + sx, cw, &D.big));
+            }
+        }
     }
     // ---- Schur form: a plain primary dimension eliminated exactly (auto, or
     // pass_kernel 1 for block Jacobi over every dimension)
@@ -418,6 +439,12 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     };
     auto finalize = [&](int d, int slot) -> int {
         ProfScope ps(ctx, B200FE_PROF_FINALIZE, fin_bytes(d));
+        if (n_big[d] > 0) {
+            const int64_t warps = static_cast<int64_t>(n_big[d]) * dims[d].nb * C;
+            slope_big_reduce_kernel<<<grid_for(ctx, warps * 32, T, 16), T, 0, s>>>(
+                dims[d], big_list[d], n_big[d], C);
+            B_LAUNCHED();
+        }
         slope_finalize_kernel<<<fin_grid[d], C * RB, 0, s>>>(
             dims[d], C, RB, pg + static_cast<size_t>(slot) * stride * C,
             pn + static_cast<size_t>(slot) * stride * C);
