@@ -21,7 +21,8 @@
 //   z_d       [n]   slope values (slope dims)
 //   perm_d    [n]   positions sorted by ids_d (stable); null for the primary
 //   chunks    per dim: ranges of <= ceil(len / nch) positions of one group,
-//             nch <= 1024 per group, so the per-group combine stays short
+//             nch <= 4096 per group; a group of more than 32 chunks has its
+//             chunk sums pre-reduced by one warp (slope_big_reduce_kernel)
 //   coefficients per dim [G][nb][C]: block 0 the intercept (if any), then the
 //             slope (if any)
 // Every sum is taken in a fixed order (chunk, then lane slots, then chunks in
