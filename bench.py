@@ -65,10 +65,11 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
-    ap.add_argument("--workload", default="akm3", choices=["akm3", "slopes", "gi"],
+    ap.add_argument("--workload", default="akm3", choices=["akm3", "slopes", "gi", "kss"],
                     help="akm3: the headline workload; slopes: the same panel with "
                          "firm-specific tenure slopes (firm##c.tenure); gi: 10M groups "
-                         "with individual FEs (group/individual design)")
+                         "with individual FEs (group/individual design); kss: the KSS firm "
+                         "system of a 10M-obs panel, 200 right-hand sides")
     return ap.parse_args()
 
 
@@ -707,8 +708,158 @@ def run_gi(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# KSS: the firm system of a 10M-obs AKM panel, 200 JL right-hand sides (1 GPU)
+# ---------------------------------------------------------------------------
+KSS_OBS = 10_000_000
+KSS_RHS = 200
+KSS_METRIC = ("KSS firm-system solves: 200 right-hand sides, grounded Jacobi-PCG to 1e-10, "
+              "10M-obs AKM panel (1M workers, 100k firms, mobility 0.15)")
+
+
+def kss_panel(n: int, seed: int):
+    panels = ge.load_module("panels")
+    return panels.akm_two_way(n, n_firms=max(1000, n // 100), n_years=10, seed=seed,
+                              move_prob=0.15)
+
+
+def kss_matches(p):
+    """Distinct (worker, firm) matches with their counts, restricted to the largest
+    connected component of the worker-firm graph, dense ids, sorted by worker."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    w = p.fes[0].astype(np.int64)
+    f = p.fes[1].astype(np.int64)
+    N, J = int(w.max()) + 1, int(f.max()) + 1
+    key, cnt = np.unique(w * J + f, return_counts=True)
+    mw, mf = key // J, key % J
+    g = coo_matrix((np.ones(key.size), (mw, N + mf)), shape=(N + J, N + J))
+    _, lab = connected_components(g, directed=False)
+    big = np.bincount(lab).argmax()
+    keep = lab[mw] == big
+    mw, mf, cnt = mw[keep], mf[keep], cnt[keep]
+    _, mw = np.unique(mw, return_inverse=True)
+    _, mf = np.unique(mf, return_inverse=True)
+    return mw.astype(np.int32), mf.astype(np.int32), cnt.astype(np.float64)
+
+
+def run_kss(args):
+    import oracle
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n_obs = args.n if args.n != N_OBS else KSS_OBS
+    sample = max(100_000, args.cpu_sample)
+
+    def ref_decompose(p, lib, use_gpu):
+        t0 = time.perf_counter()
+        r = oracle.ref_akm_kss(p.y, p.fes[0], p.fes[1], leverages="jla", jla_draws=KSS_RHS,
+                               direct_max_firms=0, use_gpu=use_gpu, threads=threads,
+                               lib_path=lib)
+        return time.perf_counter() - t0, r
+
+    def cpu_leg():
+        p = kss_panel(sample, seed=99)
+        dt, r = ref_decompose(p, oracle.REF_SO, False)
+        return {"value": dt, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": (f"the reference's akm_kss_decompose (JLA, {KSS_RHS} draws, its PCG, "
+                           f"{threads} threads) on a {sample}-obs panel of the same generator: "
+                           f"{dt:.2f} s, {r['n_matches']} matches, {r['n_firms']} firms; "
+                           "not scaled (PCG work grows faster than the sample)")}
+
+    if args.impl == "reference":
+        vals, info = [], None
+        for i in range(args.warmup + args.steps):
+            info = cpu_leg()
+            if i >= args.warmup:
+                vals.append(info["value"])
+        v = statistics.median(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": KSS_METRIC + " [reference: full decomposition on a "
+            "CPU sample]", "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1000.0, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded AKM generator)",
+            "config": {"workload": "kss_10M_200rhs", "n_obs_sample": sample},
+            "cpu_baseline": info,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import torch
+    torch.cuda.set_device(0)
+    pkg = ge.load_package()
+    p = kss_panel(n_obs, seed=0)
+    mw, mf, cnt = kss_matches(p)
+    N, J, M = int(mw.max()) + 1, int(mf.max()) + 1, int(mw.size)
+    sysd = pkg.kss_system(mw, mf, cnt, N, J)
+    solver = pkg.KssSolver(sysd)
+    L = min(pkg.max_lanes(), KSS_RHS)
+    B = np.random.default_rng(7).standard_normal((KSS_RHS, J))
+    for _ in range(max(1, args.warmup)):
+        solver.solve_multi(B[:L], tol=1e-10, max_iter=20_000)
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    times, steps, its_all = [], 0, []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for b0 in range(0, KSS_RHS, L):
+            _, its = solver.solve_multi(B[b0:b0 + L], tol=1e-10, max_iter=20_000)
+            steps += int(its.max())
+            its_all.append(its)
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    solver.close()
+    v = statistics.median(times)
+    its_all = np.concatenate(its_all)
+    # algorithmic bytes of one PCG step with l lanes: the structure once
+    # (matches: worker, firm, weight; worker and firm offsets) and per lane the
+    # match-level and node-level vectors (t, p, q, r, z, x rows)
+    steps_per_call = steps / args.steps
+    bytes_per_step = M * 16.0 + (N + J) * 8.0 + L * 8.0 * (2.0 * M + 2.0 * N + 10.0 * J)
+    achieved = bytes_per_step * steps_per_call / v / 1e9
+    peaks, peak_kind = measured_peaks()
+    drop = ref_gpu = None
+    if not args.no_reference_gpu and oracle.REF_B200_SO.exists():
+        dt, r = ref_decompose(p, oracle.REF_B200_SO, True)
+        drop = {"value": dt, "unit": UNIT, "kind": "the reference's akm_kss_decompose (JLA, "
+                f"{KSS_RHS} draws) on this library through its binding, host arrays",
+                "gpu_used": r["gpu_used"], "solver_iterations": r["solver_iterations"],
+                "kss": r["kss"]}
+    if not args.no_reference_gpu and oracle.REF_CUDA_SO.exists():
+        dt, r = ref_decompose(p, oracle.REF_CUDA_SO, True)
+        ref_gpu = {"value": dt, "unit": UNIT, "kind": "the same decomposition on the reference's "
+                   "own CUDA backend built for sm_100a", "gpu_used": r["gpu_used"],
+                   "solver_iterations": r["solver_iterations"], "kss": r["kss"]}
+    cpu = None if args.no_cpu_baseline or not oracle.ref_available() else cpu_leg()
+    print(json.dumps({
+        "metric": KSS_METRIC, "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1000.0, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded AKM generator)",
+        "config": {"workload": "kss_10M_200rhs", "n_obs": p.n, "matches": M, "workers": N,
+                   "firms": J, "rhs": KSS_RHS, "lanes_per_call": L, "tol": 1e-10,
+                   "timing": "wall time of the solve_multi calls (right-hand sides in and "
+                             "solutions out through host arrays included)",
+                   "l2_policy": "lane vectors of the match and worker levels exceed L2"},
+        "iterations": {"max": int(its_all.max()), "mean": float(its_all.mean())},
+        "pcg_steps_per_call": steps_per_call,
+        "roofline": {"kernel": "kss PCG step", "bound": "hbm", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "peak_kind": peak_kind, "bytes_per_step": bytes_per_step,
+                     "traffic": None},
+        "clocks": clocks, "dropin_decomposition": drop, "reference_gpu": ref_gpu,
+        "cpu_baseline": cpu,
+        "e2e": {"value": v, "unit": UNIT,
+                "h2d_bytes_per_step": int(KSS_RHS * J * 8), "d2h_bytes_per_step": int(KSS_RHS * J * 8)}}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "kss":
+        return run_kss(args)
     if args.workload == "gi":
         return run_gi(args)
     if args.workload == "slopes":
