@@ -65,11 +65,12 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
-    ap.add_argument("--workload", default="akm3", choices=["akm3", "slopes", "gi", "kss"],
+    ap.add_argument("--workload", default="akm3", choices=["akm3", "slopes", "gi", "kss", "ols"],
                     help="akm3: the headline workload; slopes: the same panel with "
                          "firm-specific tenure slopes (firm##c.tenure); gi: 10M groups "
                          "with individual FEs (group/individual design); kss: the KSS firm "
-                         "system of a 10M-obs panel, 200 right-hand sides")
+                         "system of a 10M-obs panel, 200 right-hand sides; ols: run_ols with "
+                         "worker-clustered SEs on the absorbed 50M panel")
     return ap.parse_args()
 
 
@@ -856,8 +857,119 @@ def run_kss(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# OLS after absorption: the absorbed 50M panel, 12 regressors, worker clusters
+# ---------------------------------------------------------------------------
+OLS_METRIC = ("run_ols after absorption: 50M obs, 12 regressors, worker-clustered SEs "
+              "(X'X, coefficients, cluster scores, VCE)")
+OLS_SAMPLE = 5_000_000
+
+
+def run_ols_bench(args):
+    import oracle
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    panel = make_panel(args.n, seed=0)
+    n, k = panel.n, panel.k
+
+    def cpu_leg(ys, Xs, cl):
+        t0 = time.perf_counter()
+        oracle.ref_run_ols(ys, Xs, None, cl, se_type="cluster")
+        dt = time.perf_counter() - t0
+        return {"value": dt * n / ys.shape[0], "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": (f"the reference's run_ols (cluster VCE) on the first {ys.shape[0]} rows "
+                           f"of the absorbed panel: {dt:.3f} s, scaled linearly to {n} rows")}
+
+    pkg = ge.load_package()
+    if args.impl == "reference":
+        # the within transform comes from this library (the input of run_ols); only
+        # the reference's run_ols is timed
+        m = min(n, OLS_SAMPLE)
+        r = pkg.absorb_fixed_effects(panel.y[:m], panel.X[:m], [f[:m] for f in panel.fes],
+                                     tol=1e-8)
+        vals, info = [], None
+        for i in range(args.warmup + args.steps):
+            info = cpu_leg(r.y_tilde, r.X_tilde, panel.cluster[:m])
+            if i >= args.warmup:
+                vals.append(info["value"])
+        v = statistics.median(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": OLS_METRIC, "value": v, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000.0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded AKM generator)",
+            "config": {"workload": "ols_50M_12reg_cluster", "n_obs": n, "regressors": k},
+            "cpu_baseline": info,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    cols = k + 1
+    v = torch.empty((cols, n), dtype=torch.float64, device=dev)
+    v[0].copy_(torch.from_numpy(panel.y))
+    v[1:].copy_(torch.from_numpy(np.ascontiguousarray(panel.X.T)))
+    gids = [torch.from_numpy(f).to(dev) for f in panel.fes]
+    absorber = pkg.Absorber(0)
+    out, _ = absorber.absorb_device(v, gids, panel.levels, None, pkg.make_options(tol=1e-8))
+    torch.cuda.synchronize()
+    del v
+    cl = torch.from_numpy(panel.cluster.astype(np.int32)).to(dev)
+    for _ in range(args.warmup):
+        pkg.run_ols(out[0], out[1:], clusters=cl, se_type="cluster")
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = pkg.run_ols(out[0], out[1:], clusters=cl, se_type="cluster")
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    val = statistics.median(times)
+    # host arrays (copies in inside the call)
+    y_h = out[0].cpu().numpy()
+    X_h = np.asfortranarray(out[1:].cpu().numpy().T)
+    cl_h = panel.cluster
+    pkg.run_ols(y_h, X_h, clusters=cl_h, se_type="cluster")
+    t0 = time.perf_counter()
+    pkg.run_ols(y_h, X_h, clusters=cl_h, se_type="cluster")
+    e2e = time.perf_counter() - t0
+    cpu = None
+    if not args.no_cpu_baseline and oracle.ref_available():
+        m = min(n, OLS_SAMPLE)
+        cpu = cpu_leg(y_h[:m], X_h[:m], cl_h[:m])
+    absorber.close()
+    # algorithmic bytes: the Gram pass reads y and X once, the residual/score pass
+    # reads them again with the cluster order (ids and permutation)
+    bytes_ = 2.0 * n * cols * 8 + n * 8.0
+    print(json.dumps({
+        "metric": OLS_METRIC, "value": val, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": val * 1000.0, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded AKM generator)",
+        "config": {"workload": "ols_50M_12reg_cluster", "n_obs": n, "regressors": k,
+                   "clusters": int(res.num_clusters),
+                   "timing": "wall time of b200fe_ols_device (synchronous; includes the "
+                             "cluster sort and the host p x p algebra)",
+                   "l2_policy": f"inputs larger than L2 ({n * cols * 8 / 1e9:.1f} GB)"},
+        "roofline": {"kernel": "run_ols (whole call)", "bound": "hbm",
+                     "achieved": bytes_ / val / 1e9, "peak": measured_peaks()[0]["hbm_gbs"],
+                     "unit": "GB/s", "frac": bytes_ / val / 1e9 / measured_peaks()[0]["hbm_gbs"],
+                     "traffic": None},
+        "clocks": clocks, "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(n * cols * 8 + n * 4),
+                "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "ols":
+        return run_ols_bench(args)
     if args.workload == "kss":
         return run_kss(args)
     if args.workload == "gi":

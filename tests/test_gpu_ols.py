@@ -86,3 +86,18 @@ def test_rank_deficient_design_like_reference(pkg, oracle_mod, within):
     assert ours.coefficients[1] == 0.0 and ours.std_errors[1] == 0.0
     assert _close(ours.coefficients, ref["coef"])
     assert _close(ours.std_errors, ref["se"])
+
+
+def test_device_cluster_ids_with_gaps(pkg, within):
+    """Cluster ids on the device need not be dense: ids with unused values in
+    between (empty clusters) give the same inference as the dense ids."""
+    import torch
+    p, yt, Xt = within
+    cl = np.asarray(p.fes[0]).astype(np.int32)  # workers: many clusters of a few rows
+    dense = pkg.run_ols(yt, Xt, None, cl, se_type="cluster")
+    dy = torch.from_numpy(np.ascontiguousarray(yt)).cuda()
+    dX = torch.from_numpy(np.ascontiguousarray(Xt.T)).cuda()
+    gaps = pkg.run_ols(dy, dX, None, torch.from_numpy(3 * cl + 1).cuda(), se_type="cluster")
+    assert gaps.num_clusters == dense.num_clusters
+    assert _close(gaps.coefficients, dense.coefficients)
+    assert _close(gaps.std_errors, dense.std_errors)

@@ -1791,9 +1791,9 @@ int ols_impl(b200fe_context* ctx, const double* d_y, const double* d_X, int64_t 
         for (int i = 0; i < p; ++i) inv[static_cast<size_t>(j) * p + i] = static_cast<double>(e[i]);
     }
     for (int i = 0; i < p * p; ++i) out->xtx_inv[i] = inv[i];
-    // 2. residual pass: RSS and the robust meat
+    // 2. residual pass: RSS, and the meat for robust inference
     m.P = p;
-    m.mode = kMomRobust;
+    m.mode = se_type == 1 ? kMomRobust : kMomRss;
     m.wfreq = wfreq;
     for (int j = 0; j < p; ++j) m.beta[j] = out->coef[j];
     std::vector<double> rm;
@@ -1830,6 +1830,8 @@ int ols_impl(b200fe_context* ctx, const double* d_y, const double* d_X, int64_t 
         B_TRY(cudaMemsetAsync(nch, 0, sizeof(int32_t) * (static_cast<size_t>(G) + 1), s));
         B_TRY(cudaMemsetAsync(mflag, 0, sizeof(int32_t) * (static_cast<size_t>(G) + 1), s));
         chunk_count_kernel<<<grid_for(ctx, G, 256), 256, 0, s>>>(off, G, kOlsChunk, nch);
+        B_LAUNCHED();
+        drop_small_chunks_kernel<<<grid_for(ctx, G, 256), 256, 0, s>>>(off, G, kOlsSmallCluster, nch);
         B_LAUNCHED();
         B_CHECK(cub_exclusive_sum(ctx, nch, ch_off, static_cast<int64_t>(G) + 1));
         multi_flag_kernel<<<grid_for(ctx, G, 256), 256, 0, s>>>(nch, G, mflag);
@@ -1870,6 +1872,9 @@ int ols_impl(b200fe_context* ctx, const double* d_y, const double* d_X, int64_t 
         for (int j = 0; j < p; ++j) c.beta[j] = out->coef[j];
         c.scores = scores;
         c.chunk_part = cpart;
+        c.small_max = kOlsSmallCluster;
+        cluster_small_kernel<<<grid_for(ctx, G, kOlsThreads, 8), kOlsThreads, 0, s>>>(c, off, G);
+        B_LAUNCHED();
         cluster_chunk_kernel<<<grid_for(ctx, nchunks * 32, kOlsThreads, 8), kOlsThreads, 0, s>>>(c);
         B_LAUNCHED();
         if (nmulti > 0) {

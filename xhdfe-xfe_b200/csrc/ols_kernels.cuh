@@ -8,7 +8,8 @@
 //                     Gram  [X y]' W [X y]      f = w,          columns X, y
 //                     robust meat               f = (w e)^2 (analytic weights)
 //                                                   or w e^2 (frequency weights)
-//                   and, in the robust mode, sum_i w_i e_i^2 (the RSS).
+//                   and, in the robust mode, sum_i w_i e_i^2 (the RSS);
+//                   the RSS mode computes the RSS alone (no pair sums).
 //   cluster_chunk_kernel  per chunk of one cluster (rows in cluster order):
 //                   the score sums sum w e x_j and sum w e, e = y - x'b.
 //
@@ -29,8 +30,9 @@ constexpr int kOlsMaxP = 32;      // regressors
 constexpr int kOlsTile = 64;      // rows staged per step
 constexpr int kOlsThreads = 256;
 constexpr int kOlsChunk = 256;    // rows per cluster chunk
+constexpr int kOlsSmallCluster = 32;  // clusters up to this many rows: one thread each
 
-enum OlsMomentMode { kMomGram = 0, kMomRobust = 1, kMomPlain = 2 };
+enum OlsMomentMode { kMomGram = 0, kMomRobust = 1, kMomPlain = 2, kMomRss = 3 };
 
 struct MomentArgs {
     int64_t n;
@@ -61,19 +63,27 @@ __device__ __forceinline__ void pair_index(int t, int P, int& a, int& b) {
 
 __global__ void __launch_bounds__(kOlsThreads)
 moments_kernel(const MomentArgs m) {
-    __shared__ double tile[kOlsMaxP + 1][kOlsTile];
+    __shared__ double tile[kOlsMaxP + 1][kOlsTile + 1];  // padded: no bank conflicts across columns
     __shared__ double fac[kOlsTile];
     __shared__ double red[kOlsThreads];
     const int tid = threadIdx.x;
     const int npairs = m.P * (m.P + 1) / 2;
+    // few pairs: R row slices of them (thread = slice x pair, slices combined
+    // in order at the end); many pairs: up to three pairs per thread, all rows
+    const int R = npairs <= kOlsThreads / 2 ? kOlsThreads / npairs : 1;
+    const int slice = R > 1 ? tid / npairs : 0;
+    const int pbase = R > 1 ? tid % npairs : tid;
     int pa[3], pb[3];
     double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int u = 0; u < 3; ++u) {
-        const int t = tid + u * kOlsThreads;
-        if (t < npairs) pair_index(t, m.P, pa[u], pb[u]);
+        const int t = pbase + u * kOlsThreads;
+        const bool mine = R > 1 ? (u == 0 && slice < R) : t < npairs;
+        if (mine) pair_index(t, m.P, pa[u], pb[u]);
         else pa[u] = pb[u] = -1;
     }
+    // row-major rows of P values (X then y at offset p, the score matrix)
+    const bool row_major = m.mode == kMomPlain && m.cs == 1 && m.rs >= m.P && !m.perm;
     const int64_t per = (m.n + gridDim.x - 1) / gridDim.x;
     const int64_t r0 = static_cast<int64_t>(blockIdx.x) * per;
     const int64_t r1 = min(m.n, r0 + per);
@@ -81,18 +91,31 @@ moments_kernel(const MomentArgs m) {
     for (int64_t base = r0; base < r1; base += kOlsTile) {
         const int nr = static_cast<int>(min(static_cast<int64_t>(kOlsTile), r1 - base));
         __syncthreads();
-        // stage the tile's columns (and y) coalesced
-        for (int i = tid; i < m.P * kOlsTile; i += kOlsThreads) {
-            const int col = i / kOlsTile, r = i - col * kOlsTile;
-            double v = 0.0;
-            if (r < nr) {
-                const int64_t row = m.perm ? m.perm[base + r] : base + r;
-                v = col < m.p ? m.X[static_cast<int64_t>(col) * m.cs + row * m.rs]
-                              : m.y[row * (m.mode == kMomPlain ? m.rs : 1)];
+        // stage the tile's columns (and y) coalesced: column by column for
+        // column-major data, row by row for row-major data (the cluster scores)
+        if (row_major) {
+            for (int i = tid; i < m.P * kOlsTile; i += kOlsThreads) {
+                const int r = i / m.P, col = i - r * m.P;
+                double v = 0.0;
+                if (r < nr) {
+                    const int64_t row = base + r;
+                    v = col < m.p ? m.X[col + row * m.rs] : m.y[row * m.rs];
+                }
+                tile[col][r] = v;
             }
-            tile[col][r] = v;
+        } else {
+            for (int i = tid; i < m.P * kOlsTile; i += kOlsThreads) {
+                const int col = i / kOlsTile, r = i - col * kOlsTile;
+                double v = 0.0;
+                if (r < nr) {
+                    const int64_t row = m.perm ? m.perm[base + r] : base + r;
+                    v = col < m.p ? m.X[static_cast<int64_t>(col) * m.cs + row * m.rs]
+                                  : m.y[row * (m.mode == kMomPlain ? m.rs : 1)];
+                }
+                tile[col][r] = v;
+            }
         }
-        if (m.mode == kMomRobust) {
+        if (m.mode == kMomRobust || m.mode == kMomRss) {
             for (int i = tid; i < kOlsTile; i += kOlsThreads) tile[m.p][i] = 0.0;
         }
         __syncthreads();
@@ -102,7 +125,7 @@ moments_kernel(const MomentArgs m) {
             if (tid < nr) {
                 const int64_t row = m.perm ? m.perm[base + tid] : base + tid;
                 const double wr = m.w ? m.w[row] : 1.0;
-                if (m.mode == kMomRobust) {
+                if (m.mode == kMomRobust || m.mode == kMomRss) {
                     double fit = 0.0;
                     for (int j = 0; j < m.p; ++j) fit = fma(tile[j][tid], m.beta[j], fit);
                     const double e = m.y[row] - fit;
@@ -117,20 +140,32 @@ moments_kernel(const MomentArgs m) {
             fac[tid] = f;
         }
         __syncthreads();
+        if (m.mode == kMomRss) continue;
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
             if (pa[u] < 0) continue;
             const double* ca = tile[pa[u]];
             const double* cb = tile[pb[u]];
             double s = acc[u];
-            for (int r = 0; r < nr; ++r) s = fma(fac[r] * ca[r], cb[r], s);
+            for (int r = slice; r < nr; r += R) s = fma(fac[r] * ca[r], cb[r], s);
             acc[u] = s;
         }
     }
+    if (R > 1) {
+        __syncthreads();
+        red[tid] = pa[0] >= 0 ? acc[0] : 0.0;
+        __syncthreads();
+        if (tid < npairs) {
+            double t = 0.0;
+            for (int sl = 0; sl < R; ++sl) t += red[sl * npairs + tid];
+            m.partial[static_cast<int64_t>(blockIdx.x) * npairs + tid] = t;
+        }
+    } else {
 #pragma unroll
-    for (int u = 0; u < 3; ++u) {
-        const int t = tid + u * kOlsThreads;
-        if (t < npairs) m.partial[static_cast<int64_t>(blockIdx.x) * npairs + t] = acc[u];
+        for (int u = 0; u < 3; ++u) {
+            const int t = tid + u * kOlsThreads;
+            if (t < npairs) m.partial[static_cast<int64_t>(blockIdx.x) * npairs + t] = acc[u];
+        }
     }
     if (m.rss_partial) {
         __syncthreads();
@@ -169,6 +204,7 @@ struct ClusterArgs {
     double beta[kOlsMaxP];
     double* scores;             // [G][p + 1]: sum w e x_j, then sum w e
     double* chunk_part;         // [nchunks][p + 1]
+    int32_t small_max;          // whole-cluster chunks this short go to cluster_small_kernel
 };
 
 // One warp per chunk: lane l takes rows l, l + 32, ... of the chunk, then the
@@ -179,6 +215,7 @@ cluster_chunk_kernel(const ClusterArgs c) {
     const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (kOlsThreads / 32);
     for (int64_t k = static_cast<int64_t>(blockIdx.x) * (kOlsThreads / 32) + (threadIdx.x >> 5);
          k < c.nchunks; k += nwarps) {
+        if (c.chunk_whole[k] && c.chunk_end[k] - c.chunk_beg[k] <= c.small_max) continue;
         double s[kOlsMaxP + 1];
 #pragma unroll
         for (int j = 0; j <= kOlsMaxP; ++j) s[j] = 0.0;
@@ -205,10 +242,50 @@ cluster_chunk_kernel(const ClusterArgs c) {
         if (lane == 0) {
             double* dst = c.chunk_whole[k] ? c.scores + static_cast<int64_t>(c.chunk_grp[k]) * (c.p + 1)
                                            : c.chunk_part + k * (c.p + 1);
-            for (int j = 0; j < c.p; ++j) dst[j] = s[j];
+#pragma unroll
+            for (int j = 0; j < kOlsMaxP; ++j)
+                if (j < c.p) dst[j] = s[j];
             dst[c.p] = s[kOlsMaxP];
         }
     }
+}
+
+// Clusters of at most small_max rows (and empty ones): one thread per cluster
+// walks its rows in cluster order; an empty cluster gets zero scores.
+__global__ void __launch_bounds__(kOlsThreads)
+cluster_small_kernel(const ClusterArgs c, const int32_t* __restrict__ off, int32_t G) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t b = off[g], e = off[g + 1];
+        if (e - b > c.small_max) continue;
+        double s[kOlsMaxP + 1];
+#pragma unroll
+        for (int j = 0; j <= kOlsMaxP; ++j) s[j] = 0.0;
+        for (int32_t r = b; r < e; ++r) {
+            const int64_t row = c.perm ? c.perm[r] : r;
+            double fit = 0.0;
+            for (int j = 0; j < c.p; ++j) fit = fma(c.X[static_cast<int64_t>(j) * c.ld + row], c.beta[j], fit);
+            const double wr = c.w ? c.w[row] : 1.0;
+            const double we = wr * (c.y[row] - fit);
+#pragma unroll
+            for (int j = 0; j < kOlsMaxP; ++j)
+                if (j < c.p) s[j] = fma(we, c.X[static_cast<int64_t>(j) * c.ld + row], s[j]);
+            s[kOlsMaxP] += we;
+        }
+        double* dst = c.scores + g * (c.p + 1);
+#pragma unroll
+        for (int j = 0; j < kOlsMaxP; ++j)
+            if (j < c.p) dst[j] = s[j];
+        dst[c.p] = s[kOlsMaxP];
+    }
+}
+
+// clusters the per-thread kernel takes get no chunks
+__global__ void drop_small_chunks_kernel(const int32_t* __restrict__ off, int32_t G,
+                                         int32_t small_max, int32_t* __restrict__ nch) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        if (off[g + 1] - off[g] <= small_max) nch[g] = 0;
 }
 
 // clusters of several chunks: chunk sums in chunk order

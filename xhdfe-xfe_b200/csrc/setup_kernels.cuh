@@ -266,7 +266,7 @@ __global__ void chunk_fill_kernel(const int32_t* __restrict__ grp_off, int32_t G
             chunk_end[c] = min(e, cb + CH);
             chunk_whole[c] = whole ? 1 : 0;
         }
-        if (!whole) {
+        if (c1 - c0 > 1) {  // several chunks (a group may also have none)
             const int32_t mi = multi_idx[g];
             multi_grp[mi] = static_cast<int32_t>(g);
             multi_c0[mi] = c0;
