@@ -65,12 +65,14 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
-    ap.add_argument("--workload", default="akm3", choices=["akm3", "slopes", "gi", "kss", "ols"],
+    ap.add_argument("--workload", default="akm3",
+                    choices=["akm3", "slopes", "gi", "kss", "ols", "prep"],
                     help="akm3: the headline workload; slopes: the same panel with "
                          "firm-specific tenure slopes (firm##c.tenure); gi: 10M groups "
                          "with individual FEs (group/individual design); kss: the KSS firm "
                          "system of a 10M-obs panel, 200 right-hand sides; ols: run_ols with "
-                         "worker-clustered SEs on the absorbed 50M panel")
+                         "worker-clustered SEs on the absorbed 50M panel; prep: dense ids, "
+                         "singleton cascade and mobility components of the 50M panel")
     return ap.parse_args()
 
 
@@ -966,8 +968,102 @@ def run_ols_bench(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# preprocessing on the device: dense ids, singleton cascade, mobility groups
+# ---------------------------------------------------------------------------
+PREP_METRIC = ("preprocessing of the 50M AKM panel on the device: dense ids of 3 raw FE "
+               "columns, the singleton cascade, the worker-firm mobility groups")
+
+
+def run_prep(args):
+    import oracle
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    panels = ge.load_module("panels")
+    firms = max(1000, int(N_FIRMS * args.n / N_OBS))
+    p = panels.akm_batched(args.n, n_firms=firms, n_years=N_YEARS, seed=0)
+    n = p.n
+    # raw ids: the dense ids spread over a sparse range (build_indexer then ranks)
+    raw = [(f.astype(np.int64) * 7 + 3).astype(np.int32) for f in p.fes]
+
+    def cpu_leg():
+        t0 = time.perf_counter()
+        oracle.ref_components(raw[0], raw[1])
+        dt = time.perf_counter() - t0
+        return {"value": dt, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": (f"the reference's compute_first_pair_component_stats on the full "
+                           f"{n}-row panel (raw ids): {dt:.2f} s; its dense ranking and singleton "
+                           "cascade run inside its fit and are not timed separately")}
+
+    if args.impl == "reference":
+        vals, info = [], None
+        for i in range(args.warmup + args.steps):
+            info = cpu_leg()
+            if i >= args.warmup:
+                vals.append(info["value"])
+        v = statistics.median(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": PREP_METRIC + " [reference: mobility groups only]",
+            "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1000.0, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded AKM generator)",
+            "config": {"workload": "prep_50M", "n_obs": n}, "cpu_baseline": info,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import torch
+    torch.cuda.set_device(0)
+    pkg = ge.load_package()
+    draw = [torch.from_numpy(r).cuda() for r in raw]
+    stats = {}
+
+    def step():
+        dense = [pkg.dense_ids_device(r) for r in draw]
+        ids = [d for d, _, _ in dense]
+        G = [g for _, g, _ in dense]
+        keep, dropped, rounds = pkg.drop_singletons_device(ids, G)
+        comp = pkg.first_pair_component_stats(ids[0], ids[1])
+        stats.update(levels=G, dropped=dropped, rounds=rounds,
+                     components=comp.num_components)
+        return comp
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    v = statistics.median(times)
+    cpu = None if args.no_cpu_baseline or not oracle.ref_available() else cpu_leg()
+    print(json.dumps({
+        "metric": PREP_METRIC, "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1000.0, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded AKM generator)",
+        "config": {"workload": "prep_50M", "n_obs": n, "levels": stats["levels"],
+                   "singletons_dropped": stats["dropped"], "cascade_rounds": stats["rounds"],
+                   "components": stats["components"],
+                   "timing": "wall time with the device synchronised before and after; the "
+                             "raw ids are resident on the device"},
+        "clocks": clocks, "cpu_baseline": cpu,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "prep":
+        return run_prep(args)
     if args.workload == "ols":
         return run_ols_bench(args)
     if args.workload == "kss":

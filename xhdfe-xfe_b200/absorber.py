@@ -591,8 +591,14 @@ def first_pair_component_stats(first_fe, second_fe, weights=None, device=0) -> F
     import torch
     ab = _thread_absorber(device)
     dev = f"cuda:{device}"
-    f1 = torch.as_tensor(np.asarray(first_fe, dtype=np.int32)).to(dev).contiguous()
-    f2 = torch.as_tensor(np.asarray(second_fe, dtype=np.int32)).to(dev).contiguous()
+
+    def on_device(a):  # torch CUDA tensors are used in place
+        if isinstance(a, torch.Tensor):
+            return a.to(device=dev, dtype=torch.int32).contiguous()
+        return torch.as_tensor(np.asarray(a, dtype=np.int32)).to(dev).contiguous()
+
+    f1 = on_device(first_fe)
+    f2 = on_device(second_fe)
     if f1.numel() != f2.numel():
         raise ValueError("First-pair FE vectors must have the same length")
     w = None if weights is None else torch.as_tensor(
