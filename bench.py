@@ -66,13 +66,14 @@ def parse():
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--workload", default="akm3",
-                    choices=["akm3", "slopes", "gi", "kss", "ols", "prep"],
+                    choices=["akm3", "slopes", "gi", "kss", "ols", "prep", "savefe"],
                     help="akm3: the headline workload; slopes: the same panel with "
                          "firm-specific tenure slopes (firm##c.tenure); gi: 10M groups "
                          "with individual FEs (group/individual design); kss: the KSS firm "
                          "system of a 10M-obs panel, 200 right-hand sides; ols: run_ols with "
                          "worker-clustered SEs on the absorbed 50M panel; prep: dense ids, "
-                         "singleton cascade and mobility components of the 50M panel")
+                         "singleton cascade and mobility components of the 50M panel; "
+                         "savefe: recover_fixed_effects of a 50M partial residual")
     return ap.parse_args()
 
 
@@ -1060,8 +1061,90 @@ def run_prep(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# saved FEs: recover_fixed_effects of one partial residual on the 50M panel
+# ---------------------------------------------------------------------------
+SAVEFE_METRIC = ("recover_fixed_effects of a 50M-row partial residual (y - X b) on the "
+                 "worker, firm and year FEs: coefficients, contributions and orthogonality check")
+SAVEFE_SAMPLE = 5_000_000
+
+
+def run_savefe(args):
+    import oracle
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    panel = make_panel(args.n, seed=0)
+    n = panel.n
+    rng = np.random.default_rng(3)
+    partial = panel.y - panel.X @ (0.01 * rng.standard_normal(panel.k))
+
+    def cpu_leg():
+        m = min(n, SAVEFE_SAMPLE)
+        t0 = time.perf_counter()
+        r = oracle.ref_recover_fe(partial[:m], [f[:m] for f in panel.fes], None, tol=1e-8,
+                                  fe_tolerance=1e-8, threads=threads)
+        dt = time.perf_counter() - t0
+        return {"value": dt * n / m, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": (f"the reference's recover_fixed_effects (CPU, {threads} threads, "
+                           f"fe_tolerance 1e-8) on the first {m} rows: {dt:.2f} s, "
+                           f"{r['iterations']} iterations, scaled linearly to {n} rows")}
+
+    if args.impl == "reference":
+        vals, info = [], None
+        for i in range(args.warmup + args.steps):
+            info = cpu_leg()
+            if i >= args.warmup:
+                vals.append(info["value"])
+        v = statistics.median(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": SAVEFE_METRIC, "value": v, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000.0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded AKM generator)",
+            "config": {"workload": "savefe_50M", "n_obs": n}, "cpu_baseline": info,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import torch
+    torch.cuda.set_device(0)
+    pkg = ge.load_package()
+    p_h = torch.from_numpy(partial).pin_memory().numpy()
+    for _ in range(max(1, args.warmup)):
+        pkg.recover_fixed_effects(p_h, panel.fes, tol=1e-8, fe_tolerance=1e-8)
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    times, r = [], None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = pkg.recover_fixed_effects(p_h, panel.fes, tol=1e-8, fe_tolerance=1e-8)
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    v = statistics.median(times)
+    cpu = None if args.no_cpu_baseline or not oracle.ref_available() else cpu_leg()
+    print(json.dumps({
+        "metric": SAVEFE_METRIC, "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1000.0, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded AKM generator)",
+        "config": {"workload": "savefe_50M", "n_obs": n, "fe_tolerance": 1e-8,
+                   "timing": "wall time of the host call: partial copied in, the absorption "
+                             "with saved FEs (solved two orders tighter), coefficients copied "
+                             "out, contributions formed on the host, the device orthogonality "
+                             "check"},
+        "iterations": r.iterations, "converged": bool(r.converged), "max_delta": r.max_delta,
+        "clocks": clocks, "cpu_baseline": cpu,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": int(2 * n * 8 + 2 * n * 4 * 3),
+                "d2h_bytes_per_step": int(n * 8)}}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "savefe":
+        return run_savefe(args)
     if args.workload == "prep":
         return run_prep(args)
     if args.workload == "ols":

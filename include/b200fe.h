@@ -62,7 +62,14 @@ typedef struct b200fe_options {
     int pass_kernel;       /* CG matvec pass: 0 auto (block level when at most one large and
                               one small FE dim besides the largest; with a small dim, its
                               dense coupling rows when they are small), 1 general tile pass,
-                              2 block level without the dense coupling                        */
+                              2 block level without the dense coupling; for the slope
+                              absorber 1 forces block Jacobi over every dimension            */
+    double fe_linf_tol;    /* > 0: a column also needs every group's weighted mean of its
+                              within transform (non-primary dims) at most this before it
+                              stops -- the check recover_fixed_effects applies to saved FEs
+                              (src/fe_absorption.cpp:15527-15548); a refinement round that
+                              raises the residual (the bound lies below what rounding
+                              allows) is undone and the L2 rule alone decides; 0 off      */
 } b200fe_options;
 
 /* Kernel categories of the profile arrays in b200fe_result. */

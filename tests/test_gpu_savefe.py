@@ -92,3 +92,34 @@ def test_reference_recovery_runs_on_b200(oracle_mod, panels):
     assert gpu["converged"] and gpu["max_delta"] <= 1e-10
     tot = gpu["contributions"].sum(axis=0)
     assert np.linalg.norm(tot - cpu["contributions"].sum(axis=0)) <= REL_TOL * np.linalg.norm(partial)
+
+
+def test_group_mean_stop_on_a_large_panel(absorber, pkg, panels):
+    """fe_linf_tol: on a 2M-row panel the relative L2 stop leaves firm means of
+    the within transform near 1e-7 for the smallest firms; with the option every
+    group mean is within it, and recover_fixed_effects meets an absolute
+    fe_tolerance of 1e-8."""
+    p = panels.akm_batched(2_000_000, n_firms=32_000, n_years=36, seed=0)
+    p = panels.subset(p, panels.drop_singletons(p.fes))
+    rng = np.random.default_rng(3)
+    partial = p.y - p.X @ (0.01 * rng.standard_normal(p.k))
+    G = np.asarray(p.levels, dtype=np.int32)
+    def max_means(r):
+        out = []
+        for d in range(len(p.fes)):
+            cnt = np.bincount(p.fes[d], minlength=G[d])
+            m = np.bincount(p.fes[d], weights=r.y_tilde, minlength=G[d])[cnt > 0] / cnt[cnt > 0]
+            out.append(np.abs(m).max())
+        return max(out)
+
+    plain = absorber.absorb(partial, None, p.fes, G, None, pkg.make_options(tol=1e-10))
+    assert plain.converged and max_means(plain) > 1e-8  # the L2 stop alone
+    r = absorber.absorb(partial, None, p.fes, G, None,
+                        pkg.make_options(tol=1e-10, fe_linf_tol=1e-9))
+    assert r.converged and max_means(r) <= 1e-9 * (1 + 1e-6)
+    # a bound below the rounding floor: the round that cannot reach it is undone
+    tight = absorber.absorb(partial, None, p.fes, G, None,
+                            pkg.make_options(tol=1e-10, fe_linf_tol=1e-15))
+    assert tight.converged and max_means(tight) <= max_means(plain)
+    rec = pkg.recover_fixed_effects(partial, p.fes, tol=1e-8, fe_tolerance=1e-8)
+    assert rec.converged and rec.max_delta <= 1e-8

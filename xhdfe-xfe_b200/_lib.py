@@ -86,6 +86,7 @@ class Options(ctypes.Structure):
         ("max_outer", ctypes.c_int),
         ("profile", ctypes.c_int),
         ("pass_kernel", ctypes.c_int),
+        ("fe_linf_tol", ctypes.c_double),
     ]
 
 

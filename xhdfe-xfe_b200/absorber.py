@@ -184,7 +184,7 @@ def cuda_backend_available() -> bool:
 def make_options(*, tol=1e-8, tolerance_mode="reghdfe-comparable", precision="mixed",
                  max_iter=10000, certify=True, check_interval=4, reuse_structure=False,
                  inner_tol=1e-5, max_outer=12, profile=False,
-                 pass_kernel=0) -> _lib.Options:
+                 pass_kernel=0, fe_linf_tol=0.0) -> _lib.Options:
     o = _lib.default_options()
     o.tol = float(tol)
     o.tolerance_mode = TOLERANCE_MODES[tolerance_mode] if isinstance(tolerance_mode, str) \
@@ -198,6 +198,7 @@ def make_options(*, tol=1e-8, tolerance_mode="reghdfe-comparable", precision="mi
     o.max_outer = int(max_outer)
     o.profile = 1 if profile else 0
     o.pass_kernel = int(pass_kernel)
+    o.fe_linf_tol = float(fe_linf_tol)
     return o
 
 
@@ -505,10 +506,12 @@ def recover_fixed_effects(partial, fes, weights=None, *, tol=1e-8, fe_tolerance=
     G = [int(g.max()) + 1 if g.size else 1 for g in gids]
     ab = _thread_absorber(device)
     fe_tol = fe_tolerance if fe_tolerance > 0.0 else tol
-    # the check below is absolute (max over groups of the residual's mean), so
-    # the solve runs two orders tighter than the tolerance it must meet
+    # the check below is absolute (the largest group mean of the residual): the
+    # solve runs two orders tighter than the tolerance it must meet and stops
+    # only when every group mean is within half of it
     solve_tol = max(min(tol, fe_tol) * 1e-2, 1e-14)
-    res = ab.absorb(partial, None, gids, G, weights, make_options(tol=solve_tol, **options),
+    res = ab.absorb(partial, None, gids, G, weights,
+                    make_options(tol=solve_tol, fe_linf_tol=0.5 * fe_tol, **options),
                     save_fe=True)
     contrib = [res.fe[d][gids[d], 0] for d in range(len(gids))]
     out = FeRecoveryResult(contributions=contrib, iterations=res.iterations)

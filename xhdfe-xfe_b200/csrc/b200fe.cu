@@ -160,6 +160,7 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
 
     double *Wall, *Eall;
     B_CHECK(get_buf(ctx, "diagW", std::max<int64_t>(st.GR, 1), &Wall));
+    st.w_rows = Wall;
     B_CHECK(get_buf(ctx, "diagE", std::max<int64_t>(st.GR, 1), &Eall));
 
     // large dims: ids in primary order, runs, sorted run order, chunks, diagonal
@@ -1070,19 +1071,49 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             for (int c = 0; c < cols && c < CP; ++c)
                 thr64[c] = std::max(tol * tol * bb[c], fl * fl * opn2 * vnorm2[c]);
         }
+        // fe_linf_tol: the largest group mean of the within transform, per column
+        const bool linf_on = o.fe_linf_tol > 0.0 && st.w_rows != nullptr;
+        std::vector<double> linf(CP, 0.0);
+        unsigned long long* linf_d = nullptr;
+        if (linf_on) B_CHECK(get_buf(ctx, "linf_bits", CP, &linf_d));
+        auto read_linf = [&]() -> int {
+            B_TRY(cudaMemsetAsync(linf_d, 0, sizeof(unsigned long long) * CP, s));
+            row_linf_kernel<<<rgrid, kRowThreads, 0, s>>>(GR, CP, cols, r64, st.w_rows, linf_d);
+            B_LAUNCHED();
+            std::vector<unsigned long long> bits(CP);
+            B_TRY(cudaMemcpyAsync(bits.data(), linf_d, sizeof(unsigned long long) * CP,
+                                  cudaMemcpyDeviceToHost, s));
+            B_TRY(cudaStreamSynchronize(s));
+            for (int c = 0; c < CP; ++c) std::memcpy(&linf[c], &bits[c], sizeof(double));
+            return B200FE_OK;
+        };
+        if (linf_on) B_CHECK(read_linf());
+        // rounds driven by the group-mean bound alone get a bounded inner budget,
+        // and one that raises the residual (its rhs was rounding noise) is undone
+        double* a_prev = nullptr;
+        double* r_prev = nullptr;
+        if (linf_on) {
+            B_CHECK(get_buf(ctx, "a64_prev", GR * CP, &a_prev));
+            B_CHECK(get_buf(ctx, "r64_prev", GR * CP, &r_prev));
+        }
+        int first_round_its = 0;
+        bool linf_stuck = false;
         const int max_outer = std::max(1, o.max_outer);
         converged = false;
         for (outer = 0; outer < max_outer; ++outer) {
-            bool all = true;
+            bool all = true, linf_only = true;
             std::vector<double> scale(CP, 0.0), inv_scale(CP, 0.0), thr(CP, 0.0);
             for (int c = 0; c < cols && c < CP; ++c) {
-                const bool done = !(rr[c] > thr64[c]);
-                if (!done) {
+                const bool l2_done = !(rr[c] > thr64[c]);
+                const bool linf_done = !linf_on || linf_stuck || !(linf[c] > o.fe_linf_tol);
+                if (!(l2_done && linf_done) && rr[c] > 0.0) {
                     all = false;
+                    if (!l2_done) linf_only = false;
                     scale[c] = std::sqrt(rr[c]);
                     inv_scale[c] = 1.0 / scale[c];
                     // inner target relative to this round's rhs
-                    double t_in = 0.5 * std::sqrt(thr64[c] / rr[c]);
+                    double t_in = l2_done ? 0.5 : 0.5 * std::sqrt(thr64[c] / rr[c]);
+                    if (!linf_done) t_in = std::min(t_in, 0.1 * o.fe_linf_tol / linf[c]);
                     if (mixed) t_in = std::max(t_in, o.inner_tol);
                     t_in = std::min(t_in, 0.5);
                     thr[c] = t_in * t_in;  // rhs is normalised to unit norm
@@ -1093,6 +1124,13 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                 break;
             }
             if (total_iters >= o.max_iter) break;
+            int round_cap = o.max_iter - total_iters;
+            const std::vector<double> rr_before = rr;
+            if (linf_on && linf_only) {
+                round_cap = std::min(round_cap, std::max(50, 2 * first_round_its));
+                B_TRY(cudaMemcpyAsync(a_prev, a64, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
+                B_TRY(cudaMemcpyAsync(r_prev, r64, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
+            }
             B_TRY(cudaMemcpyAsync(scale_d, scale.data(), sizeof(double) * CP, cudaMemcpyHostToDevice, s));
             B_TRY(cudaMemcpyAsync(inv_scale_d, inv_scale.data(), sizeof(double) * CP,
                                   cudaMemcpyHostToDevice, s));
@@ -1101,7 +1139,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                 scale_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, r32);
                 B_LAUNCHED();
                 B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.run_w32, st.block_w32, st.dinv32, x32, r32, z32, p32, q32, thr,
-                                        o.max_iter - total_iters, std::max(1, o.check_interval),
+                                        round_cap, std::max(1, o.check_interval),
                                         &its)));
                 axpy_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x32, scale_d, a64);
                 B_LAUNCHED();
@@ -1109,7 +1147,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                 scale_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, rin64);
                 B_LAUNCHED();
                 B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
-                                         o.max_iter - total_iters, std::max(1, o.check_interval),
+                                         round_cap, std::max(1, o.check_interval),
                                          &its)));
                 axpy_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x64, scale_d, a64);
                 B_LAUNCHED();
@@ -1123,11 +1161,26 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                                                                          dot_ticket, dot_res);
             B_LAUNCHED();
             B_CHECK(sync_read_double(ctx, dot_res, CP, rr.data()));
+            if (outer == 0) first_round_its = its;
+            if (linf_on && linf_only) {
+                bool worse = false;
+                for (int c = 0; c < cols && c < CP; ++c) worse = worse || rr[c] > rr_before[c];
+                if (worse) {  // the bound is below what rounding allows: keep the last a
+                    B_TRY(cudaMemcpyAsync(a64, a_prev, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
+                    B_TRY(cudaMemcpyAsync(r64, r_prev, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
+                    rr = rr_before;
+                    linf_stuck = true;
+                    continue;
+                }
+            }
+            if (linf_on) B_CHECK(read_linf());
         }
         if (!converged) {
             bool all = true;
-            for (int c = 0; c < cols && c < CP; ++c)
+            for (int c = 0; c < cols && c < CP; ++c) {
                 if (rr[c] > thr64[c]) all = false;
+                if (linf_on && !linf_stuck && linf[c] > o.fe_linf_tol && rr[c] > 0.0) all = false;
+            }
             converged = all;
         }
         // residual relative to the scale the stop rule uses (||b_c|| or the floor)

@@ -77,6 +77,7 @@ struct Structure {
     float* wp32 = nullptr;
     uint32_t* sid = nullptr;
     double* dinv64 = nullptr;
+    double* w_rows = nullptr;  // [GR] level weight of every alpha row
     float* dinv32 = nullptr;
     int32_t* gp = nullptr;  // primary ids in primary order (setup only)
     int SG = 0;             // bin rows over all small dims

@@ -14,6 +14,26 @@
 
 namespace b200fe {
 
+// out[c] = bits of max over alpha rows g with W_g > 0 of |r[g][c]| / W_g (the
+// largest group mean of the within transform, by dimension-row); the maximum
+// of non-negative doubles is taken on their bit patterns (integer atomics:
+// exact and order-free)
+__global__ void row_linf_kernel(int64_t GR, int CP, int cols, const double* __restrict__ r,
+                                const double* __restrict__ w_rows,
+                                unsigned long long* __restrict__ out) {
+    const int64_t total = GR * CP;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t g = e / CP;
+        const int c = static_cast<int>(e - g * CP);
+        const double W = w_rows[g];
+        if (c < cols && W > 0.0) {
+            const double v = fabs(r[e]) / W;
+            if (v > 0.0) atomicMax(out + c, static_cast<unsigned long long>(__double_as_longlong(v)));
+        }
+    }
+}
+
 __global__ void to_float_kernel(const double* __restrict__ src, int64_t n, float* __restrict__ dst) {
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)

@@ -117,6 +117,7 @@ bool absorb_fixed_effects_cuda(const Eigen::Ref<const Eigen::VectorXd>& y,
             // check): solve two orders tighter than that
             const double fe_tol = options.fe_tolerance > 0.0 ? options.fe_tolerance : o.tol;
             o.tol = std::max(std::min(o.tol, fe_tol) * 1e-2, 1e-14);
+            o.fe_linf_tol = 0.5 * fe_tol;  // every group mean within half the check's bound
         }
         // contiguous copies: Eigen::Ref may have an inner stride
         const Eigen::VectorXd yc = y;
