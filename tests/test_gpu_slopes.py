@@ -229,6 +229,53 @@ def test_slopes_schur_long_primary_groups(absorber, pkg, weighted):
     assert a.precision_certified
 
 
+def _slope_primary_case(k, seed, weighted, intercept, long_share):
+    """Primary groups (the most groups) with their own slope t: mostly 1-7
+    rows, long_share of them 65-300 rows; t constant inside every 97th group."""
+    rng = np.random.default_rng(seed)
+    sizes = np.where(rng.random(k) < long_share, rng.integers(65, 300, k), rng.integers(1, 8, k))
+    g1 = np.repeat(np.arange(k), sizes).astype(np.int32)
+    n = g1.size
+    g2 = rng.integers(0, max(20, k // 20), n).astype(np.int32)
+    g3 = rng.integers(0, 10, n).astype(np.int32)
+    t = rng.uniform(0.0, 5.0, n)
+    t[g1 % 97 == 5] = 2.0
+    X = rng.standard_normal((n, 3))
+    y = X @ np.array([0.5, -1.0, 0.2]) + 0.3 * t * (g1 % 5) + rng.standard_normal(n)
+    w = rng.uniform(0.3, 3.0, n) if weighted else None
+    return dict(y=y, X=X, fes=[g1, g2, g3], slopes=[(0, t, intercept)], weights=w)
+
+
+@pytest.mark.parametrize("intercept", [True, False])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_slopes_schur_slope_primary_exact(absorber, pkg, weighted, intercept):
+    """worker##c.t (2x2 primary blocks) and worker#c.t (slope only) eliminated
+    exactly: the oracle's projection, with one-row groups and groups of
+    constant t on the pseudo-inverse and long groups on the fix-up path."""
+    c = _slope_primary_case(500, 41, weighted, intercept, 0.02)
+    G = [int(f.max()) + 1 for f in c["fes"]]
+    assert G[0] > G[1] and np.bincount(c["fes"][0]).max() > 64
+    r = _oracle_check(absorber, pkg, c["y"], c["X"], c["fes"], G, c["slopes"], c["weights"])
+    assert r.converged and r.primary_dim == 0
+
+
+@pytest.mark.parametrize("intercept", [True, False])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_slopes_schur_slope_primary_agrees(absorber, pkg, weighted, intercept):
+    """A slope primary eliminated exactly vs block Jacobi over every
+    dimension on a 12k-group panel: same projection, fewer iterations."""
+    c = _slope_primary_case(12_000, 42, weighted, intercept, 0.01)
+    a = _absorb(absorber, pkg, c, tol=1e-11)
+    b = _absorb(absorber, pkg, c, tol=1e-11, pass_kernel=1)
+    assert a.converged and b.converged and a.primary_dim == 0
+    Va = np.column_stack([a.y_tilde, a.X_tilde])
+    Vb = np.column_stack([b.y_tilde, b.X_tilde])
+    scale = np.linalg.norm(np.column_stack([c["y"], c["X"]]), axis=0)
+    assert (np.linalg.norm(Va - Vb, axis=0) / scale).max() <= 1e-9
+    assert a.iterations < b.iterations
+    assert a.precision_certified
+
+
 def test_slopes_many_columns(absorber, pkg, panels):
     """40 columns (two column words per lane) through both forms."""
     p, sl = panels.akm_firm_tenure_slopes(20_000, n_firms=300, seed=31)

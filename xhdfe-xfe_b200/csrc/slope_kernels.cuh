@@ -537,17 +537,74 @@ __global__ void row_edges_kernel(const int32_t* __restrict__ gptr, const int32_t
 }
 
 // ---------------------------------------------------------------------------
-// Schur form (a plain primary dimension eliminated exactly).  The CGLS runs on
+// Schur form (the primary dimension eliminated exactly).  The CGLS runs on
 // min || (I - P_p)(v - D_r a) ||_W over the other dimensions' coefficients a,
-// P_p the W-projection on the primary groups (segment means in primary
-// order).  Its block-Jacobi preconditioner is the exact block diagonal of the
+// P_p the W-projection on the primary groups' bases (segment sums in primary
+// order times the groups' block inverses).  Its block-Jacobi preconditioner is the exact block diagonal of the
 // Schur complement D_r' W (I - P_p) D_r: for group g of dimension d,
-//   S_g = B_g - sum over primary groups j meeting g of c_jg c_jg' / W_j,
-// c_jg the sums of the basis multipliers (w, w z) over the rows in (j, g).
+//   S_g = B_g - sum over primary groups j meeting g of C_jg' M_j^-1 C_jg,
+// C_jg the sums over the rows in (j, g) of w times the primary basis (1, and
+// the primary's slope t when it has one) times g's basis (1, z), and M_j^-1
+// the primary group's block inverse (1 / W_j for a primary without slope).
 // In dimension d's stable sorted order the rows of g are in primary order, so
 // every pair (j, g) is one contiguous run there.
 // ---------------------------------------------------------------------------
 constexpr double kSchurRel = 1e-11;  // null-space test of a Schur block, relative to B
+
+// A primary with intercept and slope is eliminated in the centred basis
+// (1, t - tbar_g), tbar_g = sum w t / W_g: the same span, but a block close to
+// diag(W, SS) instead of [W Z; Z ZZ], so projecting a constant off a group
+// leaves rounding of order eps instead of eps * cond(M_g) -- which the CGLS,
+// whose search directions reach the constants shared by the primary and the
+// other dimensions' intercepts, would otherwise pump up.
+__global__ void slope_group_center_kernel(const SlopeDim d, const double* __restrict__ cm,
+                                          double* __restrict__ tbar) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < d.G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double W = 0.0, Z = 0.0;
+        for (int32_t j = d.grp_ch[g]; j < d.grp_ch[g + 1]; ++j) {
+            W += cm[static_cast<int64_t>(j) * 5];
+            Z += cm[static_cast<int64_t>(j) * 5 + 1];
+        }
+        tbar[g] = W > 0.0 ? Z / W : 0.0;
+    }
+}
+
+// zc[k] = t[k] - tbar[ids[k]] (primary order)
+__global__ void slope_center_rows_kernel(const int32_t* __restrict__ ids, const double* __restrict__ t,
+                                         const double* __restrict__ tbar, int64_t n,
+                                         double* __restrict__ zc) {
+    for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        zc[k] = t[k] - tbar[ids[k]];
+}
+
+// Block inverse in the centred basis from the centred chunk moments; the
+// slope stays in a group's basis where the reference's rule kept it on the
+// uncentred block (minv_u[g][2] != 0).
+__global__ void slope_centred_inverse_kernel(const SlopeDim d, const double* __restrict__ cm,
+                                             const double* __restrict__ minv_u,
+                                             double* __restrict__ minv) {
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < d.G;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double W = 0.0, Z = 0.0, SS = 0.0;
+        for (int32_t j = d.grp_ch[g]; j < d.grp_ch[g + 1]; ++j) {
+            W += cm[static_cast<int64_t>(j) * 5];
+            Z += cm[static_cast<int64_t>(j) * 5 + 1];
+            SS += cm[static_cast<int64_t>(j) * 5 + 2];
+        }
+        double m00 = W > 0.0 ? 1.0 / W : 0.0, m01 = 0.0, m11 = 0.0;
+        const double det = W * SS - Z * Z;
+        if (minv_u[g * 3 + 2] != 0.0 && W > 0.0 && det > 0.0) {
+            m00 = SS / det;
+            m01 = -Z / det;
+            m11 = W / det;
+        }
+        minv[g * 3 + 0] = m00;
+        minv[g * 3 + 1] = m01;
+        minv[g * 3 + 2] = m11;
+    }
+}
 
 // flag[pos] = 1 where a (primary group, group of d) pair starts in d's order
 __global__ void pair_flags_kernel(const int32_t* __restrict__ perm, const int32_t* __restrict__ ids_d,
@@ -574,26 +631,44 @@ __global__ void pair_start_kernel(const int32_t* __restrict__ flag, const int32_
     }
 }
 
-// per pair: (c_a^2, c_a c_b, c_b^2) / W_j, c = sums of w and w z over its rows
-// (three planes of npairs values)
-__global__ void pair_contrib_kernel(const SlopeDim d, const int32_t* __restrict__ ids_p,
-                                    const double* __restrict__ minv_p, const double* __restrict__ w,
+// per pair (j, g): the entries (aa, ab, bb) of C' M_j^-1 C, C[m][f] the sum over
+// the pair's rows of w times the primary basis function m (1, the primary's
+// slope t) times g's basis function f (1, z), M_j the primary group's block --
+// (c_a^2, c_a c_b, c_b^2) / W_j for a primary without slope (three planes of
+// npairs values)
+__global__ void pair_contrib_kernel(const SlopeDim d, const SlopeDim P,
+                                    const double* __restrict__ w,
                                     const int32_t* __restrict__ start, int64_t npairs,
                                     double* __restrict__ contrib) {
     for (int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < npairs;
          q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        double ca = 0.0, cb = 0.0;
+        double ca = 0.0, cb = 0.0, ta = 0.0, tb = 0.0;  // rows 1 and t of C
         const int32_t b = start[q], e = start[q + 1];
         for (int32_t pos = b; pos < e; ++pos) {
             const int32_t k = d.perm[pos];
             const double wk = w ? w[k] : 1.0;
+            const double wz = d.has_b ? wk * d.z[k] : 0.0;
             ca += wk;
-            if (d.has_b) cb = fma(wk, d.z[k], cb);
+            cb += wz;
+            if (P.has_b) {
+                ta = fma(wk, P.z[k], ta);
+                tb = fma(wz, P.z[k], tb);
+            }
         }
-        const double iw = minv_p[static_cast<int64_t>(ids_p[d.perm[b]]) * 3];  // 1 / W_j
-        contrib[q] = ca * ca * iw;
-        contrib[npairs + q] = ca * cb * iw;
-        contrib[2 * npairs + q] = cb * cb * iw;
+        const double* mj = P.minv + static_cast<int64_t>(P.ids[d.perm[b]]) * 3;
+        if (!P.has_b) {
+            contrib[q] = ca * ca * mj[0];
+            contrib[npairs + q] = ca * cb * mj[0];
+            contrib[2 * npairs + q] = cb * cb * mj[0];
+        } else {
+            // u' M v for the columns u, v of C
+            auto qf = [&](double u0, double u1, double v0, double v1) {
+                return mj[0] * u0 * v0 + mj[1] * (u0 * v1 + u1 * v0) + mj[2] * u1 * v1;
+            };
+            contrib[q] = qf(ca, ta, ca, ta);
+            contrib[npairs + q] = qf(ca, ta, cb, tb);
+            contrib[2 * npairs + q] = qf(cb, tb, cb, tb);
+        }
     }
 }
 
@@ -658,19 +733,22 @@ schur_block_inverse_kernel(const SlopeDim d, const double* __restrict__ cm,
     if (threadIdx.x == 0) part_op[blockIdx.x] = red[0];
 }
 
-// X[k][c] -= mean[ids_p[k]][c] (the primary groups' weighted means), with CTA
-// partials of sum w x^2 per column when part is not null.
+// X[k][c] -= the fit of row k on its primary group's basis (the group's
+// weighted mean, or intercept + slope t_k; P.zv[g] holds M_g^-1 B_g' W x), with
+// CTA partials of sum w x^2 per column when part is not null.
 __global__ void __launch_bounds__(kSlopeThreads)
-slope_project_kernel(double* __restrict__ X, const int32_t* __restrict__ ids_p,
-                     const double* __restrict__ mean, const double* __restrict__ w, int64_t n,
-                     int C, int RB, double* __restrict__ part) {
+slope_project_kernel(double* __restrict__ X, const SlopeDim P, const double* __restrict__ w,
+                     int64_t n, int C, int RB, double* __restrict__ part) {
     __shared__ double red[kSlopeThreads];
     const int col = threadIdx.x % C, rr = threadIdx.x / C;
     double acc = 0.0;
     if (rr < RB) {
         for (int64_t k = static_cast<int64_t>(blockIdx.x) * RB + rr; k < n;
              k += static_cast<int64_t>(gridDim.x) * RB) {
-            const double x = X[k * C + col] - mean[static_cast<int64_t>(ids_p[k]) * C + col];
+            const double* zg = P.zv + (static_cast<int64_t>(P.ids[k]) * P.nb) * C + col;
+            double fit = P.has_a ? zg[0] : 0.0;
+            if (P.has_b) fit = fma(P.z[k], zg[P.has_a ? C : 0], fit);
+            const double x = X[k * C + col] - fit;
             X[k * C + col] = x;
             const double wk = w ? w[k] : 1.0;
             acc = fma(wk * x, x, acc);
@@ -695,9 +773,11 @@ struct SchurGatherArgs {
     const int32_t* ch_end;
     const int32_t* ch_grp;    // primary chunk -> group
     const int32_t* grp_ch;    // primary group -> first chunk
-    const double* minv_p;     // [Gp][3], m00 = 1 / W
+    const double* minv_p;     // [Gp][3] block inverse of the primary groups
+    const double* z_p;        // [n] the primary's slope values, or null
+    int p_has_a, p_has_b, p_nb;
     int32_t nch;
-    double* part_p;           // [nch][C] sums of w q of multi-chunk groups' chunks
+    double* part_p;           // [nch][p_nb][C] sums of w q (and w t q) of multi-chunk groups' chunks
     int64_t n;
     int C, slots;
     const double* w;
@@ -726,6 +806,7 @@ __global__ void __launch_bounds__(kSlopeThreads)
 schur_gather_kernel(const SchurGatherArgs a) {
     constexpr int kSchurRows = CW == 1 ? 8 : (CW == 2 ? 4 : (CW == 4 ? 2 : 1));
     __shared__ double sred[kSlopeThreads / 32][32];
+    __shared__ double tred[kSlopeThreads / 32][32];
     __shared__ double dred[kSlopeThreads / 32][32 * CW];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int C = a.C;
@@ -741,9 +822,9 @@ schur_gather_kernel(const SchurGatherArgs a) {
          j += nw) {
         const int32_t b = a.ch_beg[j], e = a.ch_end[j], g = a.ch_grp[j];
         const bool single = a.grp_ch[g + 1] - a.grp_ch[g] == 1;
-        double sw[CW];
+        double sw[CW], st[CW];  // sums of w q and of w t q (t: the primary's slope values)
 #pragma unroll
-        for (int u = 0; u < CW; ++u) sw[u] = 0.0;
+        for (int u = 0; u < CW; ++u) sw[u] = st[u] = 0.0;
         // the lane's first kSchurRows rows: formed together (their loads in
         // flight at once) and kept in registers for the second phase
         double qc[kSchurRows][CW];
@@ -762,11 +843,13 @@ schur_gather_kernel(const SchurGatherArgs a) {
                 const int32_t pos = b + slot + t * S;
                 if (pos < e) {
                     const double wk = a.w ? a.w[pos] : 1.0;
+                    const double tk = a.p_has_b ? a.z_p[pos] : 0.0;
 #pragma unroll
                     for (int u = 0; u < CW; ++u) {
                         const int c = col0 + 32 * u;
                         if (c < C) {
                             sw[u] = fma(wk, qc[t][u], sw[u]);
+                            if (a.p_has_b) st[u] = fma(wk * tk, qc[t][u], st[u]);
                             if (!single) a.Q[static_cast<int64_t>(pos) * C + c] = qc[t][u];
                         }
                     }
@@ -774,36 +857,56 @@ schur_gather_kernel(const SchurGatherArgs a) {
             }
             for (int32_t pos = b + slot + kSchurRows * S; pos < e; pos += S) {
                 const double wk = a.w ? a.w[pos] : 1.0;
+                const double tk = a.p_has_b ? a.z_p[pos] : 0.0;
 #pragma unroll
                 for (int u = 0; u < CW; ++u) {
                     const int c = col0 + 32 * u;
                     if (c < C) {
                         const double q = schur_q<ND>(a, pos, c);
                         sw[u] = fma(wk, q, sw[u]);
+                        if (a.p_has_b) st[u] = fma(wk * tk, q, st[u]);
                         if (!single) a.Q[static_cast<int64_t>(pos) * C + c] = q;
                     }
                 }
             }
         }
         // column totals over the row slots, in slot order, seen by every lane
-        double tot[CW];
+        double tot[CW], tot_t[CW];
         if (CW == 1) {
             sred[wid][lane] = sw[0];
+            tred[wid][lane] = st[0];
             __syncwarp();
-            double t = 0.0;
+            double t0 = 0.0, t1 = 0.0;
             if (live && col0 < C)
-                for (int sl = 0; sl < S; ++sl) t += sred[wid][sl * C + col0];
-            tot[0] = t;
+                for (int sl = 0; sl < S; ++sl) {
+                    t0 += sred[wid][sl * C + col0];
+                    t1 += tred[wid][sl * C + col0];
+                }
+            tot[0] = t0;
+            tot_t[0] = t1;
             __syncwarp();
         } else {
 #pragma unroll
-            for (int u = 0; u < CW; ++u) tot[u] = sw[u];
+            for (int u = 0; u < CW; ++u) {
+                tot[u] = sw[u];
+                tot_t[u] = st[u];
+            }
         }
         if (single) {
-            const double iw = a.minv_p[static_cast<int64_t>(g) * 3];
+            // the group's fit al + be t, (al, be) = M_g^-1 (sum w q, sum w t q)
+            const double* mg = a.minv_p + static_cast<int64_t>(g) * 3;
+            double al[CW], be[CW];
+#pragma unroll
+            for (int u = 0; u < CW; ++u) {
+                const double sa = a.p_has_a ? tot[u] : 0.0;
+                const double sb = a.p_has_b ? tot_t[u] : 0.0;
+                al[u] = a.p_has_b ? fma(mg[0], sa, mg[1] * sb) : sa * mg[0];
+                be[u] = a.p_has_b ? fma(mg[1], sa, mg[2] * sb) : 0.0;
+            }
             if (live) {
                 for (int32_t t = 0, pos = b + slot; pos < e; ++t, pos += S) {
                     const double wk = a.w ? a.w[pos] : 1.0;
+                    const double tk = a.p_has_b ? a.z_p[pos] : 0.0;
 #pragma unroll
                     for (int u = 0; u < CW; ++u) {
                         const int c = col0 + 32 * u;
@@ -816,7 +919,7 @@ schur_gather_kernel(const SchurGatherArgs a) {
                             } else {
                                 q = schur_q<ND>(a, pos, c);
                             }
-                            const double x = q - tot[u] * iw;
+                            const double x = q - (a.p_has_b ? fma(be[u], tk, al[u]) : al[u]);
                             a.Q[static_cast<int64_t>(pos) * C + c] = x;
                             dacc[u] = fma(wk * x, x, dacc[u]);
                         }
@@ -827,7 +930,11 @@ schur_gather_kernel(const SchurGatherArgs a) {
 #pragma unroll
             for (int u = 0; u < CW; ++u) {
                 const int c = col0 + 32 * u;
-                if (c < C) a.part_p[j * C + c] = tot[u];
+                if (c < C) {
+                    double* pj = a.part_p + (j * a.p_nb) * C + c;
+                    if (a.p_has_a) pj[0] = tot[u];
+                    if (a.p_has_b) pj[a.p_has_a ? C : 0] = tot_t[u];
+                }
             }
         }
     }
@@ -849,32 +956,41 @@ schur_gather_kernel(const SchurGatherArgs a) {
     }
 }
 
-// mean[g] = (sum of g's chunk sums, in chunk order) / W_g for the listed
-// multi-chunk primary groups, into mean_p[g][C]
+// the fit of the listed multi-chunk primary groups: their chunk sums, in chunk
+// order, times the group's block inverse, into P.zv[g][nb][C]
 __global__ void schur_fix_mean_kernel(const int32_t* __restrict__ groups, int32_t ngroups,
-                                      const int32_t* __restrict__ grp_ch,
-                                      const double* __restrict__ part_p,
-                                      const double* __restrict__ minv_p, int C,
-                                      double* __restrict__ mean_p) {
+                                      const SlopeDim P, int C) {
     const int64_t total = static_cast<int64_t>(ngroups) * C;
     for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
          e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int64_t i = e / C;
         const int c = static_cast<int>(e - i * C);
         const int32_t g = groups[i];
-        double s = 0.0;
-        for (int32_t j = grp_ch[g]; j < grp_ch[g + 1]; ++j) s += part_p[static_cast<int64_t>(j) * C + c];
-        mean_p[static_cast<int64_t>(g) * C + c] = s * minv_p[static_cast<int64_t>(g) * 3];
+        const int ob = P.has_a ? C : 0;
+        double sa = 0.0, sb = 0.0;
+        for (int32_t j = P.grp_ch[g]; j < P.grp_ch[g + 1]; ++j) {
+            const double* pj = P.part + (static_cast<int64_t>(j) * P.nb) * C + c;
+            if (P.has_a) sa += pj[0];
+            if (P.has_b) sb += pj[ob];
+        }
+        const double* mg = P.minv + static_cast<int64_t>(g) * 3;
+        double* zg = P.zv + (static_cast<int64_t>(g) * P.nb) * C + c;
+        if (P.has_b) {
+            if (P.has_a) zg[0] = fma(mg[0], sa, mg[1] * sb);
+            zg[ob] = fma(mg[1], sa, mg[2] * sb);
+        } else {
+            zg[0] = sa * mg[0];
+        }
     }
 }
 
-// Q -= mean over the rows of the listed chunks (multi-chunk groups), with CTA
-// partials of q' W q; one warp per chunk, row slots as in the gather
+// Q -= the group's fit over the rows of the listed chunks (multi-chunk
+// groups), with CTA partials of q' W q; one warp per chunk, row slots as in
+// the gather
 template <int CW>
 __global__ void __launch_bounds__(kSlopeThreads)
 schur_fix_apply_kernel(const int32_t* __restrict__ chunks, int32_t nchunks,
-                       const int32_t* __restrict__ ch_beg, const int32_t* __restrict__ ch_end,
-                       const int32_t* __restrict__ ch_grp, const double* __restrict__ mean_p,
+                       const int32_t* __restrict__ ch_grp, const SlopeDim P,
                        const double* __restrict__ w, double* __restrict__ Q, int C, int S,
                        double* __restrict__ dpart) {
     __shared__ double dred[kSlopeThreads / 32][32 * CW];
@@ -891,14 +1007,18 @@ schur_fix_apply_kernel(const int32_t* __restrict__ chunks, int32_t nchunks,
         if (!live) continue;
         const int32_t j = chunks[i];
         const int32_t g = ch_grp[j];
-        for (int32_t pos = ch_beg[j] + slot; pos < ch_end[j]; pos += S) {
+        const double* zg = P.zv + (static_cast<int64_t>(g) * P.nb) * C;
+        for (int32_t pos = P.ch_beg[j] + slot; pos < P.ch_end[j]; pos += S) {
             const double wk = w ? w[pos] : 1.0;
+            const double tk = P.has_b ? P.z[pos] : 0.0;
 #pragma unroll
             for (int u = 0; u < CW; ++u) {
                 const int c = col0 + 32 * u;
                 if (c < C) {
                     const int64_t o = static_cast<int64_t>(pos) * C + c;
-                    const double x = Q[o] - mean_p[static_cast<int64_t>(g) * C + c];
+                    double fit = P.has_a ? zg[c] : 0.0;
+                    if (P.has_b) fit = fma(tk, zg[c + (P.has_a ? C : 0)], fit);
+                    const double x = Q[o] - fit;
                     Q[o] = x;
                     dacc[u] = fma(wk * x, x, dacc[u]);
                 }

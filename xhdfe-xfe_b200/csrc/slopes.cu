@@ -260,9 +260,9 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
             }
         }
     }
-    // ---- Schur form: a plain primary dimension eliminated exactly (auto, or
+    // ---- Schur form: the primary dimension eliminated exactly (auto, or
     // pass_kernel 1 for block Jacobi over every dimension)
-    const bool schur = !gi && p >= 0 && !dims[p].has_b && nd >= 2 && o.pass_kernel != 1;
+    const bool schur = !gi && p >= 0 && nd >= 2 && o.pass_kernel != 1;
     std::vector<int> cg;  // dimensions the CG runs over, in pass order (writer last)
     for (int i = 0; i < no; ++i)
         if (!(schur && order[i] == p)) cg.push_back(order[i]);
@@ -271,6 +271,28 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
     // (slope_update_kernel) and the CG dims' passes read it through their
     // permutations; otherwise the primary's in-order segment pass stores it.
     const int writer = schur ? -1 : p;
+    if (schur && dims[p].has_a && dims[p].has_b) {
+        // the primary's slope in the centred basis (same span, well-conditioned
+        // blocks); the certificate's primary share is then taken in that basis
+        SlopeDim& P = dims[p];
+        double *cm, *tbar, *zc, *minv_c;
+        B_CHECK(get_buf(ctx, "sl_cm", static_cast<size_t>(P.nch) * 5, &cm));
+        B_CHECK(get_buf(ctx, "sl_tbar", P.G, &tbar));
+        B_CHECK(get_buf(ctx, "sl_zc", n, &zc));
+        B_CHECK(get_buf(ctx, "sl_minvc", static_cast<size_t>(P.G) * 3, &minv_c));
+        slope_moments_kernel<<<grid_for(ctx, static_cast<int64_t>(P.nch) * 32, T), T, 0, s>>>(P, w, cm);
+        B_LAUNCHED();
+        slope_group_center_kernel<<<grid_for(ctx, P.G, T), T, 0, s>>>(P, cm, tbar);
+        B_LAUNCHED();
+        slope_center_rows_kernel<<<grid_for(ctx, n, T), T, 0, s>>>(P.ids, P.z, tbar, n, zc);
+        B_LAUNCHED();
+        P.z = zc;
+        slope_moments_kernel<<<grid_for(ctx, static_cast<int64_t>(P.nch) * 32, T), T, 0, s>>>(P, w, cm);
+        B_LAUNCHED();
+        slope_centred_inverse_kernel<<<grid_for(ctx, P.G, T), T, 0, s>>>(P, cm, P.minv, minv_c);
+        B_LAUNCHED();
+        P.minv = minv_c;
+    }
     if (schur) {
         for (int d : cg) {
             SlopeDim& D = dims[d];
@@ -288,8 +310,8 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
             pair_start_kernel<<<grid_for(ctx, n + 1, T), T, 0, s>>>(flag, pid, n, start);
             B_LAUNCHED();
             B_CHECK(get_buf(ctx, "sl_contrib", static_cast<size_t>(np) * 3, &contrib));
-            pair_contrib_kernel<<<grid_for(ctx, np, T), T, 0, s>>>(D, dims[p].ids, dims[p].minv, w,
-                                                                   start, np, contrib);
+            pair_contrib_kernel<<<grid_for(ctx, np, T), T, 0, s>>>(D, dims[p], w, start, np,
+                                                                   contrib);
             B_LAUNCHED();
             B_CHECK(get_buf(ctx, "sl_off" + sx, static_cast<size_t>(D.G) + 1, &off));
             // per group sums of the pair planes: one block per group, fixed order
@@ -451,14 +473,14 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         B_LAUNCHED();
         return B200FE_OK;
     };
-    // X -= its weighted primary-group means (Schur form), with partials of
-    // x' W x into pq when dots is set
+    // X -= its W-projection on the primary groups' bases (Schur form), with
+    // partials of x' W x into pq when dots is set
     auto project = [&](double* X, bool dots) -> int {
         B_CHECK(segment(p, false, X));
-        B_CHECK(finalize(p, ncg));  // zv of the primary = the group means
-        ProfScope ps(ctx, B200FE_PROF_GATHER, n * (16.0 * C + 4.0 + wb) + 8.0 * dims[p].G * C);
-        slope_project_kernel<<<gG, C * RB, 0, s>>>(X, dims[p].ids, dims[p].zv, w, n, C, RB,
-                                                   dots ? pq : nullptr);
+        B_CHECK(finalize(p, ncg));  // zv of the primary = M_g^-1 B_g' W x
+        ProfScope ps(ctx, B200FE_PROF_GATHER, n * (16.0 * C + 4.0 + wb + (dims[p].has_b ? 8.0 : 0.0)) +
+                                                   8.0 * dims[p].G * dims[p].nb * C);
+        slope_project_kernel<<<gG, C * RB, 0, s>>>(X, dims[p], w, n, C, RB, dots ? pq : nullptr);
         B_LAUNCHED();
         return B200FE_OK;
     };
@@ -532,6 +554,10 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         sga.ch_grp = p_ch_grp;
         sga.grp_ch = P.grp_ch;
         sga.minv_p = P.minv;
+        sga.z_p = P.z;
+        sga.p_has_a = P.has_a;
+        sga.p_has_b = P.has_b;
+        sga.p_nb = P.nb;
         sga.nch = P.nch;
         sga.part_p = P.part;
         sga.n = n;
@@ -561,26 +587,22 @@ int slopes_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int C,
         if (n_multi_chunks) {
             ProfScope ps(ctx, B200FE_PROF_FINALIZE, 0.0);
             schur_fix_mean_kernel<<<grid_for(ctx, static_cast<int64_t>(n_multi_groups) * C, T), T, 0, s>>>(
-                multi_groups, n_multi_groups, dims[p].grp_ch, dims[p].part, dims[p].minv, C,
-                dims[p].zv);
+                multi_groups, n_multi_groups, dims[p], C);
             B_LAUNCHED();
             const int S = CW == 1 ? 32 / C : 1;
+            const SlopeDim& P = dims[p];
             if (CW == 1)
-                schur_fix_apply_kernel<1><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, dims[p].ch_beg,
-                                                            dims[p].ch_end, p_ch_grp, dims[p].zv, w, Q,
-                                                            C, S, pq2);
+                schur_fix_apply_kernel<1><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, p_ch_grp, P, w,
+                                                            Q, C, S, pq2);
             else if (CW == 2)
-                schur_fix_apply_kernel<2><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, dims[p].ch_beg,
-                                                            dims[p].ch_end, p_ch_grp, dims[p].zv, w, Q,
-                                                            C, S, pq2);
+                schur_fix_apply_kernel<2><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, p_ch_grp, P, w,
+                                                            Q, C, S, pq2);
             else if (CW == 4)
-                schur_fix_apply_kernel<4><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, dims[p].ch_beg,
-                                                            dims[p].ch_end, p_ch_grp, dims[p].zv, w, Q,
-                                                            C, S, pq2);
+                schur_fix_apply_kernel<4><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, p_ch_grp, P, w,
+                                                            Q, C, S, pq2);
             else
-                schur_fix_apply_kernel<8><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, dims[p].ch_beg,
-                                                            dims[p].ch_end, p_ch_grp, dims[p].zv, w, Q,
-                                                            C, S, pq2);
+                schur_fix_apply_kernel<8><<<gF, T, 0, s>>>(multi_chunks, n_multi_chunks, p_ch_grp, P, w,
+                                                            Q, C, S, pq2);
             B_LAUNCHED();
         }
         return B200FE_OK;
