@@ -66,14 +66,15 @@ def parse():
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--workload", default="akm3",
-                    choices=["akm3", "slopes", "gi", "kss", "ols", "prep", "savefe"],
+                    choices=["akm3", "slopes", "gi", "kss", "ols", "prep", "savefe", "batch"],
                     help="akm3: the headline workload; slopes: the same panel with "
                          "firm-specific tenure slopes (firm##c.tenure); gi: 10M groups "
                          "with individual FEs (group/individual design); kss: the KSS firm "
                          "system of a 10M-obs panel, 200 right-hand sides; ols: run_ols with "
                          "worker-clustered SEs on the absorbed 50M panel; prep: dense ids, "
                          "singleton cascade and mobility components of the 50M panel; "
-                         "savefe: recover_fixed_effects of a 50M partial residual")
+                         "savefe: recover_fixed_effects of a 50M partial residual; batch: "
+                         "64 independent panels of uneven size, absorption + clustered OLS each")
     return ap.parse_args()
 
 
@@ -1141,8 +1142,183 @@ def run_savefe(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# an uneven batch of independent panels: absorb + worker-clustered OLS each
+# ---------------------------------------------------------------------------
+BATCH_METRIC = ("uneven batch of 64 independent panels (10k-5M obs log-uniform, 2-3 FE dims, "
+                "lognormal(0, 0.5) analytic weights): absorption to 1e-8 + worker-clustered "
+                "OLS per panel, seconds for the whole batch")
+BATCH_PANELS = 64
+BATCH_CPU_SAMPLE = 3_000_000
+
+
+def batch_panels(seed: int):
+    """The batch: sizes log-uniform over 10k-5M rows, 2 or 3 FE dims (worker,
+    firm, year), about 60 rows per firm, lognormal(0, 0.5) analytic weights,
+    singletons dropped; clusters = workers."""
+    panels = ge.load_module("panels")
+    rng = np.random.default_rng(1000 + seed)
+    sizes = np.exp(rng.uniform(np.log(10_000), np.log(5_000_000), BATCH_PANELS)).astype(int)
+    dims = rng.integers(2, 4, BATCH_PANELS)
+    out = []
+    for i, (n, d) in enumerate(zip(sizes, dims)):
+        p = panels.akm_two_way(int(n), n_firms=max(100, int(n) // 60), n_years=20,
+                               seed=seed * 1000 + i, three_way=bool(d == 3))
+        p = panels.subset(p, panels.drop_singletons(p.fes))
+        p.weights = rng.lognormal(0.0, 0.5, p.n)
+        out.append(p)
+    return out
+
+
+def run_batch(args):
+    import oracle
+
+    world, rank, local, dist = init_ranks("nccl") if args.impl == "ours" else (1, 0, 0, None)
+    if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    batch = batch_panels(rank)
+    gen_s = time.perf_counter() - t0
+    rows = sum(p.n for p in batch)
+
+    def cpu_leg():
+        t1 = time.perf_counter()
+        m, used = 0, 0
+        for p in batch:
+            oracle.ref_fit(p.y, p.X, p.fes, p.weights, p.cluster, tol=1e-8, threads=threads,
+                           drop_singletons=False)
+            m += p.n
+            used += 1
+            if m >= BATCH_CPU_SAMPLE:
+                break
+        dt = time.perf_counter() - t1
+        return {"value": dt * rows / m, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": (f"the reference's fit (CPU, {threads} threads, tol 1e-8, cluster "
+                           f"VCE) on the batch's first {used} panels ({m} rows): {dt:.2f} s, "
+                           f"scaled linearly to the batch's {rows} rows")}
+
+    config = {"workload": "batch_64_uneven_panels", "panels": len(batch), "rows": rows,
+              "sizes_min_max": [min(p.n for p in batch), max(p.n for p in batch)],
+              "dims": [len(p.fes) for p in batch], "tol": 1e-8,
+              "l2_policy": "each panel's columns are read several times per solve; the batch "
+                           f"({rows * 3 * 8 / 1e9:.1f} GB of columns) is larger than L2"}
+    if args.impl == "reference":
+        vals, info = [], None
+        for i in range(args.warmup + args.steps):
+            info = cpu_leg()
+            if i >= args.warmup:
+                vals.append(info["value"])
+        v = statistics.median(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": BATCH_METRIC, "value": v, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000.0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded AKM generator)", "config": config, "cpu_baseline": info,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pkg = ge.load_package()
+    absorber = pkg.Absorber(local)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    resident = []
+    for p in batch:
+        v = torch.empty((p.k + 1, p.n), dtype=torch.float64, device=dev)
+        v[0].copy_(torch.from_numpy(p.y))
+        v[1:].copy_(torch.from_numpy(np.ascontiguousarray(p.X.T)))
+        resident.append((v, [torch.from_numpy(f).to(dev) for f in p.fes],
+                         torch.from_numpy(p.weights).to(dev),
+                         torch.from_numpy(p.cluster.astype(np.int32)).to(dev), torch.empty_like(v)))
+    opts = pkg.make_options(tol=1e-8)
+
+    def n_eff(p):
+        return float(p.n - sum(p.levels[1:]))
+
+    def step():
+        rs = []
+        for p, (v, g, w, cl, out) in zip(batch, resident):
+            r = absorber.absorb_device(v, g, p.levels, w, opts, out=out, stream=sh)[1]
+            o = pkg.run_ols(out[0], out[1:], w, cl, se_type="cluster", n_effective=n_eff(p))
+            rs.append((r, o))
+        return rs
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier(dist)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    results = [step() for _ in range(args.steps)]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(dist)
+    clocks = sampler.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, dev)
+    last = results[-1]
+    launches = int(sum(r.kernel_launches for rs in results for r, _ in rs))
+    # end to end through the public API: host arrays, device preprocessing
+    # (dense ids, singleton cascade), absorption, clustered OLS
+    y_h = [torch.from_numpy(p.y).pin_memory().numpy() for p in batch]
+    X_h = [torch.from_numpy(np.ascontiguousarray(p.X.T)).pin_memory().numpy().T for p in batch]
+
+    def e2e_step():
+        for p, y, X in zip(batch, y_h, X_h):
+            r = pkg.partial_out(y, X, p.fes, p.weights, tol=1e-8)
+            keep = r.sample_index
+            pkg.run_ols(r.y_tilde, r.X_tilde, p.weights[keep], p.cluster[keep], se_type="cluster",
+                        n_effective=n_eff(p))
+
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e_step()
+        times = []
+        for _ in range(args.e2e_steps):
+            barrier(dist)
+            t1 = time.perf_counter()
+            e2e_step()
+            times.append(time.perf_counter() - t1)
+        et = max_over_ranks(statistics.median(times), dist, dev)
+        e2e = {"value": et, "unit": UNIT,
+               "h2d_bytes_per_step": int(sum(p.n * (3 * 8 + 8 + 4 * len(p.fes) + 4) for p in batch)),
+               "d2h_bytes_per_step": int(sum(p.n * 3 * 8 for p in batch))}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and oracle.ref_available():
+        cpu = cpu_leg()
+    absorber.close()
+    if rank == 0:
+        its = [r.iterations for r, _ in last]
+        print(json.dumps({
+            "metric": BATCH_METRIC, "value": ms / 1000.0, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner CG + f64 refinement; f64 OLS",
+            "data": "synthetic (seeded AKM generator, per-rank batch seed = rank)",
+            "config": dict(config, parallelism=f"replicas x{world}",
+                           timing="CUDA events around the batch, inputs resident in HBM; each "
+                                  "panel: b200fe_absorb_device then b200fe_ols_device (cluster)"),
+            "gpu_launches": launches, "converged": all(bool(r.converged) for r, _ in last),
+            "iterations_min_max": [min(its), max(its)],
+            "panels_per_s": len(batch) / (ms / 1000.0), "rows_per_s": rows / (ms / 1000.0),
+            "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "generate_s": gen_s}))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "batch":
+        return run_batch(args)
     if args.workload == "savefe":
         return run_savefe(args)
     if args.workload == "prep":

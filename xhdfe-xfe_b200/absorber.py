@@ -634,20 +634,41 @@ def partial_out(y, X, fes, weights=None, *, drop_singletons=True, device=0,
         w = np.asarray(weights, dtype=np.float64)
         if w.shape[0] != y.size or not np.all(np.isfinite(w)) or np.any(w < 0):
             raise ValueError("weights must be finite and non-negative")
-    # preprocessing on the device: dense ids (build_indexer), singleton cascade
+    import torch
+    # the columns go to the device once; preprocessing (dense ids as in
+    # build_indexer, the singleton cascade), the row compaction, the
+    # absorption and the within transform stay there; one copy back
+    dev = torch.device("cuda", device)
+    ab = _thread_absorber(device)
     dense = [dense_ids_device(f, device) for f in fes]
-    if drop_singletons and fes:
-        keep = drop_singletons_device([d for d, _, _ in dense], [g for _, g, _ in dense],
-                                      device)[0].cpu().numpy()
-    else:
-        keep = np.ones(y.size, bool)
-    idx = np.flatnonzero(keep).astype(np.int32)
-    ids = [d.cpu().numpy()[keep] for d, _, _ in dense]
     G = [g for _, g, _ in dense]
+    n = y.size
+    idx_d = None
+    if drop_singletons and fes:
+        keep = drop_singletons_device([d for d, _, _ in dense], G, device)[0]
+        idx_d = torch.nonzero(keep).squeeze(1)
     o = make_options(**options)
-    res = _thread_absorber(device).absorb(
-        y[keep], np.asfortranarray(X[keep]), ids, G,
-        None if weights is None else np.asarray(weights)[keep], o)
+    if idx_d is not None and idx_d.numel() == 0:
+        raise ValueError("no observations left after dropping singletons")
+    cols = 1 + X.shape[1]
+    v = torch.empty((cols, n), dtype=torch.float64, device=dev)
+    v[0].copy_(torch.from_numpy(np.ascontiguousarray(y)))
+    if cols > 1:
+        v[1:].copy_(torch.from_numpy(np.ascontiguousarray(X.T)))
+    w_d = None if weights is None else torch.from_numpy(
+        np.ascontiguousarray(weights, dtype=np.float64)).to(dev)
+    ids = [d for d, _, _ in dense]
+    if idx_d is not None and idx_d.numel() < n:
+        v = v.index_select(1, idx_d)
+        ids = [d.index_select(0, idx_d) for d in ids]
+        w_d = None if w_d is None else w_d.index_select(0, idx_d)
+        idx = idx_d.to(torch.int32).cpu().numpy()
+    else:
+        idx = np.arange(n, dtype=np.int32)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    out, r = ab.absorb_device(v, ids, G, w_d, o, stream=stream)
+    host = out.cpu().numpy()
+    res = _to_result(r, host[0], host[1:].T, G)
     res.sample_index = idx
     return res
 
