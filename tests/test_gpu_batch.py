@@ -101,3 +101,22 @@ def test_batch_context_reuse_is_bitwise_stable(pkg, batch):
         for r in (b, c):
             assert np.array_equal(a.y_tilde, r.y_tilde) and np.array_equal(a.X_tilde, r.X_tilde)
             assert a.iterations == r.iterations
+
+
+def test_graph_replay_matches_plain_launches(pkg, batch, monkeypatch):
+    """The PCG's check blocks replayed as CUDA graphs give bitwise the same
+    within transform, iteration count and kernel count as plain launches
+    (B200FE_GRAPHS=0 at context creation), across panels of different size
+    sharing one context (the executable updated in place)."""
+    opts = pkg.make_options(tol=1e-8)
+    runs = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("B200FE_GRAPHS", flag)
+        ctx = pkg.Absorber(0)
+        try:
+            runs[flag] = [ctx.absorb(p.y, p.X, p.fes, p.levels, p.weights, opts) for p in batch]
+        finally:
+            ctx.close()
+    for a, b in zip(runs["1"], runs["0"]):
+        assert np.array_equal(a.y_tilde, b.y_tilde) and np.array_equal(a.X_tilde, b.X_tilde)
+        assert a.iterations == b.iterations and a.kernel_launches == b.kernel_launches

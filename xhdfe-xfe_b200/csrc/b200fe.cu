@@ -955,24 +955,98 @@ int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, con
     B_LAUNCHED();
     cg_direction_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, p, z, sc, 1);
     B_LAUNCHED();
+    // one block of nit iterations on ctx->stream: every scalar (alpha, beta,
+    // the column masks) lives on the device, nothing is read back inside it
+    auto run_block = [&](int nit) -> int {
+        const cudaStream_t bs = ctx->stream;
+        for (int j = 0; j < nit; ++j) {
+            B_CHECK((matvec<T, CQ>(ctx, wk, wp, run_w, block_w, p, q)));
+            // pq is in wk.dot_out: copy into the scalar slot
+            B_TRY(cudaMemcpyAsync(cs.pq, wk.dot_out, sizeof(double) * CP, cudaMemcpyDeviceToDevice, bs));
+            {
+                ProfScope ps(ctx, B200FE_PROF_VECTOR,
+                             static_cast<double>(GR) * (CP * 10.0 + 1.0) * sizeof(T));
+                cg_update_kernel<T><<<rgrid, kRowThreads, 0, bs>>>(GR, CP, x, r, z, p, q, dinv, sc,
+                                                                  1.0, 0);
+                B_LAUNCHED();
+                cg_direction_kernel<T><<<rgrid, kRowThreads, 0, bs>>>(GR, CP, p, z, sc, 0);
+                B_LAUNCHED();
+            }
+        }
+        return B200FE_OK;
+    };
+    // Full blocks after the first run as one CUDA graph: captured once per
+    // call (the first block has allocated every buffer), the executable kept
+    // in the context and updated in place when the next call's kernels match.
+    // Without the event profiler only; any capture failure falls back to
+    // plain launches.
+    cudaGraphExec_t exec = nullptr;
+    long long graph_launches = 0;
+    bool graph_ok = ctx->graphs && !ctx->profiling;
+    auto capture = [&]() {
+        if (!ctx->cap_stream &&
+            cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->cap_stream = nullptr;
+            graph_ok = false;
+            return;
+        }
+        if (cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            graph_ok = false;
+            return;
+        }
+        const cudaStream_t saved = ctx->stream;
+        const long long l0 = ctx->launches;
+        const std::string err0 = ctx->err;
+        ctx->stream = ctx->cap_stream;
+        const int rc = run_block(check_interval);
+        ctx->stream = saved;
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(ctx->cap_stream, &g);
+        graph_launches = ctx->launches - l0;
+        ctx->launches = l0;
+        if (rc != B200FE_OK || ee != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            ctx->err = err0;
+            graph_ok = false;
+            return;
+        }
+        const int key = static_cast<int>(sizeof(T)) * 64 + CQ;
+        auto found = ctx->graph_exec.find(key);
+        if (found != ctx->graph_exec.end()) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(found->second, g, &info) == cudaSuccess) {
+                exec = found->second;
+            } else {
+                cudaGetLastError();
+                cudaGraphExecDestroy(found->second);
+                ctx->graph_exec.erase(found);
+            }
+        }
+        if (!exec) {
+            if (cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
+                ctx->graph_exec[key] = exec;
+            } else {
+                cudaGetLastError();
+                exec = nullptr;
+                graph_ok = false;
+            }
+        }
+        cudaGraphDestroy(g);
+    };
     int it = 0;
     int na = 0;
     B_CHECK(sync_read_int(ctx, cs.n_active, 1, &na));
     while (na > 0 && it < max_iter) {
         const int block = std::min(check_interval, max_iter - it);
-        for (int j = 0; j < block; ++j) {
-            B_CHECK((matvec<T, CQ>(ctx, wk, wp, run_w, block_w, p, q)));
-            // pq is in wk.dot_out: copy into the scalar slot
-            B_TRY(cudaMemcpyAsync(cs.pq, wk.dot_out, sizeof(double) * CP, cudaMemcpyDeviceToDevice, s));
-            {
-                ProfScope ps(ctx, B200FE_PROF_VECTOR,
-                             static_cast<double>(GR) * (CP * 10.0 + 1.0) * sizeof(T));
-                cg_update_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x, r, z, p, q, dinv, sc,
-                                                                 1.0, it + j);
-                B_LAUNCHED();
-                cg_direction_kernel<T><<<rgrid, kRowThreads, 0, s>>>(GR, CP, p, z, sc, 0);
-                B_LAUNCHED();
-            }
+        if (graph_ok && !exec && it > 0 && block == check_interval) capture();
+        if (exec && block == check_interval) {
+            B_TRY(cudaGraphLaunch(exec, s));
+            ctx->launches += graph_launches;
+        } else {
+            B_CHECK(run_block(block));
         }
         it += block;
         B_CHECK(sync_read_int(ctx, cs.n_active, 1, &na));
@@ -1411,6 +1485,7 @@ int b200fe_context_create(int device, b200fe_context** out) {
     b200fe_context* ctx = new (std::nothrow) b200fe_context();
     if (!ctx) return B200FE_CUDA_ERROR;
     ctx->device = device;
+    if (const char* g = std::getenv("B200FE_GRAPHS")) ctx->graphs = std::strcmp(g, "0") != 0;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_pinned, 64 * sizeof(int));
@@ -1432,6 +1507,8 @@ void b200fe_context_destroy(b200fe_context* ctx) {
     for (auto& kv : ctx->bufs)
         if (kv.second.p) cudaFree(kv.second.p);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    for (auto& kv : ctx->graph_exec) cudaGraphExecDestroy(kv.second);
+    if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->h_pinned_d) cudaFreeHost(ctx->h_pinned_d);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -139,6 +139,12 @@ struct b200fe_context {
     double* fe_dev[B200FE_MAX_DIMS] = {nullptr};
     int fe_cols = 0;
     int fe_c0 = 0;
+    // CUDA graphs of the PCG's check blocks (captured on cap_stream, launched
+    // on the call's stream; one executable per kernel set, updated in place
+    // for the next panel); off when B200FE_GRAPHS=0 at context creation
+    bool graphs = true;
+    cudaStream_t cap_stream = nullptr;
+    std::unordered_map<int, cudaGraphExec_t> graph_exec;
 };
 
 namespace b200fe_host {

@@ -1706,7 +1706,7 @@ cg_update_kernel(int64_t GR, int CP, T* __restrict__ x, T* __restrict__ r,
             sc.beta[cc] = old > 0.0 ? s0 / old : 0.0;
             sc.rz[cc] = s0;
             sc.rr[cc] = s1;
-            if (iter >= 0) sc.iters[cc] = iter + 1;
+            if (iter >= 0) sc.iters[cc] += 1;  // iterations while active
             if (!(s1 > tol2 * sc.bb[cc]) || !(s0 > 0.0)) sc.active[cc] = 0;
         }
     }
