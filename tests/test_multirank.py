@@ -56,7 +56,8 @@ def test_single_rank_needs_no_process_group(monkeypatch):
     assert bench.max_over_ranks(3.25, None, "cpu") == 3.25
 
 
-@pytest.mark.parametrize("workload", ["akm3", "slopes", "gi", "kss", "ols", "prep", "savefe"])
+@pytest.mark.parametrize("workload", ["akm3", "slopes", "gi", "kss", "ols", "prep", "savefe",
+                                      "batch"])
 def test_reference_arm_runs_on_rank0_only(monkeypatch, workload):
     sys.path.insert(0, str(ROOT))
     import bench
