@@ -80,31 +80,6 @@ __device__ __forceinline__ void add_quad_stream(const double* p, Acc4& acc) {
     const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
     acc.v[0] += a.x; acc.v[1] += a.y; acc.v[2] += b.x; acc.v[3] += b.y;
 }
-// a quad of one run row, loaded ahead of its addition (several rows in flight
-// per thread; the additions keep the row order)
-template <typename T>
-struct Quad;
-template <>
-struct Quad<float> {
-    float4 a;
-};
-template <>
-struct Quad<double> {
-    double2 a, b;
-};
-__device__ __forceinline__ void load_quad_stream(const float* p, Quad<float>& q) {
-    q.a = __ldcs(reinterpret_cast<const float4*>(p));
-}
-__device__ __forceinline__ void load_quad_stream(const double* p, Quad<double>& q) {
-    q.a = __ldcs(reinterpret_cast<const double2*>(p));
-    q.b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
-}
-__device__ __forceinline__ void add_quad(const Quad<float>& q, Acc4& acc) {
-    acc.v[0] += q.a.x; acc.v[1] += q.a.y; acc.v[2] += q.a.z; acc.v[3] += q.a.w;
-}
-__device__ __forceinline__ void add_quad(const Quad<double>& q, Acc4& acc) {
-    acc.v[0] += q.a.x; acc.v[1] += q.a.y; acc.v[2] += q.b.x; acc.v[3] += q.b.y;
-}
 __device__ __forceinline__ void store_quad(float* p, const Acc4& a) {
     *reinterpret_cast<float4*>(p) =
         make_float4(static_cast<float>(a.v[0]), static_cast<float>(a.v[1]),
@@ -1426,18 +1401,8 @@ run_gather_kernel(const GatherArgs<T> a) {
         const int32_t e = a.chunk_end[c];
         Acc4 acc;
         acc_zero(acc);
-        // two run rows in flight per step, added in row order (the sum is
-        // the same as the row-by-row loop)
-        int32_t j = b;
-        for (; j + 2 <= e; j += 2) {
-            const T* rp = a.R + static_cast<int64_t>(j) * a.CP + 4 * q;
-            Quad<T> r0, r1;
-            load_quad_stream(rp, r0);
-            load_quad_stream(rp + a.CP, r1);
-            add_quad(r0, acc);
-            add_quad(r1, acc);
-        }
-        if (j < e) add_quad_stream(a.R + static_cast<int64_t>(j) * a.CP + 4 * q, acc);
+        for (int32_t j = b; j < e; ++j)
+            add_quad_stream(a.R + static_cast<int64_t>(j) * a.CP + 4 * q, acc);
         if (a.chunk_whole[c]) {
             if (a.cfy) {  // + C_fy[g] x_small, four levels per load
                 const T* crow = a.cfy + static_cast<int64_t>(g) * a.SGP;
