@@ -2,7 +2,9 @@
 weighted projection with the reference's determinant rule) pinned against the
 golden vectors of the reference's absorb_fixed_effects_v6 with
 HeterogeneousSlopeTerm slopes (tests/golden/slopes_*.npz), the fixture
-generators, and the host-side slope-term checks of the package.
+generators, the host-side slope-term checks of the package, and the algebra of
+the Schur form's block diagonal for a primary with its own slope (pair sums and
+2x2 block inverses, raw and centred basis) against the dense projection.
 """
 
 import json
@@ -94,3 +96,90 @@ def test_slope_oracle_matches_reference_live(oracle_mod):
     o = slope_projection(np.column_stack([y, X]), [f1, f2], sl, w)
     scale = np.linalg.norm(o, axis=0)
     assert (np.abs(r["V"] - o).max(axis=0) / scale).max() <= ORACLE_TOL
+
+
+def _pair_blocks(tp, fp, fd, zd, w, center):
+    """Diagonal blocks of the Schur complement D_d' W (I - P_p) D_d for a
+    dimension d with intercept and slope zd, the primary fp carrying an
+    intercept and a slope tp, from per-(primary group, group) pair sums and
+    each primary group's 2x2 block inverse -- the formulas of the device's
+    pair_contrib_kernel and slope_centred_inverse_kernel -- in the raw basis
+    (1, t) or the centred one (1, t - tbar)."""
+    Gp, Gd = fp.max() + 1, fd.max() + 1
+    W = np.bincount(fp, w, Gp)
+    Z = np.bincount(fp, w * tp, Gp)
+    ZZ = np.bincount(fp, w * tp * tp, Gp)
+    keep = W * ZZ - Z * Z > 1e-12 * np.maximum(1.0, W * ZZ)  # the reference's rule
+    t = tp - (Z / W)[fp] if center else tp
+    Zt = np.bincount(fp, w * t, Gp)
+    SS = np.bincount(fp, w * t * t, Gp)
+    det = W * SS - Zt * Zt
+    m00 = np.where(keep, SS / np.where(keep, det, 1), 1 / W)
+    m01 = np.where(keep, -Zt / np.where(keep, det, 1), 0.0)
+    m11 = np.where(keep, W / np.where(keep, det, 1), 0.0)
+    S = np.zeros((Gd, 2, 2))
+    np.add.at(S, (fd, 0, 0), w)
+    np.add.at(S, (fd, 0, 1), w * zd)
+    np.add.at(S, (fd, 1, 1), w * zd * zd)
+    key = fp.astype(np.int64) * Gd + fd
+    for k in np.unique(key):
+        rows = key == k
+        j, g = divmod(int(k), Gd)
+        ca, cb = w[rows].sum(), (w * zd)[rows].sum()
+        ta, tb = (w * t)[rows].sum(), (w * zd * t)[rows].sum()
+
+        def qf(u0, u1, v0, v1):
+            return m00[j] * u0 * v0 + m01[j] * (u0 * v1 + u1 * v0) + m11[j] * u1 * v1
+
+        S[g, 0, 0] -= qf(ca, ta, ca, ta)
+        S[g, 0, 1] -= qf(ca, ta, cb, tb)
+        S[g, 1, 1] -= qf(cb, tb, cb, tb)
+    S[:, 1, 0] = S[:, 0, 1]
+    return S
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_schur_blocks_of_a_slope_primary(weighted):
+    """The pair-sum form of the Schur complement's block diagonal, for a primary
+    with intercept and slope, equals the dense D_d' W (I - P_p) D_d (P_p the
+    exact W-projection on the primary's basis under the reference's rule) in
+    the raw and the centred basis; one-row groups and groups of constant t
+    drop the slope."""
+    rng = np.random.default_rng(17)
+    sizes = rng.integers(1, 8, 120)
+    fp = np.repeat(np.arange(120), sizes).astype(np.int32)
+    n = fp.size
+    tp = rng.uniform(0.0, 5.0, n)
+    tp[fp % 13 == 4] = 2.5
+    fd = rng.integers(0, 9, n).astype(np.int32)
+    zd = rng.uniform(-1.0, 3.0, n)
+    w = rng.uniform(0.3, 3.0, n) if weighted else np.ones(n)
+    # dense reference: projection on the primary basis column by column
+    cols = []
+    for j in range(120):
+        rows = fp == j
+        e = np.zeros(n)
+        e[rows] = 1.0
+        cols.append(e)
+        W, Z, ZZ = w[rows].sum(), (w * tp)[rows].sum(), (w * tp * tp)[rows].sum()
+        if W * ZZ - Z * Z > 1e-12 * max(1.0, W * ZZ):
+            f = np.zeros(n)
+            f[rows] = tp[rows]
+            cols.append(f)
+    B = np.column_stack(cols)
+    sw = np.sqrt(w)
+    Q, _ = np.linalg.qr(B * sw[:, None])
+    Gd = int(fd.max()) + 1
+    dense = np.zeros((Gd, 2, 2))
+    for g in range(Gd):
+        D = np.zeros((n, 2))
+        rows = fd == g
+        D[rows, 0] = 1.0
+        D[rows, 1] = zd[rows]
+        A = D * sw[:, None]
+        R = A - Q @ (Q.T @ A)
+        dense[g] = R.T @ R
+    for center in (False, True):
+        S = _pair_blocks(tp, fp, fd, zd, w, center)
+        scale = np.abs(dense).max()
+        assert np.abs(S - dense).max() <= 1e-10 * scale, center
