@@ -20,7 +20,12 @@ Lines printed by rank 0 (one JSON line):
 --workload slopes times the same panel with firm-specific tenure slopes
 (firm##c.tenure) on b200fe_absorb_slopes; --workload gi a 10M-group
 group/individual design on b200fe_absorb_group_individual (one GPU each; their
-own JSON lines).
+own JSON lines).  Further workloads, each with its own JSON line and reference
+arm: kss (the KSS firm system of a 10M-obs panel, 200 right-hand sides), ols
+(clustered run_ols on the absorbed 50M panel), prep (dense ids, singleton
+cascade and mobility groups of the 50M panel), savefe (recover_fixed_effects of
+a 50M partial residual) and batch (64 independent panels of 10k-5M rows,
+absorption and clustered OLS each).
 With --gpus N > 1 every rank absorbs its own replica panel (no collective in
 the data path; replicas only), launched by torch.distributed.run.
 """
