@@ -1,9 +1,11 @@
 """CPU checks of the preprocessing oracle (oracle/preprocess_oracle.py): the
 restatement of the reference's build_indexer on hand-computed cases of its
 three branches, and its singleton cascade against the package's host mask
-(both reach the unique fixed point of the rule)."""
+(both reach the unique fixed point of the rule); partial_out's argument checks,
+which run before any device work."""
 
 import numpy as np
+import pytest
 
 
 def test_build_indexer_branches():
@@ -46,3 +48,23 @@ def test_component_oracle_matches_reference(oracle_mod, panels):
         assert ref["num_components"] == ours["num_components"] > 1
         assert ref["largest_component_n_obs"] == ours["largest_component_n_obs"]
         assert abs(ref["largest_component_weight_share"] - ours["largest_component_weight_share"]) <= 1e-12
+
+
+def test_partial_out_argument_checks(pkg):
+    """partial_out rejects what HdfeRegressorV11::partial_out rejects before any
+    device work: an empty outcome, non-finite data, X of another length,
+    negative or non-finite weights."""
+    f = [np.array([0, 0, 1, 1], dtype=np.int32)]
+    y = np.array([1.0, 2.0, 3.0, 4.0])
+    with pytest.raises(ValueError):
+        pkg.partial_out(np.zeros(0), None, f)
+    with pytest.raises(ValueError):
+        pkg.partial_out(np.array([1.0, np.nan, 3.0, 4.0]), None, f)
+    with pytest.raises(ValueError):
+        pkg.partial_out(y, np.array([[1.0], [np.inf], [0.0], [2.0]]), f)
+    with pytest.raises(ValueError):
+        pkg.partial_out(y, np.ones((3, 1)), f)
+    with pytest.raises(ValueError):
+        pkg.partial_out(y, None, f, weights=np.array([1.0, -1.0, 1.0, 1.0]))
+    with pytest.raises(ValueError):
+        pkg.partial_out(y, None, f, weights=np.ones(3))
