@@ -277,11 +277,18 @@ int b200fe_fe_recovery_max_delta(b200fe_context* ctx, const double* residual,
  * aliasing d_v).  d_out receives v minus the weighted group mean of v, per
  * column.  The only scratch is a fixed array inside the library: at most 2^20
  * groups (a larger num_groups returns B200FE_INVALID_ARG before any GPU work),
- * kept by every GPU that loads the library until the process exits.  All calls
- * on one device share that array, so calls whose GPU work overlaps race on it.
- * The first call on a device looks up the array's address with that device
- * current; make it before any stream capture.  Unsorted or out-of-range ids
- * return B200FE_INVALID_ARG.  stream: a cudaStream_t as void*, or NULL.
+ * kept until the process exits by every GPU on which it was placed.  CUDA loads
+ * device code lazily: b200fe_context_create places the array on its device,
+ * so after a context exists on a device no-alloc calls there load nothing;
+ * without one, the first no-alloc call on a device loads this code (the array
+ * and its kernels) unless CUDA_MODULE_LOADING=EAGER is set.  All calls on one
+ * device share that array, so calls whose GPU work overlaps race on it.  The
+ * array's address is looked up once per device with that device current (at
+ * context creation or by the first call); make that first call before any
+ * stream capture.  Each call waits once for its stream (the id check's status
+ * is read back).  A CUDA error pending from earlier work returns
+ * B200FE_CUDA_ERROR (and is cleared).  Unsorted or out-of-range ids return
+ * B200FE_INVALID_ARG.  stream: a cudaStream_t as void*, or NULL.
  * This entry point has no counterpart in the reference, which always
  * allocates its device workspace. */
 int b200fe_demean_sorted_noalloc(const double* d_v, int64_t n, int cols,

@@ -39,6 +39,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -151,7 +152,7 @@ def make(name: str) -> dict:
     return meta
 
 
-REF_DATA = Path("/root/reference/data/felsdvsimul.dta")
+REF_DATA = Path(os.environ.get("XHDFE_REFERENCE", "/root/reference")) / "data" / "felsdvsimul.dta"
 KSS_KEYS = ("plugin", "agsu", "kss")
 
 

@@ -9,9 +9,11 @@ the first failure has already run every other test, and it must pass both
 alone in a fresh process and after the other tests.
 
 Checked through the C ABI: two calls in a row give the same within transform
-as the regular absorber (b200fe_absorb_device with one FE dimension) within
-the relative tolerance of the other parity tests, unweighted and weighted;
-oversized and unsorted inputs are rejected.
+as the regular absorber (b200fe_absorb_device with one FE dimension) and as
+group means computed in numpy, within the relative tolerance of the other
+parity tests, unweighted and weighted; the second call leaves the device's
+free memory unchanged; oversized, unsorted, negative and out-of-range ids are
+rejected.
 """
 
 import numpy as np
@@ -50,18 +52,30 @@ def test_noalloc_matches_absorber_on_two_calls(pkg, libmod, panels, weighted):
     finally:
         ab.close()
     scale = np.linalg.norm(V, axis=1)
-    outs = []
-    for _ in range(2):
-        out = torch.empty_like(dv)
+    # the one-way within transform directly: v minus its weighted group mean
+    ww = w if weighted else np.ones(n)
+    W = np.bincount(g, weights=ww, minlength=G)
+    direct = np.empty_like(V)
+    for c in range(cols):
+        m = np.bincount(g, weights=ww * V[c], minlength=G) / np.where(W > 0, W, 1.0)
+        direct[c] = V[c] - m[g]
+    bufs = [torch.empty_like(dv) for _ in range(2)]  # no allocation between the calls
+    torch.cuda.synchronize()
+    free = []
+    for out in bufs:
         rc = lib.b200fe_demean_sorted_noalloc(
             dv.data_ptr(), n, cols, dg.data_ptr(), G, dw.data_ptr() if weighted else None,
             out.data_ptr(), None)
         torch.cuda.synchronize()
         assert rc == libmod.OK
-        outs.append(out.cpu().numpy())
+        free.append(torch.cuda.mem_get_info()[0])
+    assert free[1] == free[0]  # a repeated call places nothing on the device
+    outs = [b.cpu().numpy() for b in bufs]
     for o in outs:
         err = float((np.linalg.norm(o - ref, axis=1) / scale).max())
         assert err <= REL_TOL, err
+        err_direct = float((np.linalg.norm(o - direct, axis=1) / scale).max())
+        assert err_direct <= REL_TOL, err_direct
     assert np.array_equal(outs[0], outs[1])
 
 
@@ -80,3 +94,28 @@ def test_noalloc_rejects_oversized_and_unsorted(libmod):
     rc = lib.b200fe_demean_sorted_noalloc(dv.data_ptr(), n, 1, g_unsorted.data_ptr(), 100, None,
                                           out.data_ptr(), None)
     assert rc == libmod.INVALID_ARG
+
+
+def test_noalloc_rejects_negative_and_out_of_range_ids(libmod):
+    import torch
+
+    lib = libmod.load()
+    n = 1000
+    dv = torch.zeros((1, n), dtype=torch.float64, device="cuda")
+    out = torch.empty_like(dv)
+    g = (torch.arange(n, dtype=torch.int32, device="cuda") // 10).contiguous()  # 0..99
+    g_neg = g.clone()
+    g_neg[0] = -1  # still non-decreasing, one negative id
+    rc = lib.b200fe_demean_sorted_noalloc(dv.data_ptr(), n, 1, g_neg.data_ptr(), 100, None,
+                                          out.data_ptr(), None)
+    assert rc == libmod.INVALID_ARG
+    g_big = g.clone()
+    g_big[-1] = 100  # == num_groups
+    rc = lib.b200fe_demean_sorted_noalloc(dv.data_ptr(), n, 1, g_big.data_ptr(), 100, None,
+                                          out.data_ptr(), None)
+    assert rc == libmod.INVALID_ARG
+    # a valid call right after the rejections starts from a cleared status word
+    rc = lib.b200fe_demean_sorted_noalloc(dv.data_ptr(), n, 1, g.data_ptr(), 100, None,
+                                          out.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert rc == libmod.OK

@@ -1496,6 +1496,9 @@ int b200fe_context_create(int device, b200fe_context** out) {
         b200fe_context_destroy(ctx);
         return B200FE_CUDA_ERROR;
     }
+    // place the no-alloc entry point's scratch array on this device now, so
+    // that its later calls here load nothing (a failure is reported by them)
+    if (noalloc_scratch_for_current_device(nullptr) != B200FE_OK) cudaGetLastError();
     *out = ctx;
     return B200FE_OK;
 }

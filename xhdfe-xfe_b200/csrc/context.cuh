@@ -110,6 +110,10 @@ struct Structure {
 
 constexpr int32_t kChunkRuns = 64;
 
+// Device address of the no-alloc entry point's scratch array on the current
+// device (noalloc.cu); resolving it loads that file's device code there.
+int noalloc_scratch_for_current_device(int32_t** out);
+
 }  // namespace b200fe_host
 
 struct b200fe_context {

@@ -13,13 +13,22 @@
 // Limits and sharing rules:
 //   * at most kNoAllocMaxGroups groups (the array holds their offsets); larger
 //     calls are rejected with B200FE_INVALID_ARG before any GPU work;
-//   * every GPU that loads the library keeps the array (about 4 MiB) until the
-//     process exits;
+//   * every GPU on which this part of the library is loaded keeps the array
+//     (about 4 MiB) until the process exits.  CUDA loads a library's device
+//     code lazily, per device: creating an absorber context on a device
+//     (b200fe_context_create) loads it there and resolves the array's address,
+//     so a caller that creates a context first has nothing placed on the GPU
+//     by its no-alloc calls; without a context, the first no-alloc call on a
+//     device loads it (the array plus this file's kernels), unless the process
+//     runs with CUDA_MODULE_LOADING=EAGER, which loads it with the CUDA context;
 //   * all calls on a device share the array and it keeps the last call's
 //     contents, so calls whose GPU work overlaps (different streams or host
 //     threads without ordering between them) race on it; order such calls;
-//   * the first call on a device resolves the array's device address (with
-//     that device current); make that first call before any stream capture.
+//   * the array's device address is resolved once per device (with that
+//     device current), at context creation or else by the first call; make
+//     that first call before any stream capture;
+//   * every call waits for its stream once (it reads back the status word of
+//     the id check before the demeaning kernels are launched).
 //
 // The arithmetic is that of the absorber's segment means for a single FE
 // dimension: per group and column a weighted mean by a fixed-order reduction,
@@ -105,9 +114,16 @@ __global__ void noalloc_demean_kernel(const double* __restrict__ v, int64_t n, i
     }
 }
 
+}  // namespace
+
+namespace b200fe_host {
+
 // Resolves the scratch array's device address once per device (that device
-// current); the host-side name of the array is not a device address.
-int scratch_for_current_device(int32_t** out) {
+// current); the host-side name of the array is not a device address.  Called
+// by b200fe_context_create, so a process that creates a context on a device
+// loads this file's device code and places the array there before any
+// no-alloc call, and by every no-alloc call (a lookup once resolved).
+int noalloc_scratch_for_current_device(int32_t** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();
@@ -123,9 +139,13 @@ int scratch_for_current_device(int32_t** out) {
         }
         g_scratch_ptr[dev] = static_cast<int32_t*>(p);
     }
-    *out = g_scratch_ptr[dev];
+    if (out) *out = g_scratch_ptr[dev];
     return B200FE_OK;
 }
+
+}  // namespace b200fe_host
+
+namespace {
 
 int grid_cap(int64_t work, int threads, int cap) {
     const int64_t g = (work + threads - 1) / threads;
@@ -146,12 +166,16 @@ extern "C" int b200fe_demean_sorted_noalloc(const double* d_v, int64_t n, int co
         cudaGetLastError();
         return B200FE_UNAVAILABLE;
     }
+    // an error left by the caller's earlier CUDA work is reported, not dropped
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();
+        return B200FE_CUDA_ERROR;
+    }
     int32_t* scratch = nullptr;
-    const int rc = scratch_for_current_device(&scratch);
+    const int rc = b200fe_host::noalloc_scratch_for_current_device(&scratch);
     if (rc != B200FE_OK) return rc;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     int32_t* status = scratch + kNoAllocStatus;
-    cudaGetLastError();
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
