@@ -61,9 +61,12 @@ typedef struct b200fe_options {
     int profile;           /* 1: time every kernel category with CUDA events (default 0)      */
     int pass_kernel;       /* CG matvec pass: 0 auto (block level when at most one large and
                               one small FE dim besides the largest; with a small dim, its
-                              dense coupling rows when they are small), 1 general tile pass,
-                              2 block level without the dense coupling; for the slope
-                              absorber 1 forces block Jacobi over every dimension            */
+                              dense coupling rows when they are small; with one large dim,
+                              its Schur block built explicitly as a sparse matrix when the
+                              movers' pairs are few), 1 general tile pass, 2 block level
+                              without the dense coupling, 3 as 0 but the large dim through
+                              its runs (no explicit block); for the slope absorber 1 forces
+                              block Jacobi over every dimension                              */
     double fe_linf_tol;    /* > 0: a column also needs every group's weighted mean of its
                               within transform (non-primary dims) at most this before it
                               stops -- the check recover_fixed_effects applies to saved FEs

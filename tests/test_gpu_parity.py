@@ -171,13 +171,14 @@ def test_zipf_primary_mixed_long_and_tiles(absorber, pkg, oracle_mod, panels):
 
 @pytest.mark.parametrize("weighted", [False, True])
 def test_block_and_tile_matvec_agree(absorber, pkg, oracle_mod, panels, weighted):
-    # the CG matvec forms solve the same system: block level with the dense
-    # small-dim coupling (0, the default here), the general tile pass (1) and
-    # block level with per-block small-dim updates (2)
+    # the CG matvec forms solve the same system: the explicit sparse Schur
+    # block of the firm dim with the dense small-dim coupling (0, the default
+    # here), the general tile pass (1), block level with per-block small-dim
+    # updates (2) and block level with the dense coupling through the runs (3)
     p = _akm(panels, 30_000, True, seed=37)
     w = np.random.default_rng(5).lognormal(0.0, 0.5, size=p.n) if weighted else None
     outs = []
-    for pk in (0, 1, 2):
+    for pk in (0, 1, 2, 3):
         o = pkg.make_options(tol=1e-10, precision="fp64", pass_kernel=pk)
         r = absorber.absorb(p.y, p.X, p.fes, p.levels, w, o)
         assert r.converged

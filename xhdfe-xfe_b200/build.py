@@ -12,13 +12,14 @@ ROOT = HERE.parent
 CSRC = HERE / "csrc"
 SOURCES = ["b200fe.cu", "slopes.cu", "noalloc.cu", "kss.cu"]
 HEADERS = ["limits.cuh", "context.cuh", "common_kernels.cuh", "kernels.cuh", "setup_kernels.cuh",
-           "ols_kernels.cuh", "prep_kernels.cuh", "slope_kernels.cuh"]
+           "ols_kernels.cuh", "prep_kernels.cuh", "slope_kernels.cuh", "sparse_kernels.cuh"]
 OUT = HERE / "libb200fe.so"
+OBJ_DIR = HERE / "_build"
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -38,13 +39,27 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every translation unit for sm_100a (in parallel), then link."""
     if not force and not _stale():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, f"-I{ROOT / 'include'}", f"-I{CSRC}",
-           "-o", str(OUT), *[str(CSRC / s) for s in SOURCES]]
+    from concurrent.futures import ThreadPoolExecutor
+
+    OBJ_DIR.mkdir(exist_ok=True)
+    inc = [f"-I{ROOT / 'include'}", f"-I{CSRC}"]
+    cmds = [[nvcc(), *NVCC_FLAGS, *inc, "-c", "-o", str(OBJ_DIR / (Path(src).stem + ".o")),
+             str(CSRC / src)] for src in SOURCES]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        for c in cmds:
+            print(" ".join(c))
+    with ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed:\n{r.stdout}\n{r.stderr}")
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(OUT),
+            *[str(OBJ_DIR / (Path(src).stem + ".o")) for src in SOURCES]]
+    if verbose:
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     return OUT
 
 

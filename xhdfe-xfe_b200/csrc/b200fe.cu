@@ -10,6 +10,8 @@
 #include "setup_kernels.cuh"
 #include "ols_kernels.cuh"
 #include "prep_kernels.cuh"
+#include "sparse_kernels.cuh"
+#include "pcg_kernels.cuh"
 
 using namespace b200fe;
 using namespace b200fe_host;
@@ -19,6 +21,228 @@ namespace {
 // ---------------------------------------------------------------------------
 // Structure build
 // ---------------------------------------------------------------------------
+// Chunk lists over groups whose items are [grp_off[g], grp_off[g+1]) (runs of
+// a large dim, or nonzeros of a CSR row): chunks of at most CH items, the
+// groups with several chunks ("multi" rows, summed by finalize_kernel) and
+// their super-chunks (groups of more than kFinFewParts chunks: the Zipf-giant
+// firm owns thousands).  Fills the chunk fields of L; L.G is set by the
+// caller; buffer names end in sfx.
+int build_chunks(b200fe_context* ctx, const int32_t* grp_off, int32_t CH, const std::string& sfx,
+                 LargeDim& L) {
+    const cudaStream_t s = ctx->stream;
+    const int T256 = 256;
+    // chunk list
+    int32_t *nch, *ch_off, *mflag, *midx;
+    B_CHECK(get_buf(ctx, "nch", static_cast<size_t>(L.G) + 1, &nch));
+    B_CHECK(get_buf(ctx, "ch_off", static_cast<size_t>(L.G) + 1, &ch_off));
+    B_CHECK(get_buf(ctx, "mflag", static_cast<size_t>(L.G) + 1, &mflag));
+    B_CHECK(get_buf(ctx, "midx", static_cast<size_t>(L.G) + 1, &midx));
+    B_TRY(cudaMemsetAsync(nch, 0, sizeof(int32_t) * (static_cast<size_t>(L.G) + 1), s));
+    B_TRY(cudaMemsetAsync(mflag, 0, sizeof(int32_t) * (static_cast<size_t>(L.G) + 1), s));
+    chunk_count_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(grp_off, L.G, CH, nch);
+    B_LAUNCHED();
+    B_CHECK(cub_exclusive_sum(ctx, nch, ch_off, static_cast<int64_t>(L.G) + 1));
+    multi_flag_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(nch, L.G, mflag);
+    B_LAUNCHED();
+    B_CHECK(cub_exclusive_sum(ctx, mflag, midx, static_cast<int64_t>(L.G) + 1));
+    int hc[2];
+    B_CHECK(sync_read_int(ctx, ch_off + L.G, 1, &hc[0]));
+    B_CHECK(sync_read_int(ctx, midx + L.G, 1, &hc[1]));
+    L.nchunks = hc[0];
+    L.nmulti = hc[1];
+    B_CHECK(get_buf(ctx, "chunk_grp" + sfx, L.nchunks, &L.chunk_grp));
+    B_CHECK(get_buf(ctx, "chunk_beg" + sfx, L.nchunks, &L.chunk_beg));
+    B_CHECK(get_buf(ctx, "chunk_end" + sfx, L.nchunks, &L.chunk_end));
+    B_CHECK(get_buf(ctx, "chunk_whole" + sfx, L.nchunks, &L.chunk_whole));
+    B_CHECK(get_buf(ctx, "multi_grp" + sfx, L.nmulti, &L.multi_grp));
+    B_CHECK(get_buf(ctx, "multi_c0" + sfx, L.nmulti, &L.multi_c0));
+    B_CHECK(get_buf(ctx, "multi_c1" + sfx, L.nmulti, &L.multi_c1));
+    chunk_fill_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(
+        grp_off, L.G, CH, ch_off, L.chunk_grp, L.chunk_beg, L.chunk_end,
+        L.chunk_whole, midx, L.multi_grp, L.multi_c0, L.multi_c1);
+    B_LAUNCHED();
+    // super-chunks: a group with many chunks (Zipf sizes: one firm may own
+    // 10%+ of the runs) has its chunk partials summed in slices of
+    // kSuperParts by many lane groups before finalize adds the slices
+    L.nsup = 0;
+    if (L.nmulti > 0) {
+        std::vector<int32_t> c0(L.nmulti), c1(L.nmulti);
+        B_TRY(cudaMemcpyAsync(c0.data(), L.multi_c0, sizeof(int32_t) * L.nmulti, cudaMemcpyDeviceToHost, s));
+        B_TRY(cudaMemcpyAsync(c1.data(), L.multi_c1, sizeof(int32_t) * L.nmulti, cudaMemcpyDeviceToHost, s));
+        B_TRY(cudaStreamSynchronize(s));
+        std::vector<int32_t> s0(L.nmulti), s1(L.nmulti), sb, se;
+        for (int64_t r = 0; r < L.nmulti; ++r) {
+            s0[r] = s1[r] = static_cast<int32_t>(sb.size());
+            if (c1[r] - c0[r] <= kFinFewParts) continue;
+            for (int32_t c = c0[r]; c < c1[r]; c += kSuperParts) {
+                sb.push_back(c);
+                se.push_back(std::min(c1[r], c + kSuperParts));
+            }
+            s1[r] = static_cast<int32_t>(sb.size());
+        }
+        L.nsup = static_cast<int64_t>(sb.size());
+        B_CHECK(get_buf(ctx, "multi_s0" + sfx, L.nmulti, &L.multi_s0));
+        B_CHECK(get_buf(ctx, "multi_s1" + sfx, L.nmulti, &L.multi_s1));
+        B_CHECK(get_buf(ctx, "sup_c0" + sfx, std::max<int64_t>(L.nsup, 1), &L.sup_c0));
+        B_CHECK(get_buf(ctx, "sup_c1" + sfx, std::max<int64_t>(L.nsup, 1), &L.sup_c1));
+        B_TRY(cudaMemcpyAsync(L.multi_s0, s0.data(), sizeof(int32_t) * L.nmulti, cudaMemcpyHostToDevice, s));
+        B_TRY(cudaMemcpyAsync(L.multi_s1, s1.data(), sizeof(int32_t) * L.nmulti, cudaMemcpyHostToDevice, s));
+        if (L.nsup > 0) {
+            B_TRY(cudaMemcpyAsync(L.sup_c0, sb.data(), sizeof(int32_t) * L.nsup, cudaMemcpyHostToDevice, s));
+            B_TRY(cudaMemcpyAsync(L.sup_c1, se.data(), sizeof(int32_t) * L.nsup, cudaMemcpyHostToDevice, s));
+        }
+        B_TRY(cudaStreamSynchronize(s));  // the host vectors leave scope
+    }
+    return B200FE_OK;
+}
+
+// The explicit S_ff of the one large dim (see sparse_kernels.cuh).  Leaves
+// st.sparse false (run-level matvec) when a segment has more than
+// kSparseMaxRuns runs or the contributions would exceed eight per run.
+int build_sparse_block(b200fe_context* ctx) {
+    Structure& st = ctx->st;
+    const cudaStream_t s = ctx->stream;
+    const int T256 = 256;
+    const int32_t Gp = st.G[st.p];
+    LargeDim& L = st.L[0];
+    int32_t *count, *flag;
+    unsigned long long* total;
+    B_CHECK(get_buf(ctx, "sp_count", static_cast<size_t>(Gp) + 1, &count));
+    B_CHECK(get_buf(ctx, "sp_flag", 4, &flag));
+    B_CHECK(get_buf(ctx, "sp_total", 1, &total));
+    B_TRY(cudaMemsetAsync(flag, 0, sizeof(int32_t), s));
+    B_TRY(cudaMemsetAsync(total, 0, sizeof(unsigned long long), s));
+    B_TRY(cudaMemsetAsync(count + Gp, 0, sizeof(int32_t), s));
+    sparse_pair_count_kernel<<<grid_for(ctx, Gp, T256), T256, 0, s>>>(Gp, L.run_base, L.run_grp,
+                                                                        count, flag, total);
+    B_LAUNCHED();
+    unsigned long long htot = 0;
+    int hflag = 0;
+    B_TRY(cudaMemcpyAsync(&htot, total, sizeof(htot), cudaMemcpyDeviceToHost, s));
+    B_CHECK(sync_read_int(ctx, flag, 1, &hflag));  // synchronises htot too
+    const unsigned long long cap = std::min<unsigned long long>(
+        8ull * static_cast<unsigned long long>(L.nruns) + (1ull << 20), (1ull << 31) - 1);
+    if (hflag || htot > cap) return B200FE_OK;
+    st.sp_pairs = static_cast<int64_t>(htot);
+    st.sp.G = L.G;
+    const int64_t np = std::max<int64_t>(st.sp_pairs, 1);
+    int32_t* off;
+    B_CHECK(get_buf(ctx, "sp_off", static_cast<size_t>(Gp) + 1, &off));
+    B_CHECK(cub_exclusive_sum(ctx, count, off, static_cast<int64_t>(Gp) + 1));
+    unsigned long long *k_in, *k_out;
+    double *v_in, *v_out;
+    B_CHECK(get_buf(ctx, "sp_kin", np, &k_in));
+    B_CHECK(get_buf(ctx, "sp_kout", np, &k_out));
+    B_CHECK(get_buf(ctx, "sp_vin", np, &v_in));
+    B_CHECK(get_buf(ctx, "sp_vout", np, &v_out));
+    int32_t *ustart, *urow;
+    if (st.sp_pairs > 0) {
+        sparse_pair_fill_kernel<<<grid_for(ctx, Gp, T256), T256, 0, s>>>(
+            Gp, L.run_base, L.run_grp, L.cw_run, st.inv_wp, count, off, L.G, k_in, v_in);
+        B_LAUNCHED();
+        // stable sort by (row, column): equal keys keep segment order
+        const unsigned long long gmax = static_cast<unsigned long long>(L.G) * L.G;
+        int eb = 1;
+        while (eb < 63 && (1ull << eb) < gmax) ++eb;
+        size_t tmp = 0;
+        B_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k_in, k_out, v_in, v_out, st.sp_pairs,
+                                              0, eb, s));
+        void* t;
+        B_CHECK(get_buf(ctx, "cub_tmp", tmp, reinterpret_cast<uint8_t**>(&t)));
+        B_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, k_in, k_out, v_in, v_out, st.sp_pairs, 0, eb,
+                                              s));
+        ++ctx->lib_calls;
+        int32_t *flags, *uid;
+        B_CHECK(get_buf(ctx, "sp_flags", np, &flags));
+        B_CHECK(get_buf(ctx, "sp_uid", np, &uid));
+        sparse_key_flags_kernel<<<grid_for(ctx, st.sp_pairs, T256), T256, 0, s>>>(k_out, st.sp_pairs,
+                                                                                   flags);
+        B_LAUNCHED();
+        B_CHECK(cub_inclusive_sum(ctx, flags, uid, st.sp_pairs));
+        int nnz = 0;
+        B_CHECK(sync_read_int(ctx, uid + (st.sp_pairs - 1), 1, &nnz));
+        st.sp_nnz = nnz;
+        B_CHECK(get_buf(ctx, "sp_ustart", static_cast<size_t>(nnz) + 1, &ustart));
+        B_CHECK(get_buf(ctx, "sp_urow", nnz, &urow));
+        B_CHECK(get_buf(ctx, "sp_col", nnz, &st.sp_col));
+        sparse_unique_fill_kernel<<<grid_for(ctx, st.sp_pairs, T256), T256, 0, s>>>(
+            k_out, st.sp_pairs, flags, uid, L.G, ustart, urow, st.sp_col);
+        B_LAUNCHED();
+        int32_t* long_list;
+        B_CHECK(get_buf(ctx, "sp_val64", nnz, &st.sp_val64));
+        B_CHECK(get_buf(ctx, "sp_val32", nnz, &st.sp_val32));
+        B_CHECK(get_buf(ctx, "sp_long", nnz, &long_list));
+        B_TRY(cudaMemsetAsync(flag + 1, 0, sizeof(int32_t), s));  // long-list counter
+        sparse_merge_kernel<<<grid_for(ctx, nnz, T256), T256, 0, s>>>(nnz, ustart, v_out, st.sp_val64,
+                                                                     long_list, flag + 1);
+        B_LAUNCHED();
+        sparse_merge_long_kernel<<<ctx->num_sms * 4, 256, 0, s>>>(long_list, flag + 1, ustart, v_out,
+                                                                  st.sp_val64);
+        B_LAUNCHED();
+        to_float_kernel<<<grid_for(ctx, nnz, T256), T256, 0, s>>>(st.sp_val64, nnz, st.sp_val32);
+        B_LAUNCHED();
+    } else {
+        st.sp_nnz = 0;
+        B_CHECK(get_buf(ctx, "sp_urow", 1, &urow));
+        B_CHECK(get_buf(ctx, "sp_col", 1, &st.sp_col));
+        B_CHECK(get_buf(ctx, "sp_val64", 1, &st.sp_val64));
+        B_CHECK(get_buf(ctx, "sp_val32", 1, &st.sp_val32));
+    }
+    // CSR row offsets over the large dim's levels (rows without movers are empty)
+    B_CHECK(get_buf(ctx, "sp_row_off", static_cast<size_t>(L.G) + 1, &st.sp_row_off));
+    segment_offsets_kernel<<<grid_for(ctx, st.sp_nnz + 1, T256), T256, 0, s>>>(urow, st.sp_nnz, L.G,
+                                                                              st.sp_row_off);
+    B_LAUNCHED();
+    B_CHECK(build_chunks(ctx, st.sp_row_off, kSparseChunk, "_sp", st.sp));
+    // work lists of the persistent PCG: short rows, long rows and their chunks
+    {
+        const size_t g1 = static_cast<size_t>(L.G) + 1;
+        int32_t *is_short, *is_long, *nch, *short_idx, *long_idx, *chunk_off, *is_huge, *huge_idx;
+        B_CHECK(get_buf(ctx, "pc_is_huge", g1, &is_huge));
+        B_CHECK(get_buf(ctx, "pc_huge_idx", g1, &huge_idx));
+        B_CHECK(get_buf(ctx, "pc_is_short", g1, &is_short));
+        B_CHECK(get_buf(ctx, "pc_is_long", g1, &is_long));
+        B_CHECK(get_buf(ctx, "pc_nch", g1, &nch));
+        B_CHECK(get_buf(ctx, "pc_short_idx", g1, &short_idx));
+        B_CHECK(get_buf(ctx, "pc_long_idx", g1, &long_idx));
+        B_CHECK(get_buf(ctx, "pc_chunk_off", g1, &chunk_off));
+        B_TRY(cudaMemsetAsync(is_short + L.G, 0, sizeof(int32_t), s));
+        B_TRY(cudaMemsetAsync(is_long + L.G, 0, sizeof(int32_t), s));
+        B_TRY(cudaMemsetAsync(nch + L.G, 0, sizeof(int32_t), s));
+        B_TRY(cudaMemsetAsync(is_huge + L.G, 0, sizeof(int32_t), s));
+        pcg_lists_count_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(st.sp_row_off, L.G, is_short,
+                                                                        is_long, nch, is_huge);
+        B_LAUNCHED();
+        B_CHECK(cub_exclusive_sum(ctx, is_huge, huge_idx, static_cast<int64_t>(g1)));
+        B_CHECK(cub_exclusive_sum(ctx, is_short, short_idx, static_cast<int64_t>(g1)));
+        B_CHECK(cub_exclusive_sum(ctx, is_long, long_idx, static_cast<int64_t>(g1)));
+        B_CHECK(cub_exclusive_sum(ctx, nch, chunk_off, static_cast<int64_t>(g1)));
+        int cnt[4];
+        B_CHECK(sync_read_int(ctx, huge_idx + L.G, 1, &cnt[3]));
+        st.pc_nhuge = cnt[3];
+        B_CHECK(get_buf(ctx, "pc_huge_li", std::max<int64_t>(st.pc_nhuge, 1), &st.pc_huge_li));
+        B_CHECK(sync_read_int(ctx, short_idx + L.G, 1, &cnt[0]));
+        B_CHECK(sync_read_int(ctx, long_idx + L.G, 1, &cnt[1]));
+        B_CHECK(sync_read_int(ctx, chunk_off + L.G, 1, &cnt[2]));
+        st.pc_nshort = cnt[0];
+        st.pc_nlong = cnt[1];
+        st.pc_nlchunks = cnt[2];
+        B_CHECK(get_buf(ctx, "pc_short_rows", std::max<int64_t>(st.pc_nshort, 1), &st.pc_short_rows));
+        B_CHECK(get_buf(ctx, "pc_long_rows", std::max<int64_t>(st.pc_nlong, 1), &st.pc_long_rows));
+        B_CHECK(get_buf(ctx, "pc_long_c0", std::max<int64_t>(st.pc_nlong, 1), &st.pc_long_c0));
+        B_CHECK(get_buf(ctx, "pc_long_c1", std::max<int64_t>(st.pc_nlong, 1), &st.pc_long_c1));
+        B_CHECK(get_buf(ctx, "pc_lchunk_row", std::max<int64_t>(st.pc_nlchunks, 1), &st.pc_lchunk_row));
+        B_CHECK(get_buf(ctx, "pc_lchunk_beg", std::max<int64_t>(st.pc_nlchunks, 1), &st.pc_lchunk_beg));
+        pcg_lists_fill_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(
+            st.sp_row_off, L.G, is_short, short_idx, long_idx, chunk_off, st.pc_short_rows,
+            st.pc_long_rows, st.pc_long_c0, st.pc_long_c1, st.pc_lchunk_row, st.pc_lchunk_beg, huge_idx,
+            st.pc_huge_li);
+        B_LAUNCHED();
+    }
+    st.sparse = true;
+    return B200FE_OK;
+}
+
 int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const* gids,
                     const int32_t* G, const double* w) {
     Structure& st = ctx->st;
@@ -223,36 +447,8 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
             sorted_runs, nr, run_start, n, run_seg, st.wp64, st.inv_wp, L.run_dest, cw, ce,
             cw_run);
         B_LAUNCHED();
-        // chunk list
-        int32_t *nch, *ch_off, *mflag, *midx;
-        B_CHECK(get_buf(ctx, "nch", static_cast<size_t>(L.G) + 1, &nch));
-        B_CHECK(get_buf(ctx, "ch_off", static_cast<size_t>(L.G) + 1, &ch_off));
-        B_CHECK(get_buf(ctx, "mflag", static_cast<size_t>(L.G) + 1, &mflag));
-        B_CHECK(get_buf(ctx, "midx", static_cast<size_t>(L.G) + 1, &midx));
-        B_TRY(cudaMemsetAsync(nch, 0, sizeof(int32_t) * (static_cast<size_t>(L.G) + 1), s));
-        B_TRY(cudaMemsetAsync(mflag, 0, sizeof(int32_t) * (static_cast<size_t>(L.G) + 1), s));
-        chunk_count_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(grp_off, L.G, kChunkRuns, nch);
-        B_LAUNCHED();
-        B_CHECK(cub_exclusive_sum(ctx, nch, ch_off, static_cast<int64_t>(L.G) + 1));
-        multi_flag_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(nch, L.G, mflag);
-        B_LAUNCHED();
-        B_CHECK(cub_exclusive_sum(ctx, mflag, midx, static_cast<int64_t>(L.G) + 1));
-        int hc[2];
-        B_CHECK(sync_read_int(ctx, ch_off + L.G, 1, &hc[0]));
-        B_CHECK(sync_read_int(ctx, midx + L.G, 1, &hc[1]));
-        L.nchunks = hc[0];
-        L.nmulti = hc[1];
-        B_CHECK(get_buf(ctx, "chunk_grp" + sfx, L.nchunks, &L.chunk_grp));
-        B_CHECK(get_buf(ctx, "chunk_beg" + sfx, L.nchunks, &L.chunk_beg));
-        B_CHECK(get_buf(ctx, "chunk_end" + sfx, L.nchunks, &L.chunk_end));
-        B_CHECK(get_buf(ctx, "chunk_whole" + sfx, L.nchunks, &L.chunk_whole));
-        B_CHECK(get_buf(ctx, "multi_grp" + sfx, L.nmulti, &L.multi_grp));
-        B_CHECK(get_buf(ctx, "multi_c0" + sfx, L.nmulti, &L.multi_c0));
-        B_CHECK(get_buf(ctx, "multi_c1" + sfx, L.nmulti, &L.multi_c1));
-        chunk_fill_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(
-            grp_off, L.G, kChunkRuns, ch_off, L.chunk_grp, L.chunk_beg, L.chunk_end,
-            L.chunk_whole, midx, L.multi_grp, L.multi_c0, L.multi_c1);
-        B_LAUNCHED();
+        // chunk lists (and super-chunks) of the groups' runs
+        B_CHECK(build_chunks(ctx, grp_off, kChunkRuns, sfx, L));
         // diagonal terms W_g, E_g of the groups over the chunk list (balanced
         // however skewed the group sizes are)
         {
@@ -269,38 +465,6 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
                                                  Wall + st.lbase[l], Eall + st.lbase[l]);
                 B_LAUNCHED();
             }
-        }
-        // super-chunks: a group with many chunks (Zipf sizes: one firm may own
-        // 10%+ of the runs) has its chunk partials summed in slices of
-        // kSuperParts by many lane groups before finalize adds the slices
-        L.nsup = 0;
-        if (L.nmulti > 0) {
-            std::vector<int32_t> c0(L.nmulti), c1(L.nmulti);
-            B_TRY(cudaMemcpyAsync(c0.data(), L.multi_c0, sizeof(int32_t) * L.nmulti, cudaMemcpyDeviceToHost, s));
-            B_TRY(cudaMemcpyAsync(c1.data(), L.multi_c1, sizeof(int32_t) * L.nmulti, cudaMemcpyDeviceToHost, s));
-            B_TRY(cudaStreamSynchronize(s));
-            std::vector<int32_t> s0(L.nmulti), s1(L.nmulti), sb, se;
-            for (int64_t r = 0; r < L.nmulti; ++r) {
-                s0[r] = s1[r] = static_cast<int32_t>(sb.size());
-                if (c1[r] - c0[r] <= kFinFewParts) continue;
-                for (int32_t c = c0[r]; c < c1[r]; c += kSuperParts) {
-                    sb.push_back(c);
-                    se.push_back(std::min(c1[r], c + kSuperParts));
-                }
-                s1[r] = static_cast<int32_t>(sb.size());
-            }
-            L.nsup = static_cast<int64_t>(sb.size());
-            B_CHECK(get_buf(ctx, "multi_s0" + sfx, L.nmulti, &L.multi_s0));
-            B_CHECK(get_buf(ctx, "multi_s1" + sfx, L.nmulti, &L.multi_s1));
-            B_CHECK(get_buf(ctx, "sup_c0" + sfx, std::max<int64_t>(L.nsup, 1), &L.sup_c0));
-            B_CHECK(get_buf(ctx, "sup_c1" + sfx, std::max<int64_t>(L.nsup, 1), &L.sup_c1));
-            B_TRY(cudaMemcpyAsync(L.multi_s0, s0.data(), sizeof(int32_t) * L.nmulti, cudaMemcpyHostToDevice, s));
-            B_TRY(cudaMemcpyAsync(L.multi_s1, s1.data(), sizeof(int32_t) * L.nmulti, cudaMemcpyHostToDevice, s));
-            if (L.nsup > 0) {
-                B_TRY(cudaMemcpyAsync(L.sup_c0, sb.data(), sizeof(int32_t) * L.nsup, cudaMemcpyHostToDevice, s));
-                B_TRY(cudaMemcpyAsync(L.sup_c1, se.data(), sizeof(int32_t) * L.nsup, cudaMemcpyHostToDevice, s));
-            }
-            B_TRY(cudaStreamSynchronize(s));  // the host vectors leave scope
         }
     }
 
@@ -444,6 +608,11 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         }
     }
 
+    // explicit Schur block of the large dim (sparse_kernels.cuh): replaces the
+    // per-iteration pass over the runs when the movers' pairs fit
+    if (st.block_ok && ctx->sparse_schur && st.nL == 1 && (st.nS == 0 || st.coupled))
+        B_CHECK(build_sparse_block(ctx));
+
     if (st.GR > 0) {
         B_CHECK(get_buf(ctx, "dinv64", st.GR, &st.dinv64));
         B_CHECK(get_buf(ctx, "dinv32", st.GR, &st.dinv32));
@@ -508,6 +677,14 @@ struct Work {
     int gather_grid[kMaxLarge];
     int fin_grid;
     int64_t fin_rows;
+    // explicit Schur block (st.sparse): gather CTAs, their dot partials, the
+    // chunk and super-chunk partials of multi-chunk rows, finalize rows/CTAs
+    int sp_gather_grid;
+    double* sp_gather_partial;
+    double* sp_chunk_partial;
+    double* sp_super_partial;
+    int64_t sp_fin_rows;
+    int sp_fin_grid;
 };
 
 template <typename T, int CQ, int MODE>
@@ -581,7 +758,10 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     B_CHECK(get_buf(ctx, tag + "colsq", static_cast<size_t>(wk.nbins_ctas) * CP, &wk.colsq_partial));
     for (int l = 0; l < st.nL; ++l) {
         const std::string sfx = std::to_string(l);
-        B_CHECK(get_buf(ctx, tag + "R" + sfx, static_cast<size_t>(st.L[l].nruns) * CP, &wk.R[l]));
+        // the FP32 run rows serve only the run-level matvec
+        const bool need_R = !(st.sparse && std::is_same<T, float>::value);
+        B_CHECK(get_buf(ctx, tag + "R" + sfx, need_R ? static_cast<size_t>(st.L[l].nruns) * CP : 1,
+                        &wk.R[l]));
         wk.gather_grid[l] = grid_for(ctx, st.L[l].nchunks * CQ, kRowThreads, 8);
         B_CHECK(get_buf(ctx, tag + "gpart" + sfx, static_cast<size_t>(wk.gather_grid[l]) * CP,
                         &wk.gather_partial[l]));
@@ -594,7 +774,24 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     for (int l = 0; l < st.nL; ++l) wk.fin_rows += st.L[l].nmulti;
     wk.fin_grid = static_cast<int>(std::max<int64_t>(
         1, std::min<int64_t>(wk.fin_rows, static_cast<int64_t>(ctx->num_sms) * 8)));
-    B_CHECK(get_buf(ctx, tag + "fpart", static_cast<size_t>(wk.fin_grid) * CP, &wk.fin_partial));
+    wk.sp_gather_grid = 0;
+    wk.sp_fin_rows = 0;
+    wk.sp_fin_grid = 0;
+    if (st.sparse) {
+        wk.sp_gather_grid = grid_for(ctx, st.sp.nchunks * CQ, kRowThreads, 8);
+        B_CHECK(get_buf(ctx, tag + "sp_gpart", static_cast<size_t>(wk.sp_gather_grid) * CP,
+                        &wk.sp_gather_partial));
+        B_CHECK(get_buf(ctx, tag + "sp_cpart", static_cast<size_t>(st.sp.nchunks) * CP,
+                        &wk.sp_chunk_partial));
+        B_CHECK(get_buf(ctx, tag + "sp_spart",
+                        static_cast<size_t>(std::max<int64_t>(st.sp.nsup, 1)) * CP,
+                        &wk.sp_super_partial));
+        wk.sp_fin_rows = st.SG + st.sp.nmulti;
+        wk.sp_fin_grid = static_cast<int>(std::max<int64_t>(
+            1, std::min<int64_t>(wk.sp_fin_rows, static_cast<int64_t>(ctx->num_sms) * 8)));
+    }
+    B_CHECK(get_buf(ctx, tag + "fpart", static_cast<size_t>(std::max(wk.fin_grid, wk.sp_fin_grid)) * CP,
+                    &wk.fin_partial));
     B_CHECK(get_buf(ctx, tag + "dotout", CP, &wk.dot_out));
     B_CHECK(get_buf(ctx, tag + "ticket", 1, &wk.ticket));
     B_TRY(cudaMemsetAsync(wk.ticket, 0, sizeof(unsigned int), ctx->stream));
@@ -849,12 +1046,110 @@ int reduce_runs(b200fe_context* ctx, const Work<T>& wk, T* out, const T* dotv,
     return B200FE_OK;
 }
 
+// q = S x over the explicit Schur block: the rows of the large dim by the
+// sparse gather (+ C_fy x_small), then finalize (multi-chunk rows, small-dim
+// rows from the coupling partials, the dot x'q into wk.dot_out).
+template <typename T, int CQ>
+int reduce_sparse(b200fe_context* ctx, const Work<T>& wk, const T* x, T* q) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const cudaStream_t s = ctx->stream;
+    const LargeDim& L = st.sp;
+    const bool coupled = st.coupled && st.nS == 1;
+    SparseGatherArgs<T> g{};
+    g.CP = CP;
+    g.nchunks = L.nchunks;
+    g.chunk_grp = L.chunk_grp;
+    g.chunk_beg = L.chunk_beg;
+    g.chunk_end = L.chunk_end;
+    g.chunk_whole = L.chunk_whole;
+    g.col = st.sp_col;
+    g.val = pick_prec<T>(st.sp_val32, st.sp_val64);
+    g.x = x + st.lbase[0] * CP;
+    g.out = q + st.lbase[0] * CP;
+    g.partial = wk.sp_chunk_partial;
+    g.dot_partial = wk.sp_gather_partial;
+    if (coupled) {
+        g.cfy = pick_prec<T>(st.cfy32, st.cfy64);
+        g.xs = x + st.sbase[0] * CP;
+        g.SG = st.SG;
+        g.SGP = st.SGP;
+    }
+    {
+        // chunk meta, nonzeros (column + value), the large dim's rows of x
+        // read and of q written once, and the coupling rows
+        const double tb = static_cast<double>(sizeof(T));
+        double pb = static_cast<double>(L.nchunks) * 13.0 + static_cast<double>(st.sp_nnz) * (4.0 + tb) +
+                    2.0 * static_cast<double>(L.G) * CP * tb;
+        if (coupled) pb += static_cast<double>(L.G) * st.SGP * tb;
+        ProfScope ps(ctx, B200FE_PROF_PASS, pb);
+        const size_t gsmem = coupled ? static_cast<size_t>(st.SGP) * CP * sizeof(T) : 0;
+        sparse_gather_kernel<T, CQ><<<wk.sp_gather_grid, kRowThreads, gsmem, s>>>(g);
+        B_LAUNCHED();
+        if (L.nsup > 0) {
+            multi_super_kernel<<<grid_for(ctx, L.nsup * CP, kRowThreads), kRowThreads, 0, s>>>(
+                L.nsup, L.sup_c0, L.sup_c1, wk.sp_chunk_partial, CP, wk.sp_super_partial);
+            B_LAUNCHED();
+        }
+    }
+    FinalizeArgs<T> f{};
+    f.CP = CP;
+    f.nL = 1;
+    f.nS = st.nS;
+    f.nmulti[0] = L.nmulti;
+    f.multi_grp[0] = L.multi_grp;
+    f.multi_c0[0] = L.multi_c0;
+    f.multi_c1[0] = L.multi_c1;
+    f.partial[0] = wk.sp_chunk_partial;
+    f.multi_s0[0] = L.multi_s0;
+    f.multi_s1[0] = L.multi_s1;
+    f.super_partial[0] = wk.sp_super_partial;
+    f.lbase[0] = st.lbase[0];
+    f.gather_dot_partial[0] = wk.sp_gather_partial;
+    f.gather_ctas[0] = wk.sp_gather_grid;
+    f.SG = st.SG;
+    f.sgbase = st.nS > 0 ? st.sbase[0] : 0;
+    f.bins_partial = wk.bins_partial;
+    f.nbins_ctas = coupled ? wk.couple_grid : 0;
+    f.small_diag = nullptr;
+    f.small_dense = coupled ? st.cyy : nullptr;
+    f.cfy = coupled ? pick_prec<T>(st.cfy32, st.cfy64) : nullptr;
+    f.SGP = st.SGP;
+    f.x = x;
+    f.nrows = wk.sp_fin_rows;
+    f.out = q;
+    f.dotv = x;
+    f.dot_partial = wk.fin_partial;
+    f.dot_out = wk.dot_out;
+    f.ticket = wk.ticket;
+    double fb = static_cast<double>(f.nbins_ctas) * st.SG * CP * 8.0 +
+                static_cast<double>(L.nmulti) * CP * (8.0 + sizeof(T)) +
+                static_cast<double>(st.SG) * CP * sizeof(T);
+    ProfScope ps(ctx, B200FE_PROF_FINALIZE, fb);
+    finalize_kernel<T><<<wk.sp_fin_grid, kRowThreads, 0, s>>>(f);
+    B_LAUNCHED();
+    return B200FE_OK;
+}
+
 // q = S x ; pq = x'q (per column) into wk.dot_out
 template <typename T, int CQ>
 int matvec(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w,
            const T* block_w, const T* x, T* q) {
     const Structure& st = ctx->st;
     constexpr int CP = 4 * CQ;
+    if (st.sparse) {
+        if (st.coupled && st.nS == 1) {
+            // C_fy' x_f into the coupling partials (read by finalize)
+            ProfScope ps(ctx, B200FE_PROF_COUPLE,
+                         static_cast<double>(st.L[0].G) * (st.SGP + CP) * double(sizeof(T)) +
+                             static_cast<double>(wk.couple_grid) * st.SG * CP * 8.0);
+            coupling_xf_kernel<T, CQ><<<wk.couple_grid, 256, 0, ctx->stream>>>(
+                st.L[0].G, st.SG, st.SGP, pick_prec<T>(st.cfy32, st.cfy64), x + st.lbase[0] * CP,
+                wk.bins_partial);
+            B_LAUNCHED();
+        }
+        return reduce_sparse<T, CQ>(ctx, wk, x, q);
+    }
     PassArgs<T> a = make_pass_args<T>(st, 0, CP, wk);
     a.wp = wp;
     a.x = x;
@@ -1055,6 +1350,108 @@ int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, con
     return B200FE_OK;
 }
 
+// Algorithmic bytes of one persistent PCG iteration: the explicit block
+// (column and value per nonzero, row offsets, the p rows gathered and the q
+// rows written once), the coupling rows, and the vector updates (x, r, z, p,
+// q, dinv read; x, r, z written; z, p read and p written for the directions).
+double pcg_iter_bytes(const Structure& st, int CP, size_t tsize) {
+    const double tb = static_cast<double>(tsize);
+    const double gf = static_cast<double>(st.L[0].G);
+    const double gr = static_cast<double>(st.GR);
+    double b = static_cast<double>(st.sp_nnz) * (4.0 + tb) + gf * 4.0 + 2.0 * gf * CP * tb;
+    if (st.coupled && st.nS == 1) b += gf * st.SGP * tb;
+    b += gr * CP * tb * 11.0 + gr * tb;
+    return b;
+}
+
+// Inner PCG as one cooperative launch (pcg_kernels.cuh).  Returns
+// B200FE_UNAVAILABLE (nothing run) when the launch cannot be made, so the
+// caller falls back to the multi-kernel PCG.
+template <typename T, int CQ>
+int pcg_persistent(b200fe_context* ctx, const Work<T>& wk, const T* dinv, T* x, T* r, T* z, T* p,
+                   T* q, const std::vector<double>& thr_host, int max_iter, int* iters_out) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const cudaStream_t s = ctx->stream;
+    const bool coupled = st.coupled && st.nS == 1;
+    const int SG = coupled ? st.SG : 0;
+    const int SGP = coupled ? st.SGP : 0;
+    if (SG > kPcgMaxSG) return B200FE_UNAVAILABLE;
+    const size_t smem = pcg_smem_bytes<T>(CP, SGP);
+    auto kern = pcg_persistent_kernel<T, CQ>;
+    B_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int per_sm = 0;
+    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPcgThreads, smem));
+    if (per_sm < 1) return B200FE_UNAVAILABLE;
+    const int nb = ctx->num_sms * std::min(per_sm, 2);
+    PcgArgs<T> a{};
+    a.CP = CP;
+    a.Gf = st.L[0].G;
+    a.SG = SG;
+    a.SGP = SGP;
+    a.row_off = st.sp_row_off;
+    a.col = st.sp_col;
+    a.val = pick_prec<T>(st.sp_val32, st.sp_val64);
+    a.nshort = st.pc_nshort;
+    a.short_rows = st.pc_short_rows;
+    a.nlchunks = st.pc_nlchunks;
+    a.lchunk_row = st.pc_lchunk_row;
+    a.lchunk_beg = st.pc_lchunk_beg;
+    a.nlong = st.pc_nlong;
+    a.long_rows = st.pc_long_rows;
+    a.long_c0 = st.pc_long_c0;
+    a.long_c1 = st.pc_long_c1;
+    a.nhuge = st.pc_nhuge;
+    a.huge_li = st.pc_huge_li;
+    a.cfy = coupled ? pick_prec<T>(st.cfy32, st.cfy64) : nullptr;
+    a.cyy = coupled ? st.cyy : nullptr;
+    a.dinv = dinv;
+    a.x = x;
+    a.r = r;
+    a.z = z;
+    a.p = p;
+    a.q = q;
+    a.part_stride = CP * (3 + SG);
+    a.max_iter = max_iter;
+    const std::string tag = std::is_same<T, float>::value ? "pc32_" : "pc64_";
+    B_CHECK(get_buf(ctx, tag + "lpart", static_cast<size_t>(std::max<int64_t>(st.pc_nlchunks, 1)) * CP, &a.lpart));
+    B_CHECK(get_buf(ctx, tag + "cta_part", static_cast<size_t>(nb) * a.part_stride, &a.cta_part));
+    double* thr_d;
+    B_CHECK(get_buf(ctx, tag + "thr", CP, &thr_d));
+    B_CHECK(get_buf(ctx, tag + "rz", CP, &a.rz_out));
+    int32_t *iters_d, *ctl;
+    B_CHECK(get_buf(ctx, tag + "iters", CP, &iters_d));
+    B_CHECK(get_buf(ctx, tag + "ctl", 4, &ctl));  // loops, status, barrier[2]
+    a.iters_out = iters_d;
+    a.loops_out = ctl;
+    a.status = ctl + 1;
+    a.bar = reinterpret_cast<unsigned int*>(ctl + 2);
+    a.thr = thr_d;
+    B_TRY(cudaMemcpyAsync(thr_d, thr_host.data(), sizeof(double) * CP, cudaMemcpyHostToDevice, s));
+    B_TRY(cudaMemsetAsync(ctl, 0, 4 * sizeof(int32_t), s));
+    void* args[] = {&a};
+    {
+        ProfScope ps(ctx, B200FE_PROF_PASS, 0.0);
+        const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), dim3(nb),
+                                                          dim3(kPcgThreads), args, smem, s);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            B_TRY(cudaStreamSynchronize(s));  // thr_host copy done before the caller's fallback
+            return B200FE_UNAVAILABLE;
+        }
+        ++ctx->launches;
+        int hc[2] = {0, 0};
+        B_CHECK(sync_read_int(ctx, ctl, 2, hc));
+        if (hc[1] != 0) {
+            ctx->err = "persistent PCG: grid barrier wait timed out";
+            return B200FE_CUDA_ERROR;
+        }
+        *iters_out = hc[0];
+        ps.bytes = static_cast<double>(hc[0]) * pcg_iter_bytes(st, CP, sizeof(T));
+    }
+    return B200FE_OK;
+}
+
 template <int CQ>
 int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                 const b200fe_options& o, b200fe_result* res) {
@@ -1212,17 +1609,31 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             if (mixed) {
                 scale_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, r32);
                 B_LAUNCHED();
-                B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.run_w32, st.block_w32, st.dinv32, x32, r32, z32, p32, q32, thr,
-                                        round_cap, std::max(1, o.check_interval),
-                                        &its)));
+                int prc = B200FE_UNAVAILABLE;
+                if (st.sparse && ctx->persistent)
+                    prc = pcg_persistent<float, CQ>(ctx, w32, st.dinv32, x32, r32, z32, p32, q32, thr,
+                                                    round_cap, &its);
+                if (prc == B200FE_UNAVAILABLE)
+                    B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.run_w32, st.block_w32, st.dinv32, x32, r32, z32, p32, q32, thr,
+                                            round_cap, std::max(1, o.check_interval),
+                                            &its)));
+                else if (prc != B200FE_OK)
+                    return prc;
                 axpy_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x32, scale_d, a64);
                 B_LAUNCHED();
             } else {
                 scale_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, rin64);
                 B_LAUNCHED();
-                B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
-                                         round_cap, std::max(1, o.check_interval),
-                                         &its)));
+                int prc = B200FE_UNAVAILABLE;
+                if (st.sparse && ctx->persistent)
+                    prc = pcg_persistent<double, CQ>(ctx, w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
+                                                     round_cap, &its);
+                if (prc == B200FE_UNAVAILABLE)
+                    B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
+                                             round_cap, std::max(1, o.check_interval),
+                                             &its)));
+                else if (prc != B200FE_OK)
+                    return prc;
                 axpy_rows_kernel<double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, x64, scale_d, a64);
                 B_LAUNCHED();
             }
@@ -1397,7 +1808,9 @@ int absorb_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int co
     const bool reuse = o.reuse_structure && ctx->st.valid && ctx->st.n == n &&
                        ctx->st.D == num_dims && ctx->st.weighted == (d_w != nullptr);
     ctx->profiling = o.profile != 0;
-    ctx->pass_kernel = o.pass_kernel;
+    // 3: the run-level matvec of the automatic choice, without the explicit block
+    ctx->pass_kernel = o.pass_kernel == 3 ? 0 : o.pass_kernel;
+    ctx->sparse_schur = o.pass_kernel == 0;
     ctx->prof.clear();
     ctx->ev_used = 0;
     if (!reuse) {
@@ -1486,6 +1899,7 @@ int b200fe_context_create(int device, b200fe_context** out) {
     if (!ctx) return B200FE_CUDA_ERROR;
     ctx->device = device;
     if (const char* g = std::getenv("B200FE_GRAPHS")) ctx->graphs = std::strcmp(g, "0") != 0;
+    if (const char* g = std::getenv("B200FE_PERSISTENT")) ctx->persistent = std::strcmp(g, "0") != 0;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_pinned, 64 * sizeof(int));

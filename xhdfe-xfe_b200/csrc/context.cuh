@@ -106,6 +106,24 @@ struct Structure {
     double* cfy64 = nullptr;  // [G_f][SGP]
     float* cfy32 = nullptr;
     double* cyy = nullptr;    // [SG][SG]
+    // explicit Schur block of the one large dim (sparse_kernels.cuh): CSR rows
+    // of S_ff over the large dim's levels; the CG matvec then gathers these
+    // rows instead of passing over the runs
+    bool sparse = false;
+    int64_t sp_pairs = 0;              // contributions before merging
+    int64_t sp_nnz = 0;
+    int32_t* sp_row_off = nullptr;     // [G_f + 1]
+    int32_t* sp_col = nullptr;         // [nnz] column (level of the large dim)
+    double* sp_val64 = nullptr;        // [nnz]
+    float* sp_val32 = nullptr;
+    LargeDim sp;                       // chunk lists over the CSR rows (chunk fields only)
+    // work lists of the persistent PCG over the same rows (pcg_kernels.cuh)
+    int64_t pc_nshort = 0, pc_nlong = 0, pc_nlchunks = 0;
+    int32_t* pc_short_rows = nullptr;
+    int32_t *pc_long_rows = nullptr, *pc_long_c0 = nullptr, *pc_long_c1 = nullptr;
+    int32_t *pc_lchunk_row = nullptr, *pc_lchunk_beg = nullptr;
+    int64_t pc_nhuge = 0;
+    int32_t* pc_huge_li = nullptr;
 };
 
 constexpr int32_t kChunkRuns = 64;
@@ -135,6 +153,7 @@ struct b200fe_context {
     };
     bool profiling = false;
     int pass_kernel = 0;
+    bool sparse_schur = true;  // explicit Schur block of the large dim when it applies
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<ProfRec> prof;
@@ -147,6 +166,9 @@ struct b200fe_context {
     // on the call's stream; one executable per kernel set, updated in place
     // for the next panel); off when B200FE_GRAPHS=0 at context creation
     bool graphs = true;
+    // persistent PCG kernel over the explicit Schur block (one cooperative
+    // launch per inner solve); off when B200FE_PERSISTENT=0 at context creation
+    bool persistent = true;
     cudaStream_t cap_stream = nullptr;
     std::unordered_map<int, cudaGraphExec_t> graph_exec;
 };
