@@ -70,6 +70,10 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--no-learned", action="store_true",
+                    help="do not install the shipped learned warm start (xhdfe-xfe_b200/warmstart_mlp.npz)")
+    ap.add_argument("--learned-mode", type=int, default=1,
+                    help="warm-start mode bits: 1 start from the prediction, 2 learned Jacobi scaling")
     ap.add_argument("--workload", default="akm3",
                     choices=["akm3", "slopes", "gi", "kss", "ols", "prep", "savefe", "batch"],
                     help="akm3: the headline workload; slopes: the same panel with "
@@ -170,69 +174,107 @@ def committed_traffic():
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference's own CPU core on a bounded sample
 # ---------------------------------------------------------------------------
-def cpu_baseline(sample_n: int, threads: int):
+# The reference's CPU core cannot absorb the 50M panel inside a benchmark run:
+# its alternating projections need 67 iterations at 1M rows and 606 at 5M
+# (135 s on eight cores at 5M; its coefficient-space Krylov absorber needs 1,055
+# iterations, 262 s), and the count keeps growing with N.  So the CPU leg times
+# real absorptions of a bounded sample of the same generator, reports that
+# measurement as measured, and gives the linear scaling to 50M rows only as a
+# labelled lower bound (the iteration growth makes the true 50M time larger).
+CPU_GROWTH_EVIDENCE = {"1M_rows": {"iterations": 67}, "5M_rows": {"iterations": 606, "seconds_8_threads": 135.5},
+                       "5M_rows_krylov": {"iterations": 1055, "seconds_8_threads": 261.7}}
+
+
+def cpu_sample_run(sample_n: int, threads: int, panel=None):
+    """One absorption of the bounded sample by the reference's CPU core."""
     import oracle
     if not oracle.ref_available():
         return None
-    p = make_panel(sample_n, seed=12345)
+    p = panel if panel is not None else make_panel(sample_n, seed=0)
     t0 = time.perf_counter()
     r = oracle.ref_absorb(p.y, p.X, p.fes, None, tol=1e-8, tolerance_mode="reghdfe-comparable",
                           method="auto", threads=threads)
     dt = time.perf_counter() - t0
+    return {"seconds": dt, "rows": p.n, "levels": p.levels, "iterations": r["iterations"],
+            "converged": r["converged"], "panel": p}
+
+
+def cpu_baseline(sample_n: int, threads: int):
+    info = cpu_sample_run(sample_n, threads)
+    if info is None:
+        return None
+    dt, rows = info["seconds"], info["rows"]
     return {
-        "value": dt * (N_OBS / p.n), "unit": UNIT, "cores": threads, "kind": "reference",
+        "value": dt * (N_OBS / rows), "unit": UNIT, "cores": threads, "kind": "reference",
         "sample": (f"reference CPU core (absorb_fixed_effects_v6, reghdfe-comparable tol 1e-8, "
-                   f"{threads} threads) on a {p.n}-row panel of the same generator "
-                   f"({p.levels} levels, 13 columns): {dt:.3f} s, scaled linearly to 50M rows"),
-        "sample_seconds": dt, "sample_rows": p.n, "iterations": r["iterations"],
-        "converged": r["converged"],
+                   f"{threads} threads) on a {rows}-row panel of the same generator "
+                   f"({info['levels']} levels, 13 columns): {dt:.3f} s measured; value = that time "
+                   f"scaled linearly to 50M rows, a lower bound (the reference's iteration count "
+                   f"grows with N)"),
+        "sample_seconds": dt, "sample_rows": rows, "iterations": info["iterations"],
+        "converged": info["converged"], "scaling": "linear in N, lower bound",
+        "iteration_growth": CPU_GROWTH_EVIDENCE,
     }
 
 
-def reference_gpu(panel, threads: int):
+def reference_gpu(panel, threads: int, tol: float = 1e-8, mode: str = "reghdfe-comparable"):
     """The reference's own CUDA backend (src/fe_absorption_cuda.cu, built for
     sm_100a by oracle/Makefile target ref_cuda) on the same panel, through the
     reference's absorb_fixed_effects_v6 with host arrays (its H2D/D2H inside):
-    comparable to this arm's e2e number."""
+    comparable to this arm's e2e number.  A single call (17 s at 50M rows)."""
     import oracle
     if not oracle.REF_CUDA_SO.exists():
         return None
     t0 = time.perf_counter()
-    r = oracle.ref_absorb(panel.y, panel.X, panel.fes, None, tol=1e-8,
-                          tolerance_mode="reghdfe-comparable", method="auto", threads=threads,
-                          gpu_backend="cuda", lib_path=oracle.REF_CUDA_SO)
+    r = oracle.ref_absorb(panel.y, panel.X, panel.fes, None, tol=tol, tolerance_mode=mode,
+                          method="auto", threads=threads, gpu_backend="cuda",
+                          lib_path=oracle.REF_CUDA_SO)
     dt = time.perf_counter() - t0
     return {"value": dt, "unit": UNIT, "kind": "reference CUDA backend built for sm_100a, host arrays",
+            "repetitions": 1, "tol": tol, "tolerance_mode": mode,
             "iterations": r["iterations"], "converged": r["converged"],
             "precision_certified": r["precision_certified"],
-            "abs_residual_rel": r["abs_residual_rel"], "gpu_status_code": r["gpu_status_code"]}
+            "abs_residual_rel": r["abs_residual_rel"], "gpu_status_code": r["gpu_status_code"],
+            "V": r["V"]}
 
 
 def run_reference(args):
+    """The reference's CPU core, timed on real absorptions of a bounded sample
+    (args.cpu_sample rows of the same generator, all host threads): at most 1
+    warm-up and 5 timed absorptions whatever --warmup/--steps ask (each takes
+    seconds to minutes); the counts printed are the ones run."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    vals = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        info = cpu_baseline(args.cpu_sample, threads)
+    warm, steps = min(args.warmup, 1), max(1, min(args.steps, 5))
+    panel = make_panel(args.cpu_sample, seed=0)
+    vals, info = [], None
+    for i in range(warm + steps):
+        info = cpu_sample_run(args.cpu_sample, threads, panel)
         if info is None:
             print(json.dumps({"impl": "reference", "unavailable":
                               "reference CPU core (oracle/_ref/libxhdfe_ref.so) was not built"}))
             return 0
-        if i >= args.warmup:
-            vals.append(info["value"])
+        if i >= warm:
+            vals.append(info["seconds"])
     v = statistics.median(vals)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000.0,
+        "steps": steps, "warmup": warm, "ms_per_step": v * 1000.0,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded AKM generator)",
-        "config": {"workload": "akm_3way_50M_13col_demean", "n_obs": N_OBS, "columns": 13,
-                   "fe_dims": ["worker", "firm", "year"], "tol": 1e-8,
-                   "sample_rows": info["sample_rows"]},
-        "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "config": {"workload": "akm_3way_13col_demean_sample", "sample_of": "akm_3way_50M_13col_demean",
+                   "n_obs_after_singleton_drop": info["rows"], "columns": 13,
+                   "fe_dims": ["worker", "firm", "year"], "levels": info["levels"], "tol": 1e-8,
+                   "l2_policy": "CPU run (no GPU L2)", "parallelism": "CPU threads"},
+        "note": ("the reference's CPU core cannot absorb the 50M panel inside this run (iterations "
+                 "grow with N); value is the measured time of the sample, not an extrapolation"),
+        "scaled_to_50M_lower_bound": v * (N_OBS / info["rows"]),
+        "iteration_growth": CPU_GROWTH_EVIDENCE,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{info['rows']}-row panel of the same generator, "
+                                   f"{info['iterations']} iterations, measured"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -299,6 +341,22 @@ def run_ours(args):
     def step(opts):
         return absorber.absorb_device(v, gids, panel.levels, None, opts, out=out, stream=sh)[1]
 
+    def timed(opts, reps):
+        step(opts)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rs = [step(opts) for _ in range(reps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, rs[-1]
+
+    # the learned warm start trained by train_warmstart.py (when shipped)
+    ws_params = None if args.no_learned else pkg.learned.load_trained()
+    ws_mode = args.learned_mode
+    if ws_params is not None:
+        pkg.learned.set_warm_start(absorber, ws_params, ws_mode)
     opts = pkg.make_options(tol=1e-8, precision=args.precision, profile=True)
     for _ in range(args.warmup):
         step(opts)
@@ -347,20 +405,41 @@ def run_ours(args):
         "traffic": (traffic or {}).get(hot, {}).get("dram_bytes_per_launch") if traffic else None,
     }
 
-    # plain FP64 on the same GPU (the comparison the metric names)
+    # the headline's output, kept for the error checks below
+    out_head = out.clone() if rank == 0 and world == 1 else None
+    # the same mixed solve without the learned warm start
+    learned_ab = None
+    if ws_params is not None:
+        pkg.learned.set_warm_start(absorber, None)
+        ms_cold, r_cold = timed(pkg.make_options(tol=1e-8, precision=args.precision), 2)
+        learned_ab = {"mode": ws_mode, "ms_warm": ms, "iterations_warm": r_last.iterations,
+                      "warm_columns": r_last.warm_columns, "ms_cold": ms_cold,
+                      "iterations_cold": r_cold.iterations,
+                      "weights": "xhdfe-xfe_b200/warmstart_mlp.npz (train_warmstart.py)"}
+    # plain FP64 on the same GPU (the comparison the metric names): the same
+    # solver batched over the 13 columns, and one column at a time (no
+    # batching; the FE structure built once and reused)
     fp64 = None
     if not args.no_fp64_compare and args.precision != "fp64":
         o64 = pkg.make_options(tol=1e-8, precision="fp64")
-        step(o64)
+        ms64, r64 = timed(o64, 2)
+        fp64 = {"ms_per_step": ms64, "iterations": r64.iterations, "rel_residual": r64.rel_residual,
+                "speedup_of_value": ms64 / ms}
+        o1 = pkg.make_options(tol=1e-8, precision="fp64", reuse_structure=True)
+        step(o64)  # builds the structure the per-column calls reuse
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        r64 = [step(o64) for _ in range(2)]
+        for c in range(cols):
+            absorber.absorb_device(v[c:c + 1], gids, panel.levels, None, o1, out=out[c:c + 1], stream=sh)
         e1.record(stream)
         torch.cuda.synchronize()
-        fp64 = {"ms_per_step": e0.elapsed_time(e1) / 2, "iterations": r64[-1].iterations,
-                "rel_residual": r64[-1].rel_residual}
+        ms_pc = e0.elapsed_time(e1)
+        fp64["per_column_ms_per_step"] = ms_pc
+        fp64["per_column_speedup_of_value"] = ms_pc / ms
+    if ws_params is not None:
+        pkg.learned.set_warm_start(absorber, ws_params, ws_mode)
 
     # end to end through the C ABI with pinned host buffers
     e2e = None
@@ -388,15 +467,34 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_sample, os.cpu_count() or 1)
     ref_gpu = None
+    err_ref = None
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu(panel, os.cpu_count() or 1)
+        ref_gpu.pop("V", None)
+        # the headline output against the reference's own CUDA absorber in
+        # strict-residual mode at tol 1e-11 (an independent solve of the 50M
+        # projection; its CPU core cannot produce one inside this run)
+        tight = reference_gpu(panel, os.cpu_count() or 1, tol=1e-11, mode="strict-residual")
+        if tight is not None and out_head is not None:
+            Vr = tight.pop("V")
+            Vh = out_head.cpu().numpy().T
+            scale = np.linalg.norm(np.column_stack([panel.y, panel.X]), axis=0)
+            scale[scale == 0] = 1.0
+            err = np.linalg.norm(Vh - Vr, axis=0) / scale
+            err_ref = {"max_rel_err": float(err.max()), "per_column": [float(e) for e in err],
+                       "against": "reference CUDA absorber, strict-residual tol 1e-11",
+                       "reference_seconds": tight["value"], "reference_iterations": tight["iterations"],
+                       "reference_converged": tight["converged"],
+                       "reference_gpu_status_code": tight["gpu_status_code"]}
+            del Vr, Vh
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms / 1000.0, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 inner CG + f64 refinement" if args.precision == "mixed" else "f64",
+            "dtype": ("f32 inner CG + f64 refinement" if args.precision == "mixed" else "f64") +
+                     (", learned warm start (bf16 MLP)" if ws_params is not None else ""),
             "data": "synthetic (seeded AKM generator, per-rank replica seed = rank)",
             "config": {"workload": "akm_3way_50M_13col_demean", "n_obs_generated": args.n,
                        "n_obs_after_singleton_drop": n, "columns": cols,
@@ -411,7 +509,7 @@ def run_ours(args):
             "precision_certified": bool(r_last.precision_certified),
             "setup_ms": r_last.setup_ms, "solve_ms": r_last.solve_ms,
             "roofline": roofline, "profile": prof, "clocks": clocks,
-            "fp64_plain": fp64,
+            "fp64_plain": fp64, "learned": learned_ab, "max_rel_err_vs_reference": err_ref,
             "e2e": e2e, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "generate_s": gen_s,
         }
         print(json.dumps(line))

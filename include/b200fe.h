@@ -113,6 +113,7 @@ typedef struct b200fe_result {
     double prof_ms[B200FE_PROF_CATEGORIES];
     double prof_bytes[B200FE_PROF_CATEGORIES];
     long long prof_launches[B200FE_PROF_CATEGORIES];
+    int warm_columns;        /* columns started from the learned warm start's prediction  */
 } b200fe_result;
 
 /* Library version, e.g. 10000 for 1.0.0. */
@@ -269,6 +270,50 @@ int b200fe_fe_recovery_max_delta(b200fe_context* ctx, const double* residual,
                                  const double* weights,
                                  const int32_t* sweep_order,
                                  double* out_max_delta);
+
+/* ---------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference, which always starts its
+ * solves from zero).  A 3-hidden-layer, 64-wide MLP with BF16 weights and
+ * activations and FP32 accumulation maps per-level features of the Schur
+ * system (its first three Jacobi iterates, the level's weight and mobility)
+ * to a correction of the third Jacobi iterate and a log-scaling of the level's
+ * Jacobi diagonal.  Parameters: b200fe_mlp_num_params() FP32 values, layout
+ * W1 (64x8, row-major), b1, W2 (64x64), b2, W3 (64x64), b3, W4 (2x64), b4.
+ * The plain FP64-checked solver still runs to the stated tolerance from the
+ * predicted start: only the iteration count changes.
+ * ------------------------------------------------------------------------- */
+int b200fe_mlp_num_params(void);
+/* y[n][2] = MLP(x[n][8]) on tensor cores (device arrays). */
+int b200fe_mlp_forward(b200fe_context* ctx, const float* d_params, const float* d_x, int64_t n,
+                       float* d_y);
+/* Loss L = (1/n) sum_s sum_o w_so (y_so - t_so)^2 over targets
+ * d_targets[n][4] = (t0, t1, w0, w1), and its gradient with respect to the
+ * FP32 master parameters (BF16 roundings straight-through):
+ * d_grad_loss[0 .. P) = gradient, d_grad_loss[P] = loss (FP64, P = num_params).
+ * Deterministic (fixed-order reductions). */
+int b200fe_mlp_grad(b200fe_context* ctx, const float* d_params, const float* d_x,
+                    const float* d_targets, int64_t n, double* d_grad_loss);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 master
+ * parameters from a gradient of b200fe_mlp_grad; step counts from 1. */
+int b200fe_mlp_adam(b200fe_context* ctx, float* d_params, float* d_m, float* d_v,
+                    const double* d_grad, int step, double lr);
+/* Installs trained parameters (host array) in the context: mode bit 0 starts
+ * every later absorption's refinement from the network's prediction (a column
+ * whose predicted start has a larger residual than zero starts cold), bit 1
+ * scales the Jacobi diagonal by the network's per-level factor.  params NULL
+ * or mode 0 turns the warm start off. */
+int b200fe_warmstart_set(b200fe_context* ctx, const float* params, int mode);
+/* Training samples: runs b200fe_absorb_device on the given problem with the
+ * plain solver (the installed warm start is not used) and writes, for every
+ * level of the non-primary dims and every column, the network's 8 features
+ * (d_features[count][8]) and the targets from the converged solution
+ * (d_targets[count][4]); capacity rows at most (B200FE_INVALID_ARG beyond). */
+int b200fe_warmstart_samples(b200fe_context* ctx, const double* d_v, int64_t n, int cols,
+                             int num_dims, const int32_t* const* d_group_ids,
+                             const int32_t* num_groups, const double* d_weights,
+                             const b200fe_options* opts, double* d_out, float* d_features,
+                             float* d_targets, int64_t capacity, int64_t* count,
+                             b200fe_result* res);
 
 /* One-way within transform that allocates no device memory, for callers that
  * cannot call cudaMalloc while they use this library: a host application that

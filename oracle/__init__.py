@@ -113,11 +113,14 @@ def certify(V_orig, V_tilde, fes, G, weights=None):
 class XrefOptions(ctypes.Structure):
     _fields_ = [("tol", _dbl), ("tolerance_mode", _int), ("absorption_method", _int),
                 ("num_threads", _int), ("max_iter", _int), ("drop_singletons", _int),
-                ("se_type", _int), ("fit_intercept", _int), ("gpu_backend", _int)]
+                ("se_type", _int), ("fit_intercept", _int), ("gpu_backend", _int),
+                ("use_krylov", _int)]
 
 
 TOLERANCE_MODES = {"xhdfe-fast": 0, "reghdfe-comparable": 1, "strict-residual": 2}
 METHODS = {"auto": 0, "gauss-seidel": 1, "symmetric-gauss-seidel": 2, "jacobi": 3}
+# "krylov": the reference's coefficient-space Jacobi-PCG absorber
+# (HdfeOptions::use_krylov, src/fe_absorption.cpp:10110), CPU only
 SE_TYPES = {"unadjusted": 0, "robust": 1, "cluster": 2}
 
 
@@ -162,6 +165,10 @@ def rlib(path: Path = REF_SO) -> ctypes.CDLL:
             lib.xref_components.argtypes = [_vp, _vp, _i64, _vp, P(_int), P(ctypes.c_longlong),
                                             P(_dbl), ctypes.c_char_p, _int]
             lib.xref_components.restype = _int
+        if hasattr(lib, "xref_schwarz_demean_raw"):
+            lib.xref_schwarz_demean_raw.argtypes = [_vp, _vp, _i64, _int, _vp, _int, _vp, _int, _dbl,
+                                                    _int, P(_int)]
+            lib.xref_schwarz_demean_raw.restype = _int
         if hasattr(lib, "xref_akm_kss"):
             lib.xref_akm_kss.argtypes = [_vp, _vp, _vp, _i64, _vp, ctypes.c_uint64, _dbl, _vp, P(_int),
                                          P(ctypes.c_longlong), ctypes.c_char_p, _int]
@@ -178,7 +185,8 @@ def _xopts(tol, tolerance_mode, method, threads, max_iter=0, drop_singletons=Tru
     o = XrefOptions()
     o.tol = tol
     o.tolerance_mode = TOLERANCE_MODES[tolerance_mode]
-    o.absorption_method = METHODS[method]
+    o.absorption_method = METHODS["auto" if method == "krylov" else method]
+    o.use_krylov = 1 if method == "krylov" else 0
     o.num_threads = threads
     o.max_iter = max_iter
     o.drop_singletons = 1 if drop_singletons else 0
@@ -408,6 +416,23 @@ def ref_run_ols(y, X, weights=None, clusters=None, *, se_type="unadjusted", tss=
     return {"coef": coef, "se": se, "cov": cov, "rss": sc[0], "sigma2": sc[1], "df_resid": sc[2],
             "cov_scale": sc[3], "cluster_u2": sc[4], "r2": sc[5], "r2_within": sc[6],
             "num_clusters": int(sc[7])}
+
+
+def ref_schwarz_demean_raw(y, X, fes, levels, *, tol=1e-10, max_iter=10000, threads=1,
+                           lib_path=REF_SO):
+    """xhdfe::schwarz_demean_raw of the given build (the reference's CPU block
+    PCG in libxhdfe_ref.so; the B200 absorber through the binding in
+    libxhdfe_ref_b200.so).  Returns (ok, V (n x (1+k)), iterations)."""
+    y = np.array(y, dtype=np.float64, copy=True)
+    X = np.asfortranarray(np.array(X, dtype=np.float64, copy=True))
+    n, k = y.size, X.shape[1]
+    g = np.ascontiguousarray(np.concatenate([np.asarray(f, dtype=np.int32) for f in fes]))
+    lv = np.ascontiguousarray(levels, dtype=np.int32)
+    its = _int(0)
+    ok = rlib(lib_path).xref_schwarz_demean_raw(y.ctypes.data, X.ctypes.data if k else None, n, k,
+                                                g.ctypes.data, len(fes), lv.ctypes.data, threads,
+                                                tol, max_iter, ctypes.byref(its))
+    return bool(ok), np.column_stack([y, X]), int(its.value)
 
 
 def ref_components(fe1, fe2, weights=None, lib_path=REF_SO):

@@ -31,6 +31,7 @@
 #include "fe_absorption.hpp"
 #include "fe_absorption_cuda.hpp"
 #include "hdfe/hdfe_regressor.hpp"
+#include "schwarz_demean.hpp"
 #include "hdfe/akm_kss.hpp"
 #include "ols.hpp"
 #include "hdfe/hdfe_regressor_v11.hpp"
@@ -52,6 +53,8 @@ struct XrefOptions {
     int se_type;          // 0 homoskedastic, 1 robust, 2 cluster
     int fit_intercept;
     int gpu_backend;      // 0 library default, 1 force CPU, 2 force CUDA
+    int use_krylov;       // 1: HdfeOptions::use_krylov (the coefficient-space Jacobi-PCG
+                          //    absorber, src/fe_absorption.cpp:10110), CPU backend
 };
 
 // Thread-local backend selection through the reference's own override
@@ -77,6 +80,7 @@ hdfe::HdfeOptions to_options(const XrefOptions* o) {
     opts.drop_singletons = o->drop_singletons != 0;
     opts.se_type = static_cast<hdfe::StandardErrorType>(o->se_type);
     opts.fit_intercept = o->fit_intercept != 0;
+    opts.use_krylov = o->use_krylov != 0;
     return opts;
 }
 
@@ -507,6 +511,24 @@ int xref_components(const int32_t* fe1, const int32_t* fe2, int64_t n, const dou
     } catch (...) {
         set_err(err, err_len, "unknown exception");
         return 1;
+    }
+}
+
+// xhdfe::schwarz_demean_raw (include/schwarz_demean.hpp:30-34) on Y (n) and X
+// (n x k, column-major) in place; fe_flat holds dims id arrays of length n.
+// Returns 1 when the call returned true, 0 when false.
+int xref_schwarz_demean_raw(double* Y, double* X, int64_t n, int k, const int32_t* fe_flat, int dims,
+                            const int32_t* nlev, int threads, double tol, int max_iter, int* iters_out) {
+    std::vector<const int32_t*> fe;
+    std::vector<int> lv;
+    for (int d = 0; d < dims; ++d) {
+        fe.push_back(fe_flat + static_cast<std::size_t>(d) * n);
+        lv.push_back(nlev[d]);
+    }
+    try {
+        return xhdfe::schwarz_demean_raw(Y, X, n, k, fe, lv, threads, tol, max_iter, iters_out, -1) ? 1 : 0;
+    } catch (...) {
+        return 0;
     }
 }
 

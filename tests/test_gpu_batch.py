@@ -8,7 +8,7 @@ rows) at which the reference's CPU core checks each solve in seconds:
 * the reference's own fit (src/hdfe_regressor_v11.cpp, HdfeRegressorV11::fit)
   dispatching its absorptions to this library through the reference-side
   binding, against the same fit on its CPU core in strict-residual mode:
-  coefficients at 1e-8 relative, SEs at 1e-7;
+  coefficients and SEs at 1e-8 relative;
 * this library's partial_out + run_ols (cluster) against the reference's
   partial_out (CPU, strict-residual) + run_ols at the same n_effective:
   within transform at 1e-8 of the column norm, coefficients and SEs at 1e-8;
@@ -23,7 +23,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 REL_TOL = 1e-8  # within transform (column norm) and coefficients
-SE_TOL = 1e-7   # SEs of the reference's fit, GPU solve vs strict CPU solve
+SE_TOL = 1e-8   # SEs of the reference's fit, GPU solve vs strict CPU solve
 
 
 def _batch(panels, count=12, seed=5):

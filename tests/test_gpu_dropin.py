@@ -61,4 +61,45 @@ def test_reference_partial_out_and_fit_on_b200(oracle_mod, panels, ref_b200):
                             lib_path=ref_b200)
     assert fg["gpu_status_code"] == 1 and fg["nobs"] == fc["nobs"]
     assert np.allclose(fg["coef"], fc["coef"], rtol=REL_TOL, atol=1e-12)
-    assert np.allclose(fg["se"], fc["se"], rtol=1e-7, atol=1e-12)
+    assert np.allclose(fg["se"], fc["se"], rtol=REL_TOL, atol=1e-12)
+
+
+def test_demean_raw_matches_oracle(pkg, oracle_mod, panels):
+    """b200fe_demean_raw (the C entry behind xhdfe::schwarz_demean_raw) against
+    the oracle's tight projection, unweighted, two and three FE dims."""
+    p = _panel(panels, seed=71)
+    ref, _, ok = oracle_mod.project(p.y, p.X, p.fes, p.levels, tol=1e-13)
+    assert ok
+    scale = np.linalg.norm(np.column_stack([p.y, p.X]), axis=0)
+    for k in (2, 3):
+        fes = p.fes[:k]
+        ref_k = ref if k == 3 else oracle_mod.project(p.y, p.X, fes, p.levels[:k], tol=1e-13)[0]
+        Y = np.array(p.y, dtype=np.float64, copy=True)
+        X = np.asfortranarray(np.array(p.X, dtype=np.float64, copy=True))
+        its = pkg.demean_raw(Y, X, fes, p.levels[:k], tol=1e-10)
+        V = np.column_stack([Y, X])
+        assert (np.linalg.norm(V - ref_k, axis=0) / scale).max() <= REL_TOL
+        assert its > 0
+
+
+def test_schwarz_demean_raw_binding_on_b200(oracle_mod, panels, ref_b200):
+    """The reference's xhdfe::schwarz_demean_raw with the reference signature,
+    defined by the binding over this library (libxhdfe_ref_b200.so, where
+    src/schwarz_demean.cpp is left out), against the oracle and against the
+    reference's own CPU block-PCG (libxhdfe_ref.so) on the same call."""
+    p = _panel(panels, seed=73)
+    ok_g, Vg, its_g = oracle_mod.ref_schwarz_demean_raw(p.y, p.X, p.fes, p.levels, tol=1e-10,
+                                                        lib_path=ref_b200)
+    ok_c, Vc, _ = oracle_mod.ref_schwarz_demean_raw(p.y, p.X, p.fes, p.levels, tol=1e-10, threads=4)
+    ref, _, ok = oracle_mod.project(p.y, p.X, p.fes, p.levels, tol=1e-13)
+    assert ok_g and ok_c and ok and its_g > 0
+    scale = np.linalg.norm(np.column_stack([p.y, p.X]), axis=0)
+    assert (np.linalg.norm(Vg - ref, axis=0) / scale).max() <= REL_TOL
+    assert (np.linalg.norm(Vg - Vc, axis=0) / scale).max() <= REL_TOL
+    # unsupported calls return false and leave the inputs as they were, as the
+    # reference's: one FE dim, and more than 16 columns
+    ok1, V1, _ = oracle_mod.ref_schwarz_demean_raw(p.y, p.X, p.fes[:1], p.levels[:1], lib_path=ref_b200)
+    assert not ok1 and np.array_equal(V1, np.column_stack([p.y, p.X]))
+    X16 = np.repeat(p.X, 8, axis=1)  # 1 + 16 columns
+    ok2, V2, _ = oracle_mod.ref_schwarz_demean_raw(p.y, X16, p.fes, p.levels, lib_path=ref_b200)
+    assert not ok2 and np.array_equal(V2, np.column_stack([p.y, X16]))

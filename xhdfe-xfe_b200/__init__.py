@@ -28,5 +28,6 @@ from .absorber import (  # noqa: F401
     run_ols,
 )
 from .kss import KssSolver, kss_system, max_lanes, stable_sort_u64  # noqa: F401
+from . import learned  # noqa: F401
 
 __version__ = "1.0.0"

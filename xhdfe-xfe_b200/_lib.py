@@ -58,6 +58,12 @@ EXPORTED_SYMBOLS = (
     "b200fe_kss_solve_multi",
     "b200fe_kss_solve",
     "b200fe_stable_sort_u64",
+    "b200fe_mlp_num_params",
+    "b200fe_mlp_forward",
+    "b200fe_mlp_grad",
+    "b200fe_mlp_adam",
+    "b200fe_warmstart_set",
+    "b200fe_warmstart_samples",
 )
 
 
@@ -126,6 +132,7 @@ class Result(ctypes.Structure):
         ("prof_ms", ctypes.c_double * PROF_CATEGORIES),
         ("prof_bytes", ctypes.c_double * PROF_CATEGORIES),
         ("prof_launches", ctypes.c_longlong * PROF_CATEGORIES),
+        ("warm_columns", ctypes.c_int),
     ]
 
 
@@ -219,6 +226,20 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.b200fe_kss_solve.restype = c_int
     lib.b200fe_stable_sort_u64.argtypes = [vp, vp, i64]
     lib.b200fe_stable_sort_u64.restype = c_int
+    lib.b200fe_mlp_num_params.argtypes = []
+    lib.b200fe_mlp_num_params.restype = c_int
+    lib.b200fe_mlp_forward.argtypes = [vp, vp, vp, i64, vp]
+    lib.b200fe_mlp_forward.restype = c_int
+    lib.b200fe_mlp_grad.argtypes = [vp, vp, vp, vp, i64, vp]
+    lib.b200fe_mlp_grad.restype = c_int
+    lib.b200fe_mlp_adam.argtypes = [vp, vp, vp, vp, vp, c_int, ctypes.c_double]
+    lib.b200fe_mlp_adam.restype = c_int
+    lib.b200fe_warmstart_set.argtypes = [vp, vp, c_int]
+    lib.b200fe_warmstart_set.restype = c_int
+    lib.b200fe_warmstart_samples.argtypes = [vp, vp, i64, c_int, c_int, pp, vp, vp,
+                                             ctypes.POINTER(Options), vp, vp, vp, i64,
+                                             ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(Result)]
+    lib.b200fe_warmstart_samples.restype = c_int
     if path is None:
         _LIB = lib
     return lib

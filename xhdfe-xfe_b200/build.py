@@ -10,9 +10,10 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
-SOURCES = ["b200fe.cu", "slopes.cu", "noalloc.cu", "kss.cu"]
+SOURCES = ["b200fe.cu", "slopes.cu", "noalloc.cu", "kss.cu", "learned.cu"]
 HEADERS = ["limits.cuh", "context.cuh", "common_kernels.cuh", "kernels.cuh", "setup_kernels.cuh",
-           "ols_kernels.cuh", "prep_kernels.cuh", "slope_kernels.cuh", "sparse_kernels.cuh"]
+           "ols_kernels.cuh", "prep_kernels.cuh", "slope_kernels.cuh", "sparse_kernels.cuh",
+           "pcg_kernels.cuh", "mlp_kernels.cuh", "ws_kernels.cuh"]
 OUT = HERE / "libb200fe.so"
 OBJ_DIR = HERE / "_build"
 

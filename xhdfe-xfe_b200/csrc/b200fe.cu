@@ -12,6 +12,7 @@
 #include "prep_kernels.cuh"
 #include "sparse_kernels.cuh"
 #include "pcg_kernels.cuh"
+#include "ws_kernels.cuh"
 
 using namespace b200fe;
 using namespace b200fe_host;
@@ -1452,6 +1453,47 @@ int pcg_persistent(b200fe_context* ctx, const Work<T>& wk, const T* dinv, T* x, 
     return B200FE_OK;
 }
 
+// Learned warm start (ws_kernels.cuh): the Jacobi iterates a1..a3 of S a = b
+// in FP64, the column scales and the network's features [GR * cols][8].
+template <int CQ>
+int ws_features(b200fe_context* ctx, const Work<double>& w64, const double* b64, int cols, double* q64,
+                double* dot_part, unsigned int* dot_ticket, double* dot_res, double** a1o, double** a3o,
+                double** sigmao, float** feato) {
+    const Structure& st = ctx->st;
+    constexpr int CP = 4 * CQ;
+    const cudaStream_t s = ctx->stream;
+    const int64_t GR = st.GR;
+    double *a1, *a2, *a3, *sigma;
+    float* feat;
+    B_CHECK(get_buf(ctx, "ws_a1", GR * CP, &a1));
+    B_CHECK(get_buf(ctx, "ws_a2", GR * CP, &a2));
+    B_CHECK(get_buf(ctx, "ws_a3", GR * CP, &a3));
+    B_CHECK(get_buf(ctx, "ws_sigma", CP, &sigma));
+    B_CHECK(get_buf(ctx, "ws_feat", static_cast<size_t>(GR) * cols * kWsFeatures, &feat));
+    const int g = grid_for(ctx, GR * CP, 256);
+    ws_jacobi_kernel<<<g, 256, 0, s>>>(GR, CP, nullptr, b64, nullptr, st.dinv64, a1);
+    B_LAUNCHED();
+    B_CHECK((matvec<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, a1, q64)));
+    ws_jacobi_kernel<<<g, 256, 0, s>>>(GR, CP, a1, b64, q64, st.dinv64, a2);
+    B_LAUNCHED();
+    B_CHECK((matvec<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, a2, q64)));
+    ws_jacobi_kernel<<<g, 256, 0, s>>>(GR, CP, a2, b64, q64, st.dinv64, a3);
+    B_LAUNCHED();
+    const int rgrid = grid_for(ctx, std::max<int64_t>(GR, 1) * CP, kRowThreads, 8);
+    row_dot_kernel<double, double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, a1, a1, dot_part, dot_ticket, dot_res);
+    B_LAUNCHED();
+    ws_sigma_kernel<<<1, 32, 0, s>>>(dot_res, GR, CP, sigma);
+    B_LAUNCHED();
+    ws_features_kernel<<<grid_for(ctx, GR * cols, 256), 256, 0, s>>>(
+        GR, CP, cols, a1, a2, a3, sigma, st.w_rows, st.dinv64, st.nS > 0 ? st.sbase[0] : GR, feat);
+    B_LAUNCHED();
+    *a1o = a1;
+    *a3o = a3;
+    *sigmao = sigma;
+    *feato = feat;
+    return B200FE_OK;
+}
+
 template <int CQ>
 int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                 const b200fe_options& o, b200fe_result* res) {
@@ -1519,6 +1561,8 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
 
     int total_iters = 0, outer = 0;
     bool converged = true;
+    const double* dinv64_use = st.dinv64;  // Jacobi diagonal (scaled by the learned warm start)
+    const float* dinv32_use = st.dinv32;
     double rel_res = 0.0;
     std::vector<double> bb(CP, 0.0), rr(CP, 0.0);
     if (GR > 0) {
@@ -1529,6 +1573,53 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         B_TRY(cudaMemsetAsync(a64, 0, sizeof(double) * GR * CP, s));
         B_TRY(cudaMemcpyAsync(r64, b64, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
         rr = bb;
+        // learned warm start: start from the network's prediction (columns
+        // whose predicted start has a larger residual than zero start cold),
+        // optionally with its per-row scaling of the Jacobi diagonal
+        if (ctx->ws_mode != 0 && ctx->ws_packed) {
+            ProfScope ps(ctx, B200FE_PROF_SETUP, 0.0);
+            double *wa1, *wa3, *wsig;
+            float *feat, *wy;
+            B_CHECK(ws_features<CQ>(ctx, w64, b64, cols, q64, dot_part, dot_ticket, dot_res, &wa1, &wa3,
+                                    &wsig, &feat));
+            B_CHECK(get_buf(ctx, "ws_y", static_cast<size_t>(GR) * cols * 2, &wy));
+            B_CHECK(mlp_forward_device(ctx, ctx->ws_packed, feat, GR * cols, wy));
+            if (ctx->ws_mode & 1) {
+                double* a0;
+                B_CHECK(get_buf(ctx, "ws_a0", GR * CP, &a0));
+                ws_apply_kernel<<<grid_for(ctx, GR * CP, 256), 256, 0, s>>>(GR, CP, cols, wa3, wsig, wy, a0);
+                B_LAUNCHED();
+                B_CHECK((matvec<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, a0, q64)));
+                double* r0;
+                B_CHECK(get_buf(ctx, "ws_r0", GR * CP, &r0));
+                sub_kernel<<<rgrid, kRowThreads, 0, s>>>(GR * CP, b64, q64, r0);
+                B_LAUNCHED();
+                row_dot_kernel<double, double><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r0, r0, dot_part,
+                                                                             dot_ticket, dot_res);
+                B_LAUNCHED();
+                std::vector<double> r0r0(CP, 0.0);
+                B_CHECK(sync_read_double(ctx, dot_res, CP, r0r0.data()));
+                for (int c = 0; c < cols && c < CP; ++c) {
+                    if (!(r0r0[c] < bb[c])) continue;  // keep the cold start of this column
+                    B_TRY(cudaMemcpy2DAsync(a64 + c, CP * sizeof(double), a0 + c, CP * sizeof(double),
+                                            sizeof(double), GR, cudaMemcpyDeviceToDevice, s));
+                    B_TRY(cudaMemcpy2DAsync(r64 + c, CP * sizeof(double), r0 + c, CP * sizeof(double),
+                                            sizeof(double), GR, cudaMemcpyDeviceToDevice, s));
+                    rr[c] = r0r0[c];
+                    ++res->warm_columns;
+                }
+            }
+            if (ctx->ws_mode & 2) {
+                double* d64s;
+                float* d32s;
+                B_CHECK(get_buf(ctx, "ws_dinv64", GR, &d64s));
+                B_CHECK(get_buf(ctx, "ws_dinv32", GR, &d32s));
+                ws_scale_kernel<<<grid_for(ctx, GR, 256), 256, 0, s>>>(GR, cols, wy, st.dinv64, d64s, d32s);
+                B_LAUNCHED();
+                dinv64_use = d64s;
+                dinv32_use = d32s;
+            }
+        }
         const double tol = o.tol;
         // Stop column c when ||r_c||^2 <= thr_c = max(tol^2 ||b_c||^2, floor_c^2).
         // The floor, 1e3 eps ||D'W||_F ||v_c||, sits four orders of magnitude
@@ -1611,10 +1702,10 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                 B_LAUNCHED();
                 int prc = B200FE_UNAVAILABLE;
                 if (st.sparse && ctx->persistent)
-                    prc = pcg_persistent<float, CQ>(ctx, w32, st.dinv32, x32, r32, z32, p32, q32, thr,
+                    prc = pcg_persistent<float, CQ>(ctx, w32, dinv32_use, x32, r32, z32, p32, q32, thr,
                                                     round_cap, &its);
                 if (prc == B200FE_UNAVAILABLE)
-                    B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.run_w32, st.block_w32, st.dinv32, x32, r32, z32, p32, q32, thr,
+                    B_CHECK((pcg<float, CQ>(ctx, w32, st.wp32, st.run_w32, st.block_w32, dinv32_use, x32, r32, z32, p32, q32, thr,
                                             round_cap, std::max(1, o.check_interval),
                                             &its)));
                 else if (prc != B200FE_OK)
@@ -1626,10 +1717,10 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                 B_LAUNCHED();
                 int prc = B200FE_UNAVAILABLE;
                 if (st.sparse && ctx->persistent)
-                    prc = pcg_persistent<double, CQ>(ctx, w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
+                    prc = pcg_persistent<double, CQ>(ctx, w64, dinv64_use, x64, rin64, z64, p64, q64, thr,
                                                      round_cap, &its);
                 if (prc == B200FE_UNAVAILABLE)
-                    B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, st.dinv64, x64, rin64, z64, p64, q64, thr,
+                    B_CHECK((pcg<double, CQ>(ctx, w64, st.wp64, st.run_w64, st.block_w64, dinv64_use, x64, rin64, z64, p64, q64, thr,
                                              round_cap, std::max(1, o.check_interval),
                                              &its)));
                 else if (prc != B200FE_OK)
@@ -1671,6 +1762,26 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
         // residual relative to the scale the stop rule uses (||b_c|| or the floor)
         for (int c = 0; c < cols && c < CP; ++c)
             if (thr64[c] > 0.0) rel_res = std::max(rel_res, tol * std::sqrt(rr[c] / thr64[c]));
+    }
+
+    // training samples of the learned warm start (b200fe_warmstart_samples):
+    // features of this right-hand side and targets from the converged a
+    if (ctx->ws_feat && GR > 0) {
+        double *wa1, *wa3, *wsig;
+        float* feat;
+        B_CHECK(ws_features<CQ>(ctx, w64, b64, cols, q64, dot_part, dot_ticket, dot_res, &wa1, &wa3, &wsig,
+                                &feat));
+        const int64_t ns = GR * cols;
+        if (ctx->ws_count + ns > ctx->ws_cap) {
+            ctx->err = "warm-start sample capacity exceeded";
+            return B200FE_INVALID_ARG;
+        }
+        B_TRY(cudaMemcpyAsync(ctx->ws_feat + ctx->ws_count * kWsFeatures, feat,
+                              sizeof(float) * ns * kWsFeatures, cudaMemcpyDeviceToDevice, s));
+        ws_targets_kernel<<<grid_for(ctx, ns, 256), 256, 0, s>>>(GR, CP, cols, a64, wa1, wa3, wsig,
+                                                                 ctx->ws_targ + ctx->ws_count * 4);
+        B_LAUNCHED();
+        ctx->ws_count += ns;
     }
 
     // final pass: out = (I - P_p)(v - D_r a); certificate scatter; with saved
@@ -1972,6 +2083,30 @@ int b200fe_absorb_device(b200fe_context* ctx, const double* d_v, int64_t n, int 
     r->kernel_launches = ctx->launches - l0;
     r->library_calls = ctx->lib_calls - c0;
     return r->status = rc;
+}
+
+int b200fe_warmstart_samples(b200fe_context* ctx, const double* d_v, int64_t n, int cols,
+                             int num_dims, const int32_t* const* d_group_ids,
+                             const int32_t* num_groups, const double* d_weights,
+                             const b200fe_options* opts, double* d_out, float* d_features,
+                             float* d_targets, int64_t capacity, int64_t* count,
+                             b200fe_result* res) {
+    if (!ctx || !d_features || !d_targets || !count || capacity < 0) return B200FE_INVALID_ARG;
+    *count = 0;
+    const int saved_mode = ctx->ws_mode;
+    ctx->ws_mode = 0;  // samples come from the plain solver
+    ctx->ws_feat = d_features;
+    ctx->ws_targ = d_targets;
+    ctx->ws_cap = capacity;
+    ctx->ws_count = 0;
+    const int rc = b200fe_absorb_device(ctx, d_v, n, cols, num_dims, d_group_ids, num_groups, d_weights,
+                                        opts, d_out, res, nullptr);
+    *count = ctx->ws_count;
+    ctx->ws_feat = nullptr;
+    ctx->ws_targ = nullptr;
+    ctx->ws_cap = ctx->ws_count = 0;
+    ctx->ws_mode = saved_mode;
+    return rc;
 }
 
 int b200fe_absorb_fe(b200fe_context* ctx, const double* y, const double* X, int64_t n, int k,

@@ -128,6 +128,12 @@ struct Structure {
 
 constexpr int32_t kChunkRuns = 64;
 
+// The warm-start network (learned.cu): BF16 packing of FP32 master
+// parameters into a named workspace buffer, and the forward pass y[n][2] of
+// features x[n][8] on the context's stream.
+int mlp_pack_device(b200fe_context* ctx, const float* d_params, const char* name, void** packed);
+int mlp_forward_device(b200fe_context* ctx, const void* packed, const float* d_x, int64_t n, float* d_y);
+
 // Device address of the no-alloc entry point's scratch array on the current
 // device (noalloc.cu); resolving it loads that file's device code there.
 int noalloc_scratch_for_current_device(int32_t** out);
@@ -169,6 +175,15 @@ struct b200fe_context {
     // persistent PCG kernel over the explicit Schur block (one cooperative
     // launch per inner solve); off when B200FE_PERSISTENT=0 at context creation
     bool persistent = true;
+    // learned warm start (b200fe_warmstart_set): packed network and mode bits
+    // (1: start the refinement from its prediction, 2: scale the Jacobi
+    // diagonal by its per-row factor); training-sample collection
+    // (b200fe_warmstart_samples) while ws_feat is set
+    int ws_mode = 0;
+    void* ws_packed = nullptr;
+    float* ws_feat = nullptr;
+    float* ws_targ = nullptr;
+    int64_t ws_cap = 0, ws_count = 0;
     cudaStream_t cap_stream = nullptr;
     std::unordered_map<int, cudaGraphExec_t> graph_exec;
 };

@@ -272,3 +272,32 @@ def subset(p: Panel, keep: np.ndarray) -> Panel:
                  fes=fes, fe_names=list(p.fe_names), levels=levels,
                  weights=None if p.weights is None else p.weights[keep], cluster=cl,
                  meta=dict(p.meta, singletons_dropped=int((~keep).sum())))
+
+
+def warmstart_panel_spec(i: int, *, seed: int = 4, n_min: int = 100_000,
+                         n_max: int = 20_000_000) -> dict:
+    """The i-th panel of the learned warm start's workload: N log-uniform in
+    [n_min, n_max], 2-4 FE dims (worker, firm, year, firm x year), move
+    probability U(0.02, 0.3), firm-size Zipf exponent U(0.8, 1.5), about 62
+    observations per firm (the 50M panel's ratio), 36 years."""
+    rng = np.random.default_rng([seed, i])
+    n = int(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+    return {"n": n, "dims": int(rng.integers(2, 5)), "move_prob": float(rng.uniform(0.02, 0.3)),
+            "zipf": float(rng.uniform(0.8, 1.5)), "n_firms": max(200, n // 62), "seed": 10_000 + i}
+
+
+def warmstart_panel(spec: dict) -> Panel:
+    """The panel of ``warmstart_panel_spec`` with singletons dropped; its FE
+    list holds the spec's first ``dims`` of (worker, firm, year, firm x year)."""
+    p = akm_batched(spec["n"], n_firms=spec["n_firms"], n_years=36, seed=spec["seed"],
+                    move_prob=spec["move_prob"], zipf=spec["zipf"])
+    fes, names, levels = list(p.fes), list(p.fe_names), list(p.levels)
+    if spec["dims"] >= 4:
+        fy, g = _dense(p.fes[1].astype(np.int64) * p.levels[2] + p.fes[2], p.levels[1] * p.levels[2])
+        fes.append(fy)
+        names.append("firm_x_year")
+        levels.append(g)
+    k = spec["dims"]
+    p = Panel(y=p.y, X=p.X, fes=fes[:k], fe_names=names[:k], levels=levels[:k], cluster=p.cluster,
+              meta=dict(p.meta, spec=spec))
+    return subset(p, drop_singletons(p.fes))

@@ -13,6 +13,8 @@
 //   fe_recovery_max_delta_cuda(_cached)        (fe_absorption_cuda.hpp:152-162)
 //   cuda_cert_shadow_begin/finish/abort        (fe_absorption_cuda.hpp:74-99)
 //   akm_cuda_*                                 (akm_kss_cuda.hpp:17-74)
+//   xhdfe::schwarz_demean_raw                  (schwarz_demean.hpp:30-34; this file
+//                                               then replaces src/schwarz_demean.cpp)
 // The host certificate certify_cuda_absorption_result stays the reference's
 // own src/fe_absorption_cuda_certificate.cpp.
 //
@@ -40,6 +42,7 @@
 #include "b200fe.h"
 #include "fe_absorption_cuda.hpp"
 #include "hdfe/akm_kss_cuda.hpp"
+#include "schwarz_demean.hpp"
 
 namespace {
 
@@ -365,3 +368,42 @@ double* akm_cuda_pack_buffer(AkmCudaContext* ctx, int nb) {
 
 }  // namespace akm
 }  // namespace hdfe
+
+namespace xhdfe {
+
+// The reference's raw in-place within-demean (include/schwarz_demean.hpp:30-34,
+// src/schwarz_demean.cpp:419-438), called by its CPU absorber's Schwarz gate
+// (src/fe_absorption.cpp:5199), on the B200 absorber (b200fe_demean_raw).  Same
+// contract: Y (n) and X (n x k, column-major) overwritten with the unweighted
+// within residuals on success, iters_out set; false with Y and X untouched when
+// unsupported (fewer than two FE dims, n <= 0, k < 0, more than 16 columns,
+// mismatched level list) or when the device solve fails or does not converge.
+// threads and collapse select the reference's CPU factorisation and have no
+// meaning here.
+bool schwarz_demean_raw(double* Y, double* X, int64_t n, int k, const std::vector<const int32_t*>& fe,
+                        const std::vector<int>& nlev, int threads, double tol, int max_iter,
+                        int* iters_out, int collapse) {
+    (void)threads;
+    (void)collapse;
+    if (fe.size() < 2 || nlev.size() != fe.size() || n <= 0 || k < 0 || k + 1 > 16 ||
+        fe.size() > B200FE_MAX_DIMS || !Y || (k > 0 && !X))
+        return false;
+    try {
+        std::vector<int32_t> G(nlev.begin(), nlev.end());
+        std::vector<double> y(Y, Y + n);
+        std::vector<double> x(X ? X : Y, X ? X + static_cast<std::size_t>(n) * k : Y);
+        int its = 0;
+        const int rc = b200fe_demean_raw(y.data(), k > 0 ? x.data() : nullptr, n, k,
+                                         static_cast<int>(fe.size()), fe.data(), G.data(), tol,
+                                         max_iter, &its);
+        if (iters_out) *iters_out = its;
+        if (rc != B200FE_OK) return false;
+        std::copy(y.begin(), y.end(), Y);
+        if (k > 0) std::copy(x.begin(), x.end(), X);
+        return true;
+    } catch (...) {
+        return false;
+    }
+}
+
+}  // namespace xhdfe
