@@ -470,7 +470,8 @@ def run_ours(args):
     err_ref = None
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu(panel, os.cpu_count() or 1)
-        ref_gpu.pop("V", None)
+        if ref_gpu is not None:
+            ref_gpu.pop("V", None)
         # the headline output against the reference's own CUDA absorber in
         # strict-residual mode at tol 1e-11 (an independent solve of the 50M
         # projection; its CPU core cannot produce one inside this run)

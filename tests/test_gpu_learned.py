@@ -7,7 +7,7 @@
   column, finite, with targets built from the converged solution;
 * a network trained from scratch on small seeded panels, installed in an
   absorber: on held-out panels the warm-started solves take fewer iterations
-  than the cold ones (the gain), every solve converges to tol 1e-8, and the
+  than the cold ones (the gain), every solve converges (tol 1e-10), and the
   warm within transform equals the cold one to 1e-8 of the column norm and the
   oracle's tight projection to 1e-8 (the plain solver decides the answer).
 """
@@ -116,7 +116,11 @@ def test_warm_start_gain_on_held_out_panels(absorber, learned, panels, pkg, orac
         targs.append(t.clone())
     X, T = torch.cat(feats), torch.cat(targs)
     params = learned.train(absorber, X, T, epochs=3, batch=4096, lr=2e-3, seed=0)
-    opts = pkg.make_options(tol=1e-8)
+    # tol 1e-10, so that two solves of one projection (cold and warm) and the
+    # oracle's tight projection agree to 1e-8 of the column norm; at tol 1e-8
+    # each is within tolerance of the exact answer but two of them can differ
+    # by twice that
+    opts = pkg.make_options(tol=1e-10)
     cold_its, warm_its = [], []
     for k, s in enumerate(specs[10:]):
         p = panels.warmstart_panel(s)
