@@ -228,16 +228,14 @@ int build_sparse_block(b200fe_context* ctx) {
         st.pc_nshort = cnt[0];
         st.pc_nlong = cnt[1];
         st.pc_nlchunks = cnt[2];
-        B_CHECK(get_buf(ctx, "pc_short_rows", std::max<int64_t>(st.pc_nshort, 1), &st.pc_short_rows));
+        B_CHECK(get_buf(ctx, "pc_short_meta", std::max<int64_t>(st.pc_nshort, 1), &st.pc_short_meta));
         B_CHECK(get_buf(ctx, "pc_long_rows", std::max<int64_t>(st.pc_nlong, 1), &st.pc_long_rows));
         B_CHECK(get_buf(ctx, "pc_long_c0", std::max<int64_t>(st.pc_nlong, 1), &st.pc_long_c0));
         B_CHECK(get_buf(ctx, "pc_long_c1", std::max<int64_t>(st.pc_nlong, 1), &st.pc_long_c1));
-        B_CHECK(get_buf(ctx, "pc_lchunk_row", std::max<int64_t>(st.pc_nlchunks, 1), &st.pc_lchunk_row));
-        B_CHECK(get_buf(ctx, "pc_lchunk_beg", std::max<int64_t>(st.pc_nlchunks, 1), &st.pc_lchunk_beg));
+        B_CHECK(get_buf(ctx, "pc_lchunk_meta", std::max<int64_t>(st.pc_nlchunks, 1), &st.pc_lchunk_meta));
         pcg_lists_fill_kernel<<<grid_for(ctx, L.G, T256), T256, 0, s>>>(
-            st.sp_row_off, L.G, is_short, short_idx, long_idx, chunk_off, st.pc_short_rows,
-            st.pc_long_rows, st.pc_long_c0, st.pc_long_c1, st.pc_lchunk_row, st.pc_lchunk_beg, huge_idx,
-            st.pc_huge_li);
+            st.sp_row_off, L.G, is_short, short_idx, long_idx, chunk_off, st.pc_short_meta,
+            st.pc_long_rows, st.pc_long_c0, st.pc_long_c1, st.pc_lchunk_meta, huge_idx, st.pc_huge_li);
         B_LAUNCHED();
     }
     st.sparse = true;
@@ -1394,10 +1392,9 @@ int pcg_persistent(b200fe_context* ctx, const Work<T>& wk, const T* dinv, T* x, 
     a.col = st.sp_col;
     a.val = pick_prec<T>(st.sp_val32, st.sp_val64);
     a.nshort = st.pc_nshort;
-    a.short_rows = st.pc_short_rows;
+    a.short_meta = st.pc_short_meta;
     a.nlchunks = st.pc_nlchunks;
-    a.lchunk_row = st.pc_lchunk_row;
-    a.lchunk_beg = st.pc_lchunk_beg;
+    a.lchunk_meta = st.pc_lchunk_meta;
     a.nlong = st.pc_nlong;
     a.long_rows = st.pc_long_rows;
     a.long_c0 = st.pc_long_c0;

@@ -119,9 +119,9 @@ struct Structure {
     LargeDim sp;                       // chunk lists over the CSR rows (chunk fields only)
     // work lists of the persistent PCG over the same rows (pcg_kernels.cuh)
     int64_t pc_nshort = 0, pc_nlong = 0, pc_nlchunks = 0;
-    int32_t* pc_short_rows = nullptr;
+    int4* pc_short_meta = nullptr;     // {row, begin, end, 0} of the short rows
     int32_t *pc_long_rows = nullptr, *pc_long_c0 = nullptr, *pc_long_c1 = nullptr;
-    int32_t *pc_lchunk_row = nullptr, *pc_lchunk_beg = nullptr;
+    int4* pc_lchunk_meta = nullptr;    // {row, begin, end, first} of the long-row chunks
     int64_t pc_nhuge = 0;
     int32_t* pc_huge_li = nullptr;
 };

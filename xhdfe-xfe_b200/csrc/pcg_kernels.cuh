@@ -58,10 +58,9 @@ struct PcgArgs {
     const int32_t* col;
     const T* val;
     int64_t nshort;
-    const int32_t* short_rows;  // rows with <= kShortNnz nonzeros, ascending
+    const int4* short_meta;     // rows with <= kShortNnz nonzeros, ascending: {row, begin, end, 0}
     int64_t nlchunks;           // chunks of long rows (kLongChunk nonzeros each)
-    const int32_t* lchunk_row;
-    const int32_t* lchunk_beg;
+    const int4* lchunk_meta;    // {row, begin, end, 1 for the row's first chunk}
     int64_t nlong;
     const int32_t* long_rows;   // [nlong] row of each long row
     const int32_t* long_c0;     // [nlong] its chunk range in lchunk_*
@@ -210,6 +209,46 @@ __device__ __forceinline__ void cta_reduce_quads(const double (&v)[4], int CQ, d
         }
         if (t < CQ) out[4 * t + i] = red[t];
         __syncthreads();
+    }
+}
+
+// q += sum over nonzeros j of val[j] p[col[j]] (4 columns of this lane) for
+// j = j0, j0 + step, ... < je, U nonzeros per batch; the next batch's column
+// ids and values are loaded while the current batch's rows of p are gathered.
+template <typename T, int CP, int U>
+__device__ __forceinline__ void gather_rows(const int32_t* __restrict__ col, const T* __restrict__ val,
+                                            const T* p, int32_t j0, int32_t je, int step, int q4,
+                                            Acc4& acc) {
+    int32_t cj[U];
+    T vj[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int32_t j = j0 + u * step;
+        cj[u] = j < je ? __ldg(col + j) : -1;
+        vj[u] = j < je ? __ldg(val + j) : T(0);
+    }
+    for (int32_t jb = j0; jb < je; jb += U * step) {
+        V4<T> xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (cj[u] >= 0) v4_load_cg(p + static_cast<int64_t>(cj[u]) * CP + 4 * q4, xv[u]);
+            else v4_zero(xv[u]);
+        }
+        T vc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) vc[u] = vj[u];
+        const int32_t jn = jb + U * step;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t j = jn + u * step;
+            cj[u] = j < je ? __ldg(col + j) : -1;
+            vj[u] = j < je ? __ldg(val + j) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                acc.v[i] = fma(static_cast<double>(vc[u]), static_cast<double>(xv[u].v[i]), acc.v[i]);
     }
 }
 
@@ -366,35 +405,16 @@ pcg_persistent_kernel(const PcgArgs<T> a) {
         double dot[4] = {0.0, 0.0, 0.0, 0.0};
         const int64_t nwarps = static_cast<int64_t>(NB) * (kPcgThreads / 32);
         const int64_t wid = static_cast<int64_t>(b) * (kPcgThreads / 32) + warp;
-        // long-row chunks: a warp each, lane groups interleave the nonzeros
+        // long-row chunks: a warp each, lane groups interleave the nonzeros;
+        // the next chunk's record is loaded one chunk ahead
+        int4 lm = wid < a.nlchunks ? __ldg(a.lchunk_meta + wid) : make_int4(0, 0, 0, 0);
         for (int64_t ch = wid; ch < a.nlchunks; ch += nwarps) {
-            const int32_t g = __ldg(a.lchunk_row + ch);
-            const int32_t jb = __ldg(a.lchunk_beg + ch);
-            const int32_t je = min(__ldg(a.row_off + g + 1), jb + kLongChunk);
-            const bool first = jb == __ldg(a.row_off + g);
+            const int32_t g = lm.x, jb = lm.y, je = lm.z;
+            const bool first = lm.w != 0;
+            if (ch + nwarps < a.nlchunks) lm = __ldg(a.lchunk_meta + ch + nwarps);
             Acc4 acc;
             acc_zero(acc);
-            for (int32_t j0 = jb + gw; j0 < je; j0 += GPW * U) {
-                int32_t cj[U];
-                T vj[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int32_t j = j0 + u * GPW;
-                    cj[u] = j < je ? __ldg(a.col + j) : -1;
-                    vj[u] = j < je ? __ldg(a.val + j) : T(0);
-                }
-                V4<T> xv[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    if (cj[u] >= 0) v4_load_cg(a.p + static_cast<int64_t>(cj[u]) * CP + 4 * q4, xv[u]);
-                    else v4_zero(xv[u]);
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        acc.v[i] = fma(static_cast<double>(vj[u]), static_cast<double>(xv[u].v[i]), acc.v[i]);
-            }
+            gather_rows<T, CP, U>(a.col, a.val, a.p, jb + gw, je, GPW, q4, acc);
             // lane groups of the warp combined by a butterfly (every lane gets
             // the same sum)
 #pragma unroll
@@ -407,20 +427,26 @@ pcg_persistent_kernel(const PcgArgs<T> a) {
                 // the row's first chunk carries C_fy[g] p_small, and adds the
                 // row to the warp's C_fy' p_f
                 const T* crow = a.cfy + static_cast<int64_t>(g) * a.SGP;
-                T cs[4] = {T(0), T(0), T(0), T(0)};
-                for (int h = 0; h < a.SG; ++h) {
-                    const T cv = __ldg(crow + h);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) cs[i] = fma(cv, s_xs[h * CP + 4 * q4 + i], cs[i]);
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i) acc.v[i] += static_cast<double>(cs[i]);
                 if (gw == 0) {
 #pragma unroll
                     for (int i = 0; i < 4; ++i) slab[4 * q4 + i] = pv.v[i];
                 }
                 for (int h = lane; h < a.SGP; h += 32) slab[CP + h] = __ldg(crow + h);
                 __syncwarp();
+                T cs[4] = {T(0), T(0), T(0), T(0)};
+                for (int h0 = 0; h0 < a.SGP; h0 += 4) {
+                    T c4[4];
+                    lds4<T>(slab + CP + h0, c4);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        T xr[4];
+                        lds4<T>(s_xs + (h0 + u) * CP + 4 * q4, xr);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) cs[i] = fma(c4[u], xr[i], cs[i]);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) acc.v[i] += static_cast<double>(cs[i]);
                 couple_rows<T, CQ>(slab, 1, a.SGP, lane, cacc);
                 __syncwarp();
             }
@@ -436,10 +462,15 @@ pcg_persistent_kernel(const PcgArgs<T> a) {
         // short rows: GPW rows per warp, one lane group each.  With a coupled
         // small dim the row's C_fy row is copied into the warp's slab
         // (cp.async) while the gather runs.
+        int4 sm = wid * GPW + gw < a.nshort ? __ldg(a.short_meta + wid * GPW + gw) : make_int4(0, 0, 0, 0);
         for (int64_t base = wid * GPW; base < a.nshort; base += nwarps * GPW) {
             const int64_t si = base + gw;
             const bool valid = si < a.nshort;
-            const int32_t g = valid ? __ldg(a.short_rows + si) : 0;
+            const int32_t g = sm.x, jb = sm.y, je = sm.z;
+            {  // the next step's record, one step ahead
+                const int64_t sn = si + nwarps * GPW;
+                sm = sn < a.nshort ? __ldg(a.short_meta + sn) : make_int4(0, 0, 0, 0);
+            }
             T* srow = slab + gw * (CP + a.SGP);
             if (coupled) {
                 constexpr int VT = 16 / sizeof(T);  // elements per 16-byte copy
@@ -454,30 +485,9 @@ pcg_persistent_kernel(const PcgArgs<T> a) {
                 }
                 cp_async_commit();
             }
-            const int32_t jb = valid ? __ldg(a.row_off + g) : 0;
-            const int32_t je = valid ? __ldg(a.row_off + g + 1) : 0;
             Acc4 acc;
             acc_zero(acc);
-            for (int32_t j0 = jb; j0 < je; j0 += U) {
-                int32_t cj[U];
-                T vj[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    cj[u] = j0 + u < je ? __ldg(a.col + j0 + u) : -1;
-                    vj[u] = j0 + u < je ? __ldg(a.val + j0 + u) : T(0);
-                }
-                V4<T> xv[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    if (cj[u] >= 0) v4_load_cg(a.p + static_cast<int64_t>(cj[u]) * CP + 4 * q4, xv[u]);
-                    else v4_zero(xv[u]);
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        acc.v[i] = fma(static_cast<double>(vj[u]), static_cast<double>(xv[u].v[i]), acc.v[i]);
-            }
+            gather_rows<T, CP, U>(a.col, a.val, a.p, jb, je, 1, q4, acc);
             V4<T> pv;
             if (valid) v4_load_cg(a.p + static_cast<int64_t>(g) * CP + 4 * q4, pv);
             else v4_zero(pv);
@@ -811,14 +821,14 @@ __global__ void pcg_lists_fill_kernel(const int32_t* __restrict__ row_off, int32
                                       const int32_t* __restrict__ short_idx,
                                       const int32_t* __restrict__ long_idx,
                                       const int32_t* __restrict__ chunk_off,
-                                      int32_t* __restrict__ short_rows, int32_t* __restrict__ long_rows,
+                                      int4* __restrict__ short_meta, int32_t* __restrict__ long_rows,
                                       int32_t* __restrict__ long_c0, int32_t* __restrict__ long_c1,
-                                      int32_t* __restrict__ lchunk_row, int32_t* __restrict__ lchunk_beg,
+                                      int4* __restrict__ lchunk_meta,
                                       const int32_t* __restrict__ huge_idx, int32_t* __restrict__ huge_li) {
     for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
          g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         if (is_short[g]) {
-            short_rows[short_idx[g]] = static_cast<int32_t>(g);
+            short_meta[short_idx[g]] = make_int4(static_cast<int32_t>(g), row_off[g], row_off[g + 1], 0);
             continue;
         }
         const int32_t li = long_idx[g];
@@ -827,10 +837,10 @@ __global__ void pcg_lists_fill_kernel(const int32_t* __restrict__ row_off, int32
         long_c0[li] = c0;
         long_c1[li] = c1;
         if (c1 - c0 > kHugeChunks) huge_li[huge_idx[g]] = li;
-        const int32_t b = row_off[g];
+        const int32_t b = row_off[g], e = row_off[g + 1];
         for (int32_t c = c0; c < c1; ++c) {
-            lchunk_row[c] = static_cast<int32_t>(g);
-            lchunk_beg[c] = b + (c - c0) * kLongChunk;
+            const int32_t cb = b + (c - c0) * kLongChunk;
+            lchunk_meta[c] = make_int4(static_cast<int32_t>(g), cb, min(e, cb + kLongChunk), c == c0 ? 1 : 0);
         }
     }
 }
