@@ -186,3 +186,28 @@ def test_block_and_tile_matvec_agree(absorber, pkg, oracle_mod, panels, weighted
     scale = np.linalg.norm(np.column_stack([p.y, p.X]), axis=0)
     for o in outs[1:]:
         assert (np.linalg.norm(outs[0] - o, axis=0) / scale).max() <= 1e-9
+
+
+def test_pipelined_host_copies_match_single_stream(pkg, oracle_mod, panels, monkeypatch):
+    """Host-array calls with more than four columns copy column groups in and
+    out on their own streams while other groups are solved; the within
+    transform equals the oracle's tight projection and the single-stream call
+    (B200FE_PIPELINE=0 at context creation) to 1e-9 of the column norm."""
+    p = _akm(panels, 40_000, True, seed=41)
+    rng = np.random.default_rng(9)
+    X = np.asfortranarray(np.column_stack([p.X, rng.standard_normal((p.n, 10))]))  # 13 columns
+    o = pkg.make_options(tol=1e-10)
+    outs = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("B200FE_PIPELINE", flag)
+        ab = pkg.Absorber(0)
+        try:
+            r = ab.absorb(p.y, X, p.fes, p.levels, None, o)
+        finally:
+            ab.close()
+        assert r.converged and r.precision_certified
+        outs[flag] = np.column_stack([r.y_tilde, r.X_tilde])
+    ref, _, ok = oracle_mod.project(p.y, X, p.fes, p.levels, tol=1e-13)
+    scale = np.linalg.norm(np.column_stack([p.y, X]), axis=0)
+    assert ok and (np.linalg.norm(outs["1"] - ref, axis=0) / scale).max() <= REL_TOL
+    assert (np.linalg.norm(outs["1"] - outs["0"], axis=0) / scale).max() <= 1e-9

@@ -1224,8 +1224,8 @@ int pcg(b200fe_context* ctx, const Work<T>& wk, const T* wp, const T* run_w, con
     B_CHECK(get_buf(ctx, "cs_partial", static_cast<size_t>(rgrid) * 2 * CP, &cs.partial));
     std::vector<int> act(CP, 0);
     for (int c = 0; c < CP; ++c) act[c] = thr_host[c] > 0.0 ? 1 : 0;
-    B_TRY(cudaMemcpyAsync(cs.thr, thr_host.data(), sizeof(double) * CP, cudaMemcpyHostToDevice, s));
-    B_TRY(cudaMemcpyAsync(cs.active, act.data(), sizeof(int) * CP, cudaMemcpyHostToDevice, s));
+    B_CHECK(small_h2d(ctx, cs.thr, thr_host.data(), sizeof(double) * CP));
+    B_CHECK(small_h2d(ctx, cs.active, act.data(), sizeof(int) * CP));
     B_TRY(cudaMemsetAsync(cs.rz, 0, sizeof(double) * CP, s));
     B_TRY(cudaMemsetAsync(cs.pq, 0, sizeof(double) * CP, s));
     B_TRY(cudaMemsetAsync(cs.iters, 0, sizeof(int) * CP, s));
@@ -1425,7 +1425,7 @@ int pcg_persistent(b200fe_context* ctx, const Work<T>& wk, const T* dinv, T* x, 
     a.status = ctl + 1;
     a.bar = reinterpret_cast<unsigned int*>(ctl + 2);
     a.thr = thr_d;
-    B_TRY(cudaMemcpyAsync(thr_d, thr_host.data(), sizeof(double) * CP, cudaMemcpyHostToDevice, s));
+    B_CHECK(small_h2d(ctx, thr_d, thr_host.data(), sizeof(double) * CP));
     B_TRY(cudaMemsetAsync(ctl, 0, 4 * sizeof(int32_t), s));
     void* args[] = {&a};
     {
@@ -1547,11 +1547,9 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
     std::vector<double> vnorm2(CP, 0.0);
     {
         std::vector<double> hp(static_cast<size_t>(w64.nbins_ctas) * CP);
-        B_TRY(cudaMemcpyAsync(hp.data(), w64.colsq_partial, sizeof(double) * hp.size(),
-                              cudaMemcpyDeviceToHost, s));
         if (GR > 0)
             B_CHECK(reduce_runs<double, CQ>(ctx, w64, b64, nullptr, B200FE_PROF_RHS, B200FE_PROF_RHS));
-        B_TRY(cudaStreamSynchronize(s));
+        B_CHECK(small_d2h(ctx, w64.colsq_partial, sizeof(double) * hp.size(), hp.data()));
         for (int b = 0; b < w64.nbins_ctas; ++b)
             for (int c = 0; c < CP; ++c) vnorm2[c] += hp[static_cast<size_t>(b) * CP + c];
     }
@@ -1640,9 +1638,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             row_linf_kernel<<<rgrid, kRowThreads, 0, s>>>(GR, CP, cols, r64, st.w_rows, linf_d);
             B_LAUNCHED();
             std::vector<unsigned long long> bits(CP);
-            B_TRY(cudaMemcpyAsync(bits.data(), linf_d, sizeof(unsigned long long) * CP,
-                                  cudaMemcpyDeviceToHost, s));
-            B_TRY(cudaStreamSynchronize(s));
+            B_CHECK(small_d2h(ctx, linf_d, sizeof(unsigned long long) * CP, bits.data()));
             for (int c = 0; c < CP; ++c) std::memcpy(&linf[c], &bits[c], sizeof(double));
             return B200FE_OK;
         };
@@ -1690,9 +1686,8 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                 B_TRY(cudaMemcpyAsync(a_prev, a64, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
                 B_TRY(cudaMemcpyAsync(r_prev, r64, sizeof(double) * GR * CP, cudaMemcpyDeviceToDevice, s));
             }
-            B_TRY(cudaMemcpyAsync(scale_d, scale.data(), sizeof(double) * CP, cudaMemcpyHostToDevice, s));
-            B_TRY(cudaMemcpyAsync(inv_scale_d, inv_scale.data(), sizeof(double) * CP,
-                                  cudaMemcpyHostToDevice, s));
+            B_CHECK(small_h2d(ctx, scale_d, scale.data(), sizeof(double) * CP));
+            B_CHECK(small_h2d(ctx, inv_scale_d, inv_scale.data(), sizeof(double) * CP));
             int its = 0;
             if (mixed) {
                 scale_rows_kernel<float><<<rgrid, kRowThreads, 0, s>>>(GR, CP, r64, inv_scale_d, r32);
@@ -1807,8 +1802,6 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
     double abs_res = 0.0, abs_rel = 0.0;
     if (cert) {
         std::vector<double> hp(static_cast<size_t>(w64.nbins_ctas) * CP);
-        B_TRY(cudaMemcpyAsync(hp.data(), w64.colsq_partial, sizeof(double) * hp.size(),
-                              cudaMemcpyDeviceToHost, s));
         std::vector<double> res2(CP, 0.0);
         if (GR > 0) {
             B_CHECK(reduce_runs<double, CQ>(ctx, w64, q64, nullptr, B200FE_PROF_FINAL,
@@ -1818,7 +1811,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
             B_LAUNCHED();
             B_CHECK(sync_read_double(ctx, dot_res, CP, res2.data()));
         }
-        B_TRY(cudaStreamSynchronize(s));
+        B_CHECK(small_d2h(ctx, w64.colsq_partial, sizeof(double) * hp.size(), hp.data()));
         for (int b = 0; b < w64.nbins_ctas; ++b)
             for (int c = 0; c < CP; ++c) res2[c] += hp[static_cast<size_t>(b) * CP + c];
         const double opn = std::sqrt(static_cast<double>(st.D) * st.sum_w2);
@@ -1966,6 +1959,167 @@ int absorb_device_impl(b200fe_context* ctx, const double* d_v, int64_t n, int co
 }
 
 
+// Host arrays in and out with the copies overlapped: the ids (and weights)
+// go in first, then the columns in groups (two columns, then kPipeCols) on
+// the copy-in stream; the compute stream builds the FE structure as soon as
+// the ids are in and solves group after group on it, each group waiting for its own
+// columns; each group's within transform goes out on the copy-out stream as
+// soon as its solve is done, while later groups are still coming in (PCIe
+// copies in both directions at once).  Every group is solved to the same
+// tolerance as one batched call; results merge: iterations, rounds and
+// residuals as maxima over the groups, converged and certified only if every
+// group is, setup and solve times summed.
+constexpr int kPipeCols = 4;
+// Large copies are issued in pieces of this size: the solver's own small
+// device<->host reads share the copy engines with them, and a read queued
+// behind a whole gigabyte-sized copy would stall the compute stream until it
+// finished.
+constexpr size_t kCopyPiece = size_t(8) << 20;
+
+int copy_pieces(b200fe_context* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind,
+                cudaStream_t st) {
+    for (size_t o = 0; o < bytes; o += kCopyPiece)
+        B_TRY(cudaMemcpyAsync(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o,
+                              std::min(kCopyPiece, bytes - o), kind, st));
+    return B200FE_OK;
+}
+
+int absorb_host_pipelined(b200fe_context* ctx, const double* y, const double* X, int64_t n, int k,
+                          int num_dims, const int32_t* const* group_ids, const int32_t* G,
+                          const double* weights, const b200fe_options& o, double* y_out, double* X_out,
+                          b200fe_result* r) {
+    const cudaStream_t s = ctx->stream;
+    const int cols = k + 1;
+    for (cudaStream_t* cs : {&ctx->copy_in, &ctx->copy_out})
+        if (!*cs) B_TRY(cudaStreamCreateWithFlags(cs, cudaStreamNonBlocking));
+    const cudaStream_t sin = ctx->copy_in, sout = ctx->copy_out;
+    double *dv, *dout, *dw = nullptr;
+    B_CHECK(get_buf(ctx, "io_v", static_cast<size_t>(n) * cols, &dv));
+    B_CHECK(get_buf(ctx, "io_out", static_cast<size_t>(n) * cols, &dout));
+    int32_t* dg[B200FE_MAX_DIMS] = {nullptr};
+    for (int d = 0; d < num_dims; ++d) B_CHECK(get_buf(ctx, "io_g" + std::to_string(d), n, &dg[d]));
+    if (weights) B_CHECK(get_buf(ctx, "io_w", n, &dw));
+    B_TRY(cudaStreamSynchronize(s));  // buffers may have been reallocated
+    // column groups: a small first group (its output copies can start early),
+    // then groups of kPipeCols
+    std::vector<int> gb{0};
+    gb.push_back(std::min(cols, 2));
+    while (gb.back() < cols) gb.push_back(std::min(cols, gb.back() + kPipeCols));
+    const int ngroups = static_cast<int>(gb.size()) - 1;
+    std::vector<cudaEvent_t> ev_in(ngroups), ev_done(ngroups);
+    cudaEvent_t h0, h1, d0, d1;
+    for (auto* e : {&h0, &h1, &d0, &d1}) B_TRY(cudaEventCreate(e));
+    for (int g = 0; g < ngroups; ++g) {
+        B_TRY(cudaEventCreateWithFlags(&ev_in[g], cudaEventDisableTiming));
+        B_TRY(cudaEventCreateWithFlags(&ev_done[g], cudaEventDisableTiming));
+    }
+    auto host_col = [&](int c) { return c == 0 ? y : X + static_cast<int64_t>(c - 1) * n; };
+    auto out_col = [&](int c) { return c == 0 ? y_out : X_out + static_cast<int64_t>(c - 1) * n; };
+    // copies in: ids and weights, then the column groups
+    cudaEvent_t ev_ids;
+    B_TRY(cudaEventCreateWithFlags(&ev_ids, cudaEventDisableTiming));
+    B_TRY(cudaEventRecord(h0, sin));
+    for (int d = 0; d < num_dims; ++d)
+        B_CHECK(copy_pieces(ctx, dg[d], group_ids[d], sizeof(int32_t) * n, cudaMemcpyHostToDevice, sin));
+    if (weights) B_CHECK(copy_pieces(ctx, dw, weights, sizeof(double) * n, cudaMemcpyHostToDevice, sin));
+    B_TRY(cudaEventRecord(ev_ids, sin));
+    for (int g = 0; g < ngroups; ++g) {
+        const int c0 = gb[g], c1 = gb[g + 1];
+        for (int c = c0; c < c1; ++c)
+            B_CHECK(copy_pieces(ctx, dv + static_cast<int64_t>(c) * n, host_col(c), sizeof(double) * n,
+                                cudaMemcpyHostToDevice, sin));
+        B_TRY(cudaEventRecord(ev_in[g], sin));
+    }
+    B_TRY(cudaEventRecord(h1, sin));
+    // the FE structure as soon as the ids are in, while the columns arrive
+    int rc = B200FE_OK;
+    if (!(o.reuse_structure && ctx->st.valid && ctx->st.n == n && ctx->st.D == num_dims &&
+          ctx->st.weighted == (dw != nullptr)) && num_dims > 0) {
+        B_TRY(cudaStreamWaitEvent(s, ev_ids, 0));
+        cudaEvent_t e0, e1;
+        B_TRY(cudaEventCreate(&e0));
+        B_TRY(cudaEventCreate(&e1));
+        ctx->pass_kernel = o.pass_kernel == 3 ? 0 : o.pass_kernel;
+        ctx->sparse_schur = o.pass_kernel == 0;
+        B_TRY(cudaEventRecord(e0, s));
+        rc = build_structure(ctx, n, num_dims, dg, G, dw);
+        B_TRY(cudaEventRecord(e1, s));
+        B_TRY(cudaEventSynchronize(e1));
+        r->setup_ms = elapsed_ms(e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc != B200FE_OK) {
+            ctx->st.valid = false;
+            B_TRY(cudaStreamSynchronize(sin));
+            cudaEventDestroy(ev_ids);
+            return rc;
+        }
+    }
+    cudaEventDestroy(ev_ids);
+    bool first_out = true;
+    for (int g = 0; g < ngroups && (rc == B200FE_OK || rc == B200FE_NOT_CONVERGED); ++g) {
+        const int c0 = gb[g], c1 = gb[g + 1];
+        B_TRY(cudaStreamWaitEvent(s, ev_in[g], 0));
+        b200fe_options og = o;
+        og.reuse_structure = num_dims > 0 ? 1 : o.reuse_structure;
+        b200fe_result rg;
+        clear_result(&rg);
+        const int rcg = absorb_device_impl(ctx, dv + static_cast<int64_t>(c0) * n, n, c1 - c0, num_dims, dg, G,
+                                           dw, og, dout + static_cast<int64_t>(c0) * n, &rg);
+        if (rcg != B200FE_OK && rcg != B200FE_NOT_CONVERGED) {
+            rc = rcg;
+            break;
+        }
+        if (rcg == B200FE_NOT_CONVERGED) rc = rcg;
+        B_TRY(cudaEventRecord(ev_done[g], s));
+        B_TRY(cudaStreamWaitEvent(sout, ev_done[g], 0));
+        if (first_out) {
+            B_TRY(cudaEventRecord(d0, sout));
+            first_out = false;
+        }
+        for (int c = c0; c < c1; ++c)
+            B_CHECK(copy_pieces(ctx, out_col(c), dout + static_cast<int64_t>(c) * n, sizeof(double) * n,
+                                cudaMemcpyDeviceToHost, sout));
+        // merge
+        r->iterations = std::max(r->iterations, rg.iterations);
+        r->outer_iterations = std::max(r->outer_iterations, rg.outer_iterations);
+        r->converged = (g == 0 ? 1 : r->converged) && rg.converged;
+        r->precision_certified = (g == 0 ? 1 : r->precision_certified) && rg.precision_certified;
+        r->primary_dim = rg.primary_dim;
+        for (int d = 0; d < num_dims; ++d) r->num_levels_present[d] = rg.num_levels_present[d];
+        r->abs_residual = std::max(r->abs_residual, rg.abs_residual);
+        r->abs_residual_rel = std::max(r->abs_residual_rel, rg.abs_residual_rel);
+        r->rel_residual = std::max(r->rel_residual, rg.rel_residual);
+        r->setup_ms += rg.setup_ms;
+        r->solve_ms += rg.solve_ms;
+        r->warm_columns += rg.warm_columns;
+        for (int c = 0; c < B200FE_PROF_CATEGORIES; ++c) {
+            r->prof_ms[c] += rg.prof_ms[c];
+            r->prof_bytes[c] += rg.prof_bytes[c];
+            r->prof_launches[c] += rg.prof_launches[c];
+        }
+    }
+    B_TRY(cudaEventRecord(d1, sout));
+    const cudaError_t e1 = cudaStreamSynchronize(sout);
+    const cudaError_t e2 = cudaStreamSynchronize(sin);
+    if (e1 == cudaSuccess && e2 == cudaSuccess && !first_out) {
+        r->h2d_ms = elapsed_ms(h0, h1);
+        r->d2h_ms = elapsed_ms(d0, d1);
+    }
+    for (auto e : {h0, h1, d0, d1}) cudaEventDestroy(e);
+    for (int g = 0; g < ngroups; ++g) {
+        cudaEventDestroy(ev_in[g]);
+        cudaEventDestroy(ev_done[g]);
+    }
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = std::string("pipelined copies: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2);
+        return B200FE_CUDA_ERROR;
+    }
+    if (rc == B200FE_OK || rc == B200FE_NOT_CONVERGED) rc = r->converged ? B200FE_OK : B200FE_NOT_CONVERGED;
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2008,10 +2162,15 @@ int b200fe_context_create(int device, b200fe_context** out) {
     ctx->device = device;
     if (const char* g = std::getenv("B200FE_GRAPHS")) ctx->graphs = std::strcmp(g, "0") != 0;
     if (const char* g = std::getenv("B200FE_PERSISTENT")) ctx->persistent = std::strcmp(g, "0") != 0;
+    if (const char* g = std::getenv("B200FE_PIPELINE")) ctx->pipeline = std::strcmp(g, "0") != 0;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_pinned, 64 * sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_pinned_d, 64 * sizeof(double));
+    if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_xout, kXferOutBytes, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->h_xout_dev), ctx->h_xout, 0);
+    if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_xin, kXferInBytes, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->h_xin_dev), ctx->h_xin, 0);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -2034,8 +2193,15 @@ void b200fe_context_destroy(b200fe_context* ctx) {
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     for (auto& kv : ctx->graph_exec) cudaGraphExecDestroy(kv.second);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    for (cudaStream_t cs : {ctx->copy_in, ctx->copy_out})
+        if (cs) {
+            cudaStreamSynchronize(cs);
+            cudaStreamDestroy(cs);
+        }
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->h_pinned_d) cudaFreeHost(ctx->h_pinned_d);
+    if (ctx->h_xout) cudaFreeHost(ctx->h_xout);
+    if (ctx->h_xin) cudaFreeHost(ctx->h_xin);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     cudaGetLastError();
     delete ctx;
@@ -2135,6 +2301,13 @@ int b200fe_absorb_fe(b200fe_context* ctx, const double* y, const double* X, int6
     const cudaStream_t s = ctx->stream;
     const long long l0 = ctx->launches, c0 = ctx->lib_calls;
     const int cols = k + 1;
+    if (!fe_out && ctx->pipeline && cols > kPipeCols) {
+        rc = absorb_host_pipelined(ctx, y, X, n, k, num_dims, group_ids, num_groups, weights, o, y_out,
+                                   X_out, r);
+        r->kernel_launches = ctx->launches - l0;
+        r->library_calls = ctx->lib_calls - c0;
+        return r->status = rc;
+    }
     auto run = [&]() -> int {
         double *dv, *dout, *dw = nullptr;
         B_CHECK(get_buf(ctx, "io_v", static_cast<size_t>(n) * cols, &dv));

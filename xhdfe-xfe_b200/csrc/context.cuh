@@ -151,6 +151,13 @@ struct b200fe_context {
     long long lib_calls = 0;
     int* h_pinned = nullptr;     // small pinned scratch
     double* h_pinned_d = nullptr;
+    // mapped pinned staging of the small transfers (small_d2h / small_h2d):
+    // host pointer and the device's address of the same memory
+    char* h_xout = nullptr;
+    char* h_xout_dev = nullptr;
+    char* h_xin = nullptr;
+    char* h_xin_dev = nullptr;
+    size_t xin_pos = 0;
     // opt-in event profiler (b200fe_options.profile)
     struct ProfRec {
         cudaEvent_t a, b;
@@ -175,6 +182,10 @@ struct b200fe_context {
     // persistent PCG kernel over the explicit Schur block (one cooperative
     // launch per inner solve); off when B200FE_PERSISTENT=0 at context creation
     bool persistent = true;
+    // host-array calls copy column groups in and out on their own streams,
+    // overlapped with the solves of other groups; off when B200FE_PIPELINE=0
+    bool pipeline = true;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
     // learned warm start (b200fe_warmstart_set): packed network and mode bits
     // (1: start the refinement from its prediction, 2: scale the Jacobi
     // diagonal by its per-row factor); training-sample collection
@@ -344,20 +355,76 @@ inline int cub_sort_pairs(b200fe_context* ctx, const int32_t* keys_in, int32_t* 
     return B200FE_OK;
 }
 
-inline int sync_read_int(b200fe_context* ctx, const int32_t* dptr, int count, int* host) {
-    B_TRY(cudaMemcpyAsync(ctx->h_pinned, dptr, sizeof(int) * count, cudaMemcpyDeviceToHost,
-                          ctx->stream));
-    B_TRY(cudaStreamSynchronize(ctx->stream));
-    std::memcpy(host, ctx->h_pinned, sizeof(int) * count);
+// Small transfers between host and device that bypass the copy engines: a
+// kernel on the context's stream reads or writes the context's mapped pinned
+// staging memory.  A copy-engine transfer queues behind every large copy
+// already submitted in the same direction (on any stream), so a scalar read
+// back by the solver would wait for a gigabyte copy overlapped with it on
+// another stream; these do not.  Sizes are multiples of 4 bytes.
+constexpr size_t kXferOutBytes = size_t(1) << 20;
+constexpr size_t kXferInBytes = size_t(1) << 16;
+
+static __global__ void xfer_words_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                         int64_t nwords) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nwords;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = src[i];
+}
+
+inline int launch_xfer(b200fe_context* ctx, const void* src, void* dst, size_t bytes) {
+    const int64_t words = static_cast<int64_t>(bytes / 4);
+    const int grid = static_cast<int>(std::min<int64_t>((words + 255) / 256, 64));
+    xfer_words_kernel<<<std::max(grid, 1), 256, 0, ctx->stream>>>(static_cast<const uint32_t*>(src),
+                                                                   static_cast<uint32_t*>(dst), words);
+    ++ctx->launches;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        ctx->err = std::string("kernel launch: ") + cudaGetErrorString(e);
+        return B200FE_CUDA_ERROR;
+    }
     return B200FE_OK;
 }
 
-inline int sync_read_double(b200fe_context* ctx, const double* dptr, int count, double* host) {
-    B_TRY(cudaMemcpyAsync(ctx->h_pinned_d, dptr, sizeof(double) * count,
-                          cudaMemcpyDeviceToHost, ctx->stream));
+// device -> host, waits for the context's stream
+inline int small_d2h(b200fe_context* ctx, const void* dptr, size_t bytes, void* host) {
+    if (bytes == 0) return B200FE_OK;
+    if (!ctx->h_xout || bytes > kXferOutBytes || (bytes & 3)) {
+        B_TRY(cudaMemcpyAsync(host, dptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        B_TRY(cudaStreamSynchronize(ctx->stream));
+        return B200FE_OK;
+    }
+    B_CHECK(launch_xfer(ctx, dptr, ctx->h_xout_dev, bytes));
     B_TRY(cudaStreamSynchronize(ctx->stream));
-    std::memcpy(host, ctx->h_pinned_d, sizeof(double) * count);
+    std::memcpy(host, ctx->h_xout, bytes);
     return B200FE_OK;
+}
+
+// host -> device, stream-ordered; the host data is staged at once, so the
+// caller may reuse its buffer on return
+inline int small_h2d(b200fe_context* ctx, void* dptr, const void* host, size_t bytes) {
+    if (bytes == 0) return B200FE_OK;
+    if (!ctx->h_xin || bytes > kXferInBytes || (bytes & 3)) {
+        B_TRY(cudaMemcpyAsync(dptr, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        B_TRY(cudaStreamSynchronize(ctx->stream));
+        return B200FE_OK;
+    }
+    const size_t slot = (bytes + 255) & ~size_t(255);
+    if (ctx->xin_pos + slot > kXferInBytes) {  // earlier slots may still be read
+        B_TRY(cudaStreamSynchronize(ctx->stream));
+        ctx->xin_pos = 0;
+    }
+    std::memcpy(ctx->h_xin + ctx->xin_pos, host, bytes);
+    B_CHECK(launch_xfer(ctx, ctx->h_xin_dev + ctx->xin_pos, dptr, bytes));
+    ctx->xin_pos += slot;
+    return B200FE_OK;
+}
+
+inline int sync_read_int(b200fe_context* ctx, const int32_t* dptr, int count, int* host) {
+    return small_d2h(ctx, dptr, sizeof(int) * count, host);
+}
+
+inline int sync_read_double(b200fe_context* ctx, const double* dptr, int count, double* host) {
+    return small_d2h(ctx, dptr, sizeof(double) * count, host);
 }
 
 inline int check_common(b200fe_context* ctx, int64_t n, int cols, int num_dims, const int32_t* G) {
