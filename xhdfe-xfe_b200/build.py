@@ -13,7 +13,7 @@ CSRC = HERE / "csrc"
 SOURCES = ["b200fe.cu", "slopes.cu", "noalloc.cu", "kss.cu", "learned.cu"]
 HEADERS = ["limits.cuh", "context.cuh", "common_kernels.cuh", "kernels.cuh", "setup_kernels.cuh",
            "ols_kernels.cuh", "prep_kernels.cuh", "slope_kernels.cuh", "sparse_kernels.cuh",
-           "pcg_kernels.cuh", "mlp_kernels.cuh", "ws_kernels.cuh"]
+           "pcg_kernels.cuh", "mlp_kernels.cuh", "ws_kernels.cuh", "stream_kernels.cuh"]
 OUT = HERE / "libb200fe.so"
 OBJ_DIR = HERE / "_build"
 

@@ -13,6 +13,7 @@
 #include "sparse_kernels.cuh"
 #include "pcg_kernels.cuh"
 #include "ws_kernels.cuh"
+#include "stream_kernels.cuh"
 
 using namespace b200fe;
 using namespace b200fe_host;
@@ -94,6 +95,81 @@ int build_chunks(b200fe_context* ctx, const int32_t* grp_off, int32_t CH, const 
         }
         B_TRY(cudaStreamSynchronize(s));  // the host vectors leave scope
     }
+    return B200FE_OK;
+}
+
+// Records of the regular tiles for the bulk-copy data passes
+// (stream_kernels.cuh).  st.stream_ok stays false when a regular tile has
+// more observations or segments than a stage holds.
+int build_stream_meta(b200fe_context* ctx) {
+    Structure& st = ctx->st;
+    const cudaStream_t s = ctx->stream;
+    st.stream_ok = false;
+    st.stream_nreg = 0;
+    if (st.ntiles <= 0) return B200FE_OK;
+    int32_t *rflag, *ridx;
+    int* flags;
+    const size_t t1 = static_cast<size_t>(st.ntiles) + 1;
+    B_CHECK(get_buf(ctx, "tmp_tile_flag", t1, &rflag));
+    B_CHECK(get_buf(ctx, "tmp_tile_idx", t1, &ridx));
+    B_CHECK(get_buf(ctx, "stream_flags", 4, &flags));
+    B_TRY(cudaMemsetAsync(flags, 0, 4 * sizeof(int), s));
+    tile_regular_flag_kernel<<<grid_for(ctx, st.ntiles + 1, 256), 256, 0, s>>>(st.ntiles, st.tile_long, rflag);
+    B_LAUNCHED();
+    B_CHECK(cub_exclusive_sum(ctx, rflag, ridx, static_cast<int64_t>(t1)));
+    int nreg = 0;
+    B_CHECK(sync_read_int(ctx, ridx + st.ntiles, 1, &nreg));
+    st.stream_nreg = nreg;
+    if (nreg == 0) return B200FE_OK;
+    st.stream_aux_stride = stream_aux_stride(st.nL, st.SG, st.nS);
+    int32_t* bsize;
+    B_CHECK(get_buf(ctx, "stream_meta", 2 * static_cast<size_t>(nreg), &st.stream_meta));
+    B_CHECK(get_buf(ctx, "tmp_blob_size", static_cast<size_t>(nreg) + 1, &bsize));
+    B_CHECK(get_buf(ctx, "stream_boff", static_cast<size_t>(nreg) + 1, &st.stream_boff));
+    B_TRY(cudaMemsetAsync(bsize + nreg, 0, sizeof(int32_t), s));
+    TileMetaArgs m{};
+    m.ntiles = st.ntiles;
+    m.tile_seg = st.tile_seg;
+    m.tile_long = st.tile_long;
+    m.reg_idx = ridx;
+    m.seg_off = st.seg_off;
+    m.nL = st.nL;
+    m.nS = st.nS;
+    m.aux_stride = st.stream_aux_stride;
+    for (int l = 0; l < st.nL; ++l) m.run_base[l] = st.L[l].run_base;
+    m.tmeta = st.stream_meta;
+    m.bsize = bsize;
+    m.flags = flags;
+    tile_meta_kernel<<<grid_for(ctx, st.ntiles, 256), 256, 0, s>>>(m);
+    B_LAUNCHED();
+    B_CHECK(cub_exclusive_sum(ctx, bsize, st.stream_boff, static_cast<int64_t>(nreg) + 1));
+    int hf[2] = {0, 0}, units = 0;
+    B_CHECK(sync_read_int(ctx, flags, 2, hf));
+    B_CHECK(sync_read_int(ctx, st.stream_boff + nreg, 1, &units));
+    if (hf[0] != 0) return B200FE_OK;
+    st.stream_blob_max = hf[1];
+    B_CHECK(get_buf(ctx, "stream_blob", static_cast<size_t>(std::max(units, 1)) * 16, &st.stream_blob));
+    TileBlobArgs x{};
+    x.nreg = nreg;
+    x.tmeta = st.stream_meta;
+    x.boff = st.stream_boff;
+    x.seg_off = st.seg_off;
+    x.inv_wp = st.inv_wp;
+    x.nL = st.nL;
+    for (int l = 0; l < st.nL; ++l) {
+        x.run_base[l] = st.L[l].run_base;
+        x.run_start[l] = st.L[l].run_start;
+        x.run_dest[l] = st.L[l].run_dest;
+    }
+    x.run_grp0 = st.nL > 0 ? st.L[0].run_grp : nullptr;
+    x.sid = st.sid;
+    x.nS = st.nS;
+    for (int j = 0; j < st.nS; ++j) x.sG[j] = st.sG[j];
+    x.aux_stride = st.stream_aux_stride;
+    x.blob = st.stream_blob;
+    tile_blob_kernel<<<static_cast<int>((nreg + kBlobWarps - 1) / kBlobWarps), kBlobWarps * 32, 0, s>>>(x);
+    B_LAUNCHED();
+    st.stream_ok = true;
     return B200FE_OK;
 }
 
@@ -612,6 +688,8 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
     if (st.block_ok && ctx->sparse_schur && st.nL == 1 && (st.nS == 0 || st.coupled))
         B_CHECK(build_sparse_block(ctx));
 
+    B_CHECK(build_stream_meta(ctx));
+
     if (st.GR > 0) {
         B_CHECK(get_buf(ctx, "dinv64", st.GR, &st.dinv64));
         B_CHECK(get_buf(ctx, "dinv32", st.GR, &st.dinv32));
@@ -833,8 +911,93 @@ PassArgs<T> make_pass_args(const Structure& st, int cols, int CP, const Work<T>&
     return a;
 }
 
-// Data pass (FP64, lane = column) or tile pass over the regular tiles, then
-// the long segments (if any).  Partial slots beyond the launched grid are
+// Bulk-copy FP64 data pass over the regular tiles (stream_kernels.cuh): one
+// CTA per SM with as many stages as shared memory holds (at least two).
+// *grid = 0 (nothing launched) when it does not apply: the pass is off, the
+// observations are not in primary order, a tile exceeds the staged sizes, or
+// (kFinal) input and output differ in their offset from a 16-byte boundary.
+template <int MODE>
+int launch_stream_pass(b200fe_context* ctx, const PassArgs<double>& a, int* grid) {
+    const Structure& st = ctx->st;
+    *grid = 0;
+    if (!ctx->stream_pass || !st.stream_ok || a.pord || a.cols > 16 || a.CP > 16 || st.stream_nreg <= 0)
+        return B200FE_OK;
+    const uintptr_t pv = reinterpret_cast<uintptr_t>(a.v), po = reinterpret_cast<uintptr_t>(a.out);
+    if ((pv & 7u) || (MODE == kFinal && (((pv ^ po) & 15u) || (po & 7u)))) return B200FE_OK;
+    const bool weighted = a.wp != nullptr;
+    StreamLayout L{};
+    int off = kStreamHeader;
+    L.off_cols = off;
+    off += a.cols * kStreamPitchD * 8;
+    L.off_blob = off;
+    off += round16(st.stream_blob_max);
+    if (weighted) {
+        L.off_wp = off;
+        off += kStreamPitchD * 8;
+    }
+    if (MODE == kFinal && a.nS > 0) {
+        L.off_sid = off;
+        off += kStreamPitchI * 4;
+    }
+    for (int l = 0; l < a.nL && MODE == kFinal && a.nL > 1; ++l) {
+        L.off_rid[l] = off;
+        off += kStreamPitchI * 4;
+    }
+    L.stage_bytes = (off + 127) & ~127;
+    L.off_stages = 128;  // barriers and the abort flag
+    const int bins_bytes = std::max(a.SG, 1) * 16 * 8;
+    const int red_bytes = kStreamWarps * 16 * 8;
+    const int yt_bytes = (MODE == kFinal && a.nS > 0) ? a.SG * 16 * 8 : 0;
+    const int afb_bytes = (MODE == kFinal && a.nL == 1) ? kStreamWarps * kStreamRunRows * 16 * 8 : 0;
+    int budget = 0;
+    B_TRY(cudaDeviceGetAttribute(&budget, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const int ns = std::min(kStreamMaxStages, (budget - L.off_stages - bins_bytes - red_bytes - yt_bytes - afb_bytes) /
+                                                  L.stage_bytes);
+    if (ns < 2) return B200FE_OK;
+    L.NS = ns;
+    L.off_bins = L.off_stages + ns * L.stage_bytes;
+    L.off_red = L.off_bins + bins_bytes;
+    L.off_yt = L.off_red + red_bytes;
+    L.off_afb = L.off_yt + yt_bytes;
+    const int smem = L.off_afb + afb_bytes;
+    L.tmeta = st.stream_meta;
+    L.nreg = st.stream_nreg;
+    L.boff = st.stream_boff;
+    L.blob = st.stream_blob;
+    L.aux_stride = st.stream_aux_stride;
+    if (!ctx->stream_status) {
+        B_CHECK(get_buf(ctx, "stream_status", 4, &ctx->stream_status));
+        B_TRY(cudaMemsetAsync(ctx->stream_status, 0, 4 * sizeof(int), ctx->stream));
+    }
+    L.status = ctx->stream_status;
+    auto kern = weighted ? stream_pass_kernel<MODE, true> : stream_pass_kernel<MODE, false>;
+    const unsigned bit = 1u << (2 * (MODE == kFinal ? 1 : 0) + (weighted ? 1 : 0));
+    if (!(ctx->stream_smem_set & bit)) {
+        B_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+        ctx->stream_smem_set |= bit;
+    }
+    const int g = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(st.stream_nreg, ctx->num_sms)));
+    kern<<<g, kStreamThreads, smem, ctx->stream>>>(a, L);
+    B_LAUNCHED();
+    *grid = g;
+    return B200FE_OK;
+}
+
+// Reports a bulk-copy data pass whose pipeline wait ran out (and clears it).
+int check_stream_status(b200fe_context* ctx) {
+    if (!ctx->stream_status) return B200FE_OK;
+    int hs = 0;
+    B_CHECK(sync_read_int(ctx, ctx->stream_status, 1, &hs));
+    if (hs != 0) {
+        B_TRY(cudaMemsetAsync(ctx->stream_status, 0, sizeof(int), ctx->stream));
+        ctx->err = "FP64 data pass: a pipeline wait timed out";
+        return B200FE_CUDA_ERROR;
+    }
+    return B200FE_OK;
+}
+
+// Data pass (FP64: bulk-copy stream pass, else lane = column) or tile pass
+// over the regular tiles, then the long segments (if any).  Partial slots beyond the launched grid are
 // zeroed so finalize and the host sum a fixed number of slots.
 template <typename T, int CQ, int MODE>
 int launch_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a) {
@@ -844,13 +1007,17 @@ int launch_pass(b200fe_context* ctx, const Work<T>& wk, PassArgs<T> a) {
     int used;
     a.bins_cta0 = 0;
     if constexpr (std::is_same<T, double>::value && MODE != kMatvec) {
-        data_pass_kernel<CP, MODE><<<wk.data_grid, kDataThreads, wk.data_smem, ctx->stream>>>(a);
-        used = wk.data_grid;
+        B_CHECK(launch_stream_pass<MODE>(ctx, a, &used));
+        if (used == 0) {
+            data_pass_kernel<CP, MODE><<<wk.data_grid, kDataThreads, wk.data_smem, ctx->stream>>>(a);
+            B_LAUNCHED();
+            used = wk.data_grid;
+        }
     } else {
         tile_pass_kernel<T, CQ, MODE><<<wk.tile_grid, kTileThreads, wk.tile_smem, ctx->stream>>>(a);
+        B_LAUNCHED();
         used = wk.tile_grid;
     }
-    B_LAUNCHED();
     if (used < slots) {
         if (st.nS > 0)
             B_TRY(cudaMemsetAsync(wk.bins_partial + static_cast<int64_t>(used) * st.SG * CP, 0,
@@ -1799,6 +1966,7 @@ int solve_block(b200fe_context* ctx, const double* d_v, int cols, double* d_out,
                          (cert ? runs_write_bytes(st, CP, 8) : 0.0));
         B_CHECK((launch_pass<double, CQ, kFinal>(ctx, w64, a)));
     }
+    B_CHECK(check_stream_status(ctx));
     double abs_res = 0.0, abs_rel = 0.0;
     if (cert) {
         std::vector<double> hp(static_cast<size_t>(w64.nbins_ctas) * CP);
@@ -2163,6 +2331,7 @@ int b200fe_context_create(int device, b200fe_context** out) {
     if (const char* g = std::getenv("B200FE_GRAPHS")) ctx->graphs = std::strcmp(g, "0") != 0;
     if (const char* g = std::getenv("B200FE_PERSISTENT")) ctx->persistent = std::strcmp(g, "0") != 0;
     if (const char* g = std::getenv("B200FE_PIPELINE")) ctx->pipeline = std::strcmp(g, "0") != 0;
+    if (const char* g = std::getenv("B200FE_STREAM")) ctx->stream_pass = std::strcmp(g, "0") != 0;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_pinned, 64 * sizeof(int));

@@ -124,6 +124,15 @@ struct Structure {
     int4* pc_lchunk_meta = nullptr;    // {row, begin, end, first} of the long-row chunks
     int64_t pc_nhuge = 0;
     int32_t* pc_huge_li = nullptr;
+    // records of the regular tiles for the bulk-copy data passes
+    // (stream_kernels.cuh); stream_ok when every one fits the staged sizes
+    bool stream_ok = false;
+    int64_t stream_nreg = 0;
+    int4* stream_meta = nullptr;
+    int32_t* stream_boff = nullptr;        // [nreg + 1] record offsets (16-byte units)
+    unsigned char* stream_blob = nullptr;  // the records (stream_kernels.cuh: tile_blob_kernel)
+    int stream_blob_max = 0;               // largest record (bytes)
+    int stream_aux_stride = 0;
 };
 
 constexpr int32_t kChunkRuns = 64;
@@ -186,6 +195,13 @@ struct b200fe_context {
     // overlapped with the solves of other groups; off when B200FE_PIPELINE=0
     bool pipeline = true;
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    // FP64 data passes fed by bulk copies (stream_kernels.cuh); off when
+    // B200FE_STREAM=0 at context creation.  stream_status is set by a pass
+    // whose pipeline wait ran out; stream_smem_set marks the kernels whose
+    // shared-memory limit was raised
+    bool stream_pass = true;
+    int* stream_status = nullptr;
+    unsigned stream_smem_set = 0;
     // learned warm start (b200fe_warmstart_set): packed network and mode bits
     // (1: start the refinement from its prediction, 2: scale the Jacobi
     // diagonal by its per-row factor); training-sample collection

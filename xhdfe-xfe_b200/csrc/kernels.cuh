@@ -868,7 +868,7 @@ data_pass_kernel(const PassArgs<double> a) {
     // shared memory, so those loads are in flight while the current tile is
     // worked on.  Thread tid holds observations tid and tid + kDataThreads of
     // a tile and run table entries tid + u * kDataThreads, u < 3.
-    static_assert(kTileObs == 2 * kDataThreads, "two observations per thread");
+    static_assert(kTileObs <= 2 * kDataThreads, "at most two observations per thread");
     struct Meta {
         int32_t s0, s1;
         int64_t k0;

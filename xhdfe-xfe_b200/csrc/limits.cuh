@@ -12,8 +12,8 @@ constexpr int kMaxSmallRows = 128; // total levels over all small dims
 constexpr int kPassThreads = 128;  // long-segment pass CTA size (4 warps)
 constexpr int kTileThreads = 256;  // tile pass CTA size (8 warps)
 constexpr int kRowThreads = 256;   // alpha-space row kernels
-constexpr int kTileObs = 512;      // observations staged per tile
-constexpr int kTileStride = 384;   // tiles start within windows of this many obs
+constexpr int kTileObs = 448;      // observations staged per tile
+constexpr int kTileStride = 320;   // tiles start within windows of this many obs
 constexpr int kLongSeg = kTileObs - kTileStride;  // longer segments take the long path
 
 }  // namespace b200fe
