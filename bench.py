@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip the reference's own CUDA backend leg (kss workload)")
     ap.add_argument("--no-learned", action="store_true",
                     help="do not install the shipped learned warm start (xhdfe-xfe_b200/warmstart_mlp.npz)")
     ap.add_argument("--learned-mode", type=int, default=0,
@@ -931,6 +933,23 @@ def run_kss(args):
             its_all.append(its)
         times.append(time.perf_counter() - t0)
     clocks = sampler.stop()
+    # the JLA leverages on the device: 200 draws (600 solves) of the same
+    # system, host arrays in and out (b200fe_kss_jla)
+    cnt_i = cnt.astype(np.int64)
+    sw = np.sqrt(cnt)
+    npy = float(cnt.sum())
+    solver.jla(mw, mf, cnt_i, npy, row_sw=sw, seed=20260705, draws=21, block=21, tol=1e-10, max_iter=20_000)
+    jla_times = []
+    for _ in range(max(1, min(args.steps, 2))):
+        t0 = time.perf_counter()
+        jo = solver.jla(mw, mf, cnt_i, npy, row_sw=sw, seed=20260705, draws=KSS_RHS, block=21, tol=1e-10,
+                        max_iter=20_000)
+        jla_times.append(time.perf_counter() - t0)
+    jla = {"value": statistics.median(jla_times), "unit": UNIT, "draws": KSS_RHS, "solves": 3 * KSS_RHS,
+           "draws_per_batch": 21, "failed_lanes": jo["failed_lanes"], "pcg_iterations": jo["iterations"],
+           "mean_pii": float(jo["pii"].mean()), "max_pii": float(jo["pii"].max()),
+           "kind": "b200fe_kss_jla: the reference's JLA draw loop (SplitMix64 streams, scatters, "
+                   "3 solves per draw, per-row sums, ratio estimator) on the device, host arrays in and out"}
     solver.close()
     v = statistics.median(times)
     its_all = np.concatenate(its_all)
@@ -948,7 +967,7 @@ def run_kss(args):
                 f"{KSS_RHS} draws) on this library through its binding, host arrays",
                 "gpu_used": r["gpu_used"], "solver_iterations": r["solver_iterations"],
                 "kss": r["kss"]}
-    if not args.no_reference_gpu and oracle.REF_CUDA_SO.exists():
+    if not args.no_reference_gpu and not args.no_reference_cuda and oracle.REF_CUDA_SO.exists():
         dt, r = ref_decompose(p, oracle.REF_CUDA_SO, True)
         ref_gpu = {"value": dt, "unit": UNIT, "kind": "the same decomposition on the reference's "
                    "own CUDA backend built for sm_100a", "gpu_used": r["gpu_used"],
@@ -970,7 +989,7 @@ def run_kss(args):
                      "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                      "peak_kind": peak_kind, "bytes_per_step": bytes_per_step,
                      "traffic": None},
-        "clocks": clocks, "dropin_decomposition": drop, "reference_gpu": ref_gpu,
+        "clocks": clocks, "device_jla": jla, "dropin_decomposition": drop, "reference_gpu": ref_gpu,
         "cpu_baseline": cpu,
         "e2e": {"value": v, "unit": UNIT,
                 "h2d_bytes_per_step": int(KSS_RHS * J * 8), "d2h_bytes_per_step": int(KSS_RHS * J * 8)}}))

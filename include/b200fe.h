@@ -476,6 +476,29 @@ int b200fe_kss_solve_multi(b200fe_kss* kss, const double* rhs_pack, double* z_pa
  * Replaces akm_cuda_solve_S (akm_kss_cuda.hpp:40-44, src/akm_kss_cuda.cu:655-700). */
 int b200fe_kss_solve(b200fe_kss* kss, const double* rhs, double* z, double tol,
                      int max_iter, int* iterations);
+/* JLA leverages of the leave-out decomposition for `draws` Rademacher draws,
+ * on the device: per draw d, working row r gets the sign bit r % 64 of the
+ * SplitMix64 stream (seed, 3d, r / 64), match m the sum of m_cnt[m] signs of
+ * the stream (seed, 3d + 1, m); the worker/firm scatters of row_sw[r] * sign
+ * (row_sw NULL: 1) and of the centred match sums solve K z = (tw1, tf1),
+ * (0, tf2), (tw2, 0) in batches of `block` draws (three lanes each; 0: 8),
+ * and every row accumulates, in ascending draw order, the sums of the
+ * ratio estimator and its nonlinearity correction.  Rows are given by
+ * their worker row_w and firm row_f (0-based, the context's numbering) in
+ * the caller's row order, which indexes the streams; m_cnt[M] are the
+ * person-year counts of the matches, n_py their total.  Outputs (host, R
+ * each, any may be NULL): pii, mii (ratio estimates), corr (nonlinearity
+ * correction), bfe, bpe, bcov (sums over draws of W2^2, W1^2, W1 W2).  The
+ * solves stop as b200fe_kss_solve_multi (tol, max_iter); *failed_lanes
+ * counts lanes that did not converge (B200FE_NOT_CONVERGED when > 0) and
+ * *iterations sums the others' iterations.
+ * Replaces the JLA draw loop of hdfe::akm::akm_kss_decompose
+ * (src/akm_kss.cpp:2753-3160, the ratio estimator :3275-3289), whose solves
+ * go through akm_cuda_solve_S_multi. */
+int b200fe_kss_jla(b200fe_kss* kss, int64_t n_rows, const int32_t* row_w, const int32_t* row_f,
+                   const double* row_sw, const int64_t* m_cnt, double n_py, uint64_t seed, int draws,
+                   int block, double tol, int max_iter, double* pii, double* mii, double* corr,
+                   double* bfe, double* bpe, double* bcov, int* failed_lanes, long long* iterations);
 /* Stable ascending sort of host uint64 keys: order_out[i] is the input row of
  * the i-th smallest key, equal keys in input order.
  * Replaces akm_cuda_stable_sort_u64 (akm_kss_cuda.hpp:21-28). */

@@ -367,6 +367,38 @@ def ref_akm_kss(y, worker, firm, *, leverages="auto", jla_draws=0, seed=20260705
             "solver_iterations": int(iters.value)}
 
 
+def ref_akm_kss_rows(y, worker, firm, *, leverages="jla", jla_draws=0, seed=20260705, cg_tol=1e-10,
+                     direct_max_firms=-1, threads=0, cg_max_iter=0, lib_path=REF_SO):
+    """The working rows of the reference's akm_kss_decompose
+    (include/hdfe/akm_kss.hpp:120-124, 227-233), in its row order: pii,
+    original worker and firm ids, person-year weight."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    w = np.ascontiguousarray(worker, dtype=np.int32)
+    f = np.ascontiguousarray(firm, dtype=np.int32)
+    opts = np.array([LEVERAGE[leverages], jla_draws, direct_max_firms, 0, threads, cg_max_iter],
+                    dtype=np.int32)
+    cap = len(y)
+    pii = np.zeros(cap)
+    rw = np.zeros(cap, dtype=np.int32)
+    rf = np.zeros(cap, dtype=np.int32)
+    wt = np.zeros(cap)
+    nr = ctypes.c_int64(0)
+    err = ctypes.create_string_buffer(512)
+    lib = rlib(lib_path)
+    lib.xref_akm_kss_rows.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_void_p, ctypes.c_uint64,
+                                      ctypes.c_double, ctypes.c_int64] + [ctypes.c_void_p] * 5 + \
+        [ctypes.c_char_p, ctypes.c_int]
+    lib.xref_akm_kss_rows.restype = ctypes.c_int
+    rc = lib.xref_akm_kss_rows(y.ctypes.data, w.ctypes.data, f.ctypes.data, len(y), opts.ctypes.data, seed,
+                               cg_tol, cap, pii.ctypes.data, rw.ctypes.data, rf.ctypes.data, wt.ctypes.data,
+                               ctypes.byref(nr), err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    R = nr.value
+    return {"pii": pii[:R].copy(), "row_worker": rw[:R].copy(), "row_firm": rf[:R].copy(),
+            "row_weight": wt[:R].copy()}
+
+
 def ref_recover_fe(partial, fes, weights=None, *, tol=1e-8, fe_tolerance=0.0, threads=1,
                    gpu_backend="default", lib_path=REF_SO):
     """The reference's recover_fixed_effects (include/fe_absorption.hpp:127-130):

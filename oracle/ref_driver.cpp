@@ -348,6 +348,55 @@ int xref_fit(const double* y, const double* X, int64_t n, int k,
     }
 }
 
+// The same decomposition, returning its working rows: *n_rows rows (at most
+// cap) with their leverage pii, original worker and firm ids and person-year
+// weight, in the library's row order (hdfe::akm::AkmKssResult::pii,
+// row_worker, row_firm, row_weight; include/hdfe/akm_kss.hpp:120-124).
+int xref_akm_kss_rows(const double* y, const int32_t* worker, const int32_t* firm, int64_t n,
+                      const int* opts, uint64_t seed, double cg_tol, int64_t cap, double* pii,
+                      int32_t* row_worker, int32_t* row_firm, double* row_weight, int64_t* n_rows,
+                      char* err, int err_len) {
+    try {
+        const VectorXd yv = Map<const VectorXd>(y, n);
+        VectorXi wv(n), fv(n);
+        for (int64_t i = 0; i < n; ++i) {
+            wv[i] = worker[i];
+            fv[i] = firm[i];
+        }
+        hdfe::akm::AkmOptions o;
+        o.leverage_method = opts[0] == 1   ? hdfe::akm::LeverageMethod::Exact
+                            : opts[0] == 2 ? hdfe::akm::LeverageMethod::Jla
+                                           : hdfe::akm::LeverageMethod::Auto;
+        if (opts[1] > 0) o.jla_draws = opts[1];
+        if (opts[2] >= 0) o.direct_max_firms = opts[2];
+        o.use_gpu = opts[3] != 0;
+        o.num_threads = opts[4];
+        o.cg_max_iter = opts[5];
+        o.seed = seed;
+        if (cg_tol > 0.0) o.cg_tol = cg_tol;
+        const hdfe::akm::AkmKssResult r = hdfe::akm::akm_kss_decompose(yv, wv, fv, nullptr, o);
+        const int64_t R = static_cast<int64_t>(r.pii.size());
+        *n_rows = R;
+        if (R > cap) {
+            set_err(err, err_len, "row buffers too small");
+            return 1;
+        }
+        for (int64_t k = 0; k < R; ++k) {
+            pii[k] = r.pii[k];
+            row_worker[k] = r.row_worker[k];
+            row_firm[k] = r.row_firm[k];
+            row_weight[k] = r.row_weight[k];
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, err_len, e.what());
+        return 1;
+    } catch (...) {
+        set_err(err, err_len, "unknown exception");
+        return 1;
+    }
+}
+
 // AKM + leave-out decomposition.  opts (ints): [0] leverage method (0 auto,
 // 1 exact, 2 jla), [1] jla_draws, [2] direct_max_firms (-1: library default),
 // [3] use_gpu, [4] num_threads, [5] cg_max_iter; seed and cg_tol as given.

@@ -57,6 +57,7 @@ EXPORTED_SYMBOLS = (
     "b200fe_kss_pack_buffer",
     "b200fe_kss_solve_multi",
     "b200fe_kss_solve",
+    "b200fe_kss_jla",
     "b200fe_stable_sort_u64",
     "b200fe_mlp_num_params",
     "b200fe_mlp_forward",
@@ -224,6 +225,10 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.b200fe_kss_solve_multi.restype = c_int
     lib.b200fe_kss_solve.argtypes = [vp, vp, vp, ctypes.c_double, c_int, ctypes.POINTER(c_int)]
     lib.b200fe_kss_solve.restype = c_int
+    lib.b200fe_kss_jla.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp, ctypes.c_double, ctypes.c_uint64, c_int,
+                                   c_int, ctypes.c_double, c_int, vp, vp, vp, vp, vp, vp,
+                                   ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_longlong)]
+    lib.b200fe_kss_jla.restype = c_int
     lib.b200fe_stable_sort_u64.argtypes = [vp, vp, i64]
     lib.b200fe_stable_sort_u64.restype = c_int
     lib.b200fe_mlp_num_params.argtypes = []

@@ -410,6 +410,281 @@ int lane_pitch(int nb) {
     return lw;
 }
 
+// ---------------------------------------------------------------------------
+// JLA leverages (b200fe_kss_jla).  Per draw d the reference's driver
+// (src/akm_kss.cpp:2753-3160) draws one Rademacher sign per working row from
+// the SplitMix64 stream (seed, 3d, row block of 64), scatters sqrt(c_r) g_r
+// into worker and firm right-hand sides (tw1, tf1), draws per match the sum
+// of cnt_m signs from the stream (seed, 3d + 1, m) and scatters its centred
+// value su_m into (tw2, tf2), and solves K z = (tw1, tf1), (0, tf2) and
+// (tw2, 0).  Per row it then accumulates, in ascending draw order,
+//     Z = sqrt(c_r)(zw[w] + zf[f]), diff = g - Z:
+//     Pacc += Z^2/p, Psq += Z^4/p, Macc += diff^2/p, Msq += diff^4/p,
+//     PM += Z^2 diff^2/p, and Bfe += W2^2, Bpe += W1^2, Bcov += W1 W2
+// with W2, W1 the same products of the (0, tf2) and (tw2, 0) solutions.  Here
+// all of it runs on the device, a block of draws (three lanes each) per
+// batched solve; the streams are the reference's bit for bit.
+// ---------------------------------------------------------------------------
+
+// SplitMix64 (Steele, Lea and Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014), the generator the reference's streams use.
+__device__ __forceinline__ uint64_t jla_mix(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+// The reference's stream of (draw tag, unit): src/akm_kss.cpp:218-222.
+__device__ __forceinline__ uint64_t jla_stream(uint64_t seed, uint64_t tag, uint64_t unit) {
+    const uint64_t s = jla_mix(seed ^ (0xA24BAED4963EE407ULL * (tag + 1)));
+    return jla_mix(s ^ (0x9FB21C651E98DF25ULL * (unit + 1)));
+}
+__device__ __forceinline__ double jla_sign(const uint64_t* words, int64_t r) {
+    return ((words[r >> 6] >> (r & 63)) & 1ULL) ? 1.0 : -1.0;
+}
+
+// words[b][blk]: the sign words of draw d0 + b
+__global__ void jla_bits_kernel(uint64_t seed, int d0, int B, int64_t nblk, uint64_t* __restrict__ words) {
+    const int64_t total = static_cast<int64_t>(B) * nblk;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int b = static_cast<int>(e / nblk);
+        const int64_t blk = e - static_cast<int64_t>(b) * nblk;
+        words[e] = jla_stream(seed, 3ULL * static_cast<uint64_t>(d0 + b), static_cast<uint64_t>(blk));
+    }
+}
+
+// su[b][m] = sum of cnt_m signs of the stream (seed, 3d + 1, m), 64 per state
+// advance (src/akm_kss.cpp:224-238); tot[b] += that sum (integers: exact in
+// any order)
+__global__ void jla_msum_kernel(uint64_t seed, int d0, int B, int64_t M, const int64_t* __restrict__ cnt,
+                                double* __restrict__ su, unsigned long long* __restrict__ tot) {
+    const int64_t total = static_cast<int64_t>(B) * M;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int b = static_cast<int>(e / M);
+        const int64_t m = e - static_cast<int64_t>(b) * M;
+        uint64_t st = jla_stream(seed, 3ULL * static_cast<uint64_t>(d0 + b) + 1ULL, static_cast<uint64_t>(m));
+        long long acc = 0;
+        for (long long rem = cnt[m]; rem > 0;) {
+            st = jla_mix(st);
+            const int k = rem >= 64 ? 64 : static_cast<int>(rem);
+            const uint64_t bits = k == 64 ? st : (st & ((1ULL << k) - 1ULL));
+            acc += 2LL * __popcll(bits) - k;
+            rem -= k;
+        }
+        su[e] = static_cast<double>(acc);
+        atomicAdd(tot + b, static_cast<unsigned long long>(acc));
+    }
+}
+
+// su[b][m] = msum * scale - vbar_b cnt_m, vbar_b = (tot_b / n_py) scale
+__global__ void jla_su_kernel(int B, int64_t M, const int64_t* __restrict__ cnt,
+                              const unsigned long long* __restrict__ tot, double n_py, double scale,
+                              double* __restrict__ su) {
+    const int64_t total = static_cast<int64_t>(B) * M;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int b = static_cast<int>(e / M);
+        const int64_t m = e - static_cast<int64_t>(b) * M;
+        const double vbar = (static_cast<double>(static_cast<long long>(tot[b])) / n_py) * scale;
+        su[e] = su[e] * scale - vbar * static_cast<double>(cnt[m]);
+    }
+}
+
+// xw[w][l] = tw[w][l] / Dw[w]: lanes [0,B) the rows' signed weights, [B,2B)
+// zero, [2B,3B) su of the worker's matches; padding lanes zero
+__global__ void jla_tw_kernel(int N, int LW, int B, const int64_t* __restrict__ rw_ptr,
+                              const int32_t* __restrict__ rw_rows, const double* __restrict__ row_sw,
+                              const uint64_t* __restrict__ words, int64_t nblk, const int64_t* __restrict__ w_ptr,
+                              const double* __restrict__ su, int64_t M, const double* __restrict__ Dw,
+                              double* __restrict__ xw) {
+    const int64_t total = static_cast<int64_t>(N) * LW;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t w = e / LW;
+        const int l = static_cast<int>(e - w * LW);
+        double acc = 0.0;
+        if (l < B) {
+            const uint64_t* wd = words + static_cast<int64_t>(l) * nblk;
+            for (int64_t a = rw_ptr[w]; a < rw_ptr[w + 1]; ++a) {
+                const int64_t r = rw_rows[a];
+                acc += (row_sw ? row_sw[r] : 1.0) * jla_sign(wd, r);
+            }
+        } else if (l >= 2 * B && l < 3 * B) {
+            const double* sb = su + static_cast<int64_t>(l - 2 * B) * M;
+            for (int64_t a = w_ptr[w]; a < w_ptr[w + 1]; ++a) acc += sb[a];
+        }
+        xw[e] = acc / Dw[w];
+    }
+}
+
+// Firm-side scatters cut into chunks of at most kJlaChunk entries (a firm
+// with a large share of the rows is summed by many threads), the chunk
+// partials then added per firm in chunk order.
+constexpr int kJlaChunk = 256;
+
+__global__ void jla_chunk_count_kernel(int nseg, const int64_t* __restrict__ ptr, int32_t* __restrict__ count) {
+    for (int64_t sg = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; sg <= nseg;
+         sg += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        count[sg] = sg < nseg ? static_cast<int32_t>((ptr[sg + 1] - ptr[sg] + kJlaChunk - 1) / kJlaChunk) : 0;
+}
+
+__global__ void jla_chunk_fill_kernel(int nseg, const int64_t* __restrict__ ptr, const int32_t* __restrict__ first,
+                                      int64_t* __restrict__ cbeg) {
+    for (int64_t sg = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; sg < nseg;
+         sg += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t k0 = first[sg], k1 = first[sg + 1];
+        for (int32_t k = k0; k < k1; ++k) cbeg[k] = ptr[sg] + static_cast<int64_t>(k - k0) * kJlaChunk;
+    }
+}
+
+// part[k][l], l in [0, B): the signed row weights of chunk k (rows: idx),
+// or (su != null) the sums su[l][idx[a]] of chunk k
+__global__ void jla_chunk_sum_kernel(int64_t nchunks, int LW, int B, const int64_t* __restrict__ cbeg,
+                                     const int32_t* __restrict__ first, int nseg,
+                                     const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx32,
+                                     const int64_t* __restrict__ idx64, const double* __restrict__ row_sw,
+                                     const uint64_t* __restrict__ words, int64_t nblk, const double* __restrict__ su,
+                                     int64_t M, double* __restrict__ part) {
+    const int64_t total = nchunks * B;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t k = e / B;
+        const int l = static_cast<int>(e - k * B);
+        // end of the chunk: the next chunk's start, or the end of its segment
+        int lo = 0, hi = nseg;  // segment of chunk k: last sg with first[sg] <= k
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (first[mid] <= k) lo = mid;
+            else hi = mid;
+        }
+        const int64_t a0 = cbeg[k];
+        const int64_t a1 = min(a0 + kJlaChunk, ptr[lo + 1]);
+        double acc = 0.0;
+        if (su) {
+            const double* sb = su + static_cast<int64_t>(l) * M;
+            for (int64_t a = a0; a < a1; ++a) acc += sb[idx64[a]];
+        } else {
+            const uint64_t* wd = words + static_cast<int64_t>(l) * nblk;
+            for (int64_t a = a0; a < a1; ++a) {
+                const int64_t r = idx32[a];
+                acc += (row_sw ? row_sw[r] : 1.0) * jla_sign(wd, r);
+            }
+        }
+        part[k * LW + l] = acc;
+    }
+}
+
+// out[sg][l0 + l] = sum of the chunk partials of segment sg, in chunk order
+__global__ void jla_chunk_combine_kernel(int nseg, int LW, int B, int l0, const int32_t* __restrict__ first,
+                                         const double* __restrict__ part, double* __restrict__ out) {
+    const int64_t total = static_cast<int64_t>(nseg) * B;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t sg = e / B;
+        const int l = static_cast<int>(e - sg * B);
+        double acc = 0.0;
+        for (int32_t k = first[sg]; k < first[sg + 1]; ++k) acc += part[static_cast<int64_t>(k) * LW + l];
+        out[sg * LW + l0 + l] = acc;
+    }
+}
+
+// lane-major stage [nl][J] = tf - B' xw (Ap holds -B' xw; ground entries zero)
+__global__ void jla_rhs_kernel(int64_t J, int LW, int nl, int ground, const double* __restrict__ tf,
+                               const double* __restrict__ Ap, double* __restrict__ stage) {
+    const int64_t total = J * nl;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int l = static_cast<int>(e / J);
+        const int64_t f = e - static_cast<int64_t>(l) * J;
+        stage[e] = f == ground ? 0.0 : tf[f * LW + l] + Ap[f * LW + l];
+    }
+}
+
+__global__ void jla_sub_kernel(int64_t total, const double* __restrict__ t, double* __restrict__ xw) {
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        xw[e] -= t[e];
+}
+
+// per row, ascending draw: the eight sums acc[k][r]
+__global__ void jla_accum_kernel(int64_t R, int LW, int B, const int32_t* __restrict__ row_w,
+                                 const int32_t* __restrict__ row_f, const double* __restrict__ row_sw,
+                                 const uint64_t* __restrict__ words, int64_t nblk, const double* __restrict__ zw,
+                                 const double* __restrict__ zf, double pd, double* __restrict__ acc) {
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < R;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t w = row_w[r], f = row_f[r];
+        const double sw = row_sw ? row_sw[r] : 1.0;
+        double pa = acc[r], ps = acc[R + r], ma = acc[2 * R + r], ms = acc[3 * R + r], pm = acc[4 * R + r];
+        double bfe = acc[5 * R + r], bpe = acc[6 * R + r], bcov = acc[7 * R + r];
+        for (int b = 0; b < B; ++b) {
+            const double Z = sw * (zw[w * LW + b] + zf[f * LW + b]);
+            const double g = jla_sign(words + static_cast<int64_t>(b) * nblk, r);
+            const double diff = g - Z;
+            const double z2 = Z * Z;
+            const double m2 = diff * diff;
+            pa += z2 / pd;
+            ps += z2 * z2 / pd;
+            ma += m2 / pd;
+            ms += m2 * m2 / pd;
+            pm += z2 * m2 / pd;
+        }
+        for (int b = 0; b < B; ++b) {
+            const double W2 = sw * (zw[w * LW + B + b] + zf[f * LW + B + b]);
+            const double W1 = sw * (zw[w * LW + 2 * B + b] + zf[f * LW + 2 * B + b]);
+            bfe += W2 * W2;
+            bpe += W1 * W1;
+            bcov += W1 * W2;
+        }
+        acc[r] = pa;
+        acc[R + r] = ps;
+        acc[2 * R + r] = ma;
+        acc[3 * R + r] = ms;
+        acc[4 * R + r] = pm;
+        acc[5 * R + r] = bfe;
+        acc[6 * R + r] = bpe;
+        acc[7 * R + r] = bcov;
+    }
+}
+
+// ratio estimator and nonlinearity correction (src/akm_kss.cpp:3275-3289)
+__global__ void jla_final_kernel(int64_t R, double pd, const double* __restrict__ acc, double* __restrict__ out) {
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < R;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double Pa = acc[r], Ps = acc[R + r], Ma = acc[2 * R + r], Ms = acc[3 * R + r], PM = acc[4 * R + r];
+        const double denom = Pa + Ma;
+        const double Ph = denom > 0.0 ? Pa / denom : 0.0;
+        const double Mh = 1.0 - Ph;
+        double corr = 0.0;
+        if (Mh > 0.0) {
+            const double Vi = (Mh * Mh * Ps + Ph * Ph * Ms - 2.0 * Mh * Ph * PM) / pd;
+            const double Bi = (Mh * Ps - Ph * Ms + 2.0 * (Mh - Ph) * PM) / pd;
+            corr = 1.0 - Vi / (Mh * Mh) + Bi / Mh;
+        }
+        out[r] = Ph;
+        out[R + r] = Mh;
+        out[2 * R + r] = corr;
+    }
+}
+
+// CSR offsets of sorted keys: ptr[k] = first position with key >= k
+__global__ void jla_ptr_kernel(int64_t R, int nkeys, const int32_t* __restrict__ keys, int64_t* __restrict__ ptr) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= R;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int kp = i == 0 ? -1 : keys[i - 1];
+        const int kc = i == R ? nkeys : keys[i];
+        for (int k = kp + 1; k <= kc && k <= nkeys; ++k) ptr[k] = i;
+    }
+}
+
+__global__ void jla_iota_kernel(int32_t* out, int64_t n) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<int32_t>(i);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -439,6 +714,10 @@ struct b200fe_kss {
     int64_t nmulti = 0, nslots = 0;
     double* Df = nullptr;
     double* inv_diag = nullptr;
+    double* Dw = nullptr;
+    int64_t* f_ptr = nullptr;      // firm CSR over f_matches
+    int64_t* f_matches = nullptr;  // match ids in firm order (ascending within a firm)
+    KssScalars* sc_one = nullptr;  // nactive = 1: the matrix kernels outside a solve (JLA)
     // workspace for lw_cap lanes
     int lw_cap = 0;
     double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr, *t = nullptr;
@@ -600,6 +879,111 @@ int solve_lanes(b200fe_kss* kss, const double* rhs_pack, double* z_pack, int nb,
     return B200FE_OK;
 }
 
+// Device buffers of one b200fe_kss_jla call, freed on every return.
+struct JlaBufs {
+    std::vector<void*> ptrs;
+    ~JlaBufs() {
+        for (void* q : ptrs) cudaFree(q);
+    }
+    template <typename T>
+    cudaError_t get(T** out, size_t count) {
+        void* q = nullptr;
+        const cudaError_t e = cudaMalloc(&q, sizeof(T) * std::max<size_t>(count, 1));
+        if (e == cudaSuccess) ptrs.push_back(q);
+        *out = static_cast<T*>(q);
+        return e;
+    }
+};
+
+struct JlaState {
+    int64_t R = 0, M = 0, nblk = 0;
+    const int32_t *row_w = nullptr, *row_f = nullptr;
+    const double* row_sw = nullptr;
+    const int64_t* cnt = nullptr;
+    const int64_t *rw_ptr = nullptr, *rf_ptr = nullptr;
+    const int32_t *rw_rows = nullptr, *rf_rows = nullptr;
+    uint64_t* words = nullptr;
+    double* su = nullptr;
+    unsigned long long* tot = nullptr;
+    double* xw = nullptr;  // tw / Dw, then zw
+    double* tf = nullptr;
+    double* acc = nullptr;  // [8][R]
+    // firm chunks of the rows (r*) and of the matches (m*); part: their partials
+    int32_t *rfirst = nullptr, *mfirst = nullptr;
+    int64_t *rcbeg = nullptr, *mcbeg = nullptr;
+    int64_t nrch = 0, nmch = 0;
+    double* part = nullptr;
+    uint64_t seed = 0;
+    double n_py = 0.0, pd = 1.0, scale = 1.0;
+    double tol = 1e-10;
+    int max_iter = 1000;
+    long long iters = 0;
+    int failed = 0;
+};
+
+// draws [d0, d0 + B): the scatters, 3B batched solves and the row sums
+template <int LW>
+int jla_block(b200fe_kss* kss, JlaState& js, int d0, int B) {
+    const cudaStream_t s = kss->stream;
+    const int nl = 3 * B;
+    const int64_t N = kss->N, J = kss->J;
+    const int T = 256;
+    auto grid = [&](int64_t work) { return grid_for(kss, work, 8); };
+    jla_bits_kernel<<<grid(B * js.nblk), T, 0, s>>>(js.seed, d0, B, js.nblk, js.words);
+    K_TRY(cudaMemsetAsync(js.tot, 0, sizeof(unsigned long long) * B, s));
+    jla_msum_kernel<<<grid(B * js.M), T, 0, s>>>(js.seed, d0, B, js.M, js.cnt, js.su, js.tot);
+    jla_su_kernel<<<grid(B * js.M), T, 0, s>>>(B, js.M, js.cnt, js.tot, js.n_py, js.scale, js.su);
+    jla_tw_kernel<<<grid(N * LW), T, 0, s>>>(static_cast<int>(N), LW, B, js.rw_ptr, js.rw_rows, js.row_sw,
+                                            js.words, js.nblk, kss->w_ptr, js.su, js.M, kss->Dw, js.xw);
+    K_TRY(cudaMemsetAsync(js.tf, 0, sizeof(double) * J * LW, s));
+    jla_chunk_sum_kernel<<<grid(js.nrch * B), T, 0, s>>>(js.nrch, LW, B, js.rcbeg, js.rfirst, static_cast<int>(J),
+                                                         js.rf_ptr, js.rf_rows, nullptr, js.row_sw, js.words, js.nblk,
+                                                         nullptr, js.M, js.part);
+    jla_chunk_combine_kernel<<<grid(J * B), T, 0, s>>>(static_cast<int>(J), LW, B, 0, js.rfirst, js.part, js.tf);
+    jla_chunk_sum_kernel<<<grid(js.nmch * B), T, 0, s>>>(js.nmch, LW, B, js.mcbeg, js.mfirst, static_cast<int>(J),
+                                                         kss->f_ptr, nullptr, kss->f_matches, nullptr, js.words,
+                                                         js.nblk, js.su, js.M, js.part);
+    jla_chunk_combine_kernel<<<grid(J * B), T, 0, s>>>(static_cast<int>(J), LW, B, B, js.mfirst, js.part, js.tf);
+    K_TRY(cudaGetLastError());
+    // Ap = -B' xw (the firm pass at p = 0), then the lane-major right-hand sides
+    constexpr int TG = LaneGeom<LW>::TG;
+    K_TRY(cudaMemsetAsync(kss->z, 0, sizeof(double) * J * LW, s));
+    kss_firm_kernel<LW><<<grid_for(kss, kss->nchunks * TG, 8), kKssThreads, 0, s>>>(
+        kss->nchunks, kss->cbeg, kss->cfirm, kss->cslot, kss->mw_f, kss->mc_f, js.xw, kss->Df, kss->z, kss->Ap,
+        kss->slot_part, kss->ground, kss->sc_one);
+    if (kss->nmulti > 0)
+        kss_firm_combine_kernel<LW><<<grid_for(kss, kss->nmulti * TG, 8), kKssThreads, 0, s>>>(
+            kss->nmulti, kss->mfirm, kss->mslot0, kss->mnslot, kss->slot_part, kss->Df, kss->z, kss->Ap,
+            kss->ground, kss->sc_one);
+    jla_rhs_kernel<<<grid(J * nl), T, 0, s>>>(J, LW, nl, kss->ground, js.tf, kss->Ap, kss->stage);
+    K_TRY(cudaGetLastError());
+    // S zf = rhs for the 3B lanes
+    KssScalars init;
+    std::memset(&init, 0, sizeof(init));
+    init.nb = nl;
+    init.tol = js.tol;
+    init.max_iter = js.max_iter;
+    init.nactive = 1;
+    *kss->h_sc = init;
+    K_TRY(cudaMemcpyAsync(kss->sc, kss->h_sc, sizeof(KssScalars), cudaMemcpyHostToDevice, s));
+    K_CHECK(run_solve<LW>(kss, nl));
+    K_TRY(cudaMemcpyAsync(kss->h_sc, kss->sc, sizeof(KssScalars), cudaMemcpyDeviceToHost, s));
+    // zf interleaved (failed lanes zero), zw = xw - Dw^-1 B zf
+    kss_pack_in_kernel<<<grid(J * LW), T, 0, s>>>(J, LW, nl, kss->ground, kss->stage, kss->p);
+    kss_worker_kernel<LW><<<grid_for(kss, N * TG, 8), kKssThreads, 0, s>>>(
+        static_cast<int>(N), kss->w_ptr, kss->m_f, kss->m_c, kss->inv_dw, kss->p, kss->t, kss->sc_one);
+    jla_sub_kernel<<<grid(N * LW), T, 0, s>>>(N * LW, kss->t, js.xw);
+    jla_accum_kernel<<<grid(js.R), T, 0, s>>>(js.R, LW, B, js.row_w, js.row_f, js.row_sw, js.words, js.nblk,
+                                             js.xw, kss->p, js.pd, js.acc);
+    K_TRY(cudaGetLastError());
+    K_TRY(cudaStreamSynchronize(s));
+    for (int l = 0; l < nl; ++l) {
+        if (kss->h_sc->ok[l]) js.iters += kss->h_sc->its[l];
+        else ++js.failed;
+    }
+    return B200FE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -699,6 +1083,9 @@ int b200fe_kss_create(int n_workers, int n_firms, const int32_t* m_w, const int3
         (rc = upload(kss, &kss->mslot0, mslot0.data(), mslot0.size())) ||
         (rc = upload(kss, &kss->mnslot, mnslot.data(), mnslot.size())) ||
         (rc = upload(kss, &kss->Df, Df, static_cast<size_t>(n_firms))) ||
+        (rc = upload(kss, &kss->Dw, Dw, static_cast<size_t>(n_workers))) ||
+        (rc = upload(kss, &kss->f_ptr, f_ptr, static_cast<size_t>(n_firms) + 1)) ||
+        (rc = upload(kss, &kss->f_matches, f_matches, M)) ||
         (rc = upload(kss, &kss->inv_diag, inv_diagS, static_cast<size_t>(n_firms))))
         return fail(rc);
     void* dp = nullptr;
@@ -763,6 +1150,143 @@ int b200fe_kss_solve(b200fe_kss* kss, const double* rhs, double* z, double tol, 
     if (iterations) *iterations = it;
     if (rc != B200FE_OK) return rc;
     return it >= 0 ? B200FE_OK : B200FE_NOT_CONVERGED;
+}
+
+int b200fe_kss_jla(b200fe_kss* kss, int64_t n_rows, const int32_t* row_w, const int32_t* row_f,
+                   const double* row_sw, const int64_t* m_cnt, double n_py, uint64_t seed, int draws,
+                   int block, double tol, int max_iter, double* pii, double* mii, double* corr,
+                   double* bfe, double* bpe, double* bcov, int* failed_lanes, long long* iterations) {
+    if (!kss || n_rows < 1 || n_rows >= INT_MAX || !row_w || !row_f || !m_cnt || draws < 1 || block < 0 ||
+        !(tol >= 0.0) || max_iter < 1 || !(n_py > 0.0))
+        return B200FE_INVALID_ARG;
+    for (int64_t r = 0; r < n_rows; ++r)
+        if (row_w[r] < 0 || row_w[r] >= kss->N || row_f[r] < 0 || row_f[r] >= kss->J) return B200FE_INVALID_ARG;
+    for (int64_t m = 0; m < kss->M; ++m)
+        if (m_cnt[m] < 0) return B200FE_INVALID_ARG;
+    K_TRY(cudaSetDevice(kss->device));
+    const cudaStream_t s = kss->stream;
+    // draws per batched solve: three lanes each, at most kKssMaxLanes lanes
+    const int B = std::max(1, std::min(block > 0 ? block : 8, kKssMaxLanes / 3));
+    const int lw = lane_pitch(3 * B);
+    K_CHECK(ensure_lanes(kss, lw));
+    if (!kss->sc_one) {
+        void* q = nullptr;
+        K_TRY(cudaMalloc(&q, sizeof(KssScalars)));
+        kss->owned.push_back(q);
+        kss->sc_one = static_cast<KssScalars*>(q);
+        KssScalars one;
+        std::memset(&one, 0, sizeof(one));
+        one.nactive = 1;
+        K_TRY(cudaMemcpy(kss->sc_one, &one, sizeof(one), cudaMemcpyHostToDevice));
+    }
+    JlaBufs bufs;
+    JlaState js;
+    js.R = n_rows;
+    js.M = kss->M;
+    js.nblk = (n_rows + 63) / 64;
+    js.seed = seed;
+    js.n_py = n_py;
+    js.pd = static_cast<double>(draws);
+    js.scale = 1.0 / std::sqrt(js.pd);
+    js.tol = tol;
+    js.max_iter = max_iter;
+    const size_t R = static_cast<size_t>(n_rows);
+    int32_t *d_rw, *d_rf, *keys_sorted, *iota, *rw_rows, *rf_rows;
+    double* d_sw = nullptr;
+    int64_t *d_cnt, *rw_ptr, *rf_ptr;
+    K_TRY(bufs.get(&d_rw, R));
+    K_TRY(bufs.get(&d_rf, R));
+    K_TRY(bufs.get(&keys_sorted, R));
+    K_TRY(bufs.get(&iota, R));
+    K_TRY(bufs.get(&rw_rows, R));
+    K_TRY(bufs.get(&rf_rows, R));
+    K_TRY(bufs.get(&d_cnt, static_cast<size_t>(kss->M)));
+    K_TRY(bufs.get(&rw_ptr, static_cast<size_t>(kss->N) + 1));
+    K_TRY(bufs.get(&rf_ptr, static_cast<size_t>(kss->J) + 1));
+    K_TRY(cudaMemcpyAsync(d_rw, row_w, sizeof(int32_t) * R, cudaMemcpyHostToDevice, s));
+    K_TRY(cudaMemcpyAsync(d_rf, row_f, sizeof(int32_t) * R, cudaMemcpyHostToDevice, s));
+    K_TRY(cudaMemcpyAsync(d_cnt, m_cnt, sizeof(int64_t) * kss->M, cudaMemcpyHostToDevice, s));
+    if (row_sw) {
+        K_TRY(bufs.get(&d_sw, R));
+        K_TRY(cudaMemcpyAsync(d_sw, row_sw, sizeof(double) * R, cudaMemcpyHostToDevice, s));
+    }
+    // rows grouped by worker and by firm, ascending row order within a group
+    // (a stable sort), so every scatter adds in the reference's order
+    jla_iota_kernel<<<grid_for(kss, n_rows, 8), 256, 0, s>>>(iota, n_rows);
+    size_t tmp_bytes = 0;
+    void* tmp = nullptr;
+    K_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_rw, keys_sorted, iota, rw_rows,
+                                          static_cast<int>(n_rows), 0, 32, s));
+    K_TRY(bufs.get(reinterpret_cast<unsigned char**>(&tmp), tmp_bytes));
+    K_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, d_rw, keys_sorted, iota, rw_rows,
+                                          static_cast<int>(n_rows), 0, 32, s));
+    jla_ptr_kernel<<<grid_for(kss, n_rows + 1, 8), 256, 0, s>>>(n_rows, kss->N, keys_sorted, rw_ptr);
+    K_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, d_rf, keys_sorted, iota, rf_rows,
+                                          static_cast<int>(n_rows), 0, 32, s));
+    jla_ptr_kernel<<<grid_for(kss, n_rows + 1, 8), 256, 0, s>>>(n_rows, kss->J, keys_sorted, rf_ptr);
+    K_TRY(cudaGetLastError());
+    // firm chunks of the rows and of the matches
+    auto chunks = [&](const int64_t* ptr, int32_t** first, int64_t** cbeg, int64_t* nch) -> int {
+        int32_t* cnt;
+        K_TRY(bufs.get(&cnt, static_cast<size_t>(kss->J) + 1));
+        K_TRY(bufs.get(first, static_cast<size_t>(kss->J) + 1));
+        jla_chunk_count_kernel<<<grid_for(kss, kss->J + 1, 8), 256, 0, s>>>(kss->J, ptr, cnt);
+        size_t sb = 0;
+        K_TRY(cub::DeviceScan::ExclusiveSum(nullptr, sb, cnt, *first, kss->J + 1, s));
+        unsigned char* st;
+        K_TRY(bufs.get(&st, sb));
+        K_TRY(cub::DeviceScan::ExclusiveSum(st, sb, cnt, *first, kss->J + 1, s));
+        int32_t tot = 0;
+        K_TRY(cudaMemcpyAsync(&tot, *first + kss->J, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        K_TRY(cudaStreamSynchronize(s));
+        *nch = tot;
+        K_TRY(bufs.get(cbeg, static_cast<size_t>(std::max(tot, 1))));
+        jla_chunk_fill_kernel<<<grid_for(kss, kss->J, 8), 256, 0, s>>>(kss->J, ptr, *first, *cbeg);
+        K_TRY(cudaGetLastError());
+        return B200FE_OK;
+    };
+    K_CHECK(chunks(rf_ptr, &js.rfirst, &js.rcbeg, &js.nrch));
+    K_CHECK(chunks(kss->f_ptr, &js.mfirst, &js.mcbeg, &js.nmch));
+    K_TRY(bufs.get(&js.part, static_cast<size_t>(std::max<int64_t>(std::max(js.nrch, js.nmch), 1)) * lw));
+    js.row_w = d_rw;
+    js.row_f = d_rf;
+    js.row_sw = d_sw;
+    js.cnt = d_cnt;
+    js.rw_ptr = rw_ptr;
+    js.rf_ptr = rf_ptr;
+    js.rw_rows = rw_rows;
+    js.rf_rows = rf_rows;
+    K_TRY(bufs.get(&js.words, static_cast<size_t>(B) * js.nblk));
+    K_TRY(bufs.get(&js.su, static_cast<size_t>(B) * std::max<int64_t>(kss->M, 1)));
+    K_TRY(bufs.get(&js.tot, static_cast<size_t>(B)));
+    K_TRY(bufs.get(&js.xw, static_cast<size_t>(std::max(kss->N, 1)) * lw));
+    K_TRY(bufs.get(&js.tf, static_cast<size_t>(kss->J) * lw));
+    K_TRY(bufs.get(&js.acc, 8 * R));
+    K_TRY(cudaMemsetAsync(js.acc, 0, sizeof(double) * 8 * R, s));
+    for (int d0 = 0; d0 < draws; d0 += B) {
+        const int nb = std::min(B, draws - d0);
+        int rc = B200FE_OK;
+        switch (lw) {
+            case 4: rc = jla_block<4>(kss, js, d0, nb); break;
+            case 8: rc = jla_block<8>(kss, js, d0, nb); break;
+            case 16: rc = jla_block<16>(kss, js, d0, nb); break;
+            case 32: rc = jla_block<32>(kss, js, d0, nb); break;
+            default: rc = jla_block<64>(kss, js, d0, nb); break;
+        }
+        if (rc != B200FE_OK) return rc;
+    }
+    double* fin;
+    K_TRY(bufs.get(&fin, 3 * R));
+    jla_final_kernel<<<grid_for(kss, n_rows, 8), 256, 0, s>>>(n_rows, js.pd, js.acc, fin);
+    K_TRY(cudaGetLastError());
+    double* const outs[6] = {pii, mii, corr, bfe, bpe, bcov};
+    const double* const srcs[6] = {fin, fin + R, fin + 2 * R, js.acc + 5 * R, js.acc + 6 * R, js.acc + 7 * R};
+    for (int k = 0; k < 6; ++k)
+        if (outs[k]) K_TRY(cudaMemcpyAsync(outs[k], srcs[k], sizeof(double) * R, cudaMemcpyDeviceToHost, s));
+    K_TRY(cudaStreamSynchronize(s));
+    if (failed_lanes) *failed_lanes = js.failed;
+    if (iterations) *iterations = js.iters;
+    return js.failed == 0 ? B200FE_OK : B200FE_NOT_CONVERGED;
 }
 
 int b200fe_stable_sort_u64(const uint64_t* keys, int64_t* order_out, int64_t n) {

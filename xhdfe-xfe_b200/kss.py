@@ -130,3 +130,36 @@ class KssSolver:
         if rc != _lib.OK:
             raise AbsorberError(rc, self._err())
         return Z, its
+
+    def jla(self, row_w, row_f, m_cnt, n_py, *, row_sw=None, seed: int = 20260705, draws: int = 200,
+            block: int = 8, tol: float = 1e-10, max_iter: int = 1000) -> dict:
+        """JLA leverages of the leave-out decomposition on the device (the draw
+        loop of akm_kss_decompose, src/akm_kss.cpp:2753-3160, with the ratio
+        estimator :3275-3289): rows given by their worker / firm in this
+        solver's numbering, in the reference's row order (it indexes the
+        Rademacher streams); m_cnt the person-years of every match, n_py their
+        total; row_sw the rows' sqrt match weights at match level (None: 1).
+        Returns pii, mii, corr, bfe, bpe, bcov (one entry per row), the number
+        of solve lanes that did not converge and the summed PCG iterations."""
+        rw = np.ascontiguousarray(row_w, dtype=np.int32)
+        rf = np.ascontiguousarray(row_f, dtype=np.int32)
+        cnt = np.ascontiguousarray(m_cnt, dtype=np.int64)
+        if rw.shape != rf.shape or rw.ndim != 1 or cnt.shape != (self._keep["m_c"].size,):
+            raise ValueError("row_w / row_f must have one entry per row, m_cnt one per match")
+        sw = None if row_sw is None else np.ascontiguousarray(row_sw, dtype=np.float64)
+        if sw is not None and sw.shape != rw.shape:
+            raise ValueError("row_sw must have one entry per row")
+        R = rw.size
+        out = {k: np.zeros(R) for k in ("pii", "mii", "corr", "bfe", "bpe", "bcov")}
+        failed = ctypes.c_int(0)
+        iters = ctypes.c_longlong(0)
+        rc = self._lib.b200fe_kss_jla(
+            self._h, R, rw.ctypes.data, rf.ctypes.data, None if sw is None else sw.ctypes.data,
+            cnt.ctypes.data, float(n_py), int(seed) & 0xFFFFFFFFFFFFFFFF, int(draws), int(block), tol, max_iter,
+            out["pii"].ctypes.data, out["mii"].ctypes.data, out["corr"].ctypes.data, out["bfe"].ctypes.data,
+            out["bpe"].ctypes.data, out["bcov"].ctypes.data, ctypes.byref(failed), ctypes.byref(iters))
+        if rc not in (_lib.OK, _lib.NOT_CONVERGED):
+            raise AbsorberError(rc, self._err())
+        out["failed_lanes"] = int(failed.value)
+        out["iterations"] = int(iters.value)
+        return out
