@@ -1248,7 +1248,7 @@ int reduce_sparse(b200fe_context* ctx, const Work<T>& wk, const T* x, T* q) {
         double pb = static_cast<double>(L.nchunks) * 13.0 + static_cast<double>(st.sp_nnz) * (4.0 + tb) +
                     2.0 * static_cast<double>(L.G) * CP * tb;
         if (coupled) pb += static_cast<double>(L.G) * st.SGP * tb;
-        ProfScope ps(ctx, B200FE_PROF_PASS, pb);
+        ProfScope ps(ctx, B200FE_PROF_GATHER, pb);
         const size_t gsmem = coupled ? static_cast<size_t>(st.SGP) * CP * sizeof(T) : 0;
         sparse_gather_kernel<T, CQ><<<wk.sp_gather_grid, kRowThreads, gsmem, s>>>(g);
         B_LAUNCHED();
