@@ -70,6 +70,9 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA absorber on the same panel")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--batch-workers", type=int, default=0,
+                    help="batch workload: host threads (contexts, streams) of an extra concurrent "
+                         "run (0: none)")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip the reference's own CUDA backend leg (kss workload)")
     ap.add_argument("--no-learned", action="store_true",
@@ -1400,6 +1403,24 @@ def run_batch(args):
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, dev)
     last = results[-1]
     launches = int(sum(r.kernel_launches for rs in results for r, _ in rs))
+    # the same batch with the panels spread over host threads, each with its own
+    # context and stream (absorb_many): wall time of the whole batch, synchronized
+    conc = None
+    if args.batch_workers > 1:
+        jobs = [(v, g, p.levels, w, cl) for p, (v, g, w, cl, out) in zip(batch, resident)]
+        olsk = {"se_type": "cluster"}
+        for _ in range(max(1, args.warmup)):
+            pkg.absorb_many(jobs, workers=args.batch_workers, device=local, options=opts, ols=olsk)
+        torch.cuda.synchronize()
+        ctimes = []
+        for _ in range(args.steps):
+            t1 = time.perf_counter()
+            pkg.absorb_many(jobs, workers=args.batch_workers, device=local, options=opts, ols=olsk)
+            torch.cuda.synchronize()
+            ctimes.append(time.perf_counter() - t1)
+        conc = {"workers": args.batch_workers, "value": max_over_ranks(statistics.median(ctimes), dist, dev),
+                "unit": UNIT, "timing": "wall time of the whole batch (absorption + clustered OLS per "
+                "panel), device-resident inputs, all streams synchronized"}
     # end to end through the public API: host arrays, device preprocessing
     # (dense ids, singleton cascade), absorption, clustered OLS
     y_h = [torch.from_numpy(p.y).pin_memory().numpy() for p in batch]
@@ -1443,6 +1464,7 @@ def run_batch(args):
             "gpu_launches": launches, "converged": all(bool(r.converged) for r, _ in last),
             "iterations_min_max": [min(its), max(its)],
             "panels_per_s": len(batch) / (ms / 1000.0), "rows_per_s": rows / (ms / 1000.0),
+            "concurrent": conc,
             "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "generate_s": gen_s}))
     if dist:
         dist.barrier()

@@ -120,3 +120,33 @@ def test_graph_replay_matches_plain_launches(pkg, batch, monkeypatch):
     for a, b in zip(runs["1"], runs["0"]):
         assert np.array_equal(a.y_tilde, b.y_tilde) and np.array_equal(a.X_tilde, b.X_tilde)
         assert a.iterations == b.iterations and a.kernel_launches == b.kernel_launches
+
+
+def test_concurrent_batch_equals_sequential_calls(pkg, batch):
+    """absorb_many (three host threads, each with its own context and CUDA
+    stream) gives every panel bitwise the answer of a sequential absorb_device
+    call, and the per-panel clustered OLS equal the sequential ones."""
+    import torch
+    dev = torch.device("cuda", 0)
+    opts = pkg.make_options(tol=1e-8)
+    jobs = []
+    for p in batch:
+        v = torch.empty((p.k + 1, p.n), dtype=torch.float64, device=dev)
+        v[0].copy_(torch.from_numpy(p.y))
+        v[1:].copy_(torch.from_numpy(np.ascontiguousarray(p.X.T)))
+        jobs.append((v, [torch.from_numpy(np.ascontiguousarray(f)).to(dev) for f in p.fes], p.levels,
+                     torch.from_numpy(p.weights).to(dev),
+                     torch.from_numpy(p.fes[0].astype(np.int32)).to(dev)))
+    ols = {"se_type": "cluster"}
+    conc = pkg.absorb_many(jobs, workers=3, options=opts, ols=ols)
+    ab = pkg.Absorber(0)
+    try:
+        for (v, g, G, w, cl), (out_c, r_c, o_c) in zip(jobs, conc):
+            out_s, r_s = ab.absorb_device(v, g, G, w, opts)
+            torch.cuda.synchronize()
+            assert torch.equal(out_c, out_s) and r_c.iterations == r_s.iterations
+            o_s = pkg.run_ols(out_s[0], out_s[1:], w, cl, se_type="cluster")
+            assert np.array_equal(o_c.coefficients, o_s.coefficients)
+            assert np.array_equal(o_c.std_errors, o_s.std_errors)
+    finally:
+        ab.close()

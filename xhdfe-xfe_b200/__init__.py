@@ -14,6 +14,7 @@ from .absorber import (  # noqa: F401
     HeterogeneousSlopeTerm,
     OlsResult,
     absorb_fixed_effects,
+    absorb_many,
     build_group_individual,
     cuda_backend_available,
     demean_raw,

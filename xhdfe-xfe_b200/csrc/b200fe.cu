@@ -636,8 +636,7 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
                 B_CHECK(get_buf(ctx, "cfy32", static_cast<size_t>(L.G) * SGP, &st.cfy32));
                 B_CHECK(get_buf(ctx, "cfy_part", static_cast<size_t>(L.nchunks) * SGP, &cpart));
                 const size_t fsmem = static_cast<size_t>(kCoupleWarps) * 32 * SG * sizeof(double);
-                B_TRY(cudaFuncSetAttribute(coupling_fy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(fsmem)));
+                B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&coupling_fy_kernel), static_cast<int>(fsmem)));
                 int fps = 1;
                 B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fps, coupling_fy_kernel,
                                                                     kCoupleWarps * 32, fsmem));
@@ -661,8 +660,7 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
                 B_LAUNCHED();
             }
             const size_t ysmem = static_cast<size_t>(kCoupleYyWarps) * (SG * SG + SG + 32 * SG) * sizeof(double);
-            B_TRY(cudaFuncSetAttribute(coupling_yy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(ysmem)));
+            B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&coupling_yy_kernel), static_cast<int>(ysmem)));
             int yps = 1;
             B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&yps, coupling_yy_kernel,
                                                                 kCoupleYyWarps * 32, ysmem));
@@ -766,10 +764,8 @@ struct Work {
 
 template <typename T, int CQ, int MODE>
 int set_pass_smem(b200fe_context* ctx, int tile_smem, int long_smem) {
-    B_TRY(cudaFuncSetAttribute(tile_pass_kernel<T, CQ, MODE>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
-    B_TRY(cudaFuncSetAttribute(segment_pass_kernel<T, CQ, MODE>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, long_smem));
+    B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&tile_pass_kernel<T, CQ, MODE>), tile_smem));
+    B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&segment_pass_kernel<T, CQ, MODE>), long_smem));
     return B200FE_OK;
 }
 
@@ -793,10 +789,8 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     wk.data_smem = 0;
     if (std::is_same<T, double>::value) {
         wk.data_smem = static_cast<int>(data_smem_bytes(CP, st.SG, st.nL));
-        B_TRY(cudaFuncSetAttribute(data_pass_kernel<CP, kRhs>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   wk.data_smem));
-        B_TRY(cudaFuncSetAttribute(data_pass_kernel<CP, kFinal>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, wk.data_smem));
+        B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&data_pass_kernel<CP, kRhs>), wk.data_smem));
+        B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&data_pass_kernel<CP, kFinal>), wk.data_smem));
         int dps = 1;
         B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dps, data_pass_kernel<CP, kRhs>, kDataThreads,
                                                             wk.data_smem));
@@ -809,8 +803,7 @@ int prepare_work(b200fe_context* ctx, const std::string& tag, Work<T>& wk) {
     if (st.block_ok && (ctx->pass_kernel == 0 || ctx->pass_kernel == 2)) {
         // the coupled matvec runs the pass without the small dim: no shared memory
         wk.run_smem = st.coupled ? 0 : static_cast<int>(block_smem_bytes<T>(CP, st.SG));
-        B_TRY(cudaFuncSetAttribute(block_pass_kernel<T, CQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   wk.run_smem));
+        B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&block_pass_kernel<T, CQ>), wk.run_smem));
         int rps = 1;
         B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rps, block_pass_kernel<T, CQ>, kBlockThreads,
                                                             wk.run_smem));
@@ -973,7 +966,7 @@ int launch_stream_pass(b200fe_context* ctx, const PassArgs<double>& a, int* grid
     auto kern = weighted ? stream_pass_kernel<MODE, true> : stream_pass_kernel<MODE, false>;
     const unsigned bit = 1u << (2 * (MODE == kFinal ? 1 : 0) + (weighted ? 1 : 0));
     if (!(ctx->stream_smem_set & bit)) {
-        B_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+        B_TRY(raise_smem_limit(reinterpret_cast<const void*>(kern), budget));
         ctx->stream_smem_set |= bit;
     }
     const int g = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(st.stream_nreg, ctx->num_sms)));
@@ -1545,7 +1538,7 @@ int pcg_persistent(b200fe_context* ctx, const Work<T>& wk, const T* dinv, T* x, 
     if (SG > kPcgMaxSG) return B200FE_UNAVAILABLE;
     const size_t smem = pcg_smem_bytes<T>(CP, SGP);
     auto kern = pcg_persistent_kernel<T, CQ>;
-    B_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    B_TRY(raise_smem_limit(reinterpret_cast<const void*>(kern), static_cast<int>(smem)));
     int per_sm = 0;
     B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPcgThreads, smem));
     if (per_sm < 1) return B200FE_UNAVAILABLE;

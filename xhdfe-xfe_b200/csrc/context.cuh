@@ -17,7 +17,9 @@
 #include <cstring>
 #include <cstdlib>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <type_traits>
 #include <string>
 #include <unordered_map>
@@ -282,6 +284,24 @@ inline int get_buf(b200fe_context* ctx, const std::string& name, size_t count, T
     }
     *out = static_cast<T*>(b.p);
     return B200FE_OK;
+}
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`.  The
+// limit is process-wide per kernel and device, so it is only ever raised:
+// contexts on other host threads that launch the same kernel with more shared
+// memory are never undercut.
+inline cudaError_t raise_smem_limit(const void* func, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    int& cur = limit[{dev, func}];
+    if (cur >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
 }
 
 inline int grid_for(b200fe_context* ctx, int64_t work, int threads, int per_sm = 8) {

@@ -55,8 +55,7 @@ int b200fe_mlp_grad(b200fe_context* ctx, const float* d_params, const float* d_x
     cudaGetLastError();
     cudaSetDevice(ctx->device);
     const size_t smem = sizeof(MlpGradSmem);
-    B_TRY(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem)));
+    B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&mlp_grad_kernel), static_cast<int>(smem)));
     const int64_t blocks = (n + kMlpBlock - 1) / kMlpBlock;
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(blocks, ctx->num_sms)));
     float* partial;
