@@ -197,9 +197,25 @@ def make_options(*, tol=1e-8, tolerance_mode="reghdfe-comparable", precision="mi
     o.inner_tol = float(inner_tol)
     o.max_outer = int(max_outer)
     o.profile = 1 if profile else 0
-    o.pass_kernel = int(pass_kernel)
+    # "auto": the form tuned for the call's dims and rows (autotune.py's table),
+    # resolved by Absorber.absorb / absorb_device before the library is called
+    o.pass_kernel = PASS_KERNEL_AUTO if pass_kernel == "auto" else int(pass_kernel)
     o.fe_linf_tol = float(fe_linf_tol)
     return o
+
+
+PASS_KERNEL_AUTO = -1
+
+
+def _resolve_options(o, num_dims: int, n: int):
+    """A copy of options o with pass_kernel "auto" replaced by the tuned form."""
+    if o is None or o.pass_kernel != PASS_KERNEL_AUTO:
+        return o
+    from .autotune import choose_pass_kernel
+    r = _lib.Options()
+    ctypes.pointer(r)[0] = o
+    r.pass_kernel = choose_pass_kernel(num_dims, n)
+    return r
 
 
 def _ptr_array(ptrs):
@@ -282,7 +298,7 @@ class Absorber:
             y_out = np.empty_like(y)
         if X_out is None:
             X_out = np.empty((n, k), dtype=np.float64, order="F")
-        o = options or make_options()
+        o = _resolve_options(options or make_options(), len(gids), n)
         r = _lib.Result()
         if slopes:
             if save_fe:
@@ -327,7 +343,7 @@ class Absorber:
             if g.dtype != torch.int32 or not g.is_cuda or g.numel() != n:
                 raise ValueError("group ids must be int32 CUDA tensors of length n")
         G = np.ascontiguousarray(num_groups, dtype=np.int32)
-        o = options or make_options()
+        o = _resolve_options(options or make_options(), len(group_ids), n)
         r = _lib.Result()
         rc = self.lib.b200fe_absorb_device(
             self.handle, v.data_ptr(), n, cols, len(group_ids),
@@ -365,7 +381,7 @@ class Absorber:
             y_out = np.empty_like(y)
         if X_out is None:
             X_out = np.empty((n, k), dtype=np.float64, order="F")
-        o = options or make_options()
+        o = _resolve_options(options or make_options(), len(group_ids), n)
         r = _lib.Result()
         rc = self.lib.b200fe_absorb_group_individual(
             self.handle, y.ctypes.data, X.ctypes.data if k else None, n, k, len(gids),
@@ -404,7 +420,7 @@ class Absorber:
             zp[int(d)] = z.data_ptr()
             icpt[int(d)] = 1 if inc else 0
         G = np.ascontiguousarray(num_groups, dtype=np.int32)
-        o = options or make_options()
+        o = _resolve_options(options or make_options(), len(group_ids), n)
         r = _lib.Result()
         rc = self.lib.b200fe_absorb_slopes_device(
             self.handle, v.data_ptr(), n, cols, len(group_ids),
