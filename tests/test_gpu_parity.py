@@ -37,8 +37,8 @@ def _check(absorber, pkg, oracle_mod, y, X, fes, G, w=None, precision="mixed", t
     return res, V
 
 
-def _akm(panels, n, three_way, seed=0, firms=500):
-    p = panels.akm_two_way(n, n_firms=firms, seed=seed, three_way=three_way)
+def _akm(panels, n, three_way, seed=0, firms=500, years=10):
+    p = panels.akm_two_way(n, n_firms=firms, n_years=years, seed=seed, three_way=three_way)
     return panels.subset(p, panels.drop_singletons(p.fes))
 
 
@@ -169,13 +169,16 @@ def test_zipf_primary_mixed_long_and_tiles(absorber, pkg, oracle_mod, panels):
     _check(absorber, pkg, oracle_mod, p.y[keep], p.X[keep], fes, G, w=w)
 
 
+@pytest.mark.parametrize("years", [10, 20, 36, 50])
 @pytest.mark.parametrize("weighted", [False, True])
-def test_block_and_tile_matvec_agree(absorber, pkg, oracle_mod, panels, weighted):
+def test_block_and_tile_matvec_agree(absorber, pkg, oracle_mod, panels, weighted, years):
     # the CG matvec forms solve the same system: the explicit sparse Schur
     # block of the firm dim with the dense small-dim coupling (0, the default
     # here), the general tile pass (1), block level with per-block small-dim
-    # updates (2) and block level with the dense coupling through the runs (3)
-    p = _akm(panels, 30_000, True, seed=37)
+    # updates (2) and block level with the dense coupling through the runs (3).
+    # The year counts reach each register tile of the year-year coupling
+    # (<= 12, <= 24, <= 36 levels) and the shared-memory accumulator (> 36)
+    p = _akm(panels, 30_000, True, seed=37, years=years)
     w = np.random.default_rng(5).lognormal(0.0, 0.5, size=p.n) if weighted else None
     outs = []
     for pk in (0, 1, 2, 3):

@@ -635,7 +635,7 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
                 B_CHECK(get_buf(ctx, "cfy64", static_cast<size_t>(L.G) * SGP, &st.cfy64));
                 B_CHECK(get_buf(ctx, "cfy32", static_cast<size_t>(L.G) * SGP, &st.cfy32));
                 B_CHECK(get_buf(ctx, "cfy_part", static_cast<size_t>(L.nchunks) * SGP, &cpart));
-                const size_t fsmem = static_cast<size_t>(kCoupleWarps) * 32 * SG * sizeof(double);
+                const size_t fsmem = static_cast<size_t>(kCoupleWarps) * 32 * couple_pitch(static_cast<int>(SG)) * sizeof(double);
                 B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&coupling_fy_kernel), static_cast<int>(fsmem)));
                 int fps = 1;
                 B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fps, coupling_fy_kernel,
@@ -659,22 +659,38 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
                     st.cfy64, static_cast<int64_t>(L.G) * SGP, st.cfy32);
                 B_LAUNCHED();
             }
-            const size_t ysmem = static_cast<size_t>(kCoupleYyWarps) * (SG * SG + SG + 32 * SG) * sizeof(double);
-            B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&coupling_yy_kernel), static_cast<int>(ysmem)));
-            int yps = 1;
-            B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&yps, coupling_yy_kernel,
-                                                                kCoupleYyWarps * 32, ysmem));
-            const int ny = static_cast<int>(std::max<int64_t>(
-                1, std::min<int64_t>((static_cast<int64_t>(G[p]) + 32 * kCoupleYyWarps - 1) /
-                                         (32 * kCoupleYyWarps),
-                                     static_cast<int64_t>(ctx->num_sms) * std::max(yps, 1))));
-            double* ypart;
-            B_CHECK(get_buf(ctx, "cyy_part", static_cast<size_t>(ny) * (SG * SG + SG), &ypart));
+            // C_yy partials: the register-tiled kernel where SG fits one of its
+            // tiles, the shared-memory accumulator above that
+            int ny = 1;
+            double* ypart = nullptr;
             B_CHECK(get_buf(ctx, "cyy", static_cast<size_t>(SG) * SG, &st.cyy));
-            coupling_yy_kernel<<<ny, kCoupleYyWarps * 32, ysmem, s>>>(G[p], st.seg_meta, st.run_meta,
-                                                                      st.block_meta, st.block_w64,
-                                                                      st.inv_wp, st.SG, ypart);
-            B_LAUNCHED();
+            auto launch_yy = [&](auto kern, int warps, size_t smem) -> int {
+                B_TRY(raise_smem_limit(reinterpret_cast<const void*>(kern), static_cast<int>(smem)));
+                int yps = 1;
+                B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&yps, kern, warps * 32, smem));
+                ny = static_cast<int>(std::max<int64_t>(
+                    1, std::min<int64_t>((static_cast<int64_t>(G[p]) + 32 * warps - 1) / (32 * warps),
+                                         static_cast<int64_t>(ctx->num_sms) * std::max(yps, 1))));
+                B_CHECK(get_buf(ctx, "cyy_part", static_cast<size_t>(ny) * (SG * SG + SG), &ypart));
+                kern<<<ny, warps * 32, smem, s>>>(G[p], st.seg_meta, st.run_meta, st.block_meta,
+                                                  st.block_w64, st.inv_wp, st.SG, ypart);
+                B_LAUNCHED();
+                return B200FE_OK;
+            };
+            auto tile_smem = [&](int RT, int CT) {
+                return static_cast<size_t>(SG * SG + SG + kCoupleTileWarps * 32 * couple_tile_pitch(RT, CT)) *
+                       sizeof(double);
+            };
+            if (SG <= 12)
+                B_CHECK(launch_yy(&coupling_yy_tile_kernel<2, 3>, kCoupleTileWarps, tile_smem(2, 3)));
+            else if (SG <= 24)
+                B_CHECK(launch_yy(&coupling_yy_tile_kernel<3, 6>, kCoupleTileWarps, tile_smem(3, 6)));
+            else if (SG <= 36)
+                B_CHECK(launch_yy(&coupling_yy_tile_kernel<5, 9>, kCoupleTileWarps, tile_smem(5, 9)));
+            else
+                B_CHECK(launch_yy(&coupling_yy_kernel, kCoupleYyWarps,
+                                  static_cast<size_t>(kCoupleYyWarps) * couple_yy_warp_words(static_cast<int>(SG)) *
+                                      sizeof(double)));
             coupling_yy_reduce_kernel<<<grid_for(ctx, SG * SG, T256), T256, 0, s>>>(
                 ypart, ny, st.SG, st.cyy, Wall + st.sbase[0], Eall + st.sbase[0]);
             B_LAUNCHED();

@@ -494,8 +494,14 @@ __device__ __forceinline__ void couple_row_add(double* row, const int2 bm, doubl
 // j0 + i of the chunk: its metadata and blocks are read by the 32 lanes in
 // parallel, and lane i writes y_m - c_m Y_s / W_s into its own shared-memory
 // row; lane l then sums level l (and l + 32) over the rows in lane order.
-// Rows have stride SGP (SG rounded up to 4) and padding levels are zero.
+// Output rows have stride SGP (SG rounded up to 4) and padding levels are zero.
 constexpr int kCoupleWarps = 8;
+
+// Pitch of the per-lane shared-memory rows: odd in doubles, so that the 16
+// lanes of a 64-bit shared access that touch level h of 16 different rows fall
+// in 16 different bank pairs (an even pitch such as 36 puts lanes l and l + 4
+// in the same banks: 8-way conflicts on every row access).
+__host__ __device__ __forceinline__ int couple_pitch(int SG) { return SG | 1; }
 
 __global__ void __launch_bounds__(kCoupleWarps * 32)
 coupling_fy_kernel(int64_t nchunks, const int32_t* __restrict__ chunk_grp,
@@ -508,8 +514,9 @@ coupling_fy_kernel(int64_t nchunks, const int32_t* __restrict__ chunk_grp,
                    double* __restrict__ partial) {
     extern __shared__ double cf_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double* rows = cf_smem + static_cast<int64_t>(warp) * 32 * SG;
-    double* myrow = rows + lane * SG;
+    const int SGQ = couple_pitch(SG);
+    double* rows = cf_smem + static_cast<int64_t>(warp) * 32 * SGQ;
+    double* myrow = rows + lane * SGQ;
     const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kCoupleWarps;
     for (int64_t c = static_cast<int64_t>(blockIdx.x) * kCoupleWarps + warp; c < nchunks; c += nwarps) {
         const int32_t b = chunk_beg[c], e = chunk_end[c];
@@ -533,7 +540,7 @@ coupling_fy_kernel(int64_t nchunks, const int32_t* __restrict__ chunk_grp,
             for (int i = 0; i < nj; ++i) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k)
-                    if (lane + 32 * k < SG) acc[k] += rows[i * SG + lane + 32 * k];
+                    if (lane + 32 * k < SG) acc[k] += rows[i * SGQ + lane + 32 * k];
             }
             __syncwarp();
         }
@@ -579,10 +586,14 @@ coupling_fy_combine_kernel(int64_t nmulti, const int32_t* __restrict__ multi_grp
 // warp builds Y_s of segment s0 + i in its own shared row (the 32 lanes read
 // their blocks in parallel); then, segment by segment in lane order, lane l
 // adds Y_s[h] Y_s[h'] / W_s to rows h = l and l + 32 of the warp's SG x SG
-// accumulator, for h' in the segment's level range, and Y_s[h] to W_h.
-// Per-CTA partials [SG*SG + SG], summed in CTA order by
-// coupling_yy_reduce_kernel.
+// accumulator, for h' in the segment's level range, and Y_s[h] to W_h.  Rows of
+// Y and of the accumulator have the odd pitch couple_pitch(SG).  Per-CTA
+// partials [SG*SG + SG], summed in CTA order by coupling_yy_reduce_kernel.
 constexpr int kCoupleYyWarps = 2;
+
+__host__ __device__ __forceinline__ int couple_yy_warp_words(int SG) {
+    return SG * couple_pitch(SG) + SG + 32 * couple_pitch(SG);  // acc, W, 32 rows Y
+}
 
 __global__ void __launch_bounds__(kCoupleYyWarps * 32)
 coupling_yy_kernel(int32_t Gp, const int2* __restrict__ seg_meta, const int4* __restrict__ run_meta,
@@ -591,11 +602,12 @@ coupling_yy_kernel(int32_t Gp, const int2* __restrict__ seg_meta, const int4* __
     extern __shared__ double cy_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int SS = SG * SG;
-    const int WS = SS + SG + 32 * SG;  // per warp: acc, W, 32 rows Y
+    const int SGQ = couple_pitch(SG);
+    const int WS = couple_yy_warp_words(SG);
     double* acc = cy_smem + static_cast<int64_t>(warp) * WS;
-    double* Wh = acc + SS;
+    double* Wh = acc + SG * SGQ;
     double* Y = Wh + SG;
-    double* myY = Y + lane * SG;
+    double* myY = Y + lane * SGQ;
     for (int i = threadIdx.x; i < kCoupleYyWarps * WS; i += blockDim.x) cy_smem[i] = 0.0;
     __syncthreads();
     const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kCoupleYyWarps;
@@ -622,7 +634,7 @@ coupling_yy_kernel(int32_t Gp, const int2* __restrict__ seg_meta, const int4* __
         for (int i = 0; i < ns; ++i) {
             const int lo = __shfl_sync(0xffffffffu, hmin, i), hi = __shfl_sync(0xffffffffu, hmax, i);
             const double w_inv = __shfl_sync(0xffffffffu, iw, i);
-            const double* Yi = Y + i * SG;
+            const double* Yi = Y + i * SGQ;
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
                 const int h = lane + 32 * k;
@@ -631,7 +643,7 @@ coupling_yy_kernel(int32_t Gp, const int2* __restrict__ seg_meta, const int4* __
                     Wh[h] += yh;
                     const double a = yh * w_inv;
                     if (a != 0.0)
-                        for (int h2 = lo; h2 < hi; ++h2) acc[h * SG + h2] = fma(a, Yi[h2], acc[h * SG + h2]);
+                        for (int h2 = lo; h2 < hi; ++h2) acc[h * SGQ + h2] = fma(a, Yi[h2], acc[h * SGQ + h2]);
                 }
             }
         }
@@ -641,10 +653,111 @@ coupling_yy_kernel(int32_t Gp, const int2* __restrict__ seg_meta, const int4* __
     }
     __syncthreads();
     for (int i = threadIdx.x; i < SS + SG; i += blockDim.x) {
+        const int src = i < SS ? (i / SG) * SGQ + (i - (i / SG) * SG) : SG * SGQ + (i - SS);
         double v = 0.0;
-        for (int w = 0; w < kCoupleYyWarps; ++w) v += cy_smem[static_cast<int64_t>(w) * WS + i];
+        for (int w = 0; w < kCoupleYyWarps; ++w) v += cy_smem[static_cast<int64_t>(w) * WS + src];
         partial[static_cast<int64_t>(blockIdx.x) * (SS + SG) + i] = v;
     }
+}
+
+// The same sums with the accumulator in registers, for SG <= 8 RT and SG <= 4 CT.
+// Lane l owns the RT x CT tile of entries (h, h') with h in 8-lane row group
+// l / 4 (rows RT (l / 4) ..) and h' in column group l % 4 (columns CT (l % 4) ..);
+// the lanes with l % 4 == 0 also own W_h of their rows.  For each segment of
+// the warp's batch of 32 (in lane order) every lane adds Y_s[h] / W_s * Y_s[h']
+// to its whole tile: a level outside the segment's range has Y_s = 0 and adds
+// an exact zero (all terms are >= 0), so each entry still sums its nonzero terms
+// in segment order, as coupling_yy_kernel does, with independent FMAs in place
+// of a chain of shared-memory updates.  Rows of Y have the odd pitch
+// couple_tile_pitch(RT, CT), levels >= SG stay zero.  The warps' tiles are added
+// into the CTA's partial in warp order.
+constexpr int kCoupleTileWarps = 4;
+
+__host__ __device__ constexpr int couple_tile_pitch(int RT, int CT) {
+    return (8 * RT > 4 * CT ? 8 * RT : 4 * CT) | 1;
+}
+
+template <int RT, int CT>
+__global__ void __launch_bounds__(kCoupleTileWarps * 32)
+coupling_yy_tile_kernel(int32_t Gp, const int2* __restrict__ seg_meta, const int4* __restrict__ run_meta,
+                        const int2* __restrict__ block_meta, const double* __restrict__ block_w,
+                        const double* __restrict__ inv_wp, int SG, double* __restrict__ partial) {
+    constexpr int P = couple_tile_pitch(RT, CT);
+    extern __shared__ double ct_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int SS = SG * SG;
+    double* red = ct_smem;                                   // SS + SG
+    double* Y = ct_smem + SS + SG + static_cast<int64_t>(warp) * 32 * P;
+    double* myY = Y + lane * P;
+    for (int i = threadIdx.x; i < SS + SG + kCoupleTileWarps * 32 * P; i += blockDim.x) ct_smem[i] = 0.0;
+    __syncthreads();
+    const int R0 = RT * (lane >> 2), C0 = CT * (lane & 3);
+    double acc[RT][CT], wacc[RT];
+#pragma unroll
+    for (int r = 0; r < RT; ++r) {
+        wacc[r] = 0.0;
+#pragma unroll
+        for (int c = 0; c < CT; ++c) acc[r][c] = 0.0;
+    }
+    const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kCoupleTileWarps;
+    const int64_t wid = static_cast<int64_t>(blockIdx.x) * kCoupleTileWarps + warp;
+    for (int64_t s0 = wid * 32; s0 < Gp; s0 += nwarps * 32) {
+        int hmin = SG, hmax = 0;
+        double iw = 0.0;
+        if (s0 + lane < Gp) {
+            const int64_t sg = s0 + lane;
+            const int32_t r0 = seg_meta[sg].y, r1 = seg_meta[sg + 1].y;
+            if (r1 > r0) {
+                const int sb0 = run_meta[r0].z, sb1 = run_meta[r1 - 1].w;
+                for (int bb = sb0; bb < sb1; ++bb) {
+                    const int2 bm = block_meta[bb];
+                    couple_row_add(myY, bm, block_w ? block_w[bb] : 1.0);
+                    hmin = min(hmin, bm.x);
+                    hmax = max(hmax, bm.x + bm.y);
+                }
+            }
+            iw = inv_wp[sg];
+        }
+        __syncwarp();
+        const int ns = static_cast<int>(min(static_cast<int64_t>(32), Gp - s0));
+        for (int i = 0; i < ns; ++i) {
+            const double w_inv = __shfl_sync(0xffffffffu, iw, i);
+            const double* Yi = Y + i * P;
+            double a[RT], b[CT];
+#pragma unroll
+            for (int r = 0; r < RT; ++r) {
+                const double yh = Yi[R0 + r];
+                wacc[r] += yh;
+                a[r] = yh * w_inv;
+            }
+#pragma unroll
+            for (int c = 0; c < CT; ++c) b[c] = Yi[C0 + c];
+#pragma unroll
+            for (int r = 0; r < RT; ++r)
+#pragma unroll
+                for (int c = 0; c < CT; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        }
+        __syncwarp();
+        for (int h = lo_clear(hmin, SG); h < max(hmax, 0); ++h) myY[h] = 0.0;
+        __syncwarp();
+    }
+    for (int w = 0; w < kCoupleTileWarps; ++w) {
+        if (warp == w) {
+#pragma unroll
+            for (int r = 0; r < RT; ++r) {
+                const int h = R0 + r;
+                if (h < SG) {
+#pragma unroll
+                    for (int c = 0; c < CT; ++c)
+                        if (C0 + c < SG) red[h * SG + C0 + c] += acc[r][c];
+                    if ((lane & 3) == 0) red[SS + h] += wacc[r];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < SS + SG; i += blockDim.x)
+        partial[static_cast<int64_t>(blockIdx.x) * (SS + SG) + i] = red[i];
 }
 
 // C_yy = diag(W) - sum_s Y_s Y_s' / W_s, CTA partials summed in CTA order; the
