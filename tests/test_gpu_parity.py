@@ -191,6 +191,26 @@ def test_block_and_tile_matvec_agree(absorber, pkg, oracle_mod, panels, weighted
         assert (np.linalg.norm(outs[0] - o, axis=0) / scale).max() <= 1e-9
 
 
+def test_firm_coupling_over_run_ranges_with_gapped_ids(absorber, pkg, oracle_mod, panels):
+    # the firm-year coupling is summed over ranges of 512 runs in firm order,
+    # across firm boundaries: firm ids without runs (every even id here, and
+    # five past the last) get zero rows, and the largest firms (thousands of
+    # runs) span several ranges whose pieces are joined in range order
+    p = _akm(panels, 120_000, True, seed=53, firms=200, years=20)
+    fes = [p.fes[0], (2 * p.fes[1] + 1).astype(np.int32), p.fes[2]]
+    G = [p.levels[0], 2 * p.levels[1] + 5, p.levels[2]]
+    assert np.bincount(p.fes[1]).max() > 3 * 512  # obs of the largest firm: several ranges of runs
+    outs = []
+    for pk in (0, 1):
+        o = pkg.make_options(tol=1e-10, precision="fp64", pass_kernel=pk)
+        r = absorber.absorb(p.y, p.X, fes, G, None, o)
+        assert r.converged
+        outs.append(np.column_stack([r.y_tilde, r.X_tilde]))
+    scale = np.linalg.norm(np.column_stack([p.y, p.X]), axis=0)
+    assert (np.linalg.norm(outs[0] - outs[1], axis=0) / scale).max() <= 1e-9
+    _check(absorber, pkg, oracle_mod, p.y, p.X, fes, G)
+
+
 def test_pipelined_host_copies_match_single_stream(pkg, oracle_mod, panels, monkeypatch):
     """Host-array calls with more than four columns copy column groups in and
     out on their own streams while other groups are solved; the within

@@ -628,32 +628,45 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
             const int64_t SGP = st.SGP;
             if (lg) {
                 const LargeDim& L = st.L[0];
-                int32_t *sorted_runs, *run_seg;
-                B_CHECK(get_buf(ctx, "sorted_runs", L.nruns, &sorted_runs));
+                int32_t *sorted_grp, *run_seg, *grp_off;
+                int4* frec;
+                double* frec_cf;
+                B_CHECK(get_buf(ctx, "sorted_grp", L.nruns, &sorted_grp));
+                B_CHECK(get_buf(ctx, "fy_rec", L.nruns, &frec));
+                B_CHECK(get_buf(ctx, "fy_rec_cf", L.nruns, &frec_cf));
                 B_CHECK(get_buf(ctx, "run_seg", L.nruns, &run_seg));
+                B_CHECK(get_buf(ctx, "grp_off0", static_cast<size_t>(L.G) + 1, &grp_off));
+                const int64_t nranges = (L.nruns + kFyRangeRuns - 1) / kFyRangeRuns;
                 double* cpart;
                 B_CHECK(get_buf(ctx, "cfy64", static_cast<size_t>(L.G) * SGP, &st.cfy64));
                 B_CHECK(get_buf(ctx, "cfy32", static_cast<size_t>(L.G) * SGP, &st.cfy32));
-                B_CHECK(get_buf(ctx, "cfy_part", static_cast<size_t>(L.nchunks) * SGP, &cpart));
-                const size_t fsmem = static_cast<size_t>(kCoupleWarps) * 32 * couple_pitch(static_cast<int>(SG)) * sizeof(double);
-                B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&coupling_fy_kernel), static_cast<int>(fsmem)));
-                int fps = 1;
-                B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fps, coupling_fy_kernel,
-                                                                    kCoupleWarps * 32, fsmem));
-                const int fgrid = static_cast<int>(std::max<int64_t>(
-                    1, std::min<int64_t>((L.nchunks + kCoupleWarps - 1) / kCoupleWarps,
-                                         static_cast<int64_t>(ctx->num_sms) * std::max(fps, 1))));
-                coupling_fy_kernel<<<fgrid, kCoupleWarps * 32, fsmem, s>>>(
-                    L.nchunks, L.chunk_grp, L.chunk_beg, L.chunk_end, L.chunk_whole, sorted_runs,
-                    run_seg, st.run_meta, st.seg_meta, st.block_meta, st.block_w64, L.cw_run,
-                    st.inv_wp, st.SG, st.SGP, st.cfy64, cpart);
-                B_LAUNCHED();
-                if (L.nmulti > 0) {
-                    coupling_fy_combine_kernel<<<static_cast<int>(std::min<int64_t>(
-                                                     L.nmulti, static_cast<int64_t>(ctx->num_sms) * 8)),
-                                                 256, 0, s>>>(L.nmulti, L.multi_grp, L.multi_c0,
-                                                              L.multi_c1, cpart, st.SGP, st.cfy64);
+                B_CHECK(get_buf(ctx, "cfy_part", static_cast<size_t>(std::max<int64_t>(nranges, 1)) * 2 * SGP, &cpart));
+                if (nranges == 0) {
+                    B_TRY(cudaMemsetAsync(st.cfy64, 0, sizeof(double) * static_cast<size_t>(L.G) * SGP, s));
+                } else {
+                    const size_t fsmem = static_cast<size_t>(kCoupleWarps) * 32 * couple_pitch(static_cast<int>(SG)) * sizeof(double);
+                    B_TRY(raise_smem_limit(reinterpret_cast<const void*>(&coupling_fy_range_kernel), static_cast<int>(fsmem)));
+                    int fps = 1;
+                    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fps, coupling_fy_range_kernel,
+                                                                        kCoupleWarps * 32, fsmem));
+                    const int fgrid = static_cast<int>(std::max<int64_t>(
+                        1, std::min<int64_t>((nranges + kCoupleWarps - 1) / kCoupleWarps,
+                                             static_cast<int64_t>(ctx->num_sms) * std::max(fps, 1))));
+                    fy_run_record_kernel<<<grid_for(ctx, L.nruns, T256), T256, 0, s>>>(
+                        L.nruns, L.run_dest, run_seg, st.run_meta, st.seg_meta, L.cw_run, st.inv_wp, frec,
+                        frec_cf);
                     B_LAUNCHED();
+                    coupling_fy_range_kernel<<<fgrid, kCoupleWarps * 32, fsmem, s>>>(
+                        L.nruns, nranges, L.G, frec, frec_cf, sorted_grp, grp_off, st.block_meta,
+                        st.block_w64, st.SG, st.SGP, st.cfy64, cpart);
+                    B_LAUNCHED();
+                    if (nranges > 1) {
+                        coupling_fy_join_kernel<<<static_cast<int>(std::min<int64_t>(
+                                                      nranges, static_cast<int64_t>(ctx->num_sms) * 8)),
+                                                  256, 0, s>>>(L.nruns, nranges, sorted_grp, grp_off, cpart,
+                                                               st.SGP, st.cfy64);
+                        B_LAUNCHED();
+                    }
                 }
                 to_float_kernel<<<grid_for(ctx, static_cast<int64_t>(L.G) * SGP, T256), T256, 0, s>>>(
                     st.cfy64, static_cast<int64_t>(L.G) * SGP, st.cfy32);

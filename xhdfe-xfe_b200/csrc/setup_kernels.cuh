@@ -490,93 +490,190 @@ __device__ __forceinline__ void couple_row_add(double* row, const int2 bm, doubl
     for (int h = bm.x; h < bm.x + bm.y; ++h) row[h] += w;
 }
 
-// One warp per chunk of a firm's runs (in firm order).  Lane i takes run
-// j0 + i of the chunk: its metadata and blocks are read by the 32 lanes in
-// parallel, and lane i writes y_m - c_m Y_s / W_s into its own shared-memory
-// row; lane l then sums level l (and l + 32) over the rows in lane order.
-// Output rows have stride SGP (SG rounded up to 4) and padding levels are zero.
-constexpr int kCoupleWarps = 8;
-
 // Pitch of the per-lane shared-memory rows: odd in doubles, so that the 16
 // lanes of a 64-bit shared access that touch level h of 16 different rows fall
 // in 16 different bank pairs (an even pitch such as 36 puts lanes l and l + 4
 // in the same banks: 8-way conflicts on every row access).
 __host__ __device__ __forceinline__ int couple_pitch(int SG) { return SG | 1; }
 
+// C_fy over ranges of kFyRangeRuns consecutive runs in firm order (sorted_runs),
+// one warp per range, across firm boundaries (most firms own a few runs: one
+// warp per firm would leave most lanes idle).  Lane i takes run j0 + i of each
+// batch of 32: its metadata and blocks are read by the 32 lanes in parallel,
+// and lane i writes y_m - c_m Y_s / W_s into its own shared-memory row (levels
+// hmin .. hmax of its segment, cleared again after the batch); lane l then sums
+// level l (and l + 32) over the batch's rows in order, and writes a firm's sum
+// when the firm ends.  A firm inside the range writes its row of C_fy (stride
+// SGP = SG rounded up to 4, padding zero); the piece of a firm that begins
+// before the range goes to slot 0 of the range's partials, the piece of a firm
+// that begins in the range and ends after it to slot 1, and
+// coupling_fy_join_kernel adds the pieces of those firms in range order.  Firm
+// ids with no runs (between two consecutive firms of the order, or before the
+// first or after the last) get zero rows from the warp that passes them.
+constexpr int kCoupleWarps = 8;
+constexpr int kFyRangeRuns = 512;
+constexpr int kFyPrefetch = 4;
+
+__device__ __forceinline__ void couple_put_row(double* dst, double a0, double a1, int lane, int SG, int SGP) {
+    if (lane < SGP) dst[lane] = lane < SG ? a0 : 0.0;
+    if (lane + 32 < SGP) dst[lane + 32] = lane + 32 < SG ? a1 : 0.0;
+}
+
+__device__ __forceinline__ void couple_zero_rows(double* out_fy, int64_t g0, int64_t g1, int lane, int SGP) {
+    for (int64_t g = g0; g < g1; ++g)
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+            if (lane + 32 * k < SGP) out_fy[g * SGP + lane + 32 * k] = 0.0;
+}
+
+// Per run m, written at its sorted position j = run_dest[m]: the block range
+// of its segment [x, y), its own block range [z, w) and c_m / W_s(m) - one
+// coalesced record per lane of coupling_fy_range_kernel in place of a chain of
+// dependent gathers (run -> segment -> the segment's first and last runs).
+__global__ void fy_run_record_kernel(int64_t nruns, const int32_t* __restrict__ run_dest,
+                                     const int32_t* __restrict__ run_seg, const int4* __restrict__ run_meta,
+                                     const int2* __restrict__ seg_meta, const double* __restrict__ cw_run,
+                                     const double* __restrict__ inv_wp, int4* __restrict__ rec,
+                                     double* __restrict__ rec_cf) {
+    for (int64_t m = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; m < nruns;
+         m += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t sg = run_seg[m];
+        const int4 rm = run_meta[m];
+        const int32_t r0 = seg_meta[sg].y, r1 = seg_meta[sg + 1].y;
+        const int32_t j = run_dest[m];
+        rec[j] = make_int4(run_meta[r0].z, run_meta[r1 - 1].w, rm.z, rm.w);
+        rec_cf[j] = cw_run[m] * inv_wp[sg];
+    }
+}
+
 __global__ void __launch_bounds__(kCoupleWarps * 32)
-coupling_fy_kernel(int64_t nchunks, const int32_t* __restrict__ chunk_grp,
-                   const int32_t* __restrict__ chunk_beg, const int32_t* __restrict__ chunk_end,
-                   const uint8_t* __restrict__ chunk_whole, const int32_t* __restrict__ sorted_runs,
-                   const int32_t* __restrict__ run_seg, const int4* __restrict__ run_meta,
-                   const int2* __restrict__ seg_meta, const int2* __restrict__ block_meta,
-                   const double* __restrict__ block_w, const double* __restrict__ cw_run,
-                   const double* __restrict__ inv_wp, int SG, int SGP, double* __restrict__ out_fy,
-                   double* __restrict__ partial) {
+coupling_fy_range_kernel(int64_t nruns, int64_t nranges, int32_t G, const int4* __restrict__ rec,
+                         const double* __restrict__ rec_cf, const int32_t* __restrict__ sorted_grp,
+                         const int32_t* __restrict__ grp_off, const int2* __restrict__ block_meta,
+                         const double* __restrict__ block_w, int SG, int SGP, double* __restrict__ out_fy,
+                         double* __restrict__ part) {
     extern __shared__ double cf_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int SGQ = couple_pitch(SG);
     double* rows = cf_smem + static_cast<int64_t>(warp) * 32 * SGQ;
     double* myrow = rows + lane * SGQ;
+    for (int h = 0; h < SGQ; ++h) myrow[h] = 0.0;
+    __syncwarp();
     const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kCoupleWarps;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * kCoupleWarps + warp; c < nchunks; c += nwarps) {
-        const int32_t b = chunk_beg[c], e = chunk_end[c];
-        double acc[2] = {0.0, 0.0};
-        for (int32_t j0 = b; j0 < e; j0 += 32) {
-            for (int h = 0; h < SG; ++h) myrow[h] = 0.0;
-            if (j0 + lane < e) {
-                const int32_t m = sorted_runs[j0 + lane];
-                const int32_t sg = run_seg[m];
-                const int4 rm = run_meta[m];
-                const int32_t r0 = seg_meta[sg].y, r1 = seg_meta[sg + 1].y;
-                const int sb0 = run_meta[r0].z, sb1 = run_meta[r1 - 1].w;
-                const double cf = cw_run[m] * inv_wp[sg];
-                for (int bb = rm.z; bb < rm.w; ++bb)
-                    couple_row_add(myrow, block_meta[bb], block_w ? block_w[bb] : 1.0);
-                for (int bb = sb0; bb < sb1; ++bb)
-                    couple_row_add(myrow, block_meta[bb], -cf * (block_w ? block_w[bb] : 1.0));
+    for (int64_t rg = static_cast<int64_t>(blockIdx.x) * kCoupleWarps + warp; rg < nranges; rg += nwarps) {
+        const int64_t rb = rg * kFyRangeRuns, re = min(rb + kFyRangeRuns, nruns);
+        int32_t cur = sorted_grp[rb];
+        const int32_t prev = rb > 0 ? sorted_grp[rb - 1] : -1;
+        if (cur != prev) couple_zero_rows(out_fy, prev + 1, cur, lane, SGP);
+        // where the pieces of the current firm go
+        auto flush = [&](int32_t f, double a0, double a1) {
+            const int32_t fb = grp_off[f], fe = grp_off[f + 1];
+            double* dst = (fb >= rb && fe <= re) ? out_fy + static_cast<int64_t>(f) * SGP
+                          : (fb < rb)            ? part + (rg * 2 + 0) * SGP
+                                                 : part + (rg * 2 + 1) * SGP;
+            couple_put_row(dst, a0, a1, lane, SG, SGP);
+        };
+        double acc0 = 0.0, acc1 = 0.0;
+        for (int64_t j0 = rb; j0 < re; j0 += 32) {
+            int32_t g = -1;
+            int hmin = SG, hmax = 0;
+            if (j0 + lane < re) {
+                const int4 rc = rec[j0 + lane];
+                const double cf = rec_cf[j0 + lane];
+                g = sorted_grp[j0 + lane];
+                // the segment's first kFyPrefetch blocks are loaded together
+                int2 bq[kFyPrefetch];
+                double wq[kFyPrefetch];
+#pragma unroll
+                for (int q = 0; q < kFyPrefetch; ++q) {
+                    const bool in = rc.x + q < rc.y;
+                    bq[q] = in ? block_meta[rc.x + q] : make_int2(0, 0);
+                    wq[q] = (in && block_w) ? block_w[rc.x + q] : 1.0;
+                }
+                auto block_at = [&](int bb, int2& bm, double& w) {
+                    const int q = bb - rc.x;
+                    if (q < kFyPrefetch) {
+                        bm = bq[0];
+                        w = wq[0];
+#pragma unroll
+                        for (int t = 1; t < kFyPrefetch; ++t)
+                            if (q == t) {
+                                bm = bq[t];
+                                w = wq[t];
+                            }
+                    } else {
+                        bm = block_meta[bb];
+                        w = block_w ? block_w[bb] : 1.0;
+                    }
+                };
+                for (int bb = rc.z; bb < rc.w; ++bb) {
+                    int2 bm;
+                    double w;
+                    block_at(bb, bm, w);
+                    couple_row_add(myrow, bm, w);
+                }
+                for (int bb = rc.x; bb < rc.y; ++bb) {
+                    int2 bm;
+                    double w;
+                    block_at(bb, bm, w);
+                    couple_row_add(myrow, bm, -cf * w);
+                    hmin = min(hmin, bm.x);
+                    hmax = max(hmax, bm.x + bm.y);
+                }
             }
             __syncwarp();
-            const int nj = min(32, e - j0);
+            const int nj = static_cast<int>(min(static_cast<int64_t>(32), re - j0));
             for (int i = 0; i < nj; ++i) {
-#pragma unroll
-                for (int k = 0; k < 2; ++k)
-                    if (lane + 32 * k < SG) acc[k] += rows[i * SGQ + lane + 32 * k];
+                const int32_t gi = __shfl_sync(0xffffffffu, g, i);
+                if (gi != cur) {  // warp-uniform: the firm of run j0 + i starts here
+                    flush(cur, acc0, acc1);
+                    couple_zero_rows(out_fy, static_cast<int64_t>(cur) + 1, gi, lane, SGP);
+                    acc0 = acc1 = 0.0;
+                    cur = gi;
+                }
+                if (lane < SG) acc0 += rows[i * SGQ + lane];
+                if (lane + 32 < SG) acc1 += rows[i * SGQ + lane + 32];
             }
+            __syncwarp();
+            for (int h = lo_clear(hmin, SG); h < max(hmax, 0); ++h) myrow[h] = 0.0;
             __syncwarp();
         }
-        double* dst = chunk_whole[c] ? out_fy + static_cast<int64_t>(chunk_grp[c]) * SGP
-                                     : partial + c * SGP;
-#pragma unroll
-        for (int k = 0; k < 2; ++k)
-            if (lane + 32 * k < SGP) dst[lane + 32 * k] = (lane + 32 * k < SG) ? acc[k] : 0.0;
+        flush(cur, acc0, acc1);
+        if (re == nruns) couple_zero_rows(out_fy, static_cast<int64_t>(cur) + 1, G, lane, SGP);
     }
 }
 
-// Rows of multi-chunk firms: one CTA per row; warp w sums chunks c0 + w,
-// c0 + w + 8, ... (lanes over levels), then the eight warp sums are added in
-// warp order.
+// Rows of the firms split across ranges: the range holding a firm's first run
+// sees it as its last firm, continuing past the range; its row is slot 1 of that
+// range plus slot 0 of each following range up to the firm's last run, added in
+// range order (warp w sums ranges r + 1 + w, r + 9 + w, ...; the eight warp sums
+// are then added to slot 1 in warp order).  One CTA per range.
 __global__ void __launch_bounds__(256)
-coupling_fy_combine_kernel(int64_t nmulti, const int32_t* __restrict__ multi_grp,
-                           const int32_t* __restrict__ multi_c0, const int32_t* __restrict__ multi_c1,
-                           const double* __restrict__ partial, int SGP, double* __restrict__ out_fy) {
+coupling_fy_join_kernel(int64_t nruns, int64_t nranges, const int32_t* __restrict__ sorted_grp,
+                        const int32_t* __restrict__ grp_off, const double* __restrict__ part, int SGP,
+                        double* __restrict__ out_fy) {
     __shared__ double ws[8][kCoupleMaxSG];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int64_t r = blockIdx.x; r < nmulti; r += gridDim.x) {
-        const int32_t c0 = multi_c0[r], c1 = multi_c1[r];
+    for (int64_t r = blockIdx.x; r < nranges; r += gridDim.x) {
+        const int64_t rb = r * kFyRangeRuns, re = min(rb + kFyRangeRuns, nruns);
+        const int32_t f = sorted_grp[re - 1];
+        const int64_t fb = grp_off[f], fe = grp_off[f + 1];
+        if (fb < rb || fe <= re) continue;  // uniform over the CTA
+        const int64_t r1 = (fe - 1) / kFyRangeRuns;
         double acc[2] = {0.0, 0.0};
-        for (int32_t c = c0 + warp; c < c1; c += 8) {
+        for (int64_t q = r + 1 + warp; q <= r1; q += 8) {
 #pragma unroll
             for (int k = 0; k < 2; ++k)
-                if (lane + 32 * k < SGP) acc[k] += __ldcg(partial + static_cast<int64_t>(c) * SGP + lane + 32 * k);
+                if (lane + 32 * k < SGP) acc[k] += __ldcg(part + (q * 2 + 0) * SGP + lane + 32 * k);
         }
 #pragma unroll
         for (int k = 0; k < 2; ++k)
             if (lane + 32 * k < SGP) ws[warp][lane + 32 * k] = acc[k];
         __syncthreads();
         if (threadIdx.x < SGP) {
-            double v = 0.0;
+            double v = __ldcg(part + (r * 2 + 1) * SGP + threadIdx.x);
             for (int w = 0; w < 8; ++w) v += ws[w][threadIdx.x];
-            out_fy[static_cast<int64_t>(multi_grp[r]) * SGP + threadIdx.x] = v;
+            out_fy[static_cast<int64_t>(f) * SGP + threadIdx.x] = v;
         }
         __syncthreads();
     }
