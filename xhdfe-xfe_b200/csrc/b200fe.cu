@@ -518,10 +518,16 @@ int build_structure(b200fe_context* ctx, int64_t n, int D, const int32_t* const*
         B_CHECK(get_buf(ctx, "run_ce", nr, &ce));
         B_CHECK(get_buf(ctx, "run_cw_run" + sfx, nr, &cw_run));
         L.cw_run = cw_run;
-        run_weights_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(
-            sorted_runs, nr, run_start, n, run_seg, st.wp64, st.inv_wp, L.run_dest, cw, ce,
-            cw_run);
-        B_LAUNCHED();
+        {
+            double* ce_run;
+            B_CHECK(get_buf(ctx, "run_ce_tmp", nr, &ce_run));
+            run_weights_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(nr, run_start, n, run_seg,
+                                                                        st.wp64, st.inv_wp, cw_run, ce_run);
+            B_LAUNCHED();
+            run_sorted_weights_kernel<<<grid_for(ctx, nr, T256), T256, 0, s>>>(sorted_runs, nr, cw_run, ce_run,
+                                                                               L.run_dest, cw, ce);
+            B_LAUNCHED();
+        }
         // chunk lists (and super-chunks) of the groups' runs
         B_CHECK(build_chunks(ctx, grp_off, kChunkRuns, sfx, L));
         // diagonal terms W_g, E_g of the groups over the chunk list (balanced

@@ -159,18 +159,14 @@ __global__ void tile_fill_kernel(const int32_t* __restrict__ seg_off, int32_t G,
     }
 }
 
-// Per run: weight c_m and its diagonal term c_m^2 / W_seg, written at the
-// run's sorted position.  Also run_dest (inverse of the sorted order).
-__global__ void run_weights_kernel(const int32_t* __restrict__ sorted_runs, int64_t nruns,
-                                   const int32_t* __restrict__ run_start, int64_t n,
-                                   const int32_t* __restrict__ run_seg,
-                                   const double* __restrict__ wp, const double* __restrict__ inv_wp,
-                                   int32_t* __restrict__ run_dest, double* __restrict__ cw_sorted,
-                                   double* __restrict__ ce_sorted, double* __restrict__ cw_run) {
-    for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nruns;
-         j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int32_t m = sorted_runs[j];
-        run_dest[m] = static_cast<int32_t>(j);
+// Per run m, in run (primary) order: weight c_m (its observations' weights
+// summed in order, or their count) and its diagonal term c_m^2 / W_seg.
+__global__ void run_weights_kernel(int64_t nruns, const int32_t* __restrict__ run_start, int64_t n,
+                                   const int32_t* __restrict__ run_seg, const double* __restrict__ wp,
+                                   const double* __restrict__ inv_wp, double* __restrict__ cw_run,
+                                   double* __restrict__ ce_run) {
+    for (int64_t m = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; m < nruns;
+         m += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int32_t b = run_start[m];
         const int32_t e = (m + 1 < nruns) ? run_start[m + 1] : static_cast<int32_t>(n);
         double c = 0.0;
@@ -179,9 +175,23 @@ __global__ void run_weights_kernel(const int32_t* __restrict__ sorted_runs, int6
         } else {
             c = static_cast<double>(e - b);
         }
-        cw_sorted[j] = c;
-        ce_sorted[j] = c * c * inv_wp[run_seg[m]];
         cw_run[m] = c;
+        ce_run[m] = c * c * inv_wp[run_seg[m]];
+    }
+}
+
+// The run weights at the runs' sorted positions, and run_dest (the inverse of
+// the sorted order): one gather pair and one scatter per run.
+__global__ void run_sorted_weights_kernel(const int32_t* __restrict__ sorted_runs, int64_t nruns,
+                                          const double* __restrict__ cw_run,
+                                          const double* __restrict__ ce_run, int32_t* __restrict__ run_dest,
+                                          double* __restrict__ cw_sorted, double* __restrict__ ce_sorted) {
+    for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nruns;
+         j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t m = sorted_runs[j];
+        run_dest[m] = static_cast<int32_t>(j);
+        cw_sorted[j] = cw_run[m];
+        ce_sorted[j] = ce_run[m];
     }
 }
 
